@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Walker-steps/s of the B200 random-walk engine (one JSON line on rank 0).
+
+Workload ``production`` (default): a 256 x 256 x 2048 label lattice at 0.1 um
+(one undulating, caliber-varying axon, label 1, in extra-axonal space, label
+2), 1e7 walkers per GPU, 50,000 steps of dt = 2e-4 ms, D = 2 um^2/ms in both
+compartments, membrane permeability kappa = 0.01 um/ms, T2 = 80 / 60 ms, and
+the PGSE signal of 30 directions x b in {0..5} ms/um^2 x Delta in {4, 5, 6} ms
+at delta = 4 ms (540 gradients; Delta + delta fits the 10 ms walk).
+Workload ``single``: the 64 x 64 x 512 single-axon lattice (labels 0/1),
+1e5 walkers, 5,000 steps, impermeable, no T2, periodic walls, moments every
+10 steps.  Inputs are synthetic and seeded.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision split|compat] [--workload production|single]
+
+``value``: walker-steps/s of the whole job, lattice already resident on the
+GPU, timed with CUDA events on the launching stream (max over ranks).
+``e2e``: the same through the public API with the lattice handed over from
+pinned host memory and the results read back every step (host clock around
+synchronised steps).  ``--impl reference`` times the reference simulator's
+own step loop (hpc_code/lib/main_PGSE.cu compiled for the host, all cores)
+on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "walker-steps/s on 1 B200 (batched/split-prec vs plain) at stated D(t)/K(t) error"
+UNIT = "walker-steps/s"
+# Algorithmic work per walker-step (the step kernel's roofline model): one
+# label gather per face crossing, 0.73 crossings per step at
+# step/voxel = 0.49, each a 32-byte sector -> 23.4 B; 105 thread-ops.
+BYTES_PER_WALKER_STEP = 23.4
+OPS_PER_WALKER_STEP = 105.0
+
+
+def fib_directions(n: int) -> np.ndarray:
+    """n near-uniform unit vectors (Fibonacci sphere)."""
+    i = np.arange(n) + 0.5
+    z = 1.0 - 2.0 * i / n
+    r = np.sqrt(1.0 - z * z)
+    phi = np.pi * (1.0 + 5 ** 0.5) * i
+    return np.column_stack([r * np.cos(phi), r * np.sin(phi), z])
+
+
+def workload(name: str, world: int):
+    from rms_b200 import analysis, geometry
+    if name == "production":
+        lab = geometry.axon_lattice(256, 256, 2048, 0.1, seed=0, exterior=2)
+        dirs = fib_directions(30)
+        rows = []
+        for Delta in (4.0, 5.0, 6.0):
+            for b in (0.0, 1.0, 2.0, 3.0, 4.0, 5.0):
+                g = float(analysis.pgse_gradient_for_b(b, Delta, 4.0))
+                for d in dirs:
+                    rows.append([Delta, 4.0, g, *d])
+        per_gpu = 10_000_000
+        sim_kw = dict(dt=2e-4, tn=50_000, npar=per_gpu * world, res=0.1,
+                      diffusivity=[0.0, 2.0, 2.0], t2=[80.0, 80.0, 60.0],
+                      grad=np.array(rows), permeation="kappa", kappa=0.01)
+        cfg = dict(workload="production: 256x256x2048 lattice, 1e7 walkers/GPU, 50000 steps, "
+                            "kappa=0.01 um/ms, T2 80/60 ms, PGSE 540 gradients",
+                   lattice=[256, 256, 2048], walkers_per_gpu=per_gpu, steps_per_walk=50_000,
+                   ngrad=len(rows), mode="pgse")
+    elif name == "single":
+        lab = geometry.axon_lattice(64, 64, 512, 0.1, seed=0, exterior=0)
+        per_gpu = 100_000
+        sim_kw = dict(dt=2e-4, tn=5_000, npar=per_gpu * world, res=0.1, diffusivity=[0.0, 2.0],
+                      t2=[1e12, 1e12], bval=[], bvec=np.zeros((0, 3)), timepoints=500,
+                      boundary="periodic")
+        cfg = dict(workload="single: 64x64x512 axon, 1e5 walkers/GPU, 5000 steps, moments every 10 steps",
+                   lattice=[64, 64, 512], walkers_per_gpu=per_gpu, steps_per_walk=5_000,
+                   mode="narrow")
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return lab, sim_kw, per_gpu, cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, maxmhz, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                maxmhz = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not mhz:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": maxmhz, "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+def cpu_reference_rate(lab, sim_kw, target_s: float, nthreads: int | None = None):
+    """The reference's own step loop (oracle/_ref: hpc_code/lib/main_PGSE.cu or
+    main.cu compiled for the host) on the first n walkers of the job, all
+    cores; n is chosen so one sample takes about target_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from rms_b200 import engine
+    probe = engine.Sim(None, shape=lab.shape, **{k: v for k, v in sim_kw.items()})
+    step, pij = probe.get("step"), probe.get("pij")
+    probe.close()
+    dt, tn = sim_kw["dt"], sim_kw["tn"]
+    t2s = np.array(sim_kw["t2"], dtype=np.float64) / dt
+    timepoints = sim_kw.get("timepoints", 0) or 1000
+    kw = dict(dt=dt, tn=tn, npar=sim_kw["npar"], res=sim_kw["res"], step=step, t2_steps=t2s,
+              pij=pij, seed=1, timepoints=1000)
+    if "grad" in sim_kw:
+        job = pyoracle.Job(lab, grad=sim_kw["grad"], **kw)
+    else:
+        job = pyoracle.Job(lab, bval=sim_kw.get("bval", []), bvec=sim_kw.get("bvec", np.zeros((0, 3))), **kw)
+    kind = "reference"
+    if not pyoracle.ref_available():
+        raise RuntimeError("oracle/_ref/librmsref.so missing")
+    if timepoints != 1000 or sim_kw.get("boundary", "mirror") != "mirror":
+        # the reference build has fixed 1000 records and mirror walls: time its loop as is
+        pass
+    nthreads = nthreads or pyoracle.ref_max_threads()
+    n = max(nthreads, 2 * nthreads)
+    t0 = time.perf_counter()
+    pyoracle.run_reference_walkers(job, n, nthreads)
+    dt_probe = time.perf_counter() - t0
+    n = int(max(nthreads, min(job.npar, n * target_s / max(dt_probe, 1e-3))))
+    return job, n, nthreads, kind
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    lab, sim_kw, per_gpu, cfg = workload(args.workload, 1)
+    try:
+        job, n, cores, kind = cpu_reference_rate(lab, sim_kw, target_s=6.0)
+    except Exception as e:  # the build is missing on this machine
+        print(json.dumps({"impl": "reference", "unavailable": f"reference host build: {e}"}))
+        return
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        pyoracle.run_reference_walkers(job, n, cores)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    per_step = float(np.mean(times))
+    rate = n * job.tn / per_step
+    sample = (f"walkers [0,{n}) of the job x {job.tn} steps per timed step, reference "
+              f"propagate() (oracle/_ref) on {cores} host threads")
+    line = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": cfg, "impl": "reference",
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from rms_b200 import engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    lab, sim_kw, per_gpu, cfg = workload(args.workload, world)
+    w0, w1 = rank * per_gpu, (rank + 1) * per_gpu
+    sim = engine.Sim(lab, **sim_kw)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    precision = args.precision
+
+    def one(seed):
+        sim.run(seed=seed, precision=precision, device=local, stream=sh, walker_range=(w0, w1))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        one(1000 + i)
+    launches_per_step = 2 + (1 if sim.mode == "pgse" else 0)
+    walk_ms = []
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for i in range(args.steps):
+            flush.zero_()
+            one(2000 + i)
+            walk_ms.append(sim.timing()[0])
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    walk = float(np.mean(walk_ms))
+    if world > 1:
+        t = torch.tensor([ms, walk], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, walk = float(t[0]), float(t[1])
+    tn = sim_kw["tn"]
+    value = world * per_gpu * tn / (ms * 1e-3)
+
+    # end to end through the public API: lattice from pinned host memory,
+    # results read back, every step
+    pinned = torch.from_numpy(np.ascontiguousarray(lab)).pin_memory()
+    lab_pinned = pinned.numpy()
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        sim.set_lattice(lab_pinned)
+        one(3000 + i)
+        out = sim.outputs()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t[0])
+    d2h = int(sum(v.nbytes for v in out.values()))
+    h2d = int(lab.nbytes)
+
+    # roofline of the walk kernel (the dominant launch)
+    walker_steps = per_gpu * tn
+    achieved_gbs = walker_steps * BYTES_PER_WALKER_STEP / (walk * 1e-3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "walk_traffic.json")))
+        traffic = prof.get(f"{args.workload}/{precision}")
+    except OSError:
+        pass
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                import pyoracle
+                job, n, cores, kind = cpu_reference_rate(lab, sim_kw, target_s=15.0)
+                t0 = time.perf_counter()
+                pyoracle.run_reference_walkers(job, n, cores)
+                el = time.perf_counter() - t0
+                cpu = {"value": n * job.tn / el, "unit": UNIT, "cores": cores, "kind": kind,
+                       "sample": f"walkers [0,{n}) x {job.tn} steps, reference propagate() "
+                                 f"(oracle/_ref) on {cores} host threads, {el:.1f} s"}
+            except Exception as e:
+                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                       "sample": f"unavailable: {e}"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if precision == "compat" else "f32+i32 (f64 sums)",
+            "data": "synthetic (seeded axon lattice)",
+            "config": dict(cfg, precision=precision, parallelism=f"walker shards x{world}",
+                           l2="flushed between steps (256 MiB write); lattice 134 MB > L2"),
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": achieved_gbs / peak, "traffic": traffic,
+                         "model": f"{BYTES_PER_WALKER_STEP} B/walker-step x {walker_steps:.3g} walker-steps "
+                                  f"/ walk kernel {walk:.1f} ms (peak: measured hbm_gbs)"},
+            "issue": {"achieved_thread_ops_per_s": walker_steps * OPS_PER_WALKER_STEP / (walk * 1e-3),
+                      "ops_per_walker_step": OPS_PER_WALKER_STEP},
+            "walk_ms": walk,
+            "e2e": {"value": world * per_gpu * tn / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="compat", choices=["split", "compat"])
+    ap.add_argument("--workload", default="production", choices=["production", "single"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,187 @@
+/*
+ * rms.h -- C ABI of librms, the B200-native random-walk diffusion engine.
+ *
+ * The reference simulator (NYU-DiffusionMRI/monte-carlo-simulation-3D-RMS,
+ * hpc_code/lib/main.cu and main_PGSE.cu) has no library interface: its
+ * boundary is a process run with no arguments in a directory of text files
+ * (part1_demo3_simulation.m:86-90).  This header is the library form of that
+ * boundary; `rms_main` (the drop-in executable) is a thin client of it.
+ *
+ * Conventions
+ *  - Every call returns an int status: RMS_OK (0) or a negative RMS_ERR_*.
+ *    rms_last_error() gives a thread-local message for the last failure.
+ *    No C++ exception and no exit() crosses this boundary.
+ *  - The library owns rms_sim objects.  Caller buffers are borrowed for the
+ *    duration of the call only (inputs are copied, outputs are written).
+ *  - One rms_sim is not thread-safe; distinct rms_sim objects are independent.
+ *  - Units follow the reference: ms, um, um^2/ms, |g| in rad/(um ms).
+ */
+#ifndef RMS_H
+#define RMS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RMS_OK 0
+#define RMS_ERR_ARG (-1)      /* invalid argument or configuration */
+#define RMS_ERR_IO (-2)       /* file missing or unreadable / unwritable */
+#define RMS_ERR_FORMAT (-3)   /* file content malformed or too short */
+#define RMS_ERR_RANGE (-4)    /* value outside the supported range */
+#define RMS_ERR_CUDA (-5)     /* CUDA runtime failure */
+#define RMS_ERR_NOMEM (-6)    /* host or device allocation failed */
+#define RMS_ERR_STATE (-7)    /* call out of order (e.g. get before run) */
+#define RMS_ERR_TIMEOUT (-8)  /* a bounded device wait gave up */
+
+/* Signal form: narrow-pulse b-table (main.cu) or rectangular PGSE (main_PGSE.cu). */
+#define RMS_MODE_NARROW 0
+#define RMS_MODE_PGSE 1
+#define RMS_MODE_AUTO (-1)    /* rms_sim_load_dir: PGSE iff gradient_time.txt exists */
+
+/* Lattice walls: mirror (the reference, main.cu:249-265, 302-310) or periodic. */
+#define RMS_BOUNDARY_MIRROR 0
+#define RMS_BOUNDARY_PERIODIC 1
+
+/* Membrane permeation probability Pij between compartments a -> b.
+ *  REFERENCE: 0 if a or b is 0, 1 if a == b, else min(1, sqrt(D_b/D_a))
+ *             (main.cu:444-458).
+ *  KAPPA:     0 if a or b is 0, 1 if a == b, else, from the permeability
+ *             kappa (um/ms) and the step length ds_a = sqrt(6 D_a dt) (um),
+ *             P = (2/3) kappa ds_a / D_a, then Pij = P / (1 + P).
+ *  TABLE:     the caller's nc*nc table, used as given. */
+#define RMS_PERM_REFERENCE 0
+#define RMS_PERM_KAPPA 1
+#define RMS_PERM_TABLE 2
+
+/* Arithmetic of the walk.
+ *  COMPAT: FP64 positions, FP64 uniforms, the reference's operation order;
+ *          per-walker voxel/event sequences equal the CPU oracle's.
+ *  SPLIT:  int32 voxel index + FP32 in-voxel offset, FP32 uniforms, FP64
+ *          cross-walker sums; statistically equal to COMPAT. */
+#define RMS_PREC_COMPAT 0
+#define RMS_PREC_SPLIT 1
+
+typedef struct rms_config {
+    int mode;                  /* RMS_MODE_NARROW or RMS_MODE_PGSE */
+    double dt;                 /* time step, ms */
+    int tn;                    /* number of steps */
+    int64_t npar;              /* number of walkers */
+    int nc;                    /* number of compartments (labels 0..nc-1) */
+    double res;                /* voxel size, um */
+    int n1, n2, n3;            /* lattice size, n3 fastest */
+    const double* diffusivity; /* [nc] um^2/ms; compartment 0 is the null one */
+    const double* t2;          /* [nc] ms, > 0 */
+    /* narrow pulse (main.cu:469-482) */
+    int nbvec;
+    const double* bval;        /* [nbvec] ms/um^2 */
+    const double* bvec;        /* [nbvec*3] */
+    /* PGSE (main_PGSE.cu:495-506) */
+    int ngrad;
+    const double* grad;        /* [ngrad*6]: Delta, delta, |g|, gx, gy, gz */
+    /* extensions; 0 selects the reference's value */
+    int timepoints;            /* records; 0 -> 1000 (main.cu:35) */
+    int nite;                  /* sub-segment cap per step; 0 -> 4 (main.cu:36) */
+    int boundary;              /* RMS_BOUNDARY_* */
+    int permeation;            /* RMS_PERM_* */
+    double kappa;              /* um/ms, RMS_PERM_KAPPA */
+    const double* pij;         /* [nc*nc], RMS_PERM_TABLE */
+} rms_config;
+
+typedef struct rms_run_opts {
+    uint64_t seed;             /* RNG seed (the reference reads /dev/random) */
+    int precision;             /* RMS_PREC_* */
+    int device;                /* CUDA device ordinal */
+    void* stream;              /* cudaStream_t to run on; NULL = library stream */
+    int trace_walkers;         /* > 0: keep per-step voxel/event traces of
+                                  walkers [0, trace_walkers) (COMPAT only) */
+    int block_size;            /* threads per block; 0 = tuned default */
+    int64_t walker_begin;      /* walk walkers [walker_begin, walker_end) of */
+    int64_t walker_end;        /* the job; 0, 0 = all.  Lets ranks shard a job. */
+} rms_run_opts;
+
+typedef struct rms_sim rms_sim;
+
+/* Output fields (rms_sim_get).  Layouts follow the reference's files
+ * (main.cu:550-615, main_PGSE.cu:596-669): row-major [timepoints][cols]. */
+#define RMS_FIELD_SIG0 0        /* [T]            sig0.txt */
+#define RMS_FIELD_DX2 1         /* [T*6]          dx2.txt  xx xy xz yy yz zz */
+#define RMS_FIELD_DX4 2         /* [T*15]         dx4.txt  (readRMS.m:16-18 order) */
+#define RMS_FIELD_SIGRE 3       /* [T*nbvec]      sigRe.txt (narrow) */
+#define RMS_FIELD_SIG 4         /* [ngrad]        sig.txt   (PGSE) */
+#define RMS_FIELD_NPAR_COUNT 5  /* [T*nc]         NPar_count.txt */
+#define RMS_FIELD_TD 6          /* [T]            diff_time.txt */
+/* Derived tables, available without a run (main.cu:421-458): */
+#define RMS_FIELD_DIFFUSIVITY 7 /* [nc]           um^2/ms */
+#define RMS_FIELD_STEP 8        /* [nc]           step length in voxels */
+#define RMS_FIELD_PIJ 9         /* [nc*nc]        permeation probability a -> b */
+
+/* Build a simulation from a configuration (what main.cu:414-487 derives from
+ * the text inputs).  Replaces: the input parsing + table set-up of
+ * hpc_code/lib/main.cu:388-487 and main_PGSE.cu:414-527. */
+int rms_sim_create(const rms_config* cfg, rms_sim** out);
+
+/* Build a simulation from a run directory of reference inputs
+ * (simParamInput.txt, diffusivity.txt, T2.txt, fiber.txt, and bval/bvec.txt
+ * or gradient_Ngrad/gradient_time.txt).  mode: RMS_MODE_* or RMS_MODE_AUTO.
+ * Replaces: the ifstream readers of main.cu:414-482, main_PGSE.cu:440-506. */
+int rms_sim_load_dir(const char* dir, int mode, rms_sim** out);
+
+/* Set (copy in) the label lattice, n3 fastest.  Labels must be < nc.
+ * Replaces: fiber.txt -> APix (main.cu:461-466, :532). */
+int rms_sim_set_lattice(rms_sim* sim, const uint8_t* labels, int n1, int n2, int n3);
+
+/* Run the walk on the GPU; results stay in the sim until rms_sim_get.
+ * Replaces: setup_kernel + propagate launch + copy-back
+ * (main.cu:498-547, main_PGSE.cu:536-592). */
+int rms_sim_run(rms_sim* sim, const rms_run_opts* opts);
+
+/* Number of doubles in an output field. */
+int rms_sim_field_size(const rms_sim* sim, int field, size_t* n);
+
+/* Copy an output field into a caller buffer of n doubles (n must equal the
+ * field size).  Replaces: thrust::copy back (main.cu:542-547). */
+int rms_sim_get(const rms_sim* sim, int field, double* out, size_t n);
+
+/* Per-step traces of the first trace_walkers walkers of the last COMPAT run:
+ * init_voxel[w], voxel[w*tn+i] (linear index after step i), events[w*tn+i]
+ * (4 bits per sub-segment event: axis | type<<2, type 1 wall, 2 reflect,
+ * 3 cross; bits 28-30 event count; bit 31 remainder dropped).  No
+ * reference counterpart: the test hook for step-by-step parity. */
+int rms_sim_get_trace(const rms_sim* sim, int32_t* init_voxel, int32_t* voxel,
+                      uint32_t* events, size_t nwalkers, size_t tn);
+
+/* Write the reference's output files into dir.  Replaces: the ofstream
+ * writers of main.cu:550-615 and main_PGSE.cu:596-669. */
+int rms_sim_write_dir(const rms_sim* sim, const char* dir);
+
+/* Device time of the last run's walk kernel and of the whole run (ms), from
+ * CUDA events on the run's stream.  Replaces the clock() print of
+ * main.cu:536-540. */
+int rms_sim_last_timing(const rms_sim* sim, double* walk_ms, double* run_ms);
+
+/* Run several simulations (e.g. one per axon) on one device back to back on
+ * one stream.  Replaces: the serial per-axon loop of part1_demo3_simulation.m:83-92. */
+int rms_batch_run(rms_sim* const* sims, int n, const rms_run_opts* opts);
+
+/* Thread-local message of the last failed call ("" if none). */
+const char* rms_last_error(void);
+
+void rms_sim_destroy(rms_sim* sim);
+
+/* The engine's random stream on the host: n uniforms of walker `walker`
+ * (Philox4x32-10; doubles take two words, floats one).  Replaces the draws of
+ * curand_uniform_double (main.cu:118-120, 140, 144, 282); a test hook. */
+int rms_rng_doubles(uint64_t seed, uint64_t walker, int n, double* out);
+int rms_rng_floats(uint64_t seed, uint64_t walker, int n, float* out);
+int rms_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Library version string. */
+const char* rms_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

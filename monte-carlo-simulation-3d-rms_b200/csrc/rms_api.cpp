@@ -1,0 +1,695 @@
+// rms_api.cpp -- the C ABI of include/rms.h: configuration, derived tables,
+// device resources, launch and result unpacking.
+//
+// Host-side counterpart of the reference's main() (hpc_code/lib/main.cu:388-621,
+// main_PGSE.cu:414-675): it derives the same tables, then runs the walk
+// kernels (rms_walk_*.cu) and the ordered reduction (rms_reduce.cu) instead of
+// `propagate` with FP64 CAS atomics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <sstream>
+#include <tuple>
+
+#include "philox.cuh"
+#include "rms_internal.h"
+#include "rms_sim.h"
+
+namespace {
+thread_local std::string g_last_error;
+
+constexpr int kCompatBlock = 128;
+constexpr int kSplitBlockDefault = 256;
+constexpr int kMaxGrad = 1 << 16;
+
+// One device allocation that only grows.
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess) n = bytes;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct HostPinned {
+    void* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= n) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMallocHost(&p, bytes);
+        if (e == cudaSuccess) n = bytes;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+}  // namespace
+
+struct rms_device_state {
+    int device = -1;
+    cudaStream_t own = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    DevBuf labels, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
+        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev;
+    HostPinned h_out;
+    size_t labels_bytes = 0;
+
+    ~rms_device_state() {
+        if (device >= 0) cudaSetDevice(device);
+        for (DevBuf* b : {&labels, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
+                          &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
+                          &tr_vox, &tr_ev})
+            b->release();
+        h_out.release();
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (e2) cudaEventDestroy(e2);
+        if (own) cudaStreamDestroy(own);
+    }
+};
+
+namespace rms {
+
+int set_error(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return set_error(RMS_ERR_CUDA, m);
+}
+
+#define RMS_CUDA(call)                                      \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// Number of steps i in [0, tn) whose end time (i+1)*dt lies below x; the same
+// double comparison as main_PGSE.cu:341-343, found by bisection (monotone in i).
+int count_below(double x, int tn, double dt) {
+    int lo = 0, hi = tn;
+    while (lo < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (static_cast<double>(mid + 1) * dt < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// PGSE lobes as step windows (main_PGSE.cu:340-346): lobe 1 is the steps with
+// t < delta; lobe 2 the remaining steps with Delta <= t < Delta + delta.
+// With P(n) = sum of the first n displacements, a gradient's phase is
+// |g| dt g_hat . (P(n1) + P(a) - P(b)), lobe 2 = [a, b).  Gradients sharing
+// (n1, a, b) share one window sum ("timing pair").
+void build_pgse_schedule(rms_sim* s) {
+    std::map<std::tuple<int, int, int>, int> pairs;
+    s->gpair.assign(s->ngrad(), 0);
+    std::vector<std::tuple<int, int, int>> keys;
+    for (int j = 0; j < s->ngrad(); ++j) {
+        const double Del = s->grad[6 * j + 0], del = s->grad[6 * j + 1];
+        const int n1 = count_below(del, s->tn, s->dt);
+        const int n2 = count_below(Del, s->tn, s->dt);
+        const int n3 = count_below(Del + del, s->tn, s->dt);
+        const int a = std::max(n1, n2);
+        const int b = std::max(a, n3);
+        auto key = std::make_tuple(n1, a, b);
+        auto it = pairs.find(key);
+        if (it == pairs.end()) {
+            it = pairs.emplace(key, (int)keys.size()).first;
+            keys.push_back(key);
+        }
+        s->gpair[j] = it->second;
+    }
+    s->npairs = (int)keys.size();
+    struct Ev { int step, pair; double coef; };
+    std::vector<Ev> evs;
+    for (int p = 0; p < s->npairs; ++p) {
+        const int n1 = std::get<0>(keys[p]), a = std::get<1>(keys[p]), b = std::get<2>(keys[p]);
+        if (n1 > 0) evs.push_back({n1, p, 1.0});
+        if (a != b) {
+            if (a > 0) evs.push_back({a, p, 1.0});
+            evs.push_back({b, p, -1.0});
+        }
+    }
+    std::stable_sort(evs.begin(), evs.end(), [](const Ev& x, const Ev& y) { return x.step < y.step; });
+    s->ev_step.clear(); s->ev_pair.clear(); s->ev_coef.clear();
+    for (const Ev& e : evs) {
+        s->ev_step.push_back(e.step);
+        s->ev_pair.push_back(e.pair);
+        s->ev_coef.push_back(e.coef);
+    }
+}
+
+}  // namespace
+
+int finalize_config(rms_sim* s) {
+    std::ostringstream m;
+    if (s->mode != RMS_MODE_NARROW && s->mode != RMS_MODE_PGSE) return set_error(RMS_ERR_ARG, "mode");
+    if (!(s->dt > 0.0) || !std::isfinite(s->dt)) return set_error(RMS_ERR_RANGE, "dt must be > 0");
+    if (s->tn < 1) return set_error(RMS_ERR_RANGE, "TN must be >= 1");
+    if (s->npar < 1 || s->npar > (int64_t)1 << 40) return set_error(RMS_ERR_RANGE, "NPar out of range");
+    if (s->nc < 1 || s->nc > kNcMax) {
+        m << "Nc = " << s->nc << " outside [1, " << kNcMax << "]";
+        return set_error(RMS_ERR_RANGE, m.str());
+    }
+    if (!(s->res > 0.0)) return set_error(RMS_ERR_RANGE, "voxel size must be > 0");
+    if (s->n1 < 1 || s->n2 < 1 || s->n3 < 1) return set_error(RMS_ERR_RANGE, "lattice size must be >= 1");
+    if ((double)s->n1 * s->n2 * s->n3 >= 2147483648.0)
+        return set_error(RMS_ERR_RANGE, "lattice larger than 2^31 voxels");
+    if ((int)s->diffusivity.size() != s->nc || (int)s->t2.size() != s->nc)
+        return set_error(RMS_ERR_ARG, "diffusivity and T2 need Nc values");
+    if (s->timepoints == 0) s->timepoints = 1000;
+    if (s->nite == 0) s->nite = 4;
+    if (s->timepoints < 1 || s->timepoints > kMaxTimepoints)
+        return set_error(RMS_ERR_RANGE, "timepoints out of range");
+    if (s->tn < s->timepoints) {
+        m << "TN = " << s->tn << " is below the " << s->timepoints
+          << " recorded timepoints (the reference divides by TN/timepoints)";
+        return set_error(RMS_ERR_RANGE, m.str());
+    }
+    if (s->nite < 1 || s->nite > 7) return set_error(RMS_ERR_RANGE, "nite must be in [1, 7]");
+    if (s->boundary != RMS_BOUNDARY_MIRROR && s->boundary != RMS_BOUNDARY_PERIODIC)
+        return set_error(RMS_ERR_ARG, "boundary");
+    if (s->permeation < RMS_PERM_REFERENCE || s->permeation > RMS_PERM_TABLE)
+        return set_error(RMS_ERR_ARG, "permeation");
+    if ((int)s->bvec.size() != 3 * s->nbvec()) return set_error(RMS_ERR_ARG, "bvec needs 3 values per b-value");
+    if (s->mode == RMS_MODE_PGSE && s->ngrad() > kMaxGrad) return set_error(RMS_ERR_RANGE, "Ngrad too large");
+    if (s->grad.size() % 6) return set_error(RMS_ERR_ARG, "grad needs 6 values per gradient");
+
+    const int nc = s->nc;
+    s->tstep = s->tn / s->timepoints;                       // main.cu:68
+    s->step.assign(nc, 0.0);
+    s->t2_steps.assign(nc, 0.0);
+    for (int i = 0; i < nc; i++) {
+        const double D = s->diffusivity[i];
+        if (!(D >= 0.0) || !std::isfinite(D)) return set_error(RMS_ERR_RANGE, "diffusivity must be >= 0");
+        if (!(s->t2[i] > 0.0)) return set_error(RMS_ERR_RANGE, "T2 must be > 0 (T2 = 0 gives 0/0)");
+        s->t2_steps[i] = s->t2[i] / s->dt;                   // main.cu:433
+        s->step[i] = std::sqrt(6.0 * s->dt * D) / s->res;    // main.cu:440
+        if (i > 0 && !(s->step[i] < 1.0)) {
+            m << "step length of compartment " << i << " is " << s->step[i]
+              << " voxels; it must be below one voxel (cf. analysis/setupRMS.m:65-68)";
+            return set_error(RMS_ERR_RANGE, m.str());
+        }
+    }
+    s->pij.assign((size_t)nc * nc, 0.0);
+    for (int i = 0; i < nc; i++) {
+        for (int j = 0; j < nc; j++) {
+            double p;
+            if (s->permeation == RMS_PERM_TABLE) {
+                if ((int)s->pij_in.size() != nc * nc) return set_error(RMS_ERR_ARG, "pij table needs Nc*Nc values");
+                p = s->pij_in[(size_t)i * nc + j];
+                if (!(p >= 0.0 && p <= 1.0)) return set_error(RMS_ERR_RANGE, "pij values must be in [0, 1]");
+            } else if (i == 0 || j == 0) {                   // main.cu:448-454
+                p = 0.0;
+            } else if (i == j) {
+                p = 1.0;
+            } else if (s->permeation == RMS_PERM_REFERENCE) {
+                p = std::fmin(1.0, std::sqrt(s->diffusivity[j] / s->diffusivity[i]));
+            } else {
+                // analysis/interaction.m:437-439 (3-D): P = 2/3 kappa ds / D0, P/(1+P)
+                if (!(s->kappa >= 0.0)) return set_error(RMS_ERR_RANGE, "kappa must be >= 0");
+                const double D = s->diffusivity[i];
+                const double ds = std::sqrt(6.0 * D * s->dt);
+                double P = D > 0.0 ? 2.0 / 3.0 * s->kappa * ds / D : 0.0;
+                p = P / (1.0 + P);
+            }
+            s->pij[(size_t)i * nc + j] = p;
+        }
+    }
+    const int T = s->timepoints;
+    s->td.resize(T);
+    for (int i = 0; i < T; i++) s->td[i] = (i * s->tstep + 1) * s->dt;   // main.cu:485-487
+    const int nb = s->nbvec();
+    s->qtab.assign((size_t)T * nb, 0.0);
+    for (int t = 0; t < T; ++t)
+        for (int j = 0; j < nb; ++j) s->qtab[(size_t)t * nb + j] = std::sqrt(s->bval[j] / s->td[t]);  // main.cu:375
+    if (s->mode == RMS_MODE_PGSE) build_pgse_schedule(s);
+    else { s->npairs = 0; s->gpair.clear(); s->ev_step.clear(); s->ev_pair.clear(); s->ev_coef.clear(); }
+    return RMS_OK;
+}
+
+namespace {
+
+int validate_lattice(const uint8_t* labels, size_t n, int nc) {
+    size_t nonzero = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (labels[i] >= nc) {
+            std::ostringstream m;
+            m << "label " << (int)labels[i] << " at voxel " << i << " is not below Nc = " << nc;
+            return set_error(RMS_ERR_RANGE, m.str());
+        }
+        nonzero += labels[i] != 0;
+    }
+    if (nonzero == 0) return set_error(RMS_ERR_RANGE, "lattice has no voxel with a non-zero label");
+    if ((double)nonzero / (double)n < 1e-7)
+        return set_error(RMS_ERR_RANGE, "labelled voxels are below 1e-7 of the lattice; "
+                                        "rejection-sampled initial positions would not finish");
+    return RMS_OK;
+}
+
+int ensure_device(rms_sim* s, int device) {
+    if (s->dev && s->dev->device == device) return RMS_OK;
+    delete s->dev;
+    s->dev = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) return set_error(RMS_ERR_CUDA, "no CUDA device available");
+    if (device < 0 || device >= count) return set_error(RMS_ERR_ARG, "device ordinal out of range");
+    RMS_CUDA(cudaSetDevice(device));
+    auto* d = new rms_device_state();
+    d->device = device;
+    e = cudaStreamCreateWithFlags(&d->own, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&d->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&d->e1);
+    if (e == cudaSuccess) e = cudaEventCreate(&d->e2);
+    if (e != cudaSuccess) { delete d; return cuda_fail(e, "stream/event creation"); }
+    s->dev = d;
+    s->lattice_dirty = true;
+    return RMS_OK;
+}
+
+template <class T>
+cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+    const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+    cudaError_t e = b.ensure(bytes);
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+int run_one(rms_sim* s, const rms_run_opts* o) {
+    if (!s->have_lattice) return set_error(RMS_ERR_STATE, "no lattice: call rms_sim_set_lattice or load a run directory");
+    const int prec = o ? o->precision : RMS_PREC_COMPAT;
+    if (prec != RMS_PREC_COMPAT && prec != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "precision");
+    const int device = o ? o->device : 0;
+    int rc = ensure_device(s, device);
+    if (rc) return rc;
+    rms_device_state* d = s->dev;
+    RMS_CUDA(cudaSetDevice(device));
+    cudaStream_t st = (o && o->stream) ? (cudaStream_t)o->stream : d->own;
+
+    int64_t w0 = o ? o->walker_begin : 0, w1 = o ? o->walker_end : 0;
+    if (w0 == 0 && w1 == 0) w1 = s->npar;
+    if (w0 < 0 || w1 > s->npar || w0 >= w1) return set_error(RMS_ERR_ARG, "walker range outside [0, NPar)");
+    int64_t trace_n = (o && o->trace_walkers > 0) ? o->trace_walkers : 0;
+    if (trace_n && prec != RMS_PREC_COMPAT) return set_error(RMS_ERR_ARG, "traces are recorded by the COMPAT walk only");
+    if (trace_n && w0 != 0) return set_error(RMS_ERR_ARG, "traces need walker_begin = 0");
+    trace_n = std::min<int64_t>(trace_n, w1);
+
+    // launch shape: persistent grid, warps stride over 32-walker tiles
+    int dev_sms = 0;
+    RMS_CUDA(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
+    int block = kCompatBlock;
+    int per_sm;
+    if (prec == RMS_PREC_COMPAT) {
+        per_sm = walk_compat_blocks_per_sm(s->nc, trace_n > 0);
+    } else {
+        block = (o && o->block_size) ? o->block_size : kSplitBlockDefault;
+        if (block % 32 || block < 32 || block > 1024) return set_error(RMS_ERR_ARG, "block_size must be a multiple of 32 in [32, 1024]");
+        per_sm = walk_split_blocks_per_sm(s->nc, block);
+    }
+    if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
+    const int64_t ntiles = (w1 - w0 + 31) / 32;
+    const int64_t warps_per_block = block / 32;
+    int64_t grid64 = std::min<int64_t>((int64_t)dev_sms * per_sm, (ntiles + warps_per_block - 1) / warps_per_block);
+    const int grid = (int)std::max<int64_t>(grid64, 1);
+    const int nthr = grid * block;
+    const int nslots = nthr / 32;
+    const int T = s->timepoints;
+    const int nb = s->nbvec();
+    const int nvals = (s->mode == RMS_MODE_NARROW) ? kRowHead + ((nb + 31) / 32) * 32 : kRowHead;
+    const int ngrad = s->ngrad();
+    const int ngrad_pad = std::max(32, ((ngrad + 31) / 32) * 32);
+    const size_t row = (size_t)T * nvals;
+
+    // inputs
+    if (s->lattice_dirty || d->labels_bytes != s->labels.size()) {
+        RMS_CUDA(d->labels.ensure(s->labels.size()));
+        RMS_CUDA(cudaMemcpyAsync(d->labels.p, s->labels.data(), s->labels.size(), cudaMemcpyHostToDevice, st));
+        d->labels_bytes = s->labels.size();
+        s->lattice_dirty = false;
+    }
+    std::vector<double> tables;
+    tables.insert(tables.end(), s->step.begin(), s->step.end());
+    tables.insert(tables.end(), s->t2_steps.begin(), s->t2_steps.end());
+    tables.insert(tables.end(), s->pij.begin(), s->pij.end());
+    std::vector<float> tablesf;
+    for (double x : s->step) tablesf.push_back((float)x);
+    for (double x : s->t2_steps) tablesf.push_back((float)(1.0 / x));
+    for (double x : s->pij) tablesf.push_back((float)x);
+    RMS_CUDA(upload(d->tables, tables, st));
+    RMS_CUDA(upload(d->tablesf, tablesf, st));
+    RMS_CUDA(upload(d->qtab, s->qtab, st));
+    RMS_CUDA(upload(d->bvec, s->bvec, st));
+    RMS_CUDA(upload(d->grad, s->grad, st));
+    RMS_CUDA(upload(d->gpair, s->gpair, st));
+    RMS_CUDA(upload(d->ev_step, s->ev_step, st));
+    RMS_CUDA(upload(d->ev_pair, s->ev_pair, st));
+    RMS_CUDA(upload(d->ev_coef, s->ev_coef, st));
+
+    // accumulators
+    RMS_CUDA(d->slots.ensure((size_t)nslots * row * sizeof(double)));
+    RMS_CUDA(cudaMemsetAsync(d->slots.p, 0, (size_t)nslots * row * sizeof(double), st));
+    RMS_CUDA(d->out.ensure(row * sizeof(double)));
+    RMS_CUDA(d->err.ensure(sizeof(int)));
+    RMS_CUDA(cudaMemsetAsync(d->err.p, 0, sizeof(int), st));
+    if (s->mode == RMS_MODE_PGSE) {
+        RMS_CUDA(d->sig_slots.ensure((size_t)nslots * ngrad_pad * sizeof(double)));
+        RMS_CUDA(cudaMemsetAsync(d->sig_slots.p, 0, (size_t)nslots * ngrad_pad * sizeof(double), st));
+        RMS_CUDA(d->out_sig.ensure((size_t)ngrad_pad * sizeof(double)));
+        RMS_CUDA(d->vscr.ensure(std::max<size_t>((size_t)s->npairs * 3 * nthr * sizeof(double), 16)));
+    }
+    if (trace_n) {
+        RMS_CUDA(d->tr_init.ensure((size_t)trace_n * sizeof(int32_t)));
+        RMS_CUDA(d->tr_vox.ensure((size_t)trace_n * s->tn * sizeof(int32_t)));
+        RMS_CUDA(d->tr_ev.ensure((size_t)trace_n * s->tn * sizeof(uint32_t)));
+    }
+
+    WalkArgs a{};
+    a.labels = d->labels.as<uint8_t>();
+    a.n1 = s->n1; a.n2 = s->n2; a.n3 = s->n3;
+    a.walker_begin = w0; a.walker_end = w1;
+    a.tn = s->tn; a.tstep = s->tstep; a.timepoints = T; a.nite = s->nite; a.nc = s->nc;
+    a.boundary = s->boundary; a.mode = s->mode;
+    a.res = s->res; a.dt = s->dt;
+    a.seed = o ? o->seed : 0;
+    a.step = d->tables.as<double>();
+    a.t2 = a.step + s->nc;
+    a.pij = a.t2 + s->nc;
+    a.stepf = d->tablesf.as<float>();
+    a.t2invf = a.stepf + s->nc;
+    a.pijf = a.t2invf + s->nc;
+    a.nvals = nvals;
+    a.slots = d->slots.as<double>();
+    a.nbvec = nb;
+    a.qtab = d->qtab.as<double>();
+    a.bvec = d->bvec.as<double>();
+    a.ngrad = ngrad; a.ngrad_pad = ngrad_pad; a.npairs = s->npairs; a.nevents = (int)s->ev_step.size();
+    a.ev_step = d->ev_step.as<int>(); a.ev_pair = d->ev_pair.as<int>(); a.ev_coef = d->ev_coef.as<double>();
+    a.grad = d->grad.as<double>(); a.gpair = d->gpair.as<int>();
+    a.vscr = d->vscr.as<double>();
+    a.sig_slots = d->sig_slots.as<double>();
+    a.err = d->err.as<int>();
+    a.trace_n = trace_n;
+    a.tr_init = d->tr_init.as<int32_t>(); a.tr_vox = d->tr_vox.as<int32_t>(); a.tr_ev = d->tr_ev.as<uint32_t>();
+
+    RMS_CUDA(cudaEventRecord(d->e0, st));
+    int e = (prec == RMS_PREC_COMPAT) ? launch_walk_compat(a, grid, block, trace_n > 0, st)
+                                      : launch_walk_split(a, grid, block, st);
+    if (e) return cuda_fail((cudaError_t)e, "walk kernel launch");
+    RMS_CUDA(cudaEventRecord(d->e1, st));
+    e = launch_reduce_slots(a.slots, nslots, row, d->out.as<double>(), st);
+    if (e) return cuda_fail((cudaError_t)e, "reduce launch");
+    if (s->mode == RMS_MODE_PGSE) {
+        e = launch_reduce_slots(a.sig_slots, nslots, (size_t)ngrad_pad, d->out_sig.as<double>(), st);
+        if (e) return cuda_fail((cudaError_t)e, "reduce launch");
+    }
+    RMS_CUDA(cudaEventRecord(d->e2, st));
+
+    // results back (one pinned staging buffer: row, then sig, then the error word)
+    const size_t host_bytes = (row + ngrad_pad + 1) * sizeof(double);
+    RMS_CUDA(d->h_out.ensure(host_bytes));
+    double* h = static_cast<double*>(d->h_out.p);
+    RMS_CUDA(cudaMemcpyAsync(h, d->out.p, row * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (s->mode == RMS_MODE_PGSE)
+        RMS_CUDA(cudaMemcpyAsync(h + row, d->out_sig.p, ngrad_pad * sizeof(double), cudaMemcpyDeviceToHost, st));
+    int* herr = reinterpret_cast<int*>(h + row + ngrad_pad);
+    RMS_CUDA(cudaMemcpyAsync(herr, d->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (trace_n) {
+        s->tr_init.resize(trace_n);
+        s->tr_vox.resize((size_t)trace_n * s->tn);
+        s->tr_ev.resize((size_t)trace_n * s->tn);
+        RMS_CUDA(cudaMemcpyAsync(s->tr_init.data(), d->tr_init.p, trace_n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        RMS_CUDA(cudaMemcpyAsync(s->tr_vox.data(), d->tr_vox.p, s->tr_vox.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        RMS_CUDA(cudaMemcpyAsync(s->tr_ev.data(), d->tr_ev.p, s->tr_ev.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    }
+    RMS_CUDA(cudaStreamSynchronize(st));
+    if (*herr & kErrInitCap)
+        return set_error(RMS_ERR_RANGE, "a walker found no labelled voxel within the rejection-sampling cap");
+    if (*herr & kErrStep) return set_error(RMS_ERR_RANGE, "a step segment found no voxel face (step >= 1 voxel)");
+
+    float ms = 0.f;
+    RMS_CUDA(cudaEventElapsedTime(&ms, d->e0, d->e1));
+    s->walk_ms = ms;
+    RMS_CUDA(cudaEventElapsedTime(&ms, d->e0, d->e2));
+    s->run_ms = ms;
+    s->last_grid = grid;
+    s->last_block = block;
+
+    // unpack record rows into the reference's field layouts
+    s->sig0.assign(T, 0.0);
+    s->dx2.assign((size_t)T * 6, 0.0);
+    s->dx4.assign((size_t)T * 15, 0.0);
+    s->npar_count.assign((size_t)T * s->nc, 0.0);
+    s->sigre.assign((size_t)T * nb, 0.0);
+    for (int t = 0; t < T; ++t) {
+        const double* r = h + (size_t)t * nvals;
+        s->sig0[t] = r[kColSig0];
+        for (int k = 0; k < 6; ++k) s->dx2[t * 6 + k] = r[kColDx2 + k];
+        for (int k = 0; k < 15; ++k) s->dx4[t * 15 + k] = r[kColDx4 + k];
+        for (int c = 0; c < s->nc; ++c) s->npar_count[t * s->nc + c] = r[kColCount + c];
+        if (s->mode == RMS_MODE_NARROW)
+            for (int j = 0; j < nb; ++j) s->sigre[(size_t)t * nb + j] = r[kRowHead + j];
+    }
+    s->sig.assign(s->mode == RMS_MODE_PGSE ? ngrad : 0, 0.0);
+    for (int j = 0; j < (int)s->sig.size(); ++j) s->sig[j] = h[row + j];
+    s->trace_n = trace_n;
+    s->have_results = true;
+    return RMS_OK;
+}
+
+bool field_size(const rms_sim* s, int field, size_t& n) {
+    const size_t T = s->timepoints;
+    switch (field) {
+        case RMS_FIELD_SIG0: n = T; return true;
+        case RMS_FIELD_DX2: n = T * 6; return true;
+        case RMS_FIELD_DX4: n = T * 15; return true;
+        case RMS_FIELD_SIGRE: n = s->mode == RMS_MODE_NARROW ? T * s->nbvec() : 0; return true;
+        case RMS_FIELD_SIG: n = s->mode == RMS_MODE_PGSE ? (size_t)s->ngrad() : 0; return true;
+        case RMS_FIELD_NPAR_COUNT: n = T * s->nc; return true;
+        case RMS_FIELD_TD: n = T; return true;
+        case RMS_FIELD_DIFFUSIVITY: n = s->nc; return true;
+        case RMS_FIELD_STEP: n = s->nc; return true;
+        case RMS_FIELD_PIJ: n = (size_t)s->nc * s->nc; return true;
+        default: return false;
+    }
+}
+
+}  // namespace
+}  // namespace rms
+
+using namespace rms;
+
+extern "C" {
+
+const char* rms_last_error(void) { return g_last_error.c_str(); }
+
+const char* rms_version(void) { return "rms_b200 0.1 (sm_100a)"; }
+
+int rms_sim_create(const rms_config* cfg, rms_sim** out) {
+    if (!cfg || !out) return set_error(RMS_ERR_ARG, "null argument");
+    *out = nullptr;
+    auto* s = new (std::nothrow) rms_sim();
+    if (!s) return set_error(RMS_ERR_NOMEM, "out of host memory");
+    s->mode = cfg->mode;
+    s->dt = cfg->dt;
+    s->tn = cfg->tn;
+    s->npar = cfg->npar;
+    s->nc = cfg->nc;
+    s->res = cfg->res;
+    s->n1 = cfg->n1; s->n2 = cfg->n2; s->n3 = cfg->n3;
+    auto copy = [](const double* p, size_t n, std::vector<double>& v) -> bool {
+        if (n && !p) return false;
+        v.assign(p, p + n);
+        return true;
+    };
+    const int nc = cfg->nc > 0 ? cfg->nc : 0;
+    bool ok = copy(cfg->diffusivity, nc, s->diffusivity) && copy(cfg->t2, nc, s->t2);
+    if (cfg->mode == RMS_MODE_NARROW) {
+        ok = ok && cfg->nbvec >= 0 && copy(cfg->bval, cfg->nbvec, s->bval) &&
+             copy(cfg->bvec, (size_t)cfg->nbvec * 3, s->bvec);
+    } else {
+        ok = ok && cfg->ngrad >= 0 && copy(cfg->grad, (size_t)cfg->ngrad * 6, s->grad);
+    }
+    if (cfg->permeation == RMS_PERM_TABLE) ok = ok && copy(cfg->pij, (size_t)nc * nc, s->pij_in);
+    if (!ok) { delete s; return set_error(RMS_ERR_ARG, "missing array for a non-zero count"); }
+    s->timepoints = cfg->timepoints;
+    s->nite = cfg->nite;
+    s->boundary = cfg->boundary;
+    s->permeation = cfg->permeation;
+    s->kappa = cfg->kappa;
+    int rc = finalize_config(s);
+    if (rc) { delete s; return rc; }
+    *out = s;
+    return RMS_OK;
+}
+
+int rms_sim_load_dir(const char* dir, int mode, rms_sim** out) {
+    if (!dir || !out) return set_error(RMS_ERR_ARG, "null argument");
+    *out = nullptr;
+    auto* s = new (std::nothrow) rms_sim();
+    if (!s) return set_error(RMS_ERR_NOMEM, "out of host memory");
+    int rc = load_run_dir(dir, mode, s);
+    if (rc == RMS_OK) rc = validate_lattice(s->labels.data(), s->labels.size(), s->nc);
+    if (rc) { delete s; return rc; }
+    *out = s;
+    return RMS_OK;
+}
+
+int rms_sim_set_lattice(rms_sim* s, const uint8_t* labels, int n1, int n2, int n3) {
+    if (!s || !labels) return set_error(RMS_ERR_ARG, "null argument");
+    if (n1 != s->n1 || n2 != s->n2 || n3 != s->n3) {
+        std::ostringstream m;
+        m << "lattice " << n1 << "x" << n2 << "x" << n3 << " does not match the configured "
+          << s->n1 << "x" << s->n2 << "x" << s->n3;
+        return set_error(RMS_ERR_ARG, m.str());
+    }
+    const size_t n = (size_t)n1 * n2 * n3;
+    int rc = validate_lattice(labels, n, s->nc);
+    if (rc) return rc;
+    s->labels.assign(labels, labels + n);
+    s->have_lattice = true;
+    s->lattice_dirty = true;
+    return RMS_OK;
+}
+
+int rms_sim_run(rms_sim* s, const rms_run_opts* opts) {
+    if (!s) return set_error(RMS_ERR_ARG, "null sim");
+    try {
+        return run_one(s, opts);
+    } catch (const std::exception& e) {
+        return set_error(RMS_ERR_NOMEM, e.what());
+    }
+}
+
+int rms_batch_run(rms_sim* const* sims, int n, const rms_run_opts* opts) {
+    if (!sims || n < 0) return set_error(RMS_ERR_ARG, "null argument");
+    for (int i = 0; i < n; ++i) {
+        int rc = rms_sim_run(sims[i], opts);
+        if (rc) {
+            std::ostringstream m;
+            m << "simulation " << i << ": " << g_last_error;
+            return set_error(rc, m.str());
+        }
+    }
+    return RMS_OK;
+}
+
+int rms_sim_field_size(const rms_sim* s, int field, size_t* n) {
+    if (!s || !n) return set_error(RMS_ERR_ARG, "null argument");
+    if (!field_size(s, field, *n)) return set_error(RMS_ERR_ARG, "unknown field");
+    return RMS_OK;
+}
+
+int rms_sim_get(const rms_sim* s, int field, double* out, size_t n) {
+    if (!s || (!out && n)) return set_error(RMS_ERR_ARG, "null argument");
+    size_t want = 0;
+    if (!field_size(s, field, want)) return set_error(RMS_ERR_ARG, "unknown field");
+    if (n != want) {
+        std::ostringstream m;
+        m << "field holds " << want << " values, buffer has " << n;
+        return set_error(RMS_ERR_ARG, m.str());
+    }
+    const std::vector<double>* table = nullptr;
+    if (field == RMS_FIELD_TD) table = &s->td;
+    if (field == RMS_FIELD_DIFFUSIVITY) table = &s->diffusivity;
+    if (field == RMS_FIELD_STEP) table = &s->step;
+    if (field == RMS_FIELD_PIJ) table = &s->pij;
+    if (table) {
+        std::copy(table->begin(), table->end(), out);
+        return RMS_OK;
+    }
+    if (!s->have_results) return set_error(RMS_ERR_STATE, "no results: run the simulation first");
+    const std::vector<double>* v = nullptr;
+    switch (field) {
+        case RMS_FIELD_SIG0: v = &s->sig0; break;
+        case RMS_FIELD_DX2: v = &s->dx2; break;
+        case RMS_FIELD_DX4: v = &s->dx4; break;
+        case RMS_FIELD_SIGRE: v = &s->sigre; break;
+        case RMS_FIELD_SIG: v = &s->sig; break;
+        case RMS_FIELD_NPAR_COUNT: v = &s->npar_count; break;
+    }
+    std::copy(v->begin(), v->end(), out);
+    return RMS_OK;
+}
+
+int rms_sim_get_trace(const rms_sim* s, int32_t* init_voxel, int32_t* voxel, uint32_t* events,
+                      size_t nwalkers, size_t tn) {
+    if (!s || !init_voxel || !voxel || !events) return set_error(RMS_ERR_ARG, "null argument");
+    if (!s->have_results || s->trace_n == 0) return set_error(RMS_ERR_STATE, "the last run kept no traces");
+    if (nwalkers != (size_t)s->trace_n || tn != (size_t)s->tn)
+        return set_error(RMS_ERR_ARG, "trace buffer shape differs from the last run");
+    std::copy(s->tr_init.begin(), s->tr_init.end(), init_voxel);
+    std::copy(s->tr_vox.begin(), s->tr_vox.end(), voxel);
+    std::copy(s->tr_ev.begin(), s->tr_ev.end(), events);
+    return RMS_OK;
+}
+
+int rms_sim_write_dir(const rms_sim* s, const char* dir) {
+    if (!s || !dir) return set_error(RMS_ERR_ARG, "null argument");
+    return write_run_dir(s, dir);
+}
+
+int rms_sim_last_timing(const rms_sim* s, double* walk_ms, double* run_ms) {
+    if (!s) return set_error(RMS_ERR_ARG, "null sim");
+    if (!s->have_results) return set_error(RMS_ERR_STATE, "no run yet");
+    if (walk_ms) *walk_ms = s->walk_ms;
+    if (run_ms) *run_ms = s->run_ms;
+    return RMS_OK;
+}
+
+void rms_sim_destroy(rms_sim* s) {
+    if (!s) return;
+    delete s->dev;
+    delete s;
+}
+
+int rms_rng_doubles(uint64_t seed, uint64_t walker, int n, double* out) {
+    if (n < 0 || (n && !out)) return set_error(RMS_ERR_ARG, "bad buffer");
+    DoubleStream r;
+    r.init(seed, walker);
+    for (int i = 0; i < n; ++i) out[i] = r.next();
+    return RMS_OK;
+}
+
+int rms_rng_floats(uint64_t seed, uint64_t walker, int n, float* out) {
+    if (n < 0 || (n && !out)) return set_error(RMS_ERR_ARG, "bad buffer");
+    FloatStream r;
+    r.init(seed, walker);
+    for (int i = 0; i < n; ++i) out[i] = r.next();
+    return RMS_OK;
+}
+
+int rms_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    if (!ctr || !key || !out) return set_error(RMS_ERR_ARG, "null argument");
+    const U4 r = philox4x32_10(U4{ctr[0], ctr[1], ctr[2], ctr[3]}, key[0], key[1]);
+    out[0] = r.x; out[1] = r.y; out[2] = r.z; out[3] = r.w;
+    return RMS_OK;
+}
+
+}  // extern "C"

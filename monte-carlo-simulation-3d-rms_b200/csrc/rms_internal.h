@@ -1,0 +1,69 @@
+// rms_internal.h -- engine internals shared by the host library (C++) and the
+// kernels (CUDA).  Not part of the C ABI (include/rms.h).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace rms {
+
+constexpr int kWarp = 32;
+constexpr int kNcMax = 8;          // compartments supported by the kernels
+constexpr int kRowHead = 32;       // record row: [sig0, dx2 x6, dx4 x15, count x nc, pad] then signals
+constexpr int kColSig0 = 0;
+constexpr int kColDx2 = 1;
+constexpr int kColDx4 = 7;
+constexpr int kColCount = 22;      // + compartment
+constexpr int kMaxTimepoints = 1 << 20;
+constexpr long long kInitTryCap = 1ll << 26;   // rejection-sampling attempts per walker
+constexpr int kErrInitCap = 1;                  // a walker found no labelled voxel in kInitTryCap tries
+constexpr int kErrStep = 2;                     // a segment found no face (step >= 1 voxel)
+
+// Arguments of the walk kernels (passed by value; pointers are device memory).
+struct WalkArgs {
+    const uint8_t* labels;      // [n1*n2*n3], n3 fastest
+    int n1, n2, n3;
+    int64_t walker_begin, walker_end;
+    int tn, tstep, timepoints, nite, nc, boundary, mode;
+    double res, dt;
+    uint64_t seed;
+    const double* step;         // [nc] voxels
+    const double* t2;           // [nc] steps
+    const double* pij;          // [nc*nc]
+    int nvals;                  // doubles per record row, multiple of 32
+    double* slots;              // [nslots][timepoints][nvals]
+    // narrow pulse
+    int nbvec;
+    const double* qtab;         // [timepoints][nbvec] = sqrt(bval/TD)
+    const double* bvec;         // [nbvec*3]
+    // PGSE
+    int ngrad, ngrad_pad, npairs, nevents;
+    const int* ev_step;         // [nevents], ascending: P(ev_step) enters pair ev_pair
+    const int* ev_pair;
+    const double* ev_coef;      // +1 or -1
+    const double* grad;         // [ngrad*6]
+    const int* gpair;           // [ngrad] timing pair of each gradient
+    double* vscr;               // [npairs*3][nthreads] per-thread window sums
+    double* sig_slots;          // [nslots][ngrad_pad]
+    // split precision (FP32 arithmetic): per-compartment FP32 tables
+    const float* stepf;         // [nc]
+    const float* t2invf;        // [nc] 1 / (T2 in steps)
+    const float* pijf;          // [nc*nc]
+    int* err;                   // device error word (kErr* bits), zeroed per run
+    // traces (COMPAT)
+    int64_t trace_n;
+    int32_t* tr_init;
+    int32_t* tr_vox;
+    uint32_t* tr_ev;
+};
+
+// Launchers (rms_walk_*.cu, rms_reduce.cu).  All asynchronous on `stream`;
+// they return a cudaError_t value (0 = success).
+int launch_walk_compat(const WalkArgs& a, int grid, int block, bool trace, void* stream);
+int launch_walk_split(const WalkArgs& a, int grid, int block, void* stream);
+int launch_reduce_slots(const double* slots, int nslots, size_t row, double* out, void* stream);
+// Resident blocks per SM of the walk kernels (occupancy API); -1 on error.
+int walk_compat_blocks_per_sm(int nc, bool trace);
+int walk_split_blocks_per_sm(int nc, int block);
+const char* cuda_error_string(int code);
+
+}  // namespace rms

@@ -1,0 +1,264 @@
+"""ctypes binding of librms (include/rms.h).
+
+The engine's compute path is the compiled library; this module only marshals
+arrays across the C ABI.  There is no Python or CPU fallback: if librms.so is
+missing, or no GPU is present when a run is requested, the call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "_build", "librms.so")
+CLI_PATH = os.path.join(PKG_DIR, "_build", "rms_main")
+
+MODE = {"narrow": 0, "pgse": 1, "auto": -1}
+BOUNDARY = {"mirror": 0, "periodic": 1}
+PERMEATION = {"reference": 0, "kappa": 1, "table": 2}
+PRECISION = {"compat": 0, "split": 1}
+FIELD = {"sig0": 0, "dx2": 1, "dx4": 2, "sigre": 3, "sig": 4, "npar_count": 5, "td": 6,
+         "diffusivity": 7, "step": 8, "pij": 9}
+ERRORS = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "RANGE", -5: "CUDA", -6: "NOMEM",
+          -7: "STATE", -8: "TIMEOUT"}
+
+# The C ABI's exported names (include/rms.h), checked by the CPU tests.
+EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim_run",
+           "rms_sim_field_size", "rms_sim_get", "rms_sim_get_trace", "rms_sim_write_dir",
+           "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
+           "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version")
+
+_DP = C.POINTER(C.c_double)
+
+
+class RmsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rms error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int), ("dt", C.c_double), ("tn", C.c_int), ("npar", C.c_int64),
+        ("nc", C.c_int), ("res", C.c_double), ("n1", C.c_int), ("n2", C.c_int), ("n3", C.c_int),
+        ("diffusivity", _DP), ("t2", _DP),
+        ("nbvec", C.c_int), ("bval", _DP), ("bvec", _DP),
+        ("ngrad", C.c_int), ("grad", _DP),
+        ("timepoints", C.c_int), ("nite", C.c_int), ("boundary", C.c_int),
+        ("permeation", C.c_int), ("kappa", C.c_double), ("pij", _DP),
+    ]
+
+
+class RunOpts(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64), ("precision", C.c_int), ("device", C.c_int),
+        ("stream", C.c_void_p), ("trace_walkers", C.c_int), ("block_size", C.c_int),
+        ("walker_begin", C.c_int64), ("walker_end", C.c_int64),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load librms.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"librms.so not built: {LIB_PATH} "
+                               "(run __graft_entry__.build() or make -C monte-carlo-simulation-3d-rms_b200/csrc)")
+        L = C.CDLL(LIB_PATH)
+        L.rms_last_error.restype = C.c_char_p
+        L.rms_version.restype = C.c_char_p
+        for name in EXPORTS:
+            if name not in ("rms_last_error", "rms_version", "rms_sim_destroy"):
+                getattr(L, name).restype = C.c_int
+        L.rms_sim_destroy.restype = None
+        L.rms_sim_create.argtypes = [C.POINTER(Config), C.POINTER(C.c_void_p)]
+        L.rms_sim_load_dir.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
+        L.rms_sim_set_lattice.argtypes = [C.c_void_p, C.POINTER(C.c_uint8), C.c_int, C.c_int, C.c_int]
+        L.rms_sim_run.argtypes = [C.c_void_p, C.POINTER(RunOpts)]
+        L.rms_sim_field_size.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t)]
+        L.rms_sim_get.argtypes = [C.c_void_p, C.c_int, _DP, C.c_size_t]
+        L.rms_sim_get_trace.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_uint32), C.c_size_t, C.c_size_t]
+        L.rms_sim_write_dir.argtypes = [C.c_void_p, C.c_char_p]
+        L.rms_sim_last_timing.argtypes = [C.c_void_p, _DP, _DP]
+        L.rms_batch_run.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts)]
+        L.rms_sim_destroy.argtypes = [C.c_void_p]
+        L.rms_rng_doubles.argtypes = [C.c_uint64, C.c_uint64, C.c_int, _DP]
+        L.rms_rng_floats.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.POINTER(C.c_float)]
+        L.rms_philox4x32_10.argtypes = [C.POINTER(C.c_uint32)] * 3
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise RmsError(rc, lib().rms_last_error().decode(errors="replace"))
+
+
+def _arr(x, dtype=np.float64):
+    return np.ascontiguousarray(np.asarray(x, dtype=dtype).reshape(-1))
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return a.ctypes.data_as(_DP) if a is not None and a.size else None
+
+
+class Sim:
+    """One simulation (an ``rms_sim``): configuration, lattice, results."""
+
+    def __init__(self, labels=None, *, dt, tn, npar, res, diffusivity, t2, nc=None,
+                 shape=None, bval=None, bvec=None, grad=None, timepoints=0, nite=0,
+                 boundary="mirror", permeation="reference", kappa=0.0, pij=None):
+        self._h = C.c_void_p()
+        d = _arr(diffusivity)
+        t2a = _arr(t2)
+        mode = "pgse" if grad is not None else "narrow"
+        if labels is not None:
+            labels = np.ascontiguousarray(labels, dtype=np.uint8)
+            shape = labels.shape
+        if shape is None:
+            raise ValueError("give labels or shape")
+        self._keep = [d, t2a]
+        bv = _arr(bval if bval is not None else [])
+        bvc = _arr(bvec if bvec is not None else [])
+        gr = _arr(grad if grad is not None else [])
+        pj = _arr(pij) if pij is not None else None
+        self._keep += [bv, bvc, gr, pj]
+        cfg = Config(MODE[mode], float(dt), int(tn), int(npar), int(nc or d.size), float(res),
+                     int(shape[0]), int(shape[1]), int(shape[2]), _ptr(d), _ptr(t2a),
+                     bv.size if mode == "narrow" else 0, _ptr(bv), _ptr(bvc),
+                     gr.size // 6 if mode == "pgse" else 0, _ptr(gr),
+                     int(timepoints), int(nite), BOUNDARY[boundary], PERMEATION[permeation],
+                     float(kappa), _ptr(pj))
+        _check(lib().rms_sim_create(C.byref(cfg), C.byref(self._h)))
+        self.mode = mode
+        self.shape = tuple(int(x) for x in shape)
+        self.tn = int(tn)
+        if labels is not None:
+            self.set_lattice(labels)
+
+    @classmethod
+    def from_dir(cls, path: str, mode: str = "auto") -> "Sim":
+        self = cls.__new__(cls)
+        self._h = C.c_void_p()
+        self._keep = []
+        _check(lib().rms_sim_load_dir(path.encode(), MODE[mode], C.byref(self._h)))
+        if mode == "auto":
+            mode = "pgse" if os.path.exists(os.path.join(path, "gradient_time.txt")) else "narrow"
+        self.mode = mode
+        vals = open(os.path.join(path, "simParamInput.txt")).read().split()
+        self.tn = int(vals[1])
+        self.shape = tuple(int(v) for v in vals[-3:])
+        return self
+
+    def set_lattice(self, labels: np.ndarray):
+        lab = np.ascontiguousarray(labels, dtype=np.uint8)
+        if lab.ndim != 3:
+            raise ValueError("labels must be 3-D")
+        _check(lib().rms_sim_set_lattice(self._h, lab.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                         *[int(x) for x in lab.shape]))
+
+    def run(self, seed: int = 0, precision: str = "compat", device: int = 0, stream=None,
+            trace_walkers: int = 0, block_size: int = 0, walker_range=None):
+        w0, w1 = walker_range if walker_range is not None else (0, 0)
+        st = None if stream is None else C.c_void_p(int(stream))
+        opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION[precision], int(device), st,
+                       int(trace_walkers), int(block_size), int(w0), int(w1))
+        _check(lib().rms_sim_run(self._h, C.byref(opts)))
+        return self
+
+    def field_size(self, name: str) -> int:
+        n = C.c_size_t()
+        _check(lib().rms_sim_field_size(self._h, FIELD[name], C.byref(n)))
+        return n.value
+
+    def get(self, name: str) -> np.ndarray:
+        n = self.field_size(name)
+        out = np.zeros(n)
+        _check(lib().rms_sim_get(self._h, FIELD[name], _ptr(out) if n else None, n))
+        return out
+
+    def outputs(self) -> dict:
+        T = self.field_size("sig0")
+        o = dict(sig0=self.get("sig0"), dx2=self.get("dx2").reshape(T, 6),
+                 dx4=self.get("dx4").reshape(T, 15), td=self.get("td"))
+        nc = self.field_size("diffusivity")
+        o["npar_count"] = self.get("npar_count").reshape(T, nc)
+        if self.mode == "narrow":
+            o["sigre"] = self.get("sigre").reshape(T, -1)
+        else:
+            o["sig"] = self.get("sig")
+        return o
+
+    def trace(self, nwalkers: int) -> dict:
+        tr_init = np.zeros(nwalkers, dtype=np.int32)
+        vox = np.zeros((nwalkers, self.tn), dtype=np.int32)
+        ev = np.zeros((nwalkers, self.tn), dtype=np.uint32)
+        _check(lib().rms_sim_get_trace(self._h, tr_init.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       vox.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       ev.ctypes.data_as(C.POINTER(C.c_uint32)), nwalkers, self.tn))
+        return dict(init_voxel=tr_init, voxel=vox, events=ev)
+
+    def write_dir(self, path: str):
+        _check(lib().rms_sim_write_dir(self._h, path.encode()))
+
+    def timing(self):
+        """(walk kernel ms, whole run ms) of the last run, from CUDA events."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().rms_sim_last_timing(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().rms_sim_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def batch_run(sims, seed: int = 0, precision: str = "compat", device: int = 0, stream=None):
+    arr = (C.c_void_p * len(sims))(*[s._h.value for s in sims])
+    st = None if stream is None else C.c_void_p(int(stream))
+    opts = RunOpts(int(seed), PRECISION[precision], int(device), st, 0, 0, 0, 0)
+    _check(lib().rms_batch_run(arr, len(sims), C.byref(opts)))
+
+
+def rng_doubles(seed: int, walker: int, n: int) -> np.ndarray:
+    out = np.zeros(n)
+    _check(lib().rms_rng_doubles(seed, walker, n, _ptr(out)))
+    return out
+
+
+def rng_floats(seed: int, walker: int, n: int) -> np.ndarray:
+    out = np.zeros(n, dtype=np.float32)
+    _check(lib().rms_rng_floats(seed, walker, n, out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out
+
+
+def philox4x32_10(ctr, key) -> np.ndarray:
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    p = C.POINTER(C.c_uint32)
+    _check(lib().rms_philox4x32_10(c.ctypes.data_as(p), k.ctypes.data_as(p), out.ctypes.data_as(p)))
+    return out
+
+
+def version() -> str:
+    return lib().rms_version().decode()

@@ -1,0 +1,249 @@
+"""oracle/pyoracle.py -- TEST INFRASTRUCTURE (the oracle), not product code.
+
+ctypes front end for the two CPU checkers built by oracle/Makefile:
+
+  _build/liboracle.so  the plain-C restatement of the reference walk (rms_oracle.c)
+  _ref/librmsref.so    the reference simulator itself (hpc_code/lib/main.cu,
+                       main_PGSE.cu) compiled for the host through ref_shim/
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "librmsref.so")
+
+MODE_NARROW, MODE_PGSE = 0, 1
+BOUNDARY_MIRROR, BOUNDARY_PERIODIC = 0, 1
+
+
+class OrParams(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int), ("npar", C.c_int64), ("tn", C.c_int), ("timepoints", C.c_int),
+        ("nite", C.c_int), ("nc", C.c_int), ("n1", C.c_int), ("n2", C.c_int), ("n3", C.c_int),
+        ("boundary", C.c_int), ("res", C.c_double), ("dt", C.c_double), ("seed", C.c_uint64),
+        ("step", C.POINTER(C.c_double)), ("t2", C.POINTER(C.c_double)),
+        ("pij", C.POINTER(C.c_double)), ("labels", C.POINTER(C.c_uint8)),
+        ("nbvec", C.c_int), ("bval", C.POINTER(C.c_double)), ("bvec", C.POINTER(C.c_double)),
+        ("td", C.POINTER(C.c_double)), ("ngrad", C.c_int), ("grad", C.POINTER(C.c_double)),
+    ]
+
+
+class OrOutputs(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in
+                ("sig0", "dx2", "dx4", "sigre", "sig", "npar_count")]
+
+
+class OrTrace(C.Structure):
+    _fields_ = [("w0", C.c_int64), ("nw", C.c_int64), ("init_voxel", C.POINTER(C.c_int32)),
+                ("voxel", C.POINTER(C.c_int32)), ("events", C.POINTER(C.c_uint32))]
+
+
+_lib = None
+_ref = None
+
+
+def oracle_lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError(f"oracle library missing: {ORACLE_SO} (run make -C oracle)")
+        _lib = C.CDLL(ORACLE_SO)
+        _lib.or_run.restype = C.c_int
+        _lib.or_run_parallel.restype = C.c_int
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise RuntimeError(f"reference host build missing: {REF_SO}")
+        _ref = C.CDLL(REF_SO)
+        for f in ("ref_narrow_main_dir", "ref_pgse_main_dir", "ref_run_narrow",
+                  "ref_run_pgse", "ref_max_threads"):
+            getattr(_ref, f).restype = C.c_int
+    return _ref
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def reference_tables(dt: float, res: float, diffusivity, t2, timepoints: int = 1000,
+                     tn: Optional[int] = None):
+    """Derived tables exactly as hpc_code/lib/main.cu:421-458, 484-487 computes
+    them: step (voxels), T2/dt, Pij, TD."""
+    d = [float(x) for x in diffusivity]
+    nc = len(d)
+    step = np.array([math.sqrt(6.0 * dt * x) / res for x in d])
+    t2s = np.array([float(x) / dt for x in t2])
+    pij = np.zeros(nc * nc)
+    for i in range(nc):
+        for j in range(nc):
+            if i == 0 or j == 0:
+                pij[i * nc + j] = 0.0
+            elif i == j:
+                pij[i * nc + j] = 1.0
+            else:
+                pij[i * nc + j] = min(1.0, math.sqrt(d[j] / d[i]))
+    td = None
+    if tn is not None:
+        ts = tn // timepoints
+        td = np.array([(i * ts + 1) * dt for i in range(timepoints)])
+    return step, t2s, pij, td
+
+
+class Job:
+    """One simulation job in the oracle's terms (tables already derived)."""
+
+    def __init__(self, labels, *, dt, tn, npar, res, step, t2_steps, pij, seed,
+                 timepoints=1000, nite=4, boundary=BOUNDARY_MIRROR,
+                 bval=None, bvec=None, td=None, grad=None):
+        self.labels = np.ascontiguousarray(labels, dtype=np.uint8)
+        self.n1, self.n2, self.n3 = self.labels.shape
+        self.dt, self.tn, self.npar, self.res = float(dt), int(tn), int(npar), float(res)
+        self.step = np.ascontiguousarray(step, dtype=np.float64)
+        self.t2 = np.ascontiguousarray(t2_steps, dtype=np.float64)
+        self.pij = np.ascontiguousarray(pij, dtype=np.float64)
+        self.nc = self.step.size
+        self.seed = int(seed)
+        self.timepoints, self.nite, self.boundary = int(timepoints), int(nite), int(boundary)
+        self.mode = MODE_PGSE if grad is not None else MODE_NARROW
+        self.bval = np.ascontiguousarray(bval if bval is not None else np.zeros(0), dtype=np.float64)
+        self.bvec = np.ascontiguousarray(bvec if bvec is not None else np.zeros(0), dtype=np.float64).reshape(-1)
+        self.nbvec = self.bval.size if self.mode == MODE_NARROW else 0
+        if td is None:
+            ts = self.tn // self.timepoints
+            td = np.array([(i * ts + 1) * self.dt for i in range(self.timepoints)])
+        self.td = np.ascontiguousarray(td, dtype=np.float64)
+        self.grad = np.ascontiguousarray(grad if grad is not None else np.zeros(0), dtype=np.float64).reshape(-1)
+        self.ngrad = self.grad.size // 6
+
+    def params(self) -> OrParams:
+        return OrParams(
+            self.mode, self.npar, self.tn, self.timepoints, self.nite, self.nc, self.n1,
+            self.n2, self.n3, self.boundary, self.res, self.dt, self.seed,
+            _dp(self.step), _dp(self.t2), _dp(self.pij),
+            self.labels.ctypes.data_as(C.POINTER(C.c_uint8)),
+            self.nbvec, _dp(self.bval), _dp(self.bvec), _dp(self.td),
+            self.ngrad, _dp(self.grad))
+
+    def empty_outputs(self):
+        T = self.timepoints
+        return dict(sig0=np.zeros(T), dx2=np.zeros((T, 6)), dx4=np.zeros((T, 15)),
+                    sigre=np.zeros((T, max(self.nbvec, 0))), sig=np.zeros(self.ngrad),
+                    npar_count=np.zeros((T, self.nc)))
+
+
+def _out_struct(o):
+    return OrOutputs(*(_dp(o[k]) for k in ("sig0", "dx2", "dx4", "sigre", "sig", "npar_count")))
+
+
+def run_oracle(job: Job, w_begin: int = 0, w_end: Optional[int] = None, nthreads: int = 1,
+               trace_walkers: int = 0):
+    """Walk walkers [w_begin, w_end) with the C restatement.  With
+    ``trace_walkers`` > 0 the first that many walkers of the range also
+    return their per-step voxel and event traces (single thread)."""
+    lib = oracle_lib()
+    if w_end is None:
+        w_end = job.npar
+    o = job.empty_outputs()
+    p = job.params()
+    outs = _out_struct(o)
+    if trace_walkers:
+        nw = int(trace_walkers)
+        tr_init = np.zeros(nw, dtype=np.int32)
+        tr_vox = np.zeros((nw, job.tn), dtype=np.int32)
+        tr_ev = np.zeros((nw, job.tn), dtype=np.uint32)
+        tr = OrTrace(w_begin, nw, tr_init.ctypes.data_as(C.POINTER(C.c_int32)),
+                     tr_vox.ctypes.data_as(C.POINTER(C.c_int32)),
+                     tr_ev.ctypes.data_as(C.POINTER(C.c_uint32)))
+        rc = lib.or_run(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.byref(outs), C.byref(tr))
+        o["trace"] = dict(init_voxel=tr_init, voxel=tr_vox, events=tr_ev)
+    elif nthreads > 1:
+        rc = lib.or_run_parallel(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end),
+                                 C.c_int(nthreads), C.byref(outs))
+    else:
+        rc = lib.or_run(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.byref(outs), None)
+    if rc != 0:
+        raise RuntimeError(f"or_run failed: {rc}")
+    return o
+
+
+def stream_doubles(seed: int, walker: int, n: int) -> np.ndarray:
+    out = np.zeros(n)
+    oracle_lib().or_stream_doubles(C.c_uint64(seed), C.c_uint64(walker), C.c_int(n), _dp(out))
+    return out
+
+
+def stream_floats(seed: int, walker: int, n: int) -> np.ndarray:
+    out = np.zeros(n, dtype=np.float32)
+    oracle_lib().or_stream_floats(C.c_uint64(seed), C.c_uint64(walker), C.c_int(n),
+                                  out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def philox4x32_10(ctr, key) -> np.ndarray:
+    c = np.array(ctr, dtype=np.uint32)
+    k = np.array(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    u32p = C.POINTER(C.c_uint32)
+    oracle_lib().or_philox4x32_10(c.ctypes.data_as(u32p), k.ctypes.data_as(u32p),
+                                  out.ctypes.data_as(u32p))
+    return out
+
+
+def run_reference_main(run_dir: str, pgse: bool, seed: int) -> int:
+    """Run the reference program's main() in ``run_dir`` (the process
+    contract of part1_demo3_simulation.m:86-90), seed pinned."""
+    lib = ref_lib()
+    os.environ["RMS_REF_SEED"] = str(int(seed))
+    try:
+        fn = lib.ref_pgse_main_dir if pgse else lib.ref_narrow_main_dir
+        return fn(run_dir.encode())
+    finally:
+        os.environ.pop("RMS_REF_SEED", None)
+
+
+def run_reference_walkers(job: Job, nsample: int, nthreads: int):
+    """The reference's own propagate() on walkers [0, nsample) of the job,
+    OpenMP over walkers (the timed CPU baseline).  Labels go in as int32 like
+    the reference's APix (main.cu:461)."""
+    if job.timepoints != 1000 or job.nite != 4 or job.boundary != BOUNDARY_MIRROR:
+        raise ValueError("the reference build supports only its own constants")
+    lib = ref_lib()
+    apix = np.ascontiguousarray(job.labels, dtype=np.int32)
+    ip = apix.ctypes.data_as(C.POINTER(C.c_int))
+    o = job.empty_outputs()
+    if job.mode == MODE_NARROW:
+        rc = lib.ref_run_narrow(
+            C.c_ulonglong(job.seed), job.tn, job.npar, C.c_int64(nsample), job.nbvec, job.nc,
+            C.c_double(job.res), _dp(job.step), job.n1, job.n2, job.n3, _dp(job.t2),
+            _dp(job.pij), _dp(job.bval), _dp(job.bvec), ip, _dp(job.td), nthreads,
+            _dp(o["sig0"]), _dp(o["dx2"]), _dp(o["dx4"]), _dp(o["sigre"]), _dp(o["npar_count"]))
+    else:
+        rc = lib.ref_run_pgse(
+            C.c_ulonglong(job.seed), job.tn, job.npar, C.c_int64(nsample), job.nc,
+            C.c_double(job.res), C.c_double(job.dt), _dp(job.step), job.n1, job.n2, job.n3,
+            job.ngrad, _dp(job.grad), _dp(job.t2), _dp(job.pij), ip, nthreads,
+            _dp(o["sig0"]), _dp(o["dx2"]), _dp(o["dx4"]), _dp(o["sig"]), _dp(o["npar_count"]))
+    if rc != 0:
+        raise RuntimeError(f"reference run failed: {rc}")
+    return o
+
+
+def ref_max_threads() -> int:
+    return int(ref_lib().ref_max_threads())

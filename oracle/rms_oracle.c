@@ -1,0 +1,355 @@
+/*
+ * oracle/rms_oracle.c -- TEST INFRASTRUCTURE (the oracle), not product code.
+ *
+ * Plain-C restatement of the reference simulator's per-walker loop.  Every
+ * block cites the reference line it follows; expressions keep the reference's
+ * operand order and types so that, compiled without FMA contraction
+ * (oracle/Makefile), a job run here equals the host build of the reference
+ * (oracle/_ref) bit for bit.  See rms_oracle.h for the interface.
+ */
+#include "rms_oracle.h"
+#include "philox_stream.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+
+#define OR_PI 3.14159265 /* main.cu:34 (the reference's truncated pi) */
+#define OR_NC_MAX 16
+
+static inline int64_t lin(const or_params* p, int i, int j, int k) {
+    /* main.cu:124, 132, 272: NPix2*NPix3*i + NPix3*j + k */
+    return (int64_t)p->n2 * p->n3 * i + (int64_t)p->n3 * j + k;
+}
+
+static int check(const or_params* p) {
+    if (p->nc < 1 || p->nc > OR_NC_MAX) return -1;
+    if (p->timepoints < 1 || p->tn < p->timepoints) return -2;
+    if (p->nite < 1 || p->nite > 7) return -3;
+    if (p->n1 < 1 || p->n2 < 1 || p->n3 < 1) return -4;
+    if (p->mode == OR_MODE_PGSE && p->ngrad < 0) return -5;
+    if (p->mode == OR_MODE_NARROW && p->nbvec < 0) return -5;
+    return 0;
+}
+
+static void walk_one(const or_params* p, int64_t w, or_outputs* out, double* phase,
+                     int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev) {
+    const int Nc = p->nc;
+    const int Tstep = p->tn / p->timepoints;               /* main.cu:68 */
+    const int NPix[3] = {p->n1, p->n2, p->n3};             /* main.cu:86 */
+    const uint8_t* APix = p->labels;
+    const double* step = p->step;
+    const double* Pij = p->pij;
+    or_stream st;
+    or_stream_init(&st, p->seed, (uint64_t)w);             /* main.cu:58-61, 66 */
+
+    double xi[3] = {0}, xt[3] = {0}, vt[3] = {0};
+    int xParGi[3] = {0}, xParGj[3] = {0};
+    int flip0[3] = {0}, flip1[3] = {0};
+    double t[OR_NC_MAX] = {0};
+    int ai = 0, aj = 0, ii_hit = 0;
+
+    /* initial position: rejection sampling in the box (main.cu:117-125) */
+    for (;;) {
+        xi[0] = or_stream_double(&st) * (double)p->n1;
+        xi[1] = or_stream_double(&st) * (double)p->n2;
+        xi[2] = or_stream_double(&st) * (double)p->n3;
+        xParGi[0] = (int)floor(xi[0]);
+        xParGi[1] = (int)floor(xi[1]);
+        xParGi[2] = (int)floor(xi[2]);
+        if (APix[lin(p, xParGi[0], xParGi[1], xParGi[2])] != 0) break;
+    }
+    /* main.cu:129-132 */
+    xt[0] = xi[0]; xt[1] = xi[1]; xt[2] = xi[2];
+    xParGi[0] = (int)floor(xt[0]); xParGi[1] = (int)floor(xt[1]); xParGi[2] = (int)floor(xt[2]);
+    ai = APix[lin(p, xParGi[0], xParGi[1], xParGi[2])];
+    if (tr_init) *tr_init = (int32_t)lin(p, xParGi[0], xParGi[1], xParGi[2]);
+
+    for (int i = 0; i < p->tn; i++) {                      /* main.cu:134 */
+        double fstep = 1.0;
+        uint32_t ev = 0;
+        int nev = 0;
+        for (int jj = 0; jj < 3; jj++) { flip0[jj] = 0; flip1[jj] = 0; }
+        /* direction (main.cu:140-151) */
+        double vRand = or_stream_double(&st);
+        double cos_theta = 1.0 - 2.0 * vRand;
+        double sin_theta = 2.0 * sqrt(vRand * (1.0 - vRand));
+        vRand = or_stream_double(&st);
+        vt[0] = sin_theta * cos(2.0 * OR_PI * vRand);
+        vt[1] = sin_theta * sin(2.0 * OR_PI * vRand);
+        vt[2] = cos_theta;
+
+        int j;
+        for (j = 0; (j < p->nite) && (fstep > 0); j++) {   /* main.cu:153 */
+            /* nearest voxel face along the ray (main.cu:199-219) */
+            double tmin = 2.0, tmp, tt;
+            ii_hit = -1;
+            for (int ii = 0; ii < 3; ii++) {
+                if (vt[ii] > 0.0) {
+                    tmp = (double)xParGi[ii] + 1.0 - xt[ii];
+                } else if (vt[ii] < 0.0) {
+                    tmp = (double)xParGi[ii] - xt[ii];
+                } else {
+                    tmp = 2.0;
+                }
+                if (fabs(tmp) > fabs(vt[ii])) {
+                    tt = 2.0;
+                } else {
+                    double q = tmp / vt[ii];
+                    tt = (0.0 < q) ? q : 0.0;             /* std::max(0.0, q) */
+                }
+                if (tt < tmin) { tmin = tt; ii_hit = ii; }
+            }
+            if (tmin < 0.0) break;                         /* main.cu:226-229 */
+
+            /* advance to the face or finish the step (main.cu:231-244) */
+            if ((fstep * step[ai]) >= tmin) {
+                fstep = fstep - tmin / step[ai];
+                xt[0] = xt[0] + tmin * vt[0];
+                xt[1] = xt[1] + tmin * vt[1];
+                xt[2] = xt[2] + tmin * vt[2];
+                t[ai] = t[ai] + tmin / step[ai];
+            } else {
+                xt[0] = xt[0] + step[ai] * fstep * vt[0];
+                xt[1] = xt[1] + step[ai] * fstep * vt[1];
+                xt[2] = xt[2] + step[ai] * fstep * vt[2];
+                t[ai] = t[ai] + fstep;
+                fstep = 0.0;   /* the reference breaks here (main.cu:243) */
+                break;
+            }
+
+            /* neighbour voxel; domain wall (main.cu:246-265) */
+            xParGj[0] = xParGi[0]; xParGj[1] = xParGi[1]; xParGj[2] = xParGi[2];
+            int wall = 0;
+            if (vt[ii_hit] >= 0.0) {
+                xParGj[ii_hit] = xParGj[ii_hit] + 1;
+                if (xParGj[ii_hit] >= NPix[ii_hit]) wall = 1;
+            } else {
+                xParGj[ii_hit] = xParGj[ii_hit] - 1;
+                if (xParGj[ii_hit] < 0) wall = -1;
+            }
+            if (wall != 0 && p->boundary == OR_BOUNDARY_MIRROR) {
+                if (wall > 0) flip1[ii_hit] = 1; else flip0[ii_hit] = 1;
+                vt[ii_hit] = -vt[ii_hit];
+                ev |= (OR_EV_MIRROR << 2 | (uint32_t)ii_hit) << (4 * nev++);
+                continue;
+            }
+            if (wall != 0) {
+                /* periodic extension: the neighbour is on the far side */
+                xParGj[ii_hit] = (wall > 0) ? 0 : NPix[ii_hit] - 1;
+            }
+
+            /* membrane: cross, reflect or Bernoulli(Pij) (main.cu:272-289) */
+            aj = APix[lin(p, xParGj[0], xParGj[1], xParGj[2])];
+            int cross;
+            if (Pij[ai * Nc + aj] > 0.999999) {
+                cross = 1;
+            } else if (Pij[ai * Nc + aj] < 0.000001) {
+                cross = 0;
+            } else {
+                vRand = or_stream_double(&st);
+                cross = (vRand < Pij[ai * Nc + aj]);
+            }
+            if (cross) {
+                ai = aj;
+                xParGi[ii_hit] = xParGj[ii_hit];
+                if (wall != 0) {
+                    double shift = (wall > 0) ? -(double)NPix[ii_hit] : (double)NPix[ii_hit];
+                    xt[ii_hit] = xt[ii_hit] + shift;
+                    xi[ii_hit] = xi[ii_hit] + shift;
+                    ev |= (OR_EV_WRAP << 2 | (uint32_t)ii_hit) << (4 * nev++);
+                } else {
+                    ev |= (OR_EV_CROSS << 2 | (uint32_t)ii_hit) << (4 * nev++);
+                }
+            } else {
+                vt[ii_hit] = -vt[ii_hit];
+                ev |= (OR_EV_REFLECT << 2 | (uint32_t)ii_hit) << (4 * nev++);
+            }
+        }
+        if (fstep > 0) ev |= 1u << 31;   /* sub-segment cap hit: remainder dropped */
+        ev |= (uint32_t)nev << 28;
+
+        /* mirror the origin for every wall hit this step (main.cu:302-310) */
+        for (int jj = 0; jj < 3; jj++) {
+            if (flip0[jj]) xi[jj] = -xi[jj];
+            if (flip1[jj]) xi[jj] = 2.0 * (double)NPix[jj] - xi[jj];
+            flip0[jj] = 0; flip1[jj] = 0;
+        }
+        if (tr_vox) {
+            tr_vox[i] = (int32_t)lin(p, xParGi[0], xParGi[1], xParGi[2]);
+            tr_ev[i] = ev;
+        }
+
+        double dx = 0, dy = 0, dz = 0, s0;
+        if (p->mode == OR_MODE_PGSE) {
+            /* PGSE phase per gradient (main_PGSE.cu:336-346) */
+            dx = (xt[0] - xi[0]) * p->res;
+            dy = (xt[1] - xi[1]) * p->res;
+            dz = (xt[2] - xi[2]) * p->res;
+            const double* g = p->grad;
+            const double ti = (double)(i + 1) * p->dt;
+            for (int jg = 0; jg < p->ngrad; jg++) {
+                if (ti < g[jg * 6 + 1]) {
+                    phase[jg] += g[jg * 6 + 2] * (dx * g[jg * 6 + 3] + dy * g[jg * 6 + 4] + dz * g[jg * 6 + 5]) * p->dt;
+                } else if ((ti >= g[jg * 6]) & (ti < (g[jg * 6] + g[jg * 6 + 1]))) {
+                    phase[jg] -= g[jg * 6 + 2] * (dx * g[jg * 6 + 3] + dy * g[jg * 6 + 4] + dz * g[jg * 6 + 5]) * p->dt;
+                }
+            }
+            /* final T2-weighted signal (main_PGSE.cu:348-357) */
+            if (i == (p->tn - 1)) {
+                s0 = 0.0;
+                for (int c = 0; c < Nc; c++) s0 = s0 + (t[c] / p->t2[c]);
+                s0 = exp(-1.0 * s0);
+                for (int jg = 0; jg < p->ngrad; jg++) out->sig[jg] += s0 * cos(phase[jg]);
+            }
+        }
+
+        /* record moments every Tstep steps (main.cu:333-379) */
+        if ((i % Tstep) == 0) {
+            int tidx = i / Tstep;
+            if (tidx >= p->timepoints) continue;   /* the reference writes past its arrays here */
+            s0 = 0.0;
+            for (int c = 0; c < Nc; c++) s0 = s0 + (t[c] / p->t2[c]);
+            s0 = exp(-1.0 * s0);
+            int nidx = Nc * tidx + ai;
+            out->sig0[tidx] += s0;
+            out->npar_count[nidx] += 1;
+            dx = (xt[0] - xi[0]) * p->res;
+            dy = (xt[1] - xi[1]) * p->res;
+            dz = (xt[2] - xi[2]) * p->res;
+            double* d2 = out->dx2 + 6 * tidx;
+            d2[0] += s0 * dx * dx;
+            d2[1] += s0 * dx * dy;
+            d2[2] += s0 * dx * dz;
+            d2[3] += s0 * dy * dy;
+            d2[4] += s0 * dy * dz;
+            d2[5] += s0 * dz * dz;
+            double* d4 = out->dx4 + 15 * tidx;
+            d4[0] += s0 * dx * dx * dx * dx;
+            d4[1] += s0 * dx * dx * dx * dy;
+            d4[2] += s0 * dx * dx * dx * dz;
+            d4[3] += s0 * dx * dx * dy * dy;
+            d4[4] += s0 * dx * dx * dy * dz;
+            d4[5] += s0 * dx * dx * dz * dz;
+            d4[6] += s0 * dx * dy * dy * dy;
+            d4[7] += s0 * dx * dy * dy * dz;
+            d4[8] += s0 * dx * dy * dz * dz;
+            d4[9] += s0 * dx * dz * dz * dz;
+            d4[10] += s0 * dy * dy * dy * dy;
+            d4[11] += s0 * dy * dy * dy * dz;
+            d4[12] += s0 * dy * dy * dz * dz;
+            d4[13] += s0 * dy * dz * dz * dz;
+            d4[14] += s0 * dz * dz * dz * dz;
+            if (p->mode == OR_MODE_NARROW) {
+                /* narrow-pulse signal (main.cu:374-378) */
+                for (int jb = 0; jb < p->nbvec; jb++) {
+                    double qx = sqrt(p->bval[jb] / p->td[tidx]) *
+                                (dx * p->bvec[jb * 3 + 0] + dy * p->bvec[jb * 3 + 1] + dz * p->bvec[jb * 3 + 2]);
+                    out->sigre[p->nbvec * tidx + jb] += s0 * cos(qx);
+                }
+            }
+        }
+    }
+}
+
+int or_run(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
+           or_trace* tr) {
+    int rc = check(p);
+    if (rc) return rc;
+    double* phase = NULL;
+    if (p->mode == OR_MODE_PGSE && p->ngrad > 0) {
+        phase = (double*)malloc(sizeof(double) * (size_t)p->ngrad);
+        if (!phase) return -10;
+    }
+    for (int64_t w = w_begin; w < w_end; ++w) {
+        if (phase) memset(phase, 0, sizeof(double) * (size_t)p->ngrad);
+        int32_t* ti = NULL; int32_t* tv = NULL; uint32_t* te = NULL;
+        if (tr && w >= tr->w0 && w < tr->w0 + tr->nw) {
+            int64_t r = w - tr->w0;
+            ti = tr->init_voxel + r;
+            tv = tr->voxel + r * p->tn;
+            te = tr->events + r * p->tn;
+        }
+        walk_one(p, w, out, phase, ti, tv, te);
+    }
+    free(phase);
+    return 0;
+}
+
+static void zero_outputs(const or_params* p, or_outputs* o) {
+    memset(o->sig0, 0, sizeof(double) * p->timepoints);
+    memset(o->dx2, 0, sizeof(double) * p->timepoints * 6);
+    memset(o->dx4, 0, sizeof(double) * p->timepoints * 15);
+    memset(o->npar_count, 0, sizeof(double) * p->timepoints * p->nc);
+    if (p->mode == OR_MODE_NARROW && p->nbvec > 0)
+        memset(o->sigre, 0, sizeof(double) * p->timepoints * p->nbvec);
+    if (p->mode == OR_MODE_PGSE && p->ngrad > 0) memset(o->sig, 0, sizeof(double) * p->ngrad);
+}
+
+static void add_outputs(const or_params* p, or_outputs* dst, const or_outputs* src) {
+    for (int i = 0; i < p->timepoints; i++) dst->sig0[i] += src->sig0[i];
+    for (int i = 0; i < p->timepoints * 6; i++) dst->dx2[i] += src->dx2[i];
+    for (int i = 0; i < p->timepoints * 15; i++) dst->dx4[i] += src->dx4[i];
+    for (int i = 0; i < p->timepoints * p->nc; i++) dst->npar_count[i] += src->npar_count[i];
+    if (p->mode == OR_MODE_NARROW)
+        for (int i = 0; i < p->timepoints * p->nbvec; i++) dst->sigre[i] += src->sigre[i];
+    if (p->mode == OR_MODE_PGSE)
+        for (int i = 0; i < p->ngrad; i++) dst->sig[i] += src->sig[i];
+}
+
+int or_run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthreads,
+                    or_outputs* out) {
+    int rc = check(p);
+    if (rc) return rc;
+    if (nthreads < 1) nthreads = 1;
+    size_t per = (size_t)p->timepoints * (1 + 6 + 15 + p->nc) +
+                 (size_t)p->timepoints * (p->mode == OR_MODE_NARROW ? p->nbvec : 0) +
+                 (size_t)(p->mode == OR_MODE_PGSE ? p->ngrad : 0);
+    double* buf = (double*)calloc(per * (size_t)nthreads, sizeof(double));
+    or_outputs* priv = (or_outputs*)calloc((size_t)nthreads, sizeof(or_outputs));
+    if (!buf || !priv) { free(buf); free(priv); return -10; }
+    for (int t = 0; t < nthreads; t++) {
+        double* b = buf + per * (size_t)t;
+        priv[t].sig0 = b; b += p->timepoints;
+        priv[t].dx2 = b; b += p->timepoints * 6;
+        priv[t].dx4 = b; b += p->timepoints * 15;
+        priv[t].npar_count = b; b += p->timepoints * p->nc;
+        priv[t].sigre = b; if (p->mode == OR_MODE_NARROW) b += p->timepoints * p->nbvec;
+        priv[t].sig = b;
+    }
+    int64_t n = w_end - w_begin;
+    int err = 0;
+#pragma omp parallel num_threads(nthreads)
+    {
+        int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        int64_t lo = w_begin + n * t / nt, hi = w_begin + n * (t + 1) / nt;
+        if (or_run(p, lo, hi, &priv[t], NULL) != 0) {
+#pragma omp atomic write
+            err = 1;
+        }
+    }
+    if (!err) {
+        zero_outputs(p, out);
+        for (int t = 0; t < nthreads; t++) add_outputs(p, out, &priv[t]);
+    }
+    free(buf);
+    free(priv);
+    return err ? -11 : 0;
+}
+
+void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    or_philox4x32(ctr, key, 10, out);
+}
+
+void or_stream_doubles(uint64_t seed, uint64_t walker, int n, double* out) {
+    or_stream s;
+    or_stream_init(&s, seed, walker);
+    for (int i = 0; i < n; i++) out[i] = or_stream_double(&s);
+}
+
+void or_stream_floats(uint64_t seed, uint64_t walker, int n, float* out) {
+    or_stream s;
+    or_stream_init(&s, seed, walker);
+    for (int i = 0; i < n; i++) out[i] = or_stream_float(&s);
+}

@@ -1,0 +1,141 @@
+"""Host side of the C ABI (include/rms.h), no GPU needed: the library loads
+and exports every declared entry point, configurations are validated with
+error codes instead of the reference's silent misreads, and the derived tables
+equal the reference's (hpc_code/lib/main.cu:433-458, 484-487)."""
+import ctypes
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+import pyoracle
+from conftest import ROOT, unpack_golden
+from rms_b200 import engine, geometry, runio
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "rms.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(rms_\w+)\s*\(", src, flags=re.M))
+
+
+def test_library_exports_every_declared_function():
+    lib = engine.lib()
+    decl = declared_functions()
+    assert len(decl) >= 16
+    for name in decl:
+        assert hasattr(lib, name), name
+    assert set(engine.EXPORTS) <= decl
+
+
+def test_cli_binary_built():
+    assert os.access(engine.CLI_PATH, os.X_OK)
+
+
+def small_sim(**over):
+    lab = geometry.axon_lattice(12, 12, 16, 0.1, seed=2, exterior=2, r0=0.4)
+    kw = dict(dt=2e-4, tn=1000, npar=32, res=0.1, diffusivity=[0, 2.0, 1.0], t2=[80, 80, 40],
+              bval=[1.0], bvec=[[1, 0, 0]])
+    kw.update(over)
+    return engine.Sim(lab, **kw)
+
+
+def test_derived_tables_match_reference_formulas():
+    s = small_sim(diffusivity=[0, 2.0, 1.0, 0.5], t2=[80, 80, 40, 20])
+    step, t2s, pij, td = pyoracle.reference_tables(2e-4, 0.1, [0, 2.0, 1.0, 0.5], [80, 80, 40, 20], 1000, 1000)
+    assert np.array_equal(s.get("step"), step)
+    assert np.array_equal(s.get("pij"), pij)
+    assert np.array_equal(s.get("td"), td)
+    assert np.array_equal(s.get("diffusivity"), [0, 2.0, 1.0, 0.5])
+
+
+def test_kappa_permeation_formula():
+    # analysis/interaction.m:437-439: P = 2/3 kappa ds / D0, then P / (1 + P)
+    s = small_sim(permeation="kappa", kappa=0.01)
+    p = s.get("pij").reshape(3, 3)
+    for a, D in ((1, 2.0), (2, 1.0)):
+        ds = math.sqrt(6 * D * 2e-4)
+        P = 2.0 / 3.0 * 0.01 * ds / D
+        assert p[a, 3 - a] == pytest.approx(P / (1 + P), rel=1e-15)
+    assert p[1, 1] == 1.0 and p[0, 1] == 0.0 and p[1, 0] == 0.0
+
+
+def test_pij_table_is_used_as_given():
+    t = np.array([[0, 0, 0], [0, 1, 0.25], [0, 0.5, 1]], dtype=float)
+    s = small_sim(permeation="table", pij=t)
+    assert np.array_equal(s.get("pij"), t.ravel())
+
+
+@pytest.mark.parametrize("over,code", [
+    (dict(t2=[80, 0, 40]), -4),                      # T2 = 0 -> 0/0 in the reference
+    (dict(tn=999), -4),                              # TN below the 1000 records
+    (dict(diffusivity=[0, 2.0, 300.0]), -4),         # step >= one voxel
+    (dict(dt=-1.0), -4),
+    (dict(diffusivity=[0] + [1.0] * 9, t2=[80] * 10), -4),   # Nc above the kernels' limit
+])
+def test_invalid_configurations_are_rejected(over, code):
+    with pytest.raises(engine.RmsError) as e:
+        small_sim(**over)
+    assert e.value.code == code
+
+
+def test_lattice_validation():
+    s = small_sim()
+    with pytest.raises(engine.RmsError) as e:
+        s.set_lattice(np.full((12, 12, 16), 3, dtype=np.uint8))   # label >= Nc
+    assert e.value.code == -4
+    with pytest.raises(engine.RmsError):
+        s.set_lattice(np.zeros((12, 12, 16), dtype=np.uint8))     # nothing to start in
+    with pytest.raises(engine.RmsError) as e:
+        s.set_lattice(np.ones((12, 12, 15), dtype=np.uint8))      # wrong shape
+    assert e.value.code == -1
+
+
+def test_results_before_run_are_an_error():
+    s = small_sim()
+    with pytest.raises(engine.RmsError) as e:
+        s.get("sig0")
+    assert e.value.code == -7
+
+
+@pytest.mark.parametrize("case", ["narrow_3comp", "pgse_3comp"])
+def test_load_dir_reads_reference_inputs(case, tmp_path):
+    d = unpack_golden(case, str(tmp_path), inputs_only=True)
+    s = engine.Sim.from_dir(d)
+    assert s.mode == ("pgse" if case.startswith("pgse") else "narrow")
+    assert s.field_size("sig0") == 1000
+    D = np.loadtxt(os.path.join(d, "diffusivity.txt"))
+    assert np.array_equal(s.get("diffusivity"), D)
+
+
+def test_load_dir_errors(tmp_path):
+    d = unpack_golden("narrow_3comp", str(tmp_path / "a"), inputs_only=True)
+    os.remove(os.path.join(d, "T2.txt"))
+    with pytest.raises(engine.RmsError) as e:
+        engine.Sim.from_dir(d)
+    assert e.value.code == -2
+    d = unpack_golden("narrow_3comp", str(tmp_path / "b"), inputs_only=True)
+    txt = open(os.path.join(d, "fiber.txt")).read().split()
+    open(os.path.join(d, "fiber.txt"), "w").write(" ".join(txt[:-5]))
+    with pytest.raises(engine.RmsError) as e:
+        engine.Sim.from_dir(d)
+    assert e.value.code == -3
+    # a narrow-pulse simParamInput.txt given to the PGSE reader: the reference
+    # would read Nbvec as Nc (main_PGSE.cu:442); here it is an error
+    d = unpack_golden("narrow_3comp", str(tmp_path / "c"), inputs_only=True)
+    with pytest.raises(engine.RmsError) as e:
+        engine.Sim.from_dir(d, mode="pgse")
+    assert e.value.code == -3
+
+
+def test_run_without_gpu_fails_loudly():
+    pytest.importorskip("torch")
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    s = small_sim()
+    with pytest.raises(engine.RmsError) as e:
+        s.run(seed=1)
+    assert e.value.code == -5

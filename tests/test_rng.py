@@ -1,0 +1,49 @@
+"""The random stream: published Philox4x32-10 known answers, and the
+product's stream against the oracle's (both replace cuRAND's draws of
+hpc_code/lib/main.cu:118-120, 140, 144, 282)."""
+import numpy as np
+import pytest
+
+import pyoracle
+from rms_b200 import engine
+
+# Known-answer vectors published with Random123 (Salmon et al., SC'11):
+# counter (4 words), key (2 words) -> output (4 words), Philox4x32 with 10 rounds.
+KAT = [
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+@pytest.mark.parametrize("ctr,key,want", KAT)
+def test_philox_kat_oracle(ctr, key, want):
+    assert list(pyoracle.philox4x32_10(ctr, key)) == list(want)
+
+
+@pytest.mark.parametrize("ctr,key,want", KAT)
+def test_philox_kat_product(ctr, key, want):
+    assert list(engine.philox4x32_10(ctr, key)) == list(want)
+
+
+@pytest.mark.parametrize("seed,walker", [(0, 0), (12345, 7), (2**63 + 5, 2**40 + 3)])
+def test_streams_match_oracle(seed, walker):
+    assert np.array_equal(engine.rng_doubles(seed, walker, 257), pyoracle.stream_doubles(seed, walker, 257))
+    assert np.array_equal(engine.rng_floats(seed, walker, 257), pyoracle.stream_floats(seed, walker, 257))
+
+
+def test_uniform_maps_open_interval_and_moments():
+    d = np.concatenate([engine.rng_doubles(3, w, 2000) for w in range(20)])
+    f = np.concatenate([engine.rng_floats(3, w, 2000) for w in range(20)]).astype(np.float64)
+    for u in (d, f):
+        assert u.min() > 0.0 and u.max() < 1.0
+        assert abs(u.mean() - 0.5) < 0.01
+        assert abs(u.var() - 1.0 / 12.0) < 0.003
+
+
+def test_double_map_is_exact():
+    # u = (2m+1) 2^-53 with m the top 52 bits of (hi:lo)
+    lo, hi = 0x6627E8D5, 0xE169C58D
+    m = ((hi << 32) | lo) >> 12
+    assert engine.rng_doubles(0, 0, 1)[0] == (2 * m + 1) * 2.0 ** -53
