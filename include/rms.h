@@ -153,6 +153,10 @@ int rms_sim_get(const rms_sim* sim, int field, double* out, size_t n);
 int rms_sim_get_trace(const rms_sim* sim, int32_t* init_voxel, int32_t* voxel,
                       uint32_t* events, size_t nwalkers, size_t tn);
 
+/* Position (voxel units, [w][i][xyz]) after each step of the traced walkers
+ * of the last COMPAT run.  No reference counterpart: a parity test hook. */
+int rms_sim_get_trace_positions(const rms_sim* sim, double* pos, size_t nwalkers, size_t tn);
+
 /* Write the reference's output files into dir.  Replaces: the ofstream
  * writers of main.cu:550-615 and main_PGSE.cu:596-669. */
 int rms_sim_write_dir(const rms_sim* sim, const char* dir);

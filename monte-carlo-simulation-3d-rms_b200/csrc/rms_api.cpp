@@ -71,7 +71,7 @@ struct rms_device_state {
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     DevBuf labels, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
-        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev;
+        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos;
     HostPinned h_out;
     size_t labels_bytes = 0;
 
@@ -79,7 +79,7 @@ struct rms_device_state {
         if (device >= 0) cudaSetDevice(device);
         for (DevBuf* b : {&labels, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
-                          &tr_vox, &tr_ev})
+                          &tr_vox, &tr_ev, &tr_pos})
             b->release();
         h_out.release();
         if (e0) cudaEventDestroy(e0);
@@ -388,6 +388,7 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
         RMS_CUDA(d->tr_init.ensure((size_t)trace_n * sizeof(int32_t)));
         RMS_CUDA(d->tr_vox.ensure((size_t)trace_n * s->tn * sizeof(int32_t)));
         RMS_CUDA(d->tr_ev.ensure((size_t)trace_n * s->tn * sizeof(uint32_t)));
+        RMS_CUDA(d->tr_pos.ensure((size_t)trace_n * s->tn * 3 * sizeof(double)));
     }
 
     WalkArgs a{};
@@ -417,6 +418,7 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
     a.err = d->err.as<int>();
     a.trace_n = trace_n;
     a.tr_init = d->tr_init.as<int32_t>(); a.tr_vox = d->tr_vox.as<int32_t>(); a.tr_ev = d->tr_ev.as<uint32_t>();
+    a.tr_pos = d->tr_pos.as<double>();
 
     RMS_CUDA(cudaEventRecord(d->e0, st));
     int e = (prec == RMS_PREC_COMPAT) ? launch_walk_compat(a, grid, block, trace_n > 0, st)
@@ -444,9 +446,11 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
         s->tr_init.resize(trace_n);
         s->tr_vox.resize((size_t)trace_n * s->tn);
         s->tr_ev.resize((size_t)trace_n * s->tn);
+        s->tr_pos.resize((size_t)trace_n * s->tn * 3);
         RMS_CUDA(cudaMemcpyAsync(s->tr_init.data(), d->tr_init.p, trace_n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         RMS_CUDA(cudaMemcpyAsync(s->tr_vox.data(), d->tr_vox.p, s->tr_vox.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         RMS_CUDA(cudaMemcpyAsync(s->tr_ev.data(), d->tr_ev.p, s->tr_ev.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        RMS_CUDA(cudaMemcpyAsync(s->tr_pos.data(), d->tr_pos.p, s->tr_pos.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
     RMS_CUDA(cudaStreamSynchronize(st));
     if (*herr & kErrInitCap)
@@ -647,6 +651,15 @@ int rms_sim_get_trace(const rms_sim* s, int32_t* init_voxel, int32_t* voxel, uin
     std::copy(s->tr_init.begin(), s->tr_init.end(), init_voxel);
     std::copy(s->tr_vox.begin(), s->tr_vox.end(), voxel);
     std::copy(s->tr_ev.begin(), s->tr_ev.end(), events);
+    return RMS_OK;
+}
+
+int rms_sim_get_trace_positions(const rms_sim* s, double* pos, size_t nwalkers, size_t tn) {
+    if (!s || !pos) return set_error(RMS_ERR_ARG, "null argument");
+    if (!s->have_results || s->trace_n == 0) return set_error(RMS_ERR_STATE, "the last run kept no traces");
+    if (nwalkers != (size_t)s->trace_n || tn != (size_t)s->tn)
+        return set_error(RMS_ERR_ARG, "trace buffer shape differs from the last run");
+    std::copy(s->tr_pos.begin(), s->tr_pos.end(), pos);
     return RMS_OK;
 }
 

@@ -54,6 +54,7 @@ struct WalkArgs {
     int32_t* tr_init;
     int32_t* tr_vox;
     uint32_t* tr_ev;
+    double* tr_pos;             // [trace_n*tn*3] position after each step (voxels)
 };
 
 // Launchers (rms_walk_*.cu, rms_reduce.cu).  All asynchronous on `stream`;

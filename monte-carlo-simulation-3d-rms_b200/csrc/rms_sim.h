@@ -51,6 +51,7 @@ struct rms_sim {
     int64_t trace_n = 0;
     std::vector<int32_t> tr_init, tr_vox;
     std::vector<uint32_t> tr_ev;
+    std::vector<double> tr_pos;
     double walk_ms = 0.0, run_ms = 0.0;
     int last_grid = 0, last_block = 0;
 

@@ -223,6 +223,8 @@ __global__ void __launch_bounds__(kBlock) walk_compat_kernel(const WalkArgs a) {
                 if (TRACE && w < a.trace_n) {
                     a.tr_vox[(size_t)w * a.tn + i] = (int32_t)lin3(g0, g1, g2, a.n2, a.n3);
                     a.tr_ev[(size_t)w * a.tn + i] = ev;
+                    double* tp = a.tr_pos + ((size_t)w * a.tn + i) * 3;
+                    tp[0] = xt0; tp[1] = xt1; tp[2] = xt2;
                 }
             }
 

@@ -27,7 +27,8 @@ ERRORS = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "RANGE", -5: "CUDA", -6: "NOMEM
 
 # The C ABI's exported names (include/rms.h), checked by the CPU tests.
 EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim_run",
-           "rms_sim_field_size", "rms_sim_get", "rms_sim_get_trace", "rms_sim_write_dir",
+           "rms_sim_field_size", "rms_sim_get", "rms_sim_get_trace", "rms_sim_get_trace_positions",
+           "rms_sim_write_dir",
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version")
 
@@ -85,6 +86,7 @@ def lib():
         L.rms_sim_get.argtypes = [C.c_void_p, C.c_int, _DP, C.c_size_t]
         L.rms_sim_get_trace.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_uint32), C.c_size_t, C.c_size_t]
+        L.rms_sim_get_trace_positions.argtypes = [C.c_void_p, _DP, C.c_size_t, C.c_size_t]
         L.rms_sim_write_dir.argtypes = [C.c_void_p, C.c_char_p]
         L.rms_sim_last_timing.argtypes = [C.c_void_p, _DP, _DP]
         L.rms_batch_run.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts)]
@@ -203,7 +205,9 @@ class Sim:
         _check(lib().rms_sim_get_trace(self._h, tr_init.ctypes.data_as(C.POINTER(C.c_int32)),
                                        vox.ctypes.data_as(C.POINTER(C.c_int32)),
                                        ev.ctypes.data_as(C.POINTER(C.c_uint32)), nwalkers, self.tn))
-        return dict(init_voxel=tr_init, voxel=vox, events=ev)
+        pos = np.zeros((nwalkers, self.tn, 3))
+        _check(lib().rms_sim_get_trace_positions(self._h, _ptr(pos), nwalkers, self.tn))
+        return dict(init_voxel=tr_init, voxel=vox, events=ev, pos=pos)
 
     def write_dir(self, path: str):
         _check(lib().rms_sim_write_dir(self._h, path.encode()))

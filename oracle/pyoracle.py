@@ -44,7 +44,8 @@ class OrOutputs(C.Structure):
 
 class OrTrace(C.Structure):
     _fields_ = [("w0", C.c_int64), ("nw", C.c_int64), ("init_voxel", C.POINTER(C.c_int32)),
-                ("voxel", C.POINTER(C.c_int32)), ("events", C.POINTER(C.c_uint32))]
+                ("voxel", C.POINTER(C.c_int32)), ("events", C.POINTER(C.c_uint32)),
+                ("pos", C.POINTER(C.c_double))]
 
 
 _lib = None
@@ -168,11 +169,12 @@ def run_oracle(job: Job, w_begin: int = 0, w_end: Optional[int] = None, nthreads
         tr_init = np.zeros(nw, dtype=np.int32)
         tr_vox = np.zeros((nw, job.tn), dtype=np.int32)
         tr_ev = np.zeros((nw, job.tn), dtype=np.uint32)
+        tr_pos = np.zeros((nw, job.tn, 3))
         tr = OrTrace(w_begin, nw, tr_init.ctypes.data_as(C.POINTER(C.c_int32)),
                      tr_vox.ctypes.data_as(C.POINTER(C.c_int32)),
-                     tr_ev.ctypes.data_as(C.POINTER(C.c_uint32)))
+                     tr_ev.ctypes.data_as(C.POINTER(C.c_uint32)), _dp(tr_pos))
         rc = lib.or_run(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.byref(outs), C.byref(tr))
-        o["trace"] = dict(init_voxel=tr_init, voxel=tr_vox, events=tr_ev)
+        o["trace"] = dict(init_voxel=tr_init, voxel=tr_vox, events=tr_ev, pos=tr_pos)
     elif nthreads > 1:
         rc = lib.or_run_parallel(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end),
                                  C.c_int(nthreads), C.byref(outs))

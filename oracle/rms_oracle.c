@@ -34,7 +34,7 @@ static int check(const or_params* p) {
 }
 
 static void walk_one(const or_params* p, int64_t w, or_outputs* out, double* phase,
-                     int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev) {
+                     int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev, double* tr_pos) {
     const int Nc = p->nc;
     const int Tstep = p->tn / p->timepoints;               /* main.cu:68 */
     const int NPix[3] = {p->n1, p->n2, p->n3};             /* main.cu:86 */
@@ -180,6 +180,11 @@ static void walk_one(const or_params* p, int64_t w, or_outputs* out, double* pha
             tr_vox[i] = (int32_t)lin(p, xParGi[0], xParGi[1], xParGi[2]);
             tr_ev[i] = ev;
         }
+        if (tr_pos) {
+            tr_pos[3 * i + 0] = xt[0];
+            tr_pos[3 * i + 1] = xt[1];
+            tr_pos[3 * i + 2] = xt[2];
+        }
 
         double dx = 0, dy = 0, dz = 0, s0;
         if (p->mode == OR_MODE_PGSE) {
@@ -264,14 +269,15 @@ int or_run(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
     }
     for (int64_t w = w_begin; w < w_end; ++w) {
         if (phase) memset(phase, 0, sizeof(double) * (size_t)p->ngrad);
-        int32_t* ti = NULL; int32_t* tv = NULL; uint32_t* te = NULL;
+        int32_t* ti = NULL; int32_t* tv = NULL; uint32_t* te = NULL; double* tp = NULL;
         if (tr && w >= tr->w0 && w < tr->w0 + tr->nw) {
             int64_t r = w - tr->w0;
             ti = tr->init_voxel + r;
             tv = tr->voxel + r * p->tn;
             te = tr->events + r * p->tn;
+            if (tr->pos) tp = tr->pos + r * p->tn * 3;
         }
-        walk_one(p, w, out, phase, ti, tv, te);
+        walk_one(p, w, out, phase, ti, tv, te, tp);
     }
     free(phase);
     return 0;

@@ -72,6 +72,7 @@ typedef struct or_trace {
     int32_t* init_voxel; /* [nw] voxel of the initial position */
     int32_t* voxel;      /* [nw*tn] voxel after each step */
     uint32_t* events;    /* [nw*tn] event code of each step */
+    double* pos;         /* [nw*tn*3] position (voxel units) after each step, or NULL */
 } or_trace;
 
 /* Walk walkers [w_begin, w_end) in order, adding into *out (which the caller
