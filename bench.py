@@ -55,7 +55,21 @@ def fib_directions(n: int) -> np.ndarray:
     return np.column_stack([r * np.cos(phi), r * np.sin(phi), z])
 
 
-def workload(name: str, world: int):
+def workload(name: str, world: int, walkers: int | None = None, tn: int | None = None):
+    lab, sim_kw, per_gpu, cfg = _workload(name, world)
+    if walkers:
+        per_gpu = int(walkers)
+        sim_kw["npar"] = per_gpu * world
+        cfg["walkers_per_gpu"] = per_gpu
+        cfg["workload"] += f" [walkers/GPU overridden: {per_gpu}]"
+    if tn:
+        sim_kw["tn"] = int(tn)
+        cfg["steps_per_walk"] = int(tn)
+        cfg["workload"] += f" [steps overridden: {tn}]"
+    return lab, sim_kw, per_gpu, cfg
+
+
+def _workload(name: str, world: int):
     from rms_b200 import analysis, geometry
     if name == "production":
         lab = geometry.axon_lattice(256, 256, 2048, 0.1, seed=0, exterior=2)
@@ -184,7 +198,7 @@ def run_reference_arm(args):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    lab, sim_kw, per_gpu, cfg = workload(args.workload, 1)
+    lab, sim_kw, per_gpu, cfg = workload(args.workload, 1, args.walkers, args.tn)
     try:
         job, n, cores, kind = cpu_reference_rate(lab, sim_kw, target_s=6.0)
     except Exception as e:  # the build is missing on this machine
@@ -223,7 +237,7 @@ def run_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    lab, sim_kw, per_gpu, cfg = workload(args.workload, world)
+    lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn)
     w0, w1 = rank * per_gpu, (rank + 1) * per_gpu
     sim = engine.Sim(lab, **sim_kw)
     stream = torch.cuda.current_stream()
@@ -262,6 +276,22 @@ def run_ours(args):
         ms, walk = float(t[0]), float(t[1])
     tn = sim_kw["tn"]
     value = world * per_gpu * tn / (ms * 1e-3)
+    # the plain FP64 walk on the same workload, for the split / plain ratio
+    plain = None
+    if args.plain_ratio and precision == "split":
+        sim.run(seed=999, precision="compat", device=local, stream=sh, walker_range=(w0, w1))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim.run(seed=998, precision="compat", device=local, stream=sh, walker_range=(w0, w1))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([pms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pms = float(t[0])
+        plain = {"value": world * per_gpu * tn / (pms * 1e-3), "ms_per_step": pms, "precision": "compat (FP64)",
+                 "steps": 1}
 
     # end to end through the public API: lattice from pinned host memory,
     # results read back, every step
@@ -304,6 +334,7 @@ def run_ours(args):
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             try:
+                sys.path.insert(0, os.path.join(ROOT, "oracle"))
                 import pyoracle
                 job, n, cores, kind = cpu_reference_rate(lab, sim_kw, target_s=15.0)
                 t0 = time.perf_counter()
@@ -329,6 +360,7 @@ def run_ours(args):
             "issue": {"achieved_thread_ops_per_s": walker_steps * OPS_PER_WALKER_STEP / (walk * 1e-3),
                       "ops_per_walker_step": OPS_PER_WALKER_STEP},
             "walk_ms": walk,
+            "plain": plain,
             "e2e": {"value": world * per_gpu * tn / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,
@@ -347,9 +379,13 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="compat", choices=["split", "compat"])
+    ap.add_argument("--precision", default="split", choices=["split", "compat"])
     ap.add_argument("--workload", default="production", choices=["production", "single"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--walkers", type=int, default=None, help="walkers per GPU (smaller case, e.g. for ncu)")
+    ap.add_argument("--plain-ratio", action="store_true",
+                    help="also time one run of the plain FP64 walk on the same workload")
+    ap.add_argument("--tn", type=int, default=None, help="steps per walk (smaller case, e.g. for ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

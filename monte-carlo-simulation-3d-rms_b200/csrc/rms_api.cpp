@@ -70,14 +70,15 @@ struct rms_device_state {
     int device = -1;
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
-    DevBuf labels, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
+    DevBuf labels, packed, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
         ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos;
     HostPinned h_out;
     size_t labels_bytes = 0;
+    bool packed_valid = false;
 
     ~rms_device_state() {
         if (device >= 0) cudaSetDevice(device);
-        for (DevBuf* b : {&labels, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
+        for (DevBuf* b : {&labels, &packed, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
                           &tr_vox, &tr_ev, &tr_pos})
             b->release();
@@ -330,7 +331,7 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
         per_sm = walk_compat_blocks_per_sm(s->nc, trace_n > 0);
     } else {
         block = (o && o->block_size) ? o->block_size : kSplitBlockDefault;
-        if (block % 32 || block < 32 || block > 1024) return set_error(RMS_ERR_ARG, "block_size must be a multiple of 32 in [32, 1024]");
+        if (block % 32 || block < 32 || block > 256) return set_error(RMS_ERR_ARG, "block_size must be a multiple of 32 in [32, 256]");
         per_sm = walk_split_blocks_per_sm(s->nc, block);
     }
     if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
@@ -352,7 +353,16 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
         RMS_CUDA(d->labels.ensure(s->labels.size()));
         RMS_CUDA(cudaMemcpyAsync(d->labels.p, s->labels.data(), s->labels.size(), cudaMemcpyHostToDevice, st));
         d->labels_bytes = s->labels.size();
+        d->packed_valid = false;
         s->lattice_dirty = false;
+    }
+    const int lattice_bits = (prec == RMS_PREC_SPLIT && s->nc <= 4) ? 2 : 8;
+    if (lattice_bits == 2 && !d->packed_valid) {
+        const size_t nvox = s->labels.size();
+        RMS_CUDA(d->packed.ensure((nvox + 3) / 4));
+        int pe = pack_labels_2bit(d->labels.as<uint8_t>(), nvox, d->packed.as<uint8_t>(), st);
+        if (pe) return cuda_fail((cudaError_t)pe, "label packing");
+        d->packed_valid = true;
     }
     std::vector<double> tables;
     tables.insert(tables.end(), s->step.begin(), s->step.end());
@@ -422,7 +432,8 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
 
     RMS_CUDA(cudaEventRecord(d->e0, st));
     int e = (prec == RMS_PREC_COMPAT) ? launch_walk_compat(a, grid, block, trace_n > 0, st)
-                                      : launch_walk_split(a, grid, block, st);
+                                      : launch_walk_split(a, lattice_bits == 2 ? d->packed.as<uint8_t>() : a.labels,
+                                                          lattice_bits, grid, block, st);
     if (e) return cuda_fail((cudaError_t)e, "walk kernel launch");
     RMS_CUDA(cudaEventRecord(d->e1, st));
     e = launch_reduce_slots(a.slots, nslots, row, d->out.as<double>(), st);

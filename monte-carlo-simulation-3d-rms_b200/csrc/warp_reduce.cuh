@@ -43,4 +43,21 @@ __device__ __forceinline__ double warp_reduce_scatter32(double (&v)[32], int lan
     return v[0];
 }
 
+// Reduce-scatter of 16 values: on return lanes l and l ^ 16 both hold the
+// warp-wide sum of v[l & 15] (8 + 4 + 2 + 1 halving shuffles, then one
+// butterfly across the half-warps).  Half the registers of the 32-value form.
+__device__ __forceinline__ double warp_reduce_scatter16(double (&v)[16], int lane) {
+#pragma unroll
+    for (int half = 8; half > 0; half >>= 1) {
+        const bool upper = (lane & half) != 0;
+#pragma unroll
+        for (int k = 0; k < half; ++k) {
+            const double send = upper ? v[k] : v[k + half];
+            const double keep = upper ? v[k + half] : v[k];
+            v[k] = keep + __shfl_xor_sync(kFullMask, send, half);
+        }
+    }
+    return v[0] + __shfl_xor_sync(kFullMask, v[0], 16);
+}
+
 }  // namespace rms

@@ -7,6 +7,11 @@
    b = |g|^2 delta^2 (Delta - delta/3) (analysis/readRMS_pgse.m:53);
  - impermeable parallel planes a apart: D_parallel = D0 and
    D_perp -> a^2 / (12 t) (part2_demo1_2_diffusivity.m fits a_eff this way).
+
+The signal tests use periodic walls: under the reference's mirror walls the
+displacement is taken against the mirrored origin (hpc_code/lib/main.cu:302-310),
+so each wall hit flips the sign of that axis's displacement -- harmless for the
+even moments, not for the phase once walkers reach the lattice edge.
 """
 import numpy as np
 import pytest
@@ -14,7 +19,7 @@ import pytest
 from rms_b200 import analysis, engine
 
 pytestmark = pytest.mark.gpu
-PRECISIONS = ["compat"]
+PRECISIONS = ["compat", "split"]
 
 
 def free_sim(npar, tn, D0=2.0, T2=1e9, shape=(32, 32, 32), **kw):
@@ -37,7 +42,7 @@ def test_free_diffusion_moments(precision):
     assert np.abs(K[sl] - k_expect).mean() < 0.05
     # first record: one step of exactly sqrt(6 D0 dt) length
     r2 = o["dx2"][0, 0] + o["dx2"][0, 3] + o["dx2"][0, 5]
-    assert r2 / N == pytest.approx(6 * 2.0 * 2e-4, rel=1e-9)
+    assert r2 / N == pytest.approx(6 * 2.0 * 2e-4, rel=1e-9 if precision == "compat" else 1e-6)
 
 
 @pytest.mark.parametrize("precision", PRECISIONS)
@@ -54,7 +59,7 @@ def test_sig0_is_t2_decay(precision):
 def test_narrow_pulse_free_signal(precision):
     N, tn = 40000, 2000
     b = np.array([0.2, 0.5, 1.0, 1.5])
-    sim = free_sim(N, tn, bval=b, bvec=np.tile([[0.0, 0.6, 0.8]], (4, 1)))
+    sim = free_sim(N, tn, bval=b, bvec=np.tile([[0.0, 0.6, 0.8]], (4, 1)), boundary="periodic")
     o = sim.run(seed=77, precision=precision).outputs()
     S = o["sigre"] / o["sig0"][:, None]
     # standard error of a mean of cosines over 4e4 walkers is below 0.004
@@ -68,7 +73,7 @@ def test_pgse_free_signal(precision):
     bv = np.array([0.2, 0.5, 1.0, 2.0])
     g = analysis.pgse_gradient_for_b(bv, Delta, delta)
     grad = np.column_stack([np.full(4, Delta), np.full(4, delta), g, np.tile([0.0, 0.0, 1.0], (4, 1))])
-    sim = free_sim(N, tn, grad=grad)
+    sim = free_sim(N, tn, grad=grad, boundary="periodic")
     o = sim.run(seed=31, precision=precision).outputs()
     S = o["sig"] / N
     # discrete-time b: sum over the lobe steps, as the walk accumulates phase
