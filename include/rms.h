@@ -97,7 +97,8 @@ typedef struct rms_run_opts {
     void* stream;              /* cudaStream_t to run on; NULL = library stream */
     int trace_walkers;         /* > 0: keep per-step voxel/event traces of
                                   walkers [0, trace_walkers) (COMPAT only) */
-    int block_size;            /* threads per block; 0 = tuned default */
+    int variant;               /* SPLIT walk launch variant: 0 = tuned default,
+                                  k >= 1 = entry k of rms_split_variant() */
     int64_t walker_begin;      /* walk walkers [walker_begin, walker_end) of */
     int64_t walker_end;        /* the job; 0, 0 = all.  Lets ranks shard a job. */
 } rms_run_opts;
@@ -181,6 +182,16 @@ void rms_sim_destroy(rms_sim* sim);
 int rms_rng_doubles(uint64_t seed, uint64_t walker, int n, double* out);
 int rms_rng_floats(uint64_t seed, uint64_t walker, int n, float* out);
 int rms_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* The SPLIT walk's streams on the host: domain 0 gives the direction
+ * uniforms of steps 0, 1, ... (two per step, n values), domain 1 the start
+ * position draws, domain 2 the partial-permeation draws.  A test hook. */
+int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out);
+
+/* Launch variants of the SPLIT walk (block size x minimum resident blocks per
+ * SM).  rms_split_variant(k, ...) describes entry k >= 1; returns RMS_ERR_ARG
+ * past the end.  No reference counterpart (the reference launches one fixed
+ * shape, hpc_code/lib/main.cu:499-504). */
+int rms_split_variant(int k, int* block, int* min_blocks_per_sm);
 
 /* Library version string. */
 const char* rms_version(void);

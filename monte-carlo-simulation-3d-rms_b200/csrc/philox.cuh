@@ -111,4 +111,46 @@ struct FloatStream {
     RMS_HD float next() { return u32_to_float(next_word()); }
 };
 
+// Streams of the split-precision walk.  Three counter domains per walker
+// (counter word 1 = domain), all read as floats:
+//   kDomDir  block k = the direction uniforms of steps 2k and 2k+1
+//            (x, y -> step 2k; z, w -> step 2k+1): a pure function of the step
+//            index, so the lanes of a warp generate blocks in lock step however
+//            many other draws each lane made;
+//   kDomInit sequential words for the rejection-sampled start position;
+//   kDomPerm sequential words for partial-permeation draws.
+// counter = (k, domain, walker_lo, walker_hi), key = (seed_lo, seed_hi).
+constexpr uint32_t kDomDir = 0u;
+constexpr uint32_t kDomInit = 1u;
+constexpr uint32_t kDomPerm = 2u;
+
+RMS_HD U4 dir_block(uint32_t k, uint32_t k0, uint32_t k1, uint32_t w0, uint32_t w1) {
+    return philox4x32_10(U4{k, kDomDir, w0, w1}, k0, k1);
+}
+
+// Sequential floats of one counter domain.
+struct DomainStream {
+    uint32_t k0, k1, w0, w1, dom, block;
+    uint32_t q1, q2, q3;
+    int left;
+
+    RMS_HD void init(uint64_t seed, uint64_t walker, uint32_t domain) {
+        k0 = (uint32_t)seed; k1 = (uint32_t)(seed >> 32);
+        w0 = (uint32_t)walker; w1 = (uint32_t)(walker >> 32);
+        dom = domain; block = 0; q1 = q2 = q3 = 0; left = 0;
+    }
+    RMS_HD uint32_t next_word() {
+        if (left == 0) {
+            const U4 r = philox4x32_10(U4{block, dom, w0, w1}, k0, k1);
+            ++block;
+            q1 = r.y; q2 = r.z; q3 = r.w; left = 3;
+            return r.x;
+        }
+        const uint32_t x = q1;
+        q1 = q2; q2 = q3; --left;
+        return x;
+    }
+    RMS_HD float next() { return u32_to_float(next_word()); }
+};
+
 }  // namespace rms

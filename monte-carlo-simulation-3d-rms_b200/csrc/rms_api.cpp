@@ -22,7 +22,7 @@ namespace {
 thread_local std::string g_last_error;
 
 constexpr int kCompatBlock = 128;
-constexpr int kSplitBlockDefault = 256;
+constexpr int kSplitVariantDefault = 3;   // 256 threads, >= 4 blocks per SM (64 registers): fastest measured
 constexpr int kMaxGrad = 1 << 16;
 
 // One device allocation that only grows.
@@ -327,12 +327,15 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
     RMS_CUDA(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
     int block = kCompatBlock;
     int per_sm;
+    const int lattice_bits = (prec == RMS_PREC_SPLIT && s->nc <= 4) ? 2 : 8;
+    int variant = 0;
     if (prec == RMS_PREC_COMPAT) {
         per_sm = walk_compat_blocks_per_sm(s->nc, trace_n > 0);
     } else {
-        block = (o && o->block_size) ? o->block_size : kSplitBlockDefault;
-        if (block % 32 || block < 32 || block > 256) return set_error(RMS_ERR_ARG, "block_size must be a multiple of 32 in [32, 256]");
-        per_sm = walk_split_blocks_per_sm(s->nc, block);
+        variant = (o && o->variant > 0) ? o->variant - 1 : kSplitVariantDefault;
+        if (variant >= split_variant_count()) return set_error(RMS_ERR_ARG, "variant out of range");
+        block = split_variant_block(variant);
+        per_sm = walk_split_blocks_per_sm(s->nc, lattice_bits, variant);
     }
     if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
     const int64_t ntiles = (w1 - w0 + 31) / 32;
@@ -356,7 +359,6 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
         d->packed_valid = false;
         s->lattice_dirty = false;
     }
-    const int lattice_bits = (prec == RMS_PREC_SPLIT && s->nc <= 4) ? 2 : 8;
     if (lattice_bits == 2 && !d->packed_valid) {
         const size_t nvox = s->labels.size();
         RMS_CUDA(d->packed.ensure((nvox + 3) / 4));
@@ -433,7 +435,7 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
     RMS_CUDA(cudaEventRecord(d->e0, st));
     int e = (prec == RMS_PREC_COMPAT) ? launch_walk_compat(a, grid, block, trace_n > 0, st)
                                       : launch_walk_split(a, lattice_bits == 2 ? d->packed.as<uint8_t>() : a.labels,
-                                                          lattice_bits, grid, block, st);
+                                                          lattice_bits, variant, grid, st);
     if (e) return cuda_fail((cudaError_t)e, "walk kernel launch");
     RMS_CUDA(cudaEventRecord(d->e1, st));
     e = launch_reduce_slots(a.slots, nslots, row, d->out.as<double>(), st);
@@ -525,6 +527,13 @@ extern "C" {
 const char* rms_last_error(void) { return g_last_error.c_str(); }
 
 const char* rms_version(void) { return "rms_b200 0.1 (sm_100a)"; }
+
+int rms_split_variant(int k, int* block, int* min_blocks_per_sm) {
+    if (k < 1 || k > split_variant_count()) return set_error(RMS_ERR_ARG, "no such variant");
+    if (block) *block = split_variant_block(k - 1);
+    if (min_blocks_per_sm) *min_blocks_per_sm = split_variant_minb(k - 1);
+    return RMS_OK;
+}
 
 int rms_sim_create(const rms_config* cfg, rms_sim** out) {
     if (!cfg || !out) return set_error(RMS_ERR_ARG, "null argument");
@@ -705,6 +714,25 @@ int rms_rng_floats(uint64_t seed, uint64_t walker, int n, float* out) {
     if (n < 0 || (n && !out)) return set_error(RMS_ERR_ARG, "bad buffer");
     FloatStream r;
     r.init(seed, walker);
+    for (int i = 0; i < n; ++i) out[i] = r.next();
+    return RMS_OK;
+}
+
+int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out) {
+    if (n < 0 || (n && !out)) return set_error(RMS_ERR_ARG, "bad buffer");
+    if (domain < 0 || domain > 2) return set_error(RMS_ERR_ARG, "domain must be 0, 1 or 2");
+    if (domain == (int)kDomDir) {
+        for (int i = 0; 2 * i < n; ++i) {
+            const U4 b = dir_block((uint32_t)(i >> 1), (uint32_t)seed, (uint32_t)(seed >> 32),
+                                   (uint32_t)walker, (uint32_t)(walker >> 32));
+            const uint32_t x = (i & 1) ? b.z : b.x, y = (i & 1) ? b.w : b.y;
+            out[2 * i] = u32_to_float(x);
+            if (2 * i + 1 < n) out[2 * i + 1] = u32_to_float(y);
+        }
+        return RMS_OK;
+    }
+    DomainStream r;
+    r.init(seed, walker, (uint32_t)domain);
     for (int i = 0; i < n; ++i) out[i] = r.next();
     return RMS_OK;
 }

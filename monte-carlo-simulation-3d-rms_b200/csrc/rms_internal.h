@@ -60,14 +60,17 @@ struct WalkArgs {
 // Launchers (rms_walk_*.cu, rms_reduce.cu).  All asynchronous on `stream`;
 // they return a cudaError_t value (0 = success).
 int launch_walk_compat(const WalkArgs& a, int grid, int block, bool trace, void* stream);
-int launch_walk_split(const WalkArgs& a, const uint8_t* lattice, int lattice_bits, int grid, int block,
+int launch_walk_split(const WalkArgs& a, const uint8_t* lattice, int lattice_bits, int variant, int grid,
                       void* stream);
+int split_variant_count();
+int split_variant_block(int variant);   // threads per block of a launch variant
+int split_variant_minb(int variant);    // its minimum resident blocks per SM
 // Pack one-byte labels (< 4) into 2 bits per voxel, voxel i in bits 2(i%4) of byte i/4.
 int pack_labels_2bit(const uint8_t* labels, size_t n, uint8_t* out, void* stream);
 int launch_reduce_slots(const double* slots, int nslots, size_t row, double* out, void* stream);
 // Resident blocks per SM of the walk kernels (occupancy API); -1 on error.
 int walk_compat_blocks_per_sm(int nc, bool trace);
-int walk_split_blocks_per_sm(int nc, int block);
+int walk_split_blocks_per_sm(int nc, int lattice_bits, int variant);
 const char* cuda_error_string(int code);
 
 }  // namespace rms

@@ -9,8 +9,8 @@
 //  - position = int32 voxel index + FP32 offset inside the voxel, so FP32
 //    keeps ~1e-7 voxel resolution anywhere in a 2048-voxel lattice; a walker
 //    that crosses or reflects at a face is put exactly on it (offset 0 or 1);
-//  - FP32 uniforms (one Philox4x32-10 block per two steps), sincospif for the
-//    azimuth, one reciprocal per axis per step for the face distances;
+//  - FP32 uniforms (one Philox4x32-10 block per two steps), hardware
+//    sine/cosine and reciprocal for the direction and face distances;
 //  - labels packed 2 bits per voxel when Nc <= 4 (a 256x256x2048 lattice is
 //    33.5 MB and stays in the 126 MB L2), else one byte per voxel;
 //  - per-walker sums that grow over the walk (T2 exponent, PGSE displacement
@@ -18,9 +18,10 @@
 //  - cross-walker sums: FP32 products per walker, warp reduce-scatter in
 //    FP64, per-warp FP64 rows, ordered FP64 reduction (rms_reduce.cu).
 //
-// Random stream: the same Philox4x32-10 stream as the FP64 walk, read as
-// floats (one word each); draw order per walker: 3 per initial-position try,
-// 2 per step, 1 per partial-permeation face.
+// Random streams (philox.cuh): per walker, direction uniforms of steps 2k and
+// 2k+1 come from one Philox4x32-10 block indexed by k, so all lanes of a warp
+// generate in lock step; start positions and partial-permeation draws read
+// their own sequential counter domains.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -31,7 +32,13 @@
 namespace rms {
 namespace {
 
-constexpr int kSplitBlockMax = 512;
+// Launch variants (block size, minimum resident blocks per SM): the second
+// number caps registers per thread at 65536 / (block * minb), trading spills
+// in the rare record path for more resident warps to hide gather latency.
+struct SplitVariant { int block, minb; };
+constexpr SplitVariant kVariants[] = {
+    {256, 1}, {256, 2}, {256, 3}, {256, 4}, {128, 4}, {128, 6}, {128, 8}, {512, 1}, {512, 2}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 __device__ __forceinline__ unsigned lin3(int i, int j, int k, int n2, int n3) {
     return ((unsigned)i * (unsigned)n2 + (unsigned)j) * (unsigned)n3 + (unsigned)k;
@@ -62,16 +69,20 @@ __device__ __forceinline__ void mirror_origin(int& I, float& F, bool hi, int n) 
     else { I = base - I; }
 }
 
-template <int NCMAX, int BITS>
-__global__ void __launch_bounds__(256) walk_split_kernel(const WalkArgs a, const uint8_t* __restrict__ lat) {
-    __shared__ float s_step[NCMAX], s_istep[NCMAX], s_k[NCMAX], s_pij[NCMAX * NCMAX];
+template <int NCMAX, int BITS, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs a, const uint8_t* __restrict__ lat) {
+    // per compartment: step (voxels), T2 exponent per voxel of path; per pair:
+    // Pij and the step-length ratio that rescales the rest of a step
+    __shared__ float s_step[NCMAX], s_k[NCMAX], s_pij[NCMAX * NCMAX], s_ratio[NCMAX * NCMAX];
     for (int i = threadIdx.x; i < NCMAX * NCMAX; i += blockDim.x) {
-        s_pij[i] = (i < a.nc * a.nc) ? a.pijf[i] : 0.0f;
+        const int r = i / NCMAX, c = i % NCMAX;
+        const bool in = r < a.nc && c < a.nc;
+        s_pij[i] = in ? a.pijf[r * a.nc + c] : 0.0f;
+        const float sr = (r < a.nc) ? a.stepf[r] : 0.0f, sc = (c < a.nc) ? a.stepf[c] : 0.0f;
+        s_ratio[i] = (in && sr > 0.0f) ? sc / sr : 0.0f;
         if (i < NCMAX) {
             const float st = (i < a.nc) ? a.stepf[i] : 0.0f;
             s_step[i] = st;
-            s_istep[i] = st > 0.0f ? 1.0f / st : 0.0f;
-            // T2 exponent per voxel of path: (1/step) * (1/T2 in steps)
             s_k[i] = st > 0.0f ? (1.0f / st) * ((i < a.nc) ? a.t2invf[i] : 0.0f) : 0.0f;
         }
     }
@@ -88,24 +99,26 @@ __global__ void __launch_bounds__(256) walk_split_kernel(const WalkArgs a, const
     const int n1 = a.n1, n2 = a.n2, n3 = a.n3;
     const unsigned stride0 = (unsigned)n2 * (unsigned)n3, stride1 = (unsigned)n3;
     const float res = (float)a.res;
+    const uint32_t key0 = (uint32_t)a.seed, key1 = (uint32_t)(a.seed >> 32);
     double* slot = a.slots + (size_t)warp_global * a.timepoints * a.nvals;
     double* sig_slot = pgse ? a.sig_slots + (size_t)warp_global * a.ngrad_pad : nullptr;
 
     for (int64_t tile = warp_global; tile < ntiles; tile += nwarps) {
         const int64_t w = a.walker_begin + tile * 32 + lane;
         bool active = w < a.walker_end;
-        FloatStream rng;
-        rng.init(a.seed, (uint64_t)w);
+        const uint32_t wlo = (uint32_t)w, whi = (uint32_t)((uint64_t)w >> 32);
 
         // initial position: uniform in the labelled voxels (rejection sampling)
         int g0 = 0, g1 = 0, g2 = 0;
         float f0 = 0.5f, f1 = 0.5f, f2 = 0.5f;
         if (active) {
+            DomainStream init;
+            init.init(a.seed, (uint64_t)w, kDomInit);
             long long tries = 0;
             for (;;) {
-                const float x0 = rng.next() * (float)n1;
-                const float x1 = rng.next() * (float)n2;
-                const float x2 = rng.next() * (float)n3;
+                const float x0 = init.next() * (float)n1;
+                const float x1 = init.next() * (float)n2;
+                const float x2 = init.next() * (float)n3;
                 g0 = min((int)x0, n1 - 1); g1 = min((int)x1, n2 - 1); g2 = min((int)x2, n3 - 1);
                 f0 = x0 - (float)g0; f1 = x1 - (float)g1; f2 = x2 - (float)g2;
                 if (label_at<BITS>(lat, lin3(g0, g1, g2, n2, n3)) != 0) break;
@@ -114,9 +127,12 @@ __global__ void __launch_bounds__(256) walk_split_kernel(const WalkArgs a, const
         }
         unsigned lin = lin3(g0, g1, g2, n2, n3);
         int ai = active ? label_at<BITS>(lat, lin) : 0;
+        float cur_step = s_step[ai], cur_k = s_k[ai];
         // origin image (I + F per axis); displacement = (g - I) + (f - F)
         int I0 = g0, I1 = g1, I2 = g2;
         float F0 = f0, F1 = f1, F2 = f2;
+        DomainStream perm;
+        perm.init(a.seed, (uint64_t)w, kDomPerm);
 
         double w64 = 0.0;          // T2 exponent, folded
         float w32 = 0.0f;          // T2 exponent since the last fold
@@ -126,83 +142,93 @@ __global__ void __launch_bounds__(256) walk_split_kernel(const WalkArgs a, const
         int next_ev = (pgse && a.nevents > 0) ? a.ev_step[0] : -1;
         if (pgse)
             for (int k = 0; k < a.npairs * 3; ++k) a.vscr[(size_t)k * nthr + gtid] = 0.0;
+        uint32_t spare_u1 = 0u, spare_u2 = 0u;
 
         for (int i = 0; i < a.tn; ++i) {
+            // direction uniforms: one Philox block per two steps, in lock step
+            uint32_t r1, r2;
+            if ((i & 1) == 0) {
+                const U4 b = dir_block((uint32_t)(i >> 1), key0, key1, wlo, whi);
+                r1 = b.x; r2 = b.y; spare_u1 = b.z; spare_u2 = b.w;
+            } else {
+                r1 = spare_u1; r2 = spare_u2;
+            }
             if (active) {
-                const float u1 = rng.next();
-                const float u2 = rng.next();
+                const float u1 = u32_to_float(r1), u2 = u32_to_float(r2);
                 const float cz = 1.0f - 2.0f * u1;
-                const float sz = 2.0f * sqrtf(u1 * (1.0f - u1));
+                const float s2 = u1 * (1.0f - u1);
+                const float sz = 2.0f * s2 * rsqrtf(s2);
                 float sp, cp;
-                sincospif(2.0f * u2, &sp, &cp);
+                // azimuth 2 pi (u2 - 1/2): uniform on [-pi, pi), within the
+                // hardware sine/cosine's accurate range
+                __sincosf(6.283185307179586f * (u2 - 0.5f), &sp, &cp);
                 float v0 = sz * cp, v1 = sz * sp, v2 = cz;
-                const float iv0 = __frcp_rn(fabsf(v0)), iv1 = __frcp_rn(fabsf(v1)), iv2 = __frcp_rn(fabsf(v2));
-                float fstep = 1.0f;
+                const float iv0 = __fdividef(1.0f, fabsf(v0));
+                const float iv1 = __fdividef(1.0f, fabsf(v1));
+                const float iv2 = __fdividef(1.0f, fabsf(v2));
+                float rem = cur_step;        // path left in this step, voxels
                 unsigned flo = 0u, fhi = 0u;
-                for (int j = 0; (j < a.nite) && (fstep > 0.0f); ++j) {
+                for (int j = 0; j < a.nite; ++j) {
                     const float t0 = face_dist(f0, v0, iv0);
                     const float t1 = face_dist(f1, v1, iv1);
                     const float t2 = face_dist(f2, v2, iv2);
-                    float tmin = t0;
-                    int hit = 0;
-                    if (t1 < tmin) { tmin = t1; hit = 1; }
-                    if (t2 < tmin) { tmin = t2; hit = 2; }
-                    const float st = s_step[ai];
-                    const float rem = fstep * st;
-                    if (!(rem >= tmin)) {
+                    const float tmin = fminf(t0, fminf(t1, t2));
+                    if (rem < tmin) {
                         // the step ends inside the voxel
                         f0 = fmaf(rem, v0, f0); f1 = fmaf(rem, v1, f1); f2 = fmaf(rem, v2, f2);
-                        w32 = fmaf(rem, s_k[ai], w32);
-                        fstep = 0.0f;
+                        w32 = fmaf(rem, cur_k, w32);
+                        rem = 0.0f;
                         break;
                     }
-                    // move onto the face
+                    // onto the nearest face (lowest axis on ties, like the reference's scan)
+                    const int hit = (t0 == tmin) ? 0 : ((t1 == tmin) ? 1 : 2);
                     f0 = fmaf(tmin, v0, f0); f1 = fmaf(tmin, v1, f1); f2 = fmaf(tmin, v2, f2);
-                    w32 = fmaf(tmin, s_k[ai], w32);
-                    fstep = fmaxf(fstep - tmin * s_istep[ai], 0.0f);
+                    w32 = fmaf(tmin, cur_k, w32);
+                    rem -= tmin;
                     const float vh = hit == 0 ? v0 : (hit == 1 ? v1 : v2);
-                    const bool up = vh >= 0.0f;
-                    if (hit == 0) f0 = up ? 1.0f : 0.0f;
-                    else if (hit == 1) f1 = up ? 1.0f : 0.0f;
-                    else f2 = up ? 1.0f : 0.0f;
+                    const bool up = vh > 0.0f;
+                    const float on_face = up ? 1.0f : 0.0f;
+                    if (hit == 0) f0 = on_face; else if (hit == 1) f1 = on_face; else f2 = on_face;
                     const int gh = hit == 0 ? g0 : (hit == 1 ? g1 : g2);
                     const int nh = hit == 0 ? n1 : (hit == 1 ? n2 : n3);
-                    int gj = up ? gh + 1 : gh - 1;
-                    const int wall = (gj >= nh) ? 1 : ((gj < 0) ? -1 : 0);
-                    if (wall != 0 && mirror) {
-                        if (wall > 0) fhi |= 1u << hit; else flo |= 1u << hit;
-                        if (hit == 0) v0 = -v0; else if (hit == 1) v1 = -v1; else v2 = -v2;
-                        continue;
-                    }
                     const unsigned st_h = hit == 0 ? stride0 : (hit == 1 ? stride1 : 1u);
-                    unsigned lj;
-                    if (wall == 0) {
-                        lj = up ? lin + st_h : lin - st_h;
-                    } else {
-                        gj = (wall > 0) ? 0 : nh - 1;   // periodic neighbour
-                        lj = (wall > 0) ? lin - (unsigned)(nh - 1) * st_h : lin + (unsigned)(nh - 1) * st_h;
+                    int gj = up ? gh + 1 : gh - 1;
+                    unsigned lj = up ? lin + st_h : lin - st_h;
+                    const bool wall = (unsigned)gj >= (unsigned)nh;
+                    if (wall) {
+                        if (mirror) {
+                            if (up) fhi |= 1u << hit; else flo |= 1u << hit;
+                            if (hit == 0) v0 = -v0; else if (hit == 1) v1 = -v1; else v2 = -v2;
+                            if (!(rem > 0.0f)) break;
+                            continue;
+                        }
+                        gj = up ? 0 : nh - 1;   // periodic neighbour
+                        lj = up ? lin - (unsigned)(nh - 1) * st_h : lin + (unsigned)(nh - 1) * st_h;
                     }
                     const int aj = label_at<BITS>(lat, lj);
-                    const float P = s_pij[ai * a.nc + aj];
-                    bool cross;
-                    if (P > 0.999999f) cross = true;
-                    else if (P < 0.000001f) cross = false;
-                    else cross = rng.next() < P;
+                    const float P = s_pij[ai * NCMAX + aj];
+                    const bool cross = (P > 0.999999f) || (P >= 0.000001f && perm.next() < P);
                     if (cross) {
-                        ai = aj;
+                        if (aj != ai) {
+                            rem *= s_ratio[ai * NCMAX + aj];
+                            cur_step = s_step[aj];
+                            cur_k = s_k[aj];
+                            ai = aj;
+                        }
                         lin = lj;
                         const float fin = up ? 0.0f : 1.0f;
                         if (hit == 0) { g0 = gj; f0 = fin; }
                         else if (hit == 1) { g1 = gj; f1 = fin; }
                         else { g2 = gj; f2 = fin; }
-                        if (wall != 0) {
+                        if (wall) {
                             // periodic: shift the origin with the walker
-                            const int sh = (wall > 0) ? -nh : nh;
+                            const int sh = up ? -nh : nh;
                             if (hit == 0) I0 += sh; else if (hit == 1) I1 += sh; else I2 += sh;
                         }
                     } else {
                         if (hit == 0) v0 = -v0; else if (hit == 1) v1 = -v1; else v2 = -v2;
                     }
+                    if (!(rem > 0.0f)) break;
                 }
                 // mirror the origin for each wall hit this step (main.cu:302-310)
                 if (flo | fhi) {
@@ -325,10 +351,40 @@ __global__ void pack2_kernel(const uint8_t* __restrict__ labels, size_t n, uint8
     }
 }
 
-template <int NCMAX, int BITS>
-int launch_t(const WalkArgs& a, const uint8_t* lat, int grid, int block, void* stream) {
-    walk_split_kernel<NCMAX, BITS><<<grid, block, 0, (cudaStream_t)stream>>>(a, lat);
+template <int NCMAX, int BITS, int BLOCK, int MINB>
+int launch_t(const WalkArgs& a, const uint8_t* lat, int grid, void* stream) {
+    walk_split_kernel<NCMAX, BITS, BLOCK, MINB><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a, lat);
     return (int)cudaGetLastError();
+}
+
+template <int BLOCK, int MINB>
+const void* kernel_ptr(int nc, int bits) {
+    if (bits == 2) return (const void*)walk_split_kernel<4, 2, BLOCK, MINB>;
+    if (nc <= 4) return (const void*)walk_split_kernel<4, 8, BLOCK, MINB>;
+    return (const void*)walk_split_kernel<8, 8, BLOCK, MINB>;
+}
+
+template <int BLOCK, int MINB>
+int launch_v(const WalkArgs& a, const uint8_t* lat, int bits, int grid, void* stream) {
+    if (bits == 2) return a.nc <= 4 ? launch_t<4, 2, BLOCK, MINB>(a, lat, grid, stream) : (int)cudaErrorInvalidValue;
+    return a.nc <= 4 ? launch_t<4, 8, BLOCK, MINB>(a, lat, grid, stream)
+                     : launch_t<8, 8, BLOCK, MINB>(a, lat, grid, stream);
+}
+
+// Dispatch over the variant table (index v, 0-based).
+template <class F>
+auto by_variant(int v, F&& f) {
+    switch (v) {
+        case 0: return f.template operator()<256, 1>();
+        case 1: return f.template operator()<256, 2>();
+        case 2: return f.template operator()<256, 3>();
+        case 3: return f.template operator()<256, 4>();
+        case 4: return f.template operator()<128, 4>();
+        case 5: return f.template operator()<128, 6>();
+        case 6: return f.template operator()<128, 8>();
+        case 7: return f.template operator()<512, 1>();
+        default: return f.template operator()<512, 2>();
+    }
 }
 
 }  // namespace
@@ -341,20 +397,21 @@ int pack_labels_2bit(const uint8_t* labels, size_t n, uint8_t* out, void* stream
     return (int)cudaGetLastError();
 }
 
-int launch_walk_split(const WalkArgs& a, const uint8_t* lattice, int lattice_bits, int grid, int block,
+int split_variant_count() { return kNumVariants; }
+int split_variant_block(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].block : -1; }
+int split_variant_minb(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].minb : -1; }
+
+int launch_walk_split(const WalkArgs& a, const uint8_t* lattice, int lattice_bits, int variant, int grid,
                       void* stream) {
-    if (block > 256 || block % 32) return (int)cudaErrorInvalidValue;
-    if (lattice_bits == 2) return a.nc <= 4 ? launch_t<4, 2>(a, lattice, grid, block, stream)
-                                            : (int)cudaErrorInvalidValue;
-    return a.nc <= 4 ? launch_t<4, 8>(a, lattice, grid, block, stream)
-                     : launch_t<8, 8>(a, lattice, grid, block, stream);
+    if (variant < 0 || variant >= kNumVariants) return (int)cudaErrorInvalidValue;
+    return by_variant(variant, [&]<int B, int M>() { return launch_v<B, M>(a, lattice, lattice_bits, grid, stream); });
 }
 
-int walk_split_blocks_per_sm(int nc, int block) {
+int walk_split_blocks_per_sm(int nc, int lattice_bits, int variant) {
+    if (variant < 0 || variant >= kNumVariants) return -1;
+    const void* k = by_variant(variant, [&]<int B, int M>() { return kernel_ptr<B, M>(nc, lattice_bits); });
     int n = 0;
-    cudaError_t e;
-    if (nc <= 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, walk_split_kernel<4, 2>, block, 0);
-    else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, walk_split_kernel<8, 8>, block, 0);
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kVariants[variant].block, 0);
     return e == cudaSuccess ? n : -1;
 }
 

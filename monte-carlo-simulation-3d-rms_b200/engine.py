@@ -30,7 +30,8 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_sim_field_size", "rms_sim_get", "rms_sim_get_trace", "rms_sim_get_trace_positions",
            "rms_sim_write_dir",
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
-           "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version")
+           "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
+           "rms_split_variant", "rms_rng_split")
 
 _DP = C.POINTER(C.c_double)
 
@@ -56,7 +57,7 @@ class Config(C.Structure):
 class RunOpts(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64), ("precision", C.c_int), ("device", C.c_int),
-        ("stream", C.c_void_p), ("trace_walkers", C.c_int), ("block_size", C.c_int),
+        ("stream", C.c_void_p), ("trace_walkers", C.c_int), ("variant", C.c_int),
         ("walker_begin", C.c_int64), ("walker_end", C.c_int64),
     ]
 
@@ -94,6 +95,8 @@ def lib():
         L.rms_rng_doubles.argtypes = [C.c_uint64, C.c_uint64, C.c_int, _DP]
         L.rms_rng_floats.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.POINTER(C.c_float)]
         L.rms_philox4x32_10.argtypes = [C.POINTER(C.c_uint32)] * 3
+        L.rms_rng_split.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_float)]
+        L.rms_split_variant.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -167,11 +170,11 @@ class Sim:
                                          *[int(x) for x in lab.shape]))
 
     def run(self, seed: int = 0, precision: str = "compat", device: int = 0, stream=None,
-            trace_walkers: int = 0, block_size: int = 0, walker_range=None):
+            trace_walkers: int = 0, variant: int = 0, walker_range=None):
         w0, w1 = walker_range if walker_range is not None else (0, 0)
         st = None if stream is None else C.c_void_p(int(stream))
         opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION[precision], int(device), st,
-                       int(trace_walkers), int(block_size), int(w0), int(w1))
+                       int(trace_walkers), int(variant), int(w0), int(w1))
         _check(lib().rms_sim_run(self._h, C.byref(opts)))
         return self
 
@@ -255,6 +258,12 @@ def rng_floats(seed: int, walker: int, n: int) -> np.ndarray:
     return out
 
 
+def rng_split(seed: int, walker: int, domain: int, n: int) -> np.ndarray:
+    out = np.zeros(n, dtype=np.float32)
+    _check(lib().rms_rng_split(seed, walker, domain, n, out.ctypes.data_as(C.POINTER(C.c_float))))
+    return out
+
+
 def philox4x32_10(ctr, key) -> np.ndarray:
     c = np.ascontiguousarray(ctr, dtype=np.uint32)
     k = np.ascontiguousarray(key, dtype=np.uint32)
@@ -262,6 +271,17 @@ def philox4x32_10(ctr, key) -> np.ndarray:
     p = C.POINTER(C.c_uint32)
     _check(lib().rms_philox4x32_10(c.ctypes.data_as(p), k.ctypes.data_as(p), out.ctypes.data_as(p)))
     return out
+
+
+def split_variants():
+    """[(k, block, min_blocks_per_sm)] of the SPLIT walk's launch variants."""
+    out, k = [], 1
+    while True:
+        b, m = C.c_int(), C.c_int()
+        if lib().rms_split_variant(k, C.byref(b), C.byref(m)) != 0:
+            return out
+        out.append((k, b.value, m.value))
+        k += 1
 
 
 def version() -> str:

@@ -117,6 +117,46 @@ static inline float or_stream_float(or_stream* s) {
     return or_u32_to_float(or_stream_word(s));
 }
 
+/* Streams of the engine's split-precision walk: Philox counter
+ * (k, domain, walker_lo, walker_hi).  Domain 0: block k holds the direction
+ * uniforms of steps 2k (words 0, 1) and 2k+1 (words 2, 3).  Domain 1: start
+ * positions, sequential.  Domain 2: partial-permeation draws, sequential. */
+#define OR_DOM_DIR 0u
+#define OR_DOM_INIT 1u
+#define OR_DOM_PERM 2u
+
+static inline void or_dir_uniforms(uint64_t seed, uint64_t walker, uint32_t step, float* u1, float* u2) {
+    uint32_t ctr[4] = {step >> 1, OR_DOM_DIR, (uint32_t)walker, (uint32_t)(walker >> 32)};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t out[4];
+    or_philox4x32(ctr, key, 10, out);
+    *u1 = or_u32_to_float(out[(step & 1) ? 2 : 0]);
+    *u2 = or_u32_to_float(out[(step & 1) ? 3 : 1]);
+}
+
+typedef struct or_dstream {
+    uint32_t key[2];
+    uint64_t walker;
+    uint32_t dom, block;
+    uint32_t buf[4];
+    int pos;
+} or_dstream;
+
+static inline void or_dstream_init(or_dstream* s, uint64_t seed, uint64_t walker, uint32_t dom) {
+    s->key[0] = (uint32_t)seed; s->key[1] = (uint32_t)(seed >> 32);
+    s->walker = walker; s->dom = dom; s->block = 0; s->pos = 4;
+}
+
+static inline float or_dstream_float(or_dstream* s) {
+    if (s->pos >= 4) {
+        uint32_t ctr[4] = {s->block, s->dom, (uint32_t)s->walker, (uint32_t)(s->walker >> 32)};
+        or_philox4x32(ctr, s->key, 10, s->buf);
+        s->block++;
+        s->pos = 0;
+    }
+    return or_u32_to_float(s->buf[s->pos++]);
+}
+
 #ifdef __cplusplus
 }
 #endif

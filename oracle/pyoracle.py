@@ -154,11 +154,15 @@ def _out_struct(o):
 
 
 def run_oracle(job: Job, w_begin: int = 0, w_end: Optional[int] = None, nthreads: int = 1,
-               trace_walkers: int = 0):
+               trace_walkers: int = 0, split: bool = False):
     """Walk walkers [w_begin, w_end) with the C restatement.  With
     ``trace_walkers`` > 0 the first that many walkers of the range also
-    return their per-step voxel and event traces (single thread)."""
+    return their per-step voxel and event traces (single thread).  With
+    ``split`` the FP64 replay of the engine's split-precision walk runs instead
+    of the reference walk."""
     lib = oracle_lib()
+    run1 = lib.or_run_split if split else lib.or_run
+    runp = lib.or_run_split_parallel if split else lib.or_run_parallel
     if w_end is None:
         w_end = job.npar
     o = job.empty_outputs()
@@ -173,13 +177,12 @@ def run_oracle(job: Job, w_begin: int = 0, w_end: Optional[int] = None, nthreads
         tr = OrTrace(w_begin, nw, tr_init.ctypes.data_as(C.POINTER(C.c_int32)),
                      tr_vox.ctypes.data_as(C.POINTER(C.c_int32)),
                      tr_ev.ctypes.data_as(C.POINTER(C.c_uint32)), _dp(tr_pos))
-        rc = lib.or_run(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.byref(outs), C.byref(tr))
+        rc = run1(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.byref(outs), C.byref(tr))
         o["trace"] = dict(init_voxel=tr_init, voxel=tr_vox, events=tr_ev, pos=tr_pos)
     elif nthreads > 1:
-        rc = lib.or_run_parallel(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end),
-                                 C.c_int(nthreads), C.byref(outs))
+        rc = runp(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.c_int(nthreads), C.byref(outs))
     else:
-        rc = lib.or_run(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.byref(outs), None)
+        rc = run1(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.byref(outs), None)
     if rc != 0:
         raise RuntimeError(f"or_run failed: {rc}")
     return o
@@ -195,6 +198,20 @@ def stream_floats(seed: int, walker: int, n: int) -> np.ndarray:
     out = np.zeros(n, dtype=np.float32)
     oracle_lib().or_stream_floats(C.c_uint64(seed), C.c_uint64(walker), C.c_int(n),
                                   out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def split_dir_uniforms(seed: int, walker: int, nsteps: int) -> np.ndarray:
+    out = np.zeros(2 * nsteps, dtype=np.float32)
+    oracle_lib().or_split_dir_uniforms(C.c_uint64(seed), C.c_uint64(walker), C.c_int(nsteps),
+                                       out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def split_domain_floats(seed: int, walker: int, dom: int, n: int) -> np.ndarray:
+    out = np.zeros(n, dtype=np.float32)
+    oracle_lib().or_split_domain_floats(C.c_uint64(seed), C.c_uint64(walker), C.c_uint32(dom), C.c_int(n),
+                                        out.ctypes.data_as(C.POINTER(C.c_float)))
     return out
 
 

@@ -258,10 +258,180 @@ static void walk_one(const or_params* p, int64_t w, or_outputs* out, double* pha
     }
 }
 
+/* ---------------- FP64 replay of the split-precision walk ---------------- */
+
+static void split_mirror_origin(double* xi, int hi, int n) {
+    /* origin image x -> -x (lo wall) or 2N - x (hi wall), main.cu:302-310 */
+    *xi = hi ? 2.0 * (double)n - *xi : -*xi;
+}
+
+static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, double* phase,
+                           int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev, double* tr_pos) {
+    const int Nc = p->nc;
+    const int Tstep = p->tn / p->timepoints;
+    const int NPix[3] = {p->n1, p->n2, p->n3};
+    const uint8_t* APix = p->labels;
+    or_dstream init, perm;
+    or_dstream_init(&init, p->seed, (uint64_t)w, OR_DOM_INIT);
+    or_dstream_init(&perm, p->seed, (uint64_t)w, OR_DOM_PERM);
+    int g[3];
+    double f[3], xi[3];
+    /* start position, formed in FP32 like the GPU */
+    for (;;) {
+        float x[3];
+        for (int a = 0; a < 3; a++) {
+            x[a] = or_dstream_float(&init) * (float)NPix[a];
+            g[a] = (int)x[a];
+            if (g[a] > NPix[a] - 1) g[a] = NPix[a] - 1;
+            f[a] = (double)(x[a] - (float)g[a]);
+        }
+        if (APix[lin(p, g[0], g[1], g[2])] != 0) break;
+    }
+    for (int a = 0; a < 3; a++) xi[a] = (double)g[a] + f[a];
+    int ai = APix[lin(p, g[0], g[1], g[2])];
+    if (tr_init) *tr_init = (int32_t)lin(p, g[0], g[1], g[2]);
+    double wexp = 0.0;   /* T2 exponent */
+    for (int i = 0; i < p->tn; i++) {
+        float u1f, u2f;
+        or_dir_uniforms(p->seed, (uint64_t)w, (uint32_t)i, &u1f, &u2f);
+        const double u1 = u1f, u2 = u2f;
+        const double cz = 1.0 - 2.0 * u1;
+        const double sz = 2.0 * sqrt(u1 * (1.0 - u1));
+        const double phi = 6.283185307179586 * (u2 - 0.5);
+        double v[3] = {sz * cos(phi), sz * sin(phi), cz};
+        double rem = p->step[ai];
+        int flo = 0, fhi = 0, nev = 0;
+        uint32_t ev = 0;
+        for (int j = 0; j < p->nite; j++) {
+            double t[3], tmin;
+            for (int a = 0; a < 3; a++) {
+                double d = (v[a] > 0.0) ? 1.0 - f[a] : f[a];
+                if (d < 0.0) d = 0.0;
+                t[a] = (v[a] == 0.0) ? INFINITY : d / fabs(v[a]);
+            }
+            tmin = fmin(t[0], fmin(t[1], t[2]));
+            if (rem < tmin) {
+                for (int a = 0; a < 3; a++) f[a] += rem * v[a];
+                wexp += rem / p->step[ai] / p->t2[ai];
+                rem = 0.0;
+                break;
+            }
+            const int hit = (t[0] == tmin) ? 0 : ((t[1] == tmin) ? 1 : 2);
+            for (int a = 0; a < 3; a++) f[a] += tmin * v[a];
+            wexp += tmin / p->step[ai] / p->t2[ai];
+            rem -= tmin;
+            const int up = v[hit] > 0.0;
+            f[hit] = up ? 1.0 : 0.0;
+            int gj = up ? g[hit] + 1 : g[hit] - 1;
+            const int wall = (gj < 0 || gj >= NPix[hit]);
+            if (wall && p->boundary == OR_BOUNDARY_MIRROR) {
+                if (up) fhi |= 1 << hit; else flo |= 1 << hit;
+                v[hit] = -v[hit];
+                ev |= (OR_EV_MIRROR << 2 | (uint32_t)hit) << (4 * nev++);
+                if (!(rem > 0.0)) break;
+                continue;
+            }
+            if (wall) gj = up ? 0 : NPix[hit] - 1;
+            int gn[3] = {g[0], g[1], g[2]};
+            gn[hit] = gj;
+            const int aj = APix[lin(p, gn[0], gn[1], gn[2])];
+            const double P = p->pij[ai * Nc + aj];
+            const int cross = (P > 0.999999) || (P >= 0.000001 && (double)or_dstream_float(&perm) < P);
+            if (cross) {
+                if (aj != ai) {
+                    rem *= p->step[aj] / p->step[ai];
+                    ai = aj;
+                }
+                g[hit] = gj;
+                f[hit] = up ? 0.0 : 1.0;
+                if (wall) {
+                    xi[hit] += up ? -(double)NPix[hit] : (double)NPix[hit];
+                    ev |= (OR_EV_WRAP << 2 | (uint32_t)hit) << (4 * nev++);
+                } else {
+                    ev |= (OR_EV_CROSS << 2 | (uint32_t)hit) << (4 * nev++);
+                }
+            } else {
+                v[hit] = -v[hit];
+                ev |= (OR_EV_REFLECT << 2 | (uint32_t)hit) << (4 * nev++);
+            }
+            if (!(rem > 0.0)) break;
+        }
+        if (rem > 0.0) ev |= 1u << 31;
+        ev |= (uint32_t)nev << 28;
+        for (int a = 0; a < 3; a++) {
+            if (flo & (1 << a)) split_mirror_origin(&xi[a], 0, NPix[a]);
+            if (fhi & (1 << a)) split_mirror_origin(&xi[a], 1, NPix[a]);
+        }
+        if (tr_vox) {
+            tr_vox[i] = (int32_t)lin(p, g[0], g[1], g[2]);
+            tr_ev[i] = ev;
+        }
+        if (tr_pos) for (int a = 0; a < 3; a++) tr_pos[3 * i + a] = (double)g[a] + f[a];
+        const double dx = ((double)g[0] + f[0] - xi[0]) * p->res;
+        const double dy = ((double)g[1] + f[1] - xi[1]) * p->res;
+        const double dz = ((double)g[2] + f[2] - xi[2]) * p->res;
+        if (p->mode == OR_MODE_PGSE) {
+            const double* gr = p->grad;
+            const double ti = (double)(i + 1) * p->dt;
+            for (int jg = 0; jg < p->ngrad; jg++) {
+                const double q = gr[jg * 6 + 2] * (dx * gr[jg * 6 + 3] + dy * gr[jg * 6 + 4] + dz * gr[jg * 6 + 5]) * p->dt;
+                if (ti < gr[jg * 6 + 1]) phase[jg] += q;
+                else if ((ti >= gr[jg * 6]) && (ti < (gr[jg * 6] + gr[jg * 6 + 1]))) phase[jg] -= q;
+            }
+            if (i == p->tn - 1) {
+                const double s0 = exp(-wexp);
+                for (int jg = 0; jg < p->ngrad; jg++) out->sig[jg] += s0 * cos(phase[jg]);
+            }
+        }
+        if ((i % Tstep) == 0) {
+            const int tidx = i / Tstep;
+            if (tidx >= p->timepoints) continue;
+            const double s0 = exp(-wexp);
+            out->sig0[tidx] += s0;
+            out->npar_count[Nc * tidx + ai] += 1;
+            const double d[3] = {dx, dy, dz};
+            double* d2 = out->dx2 + 6 * tidx;
+            double* d4 = out->dx4 + 15 * tidx;
+            int k2 = 0, k4 = 0;
+            for (int a = 0; a < 3; a++)
+                for (int b = a; b < 3; b++) d2[k2++] += s0 * d[a] * d[b];
+            for (int a = 0; a < 3; a++)
+                for (int b = a; b < 3; b++)
+                    for (int c = b; c < 3; c++)
+                        for (int e = c; e < 3; e++) d4[k4++] += s0 * d[a] * d[b] * d[c] * d[e];
+            if (p->mode == OR_MODE_NARROW) {
+                for (int jb = 0; jb < p->nbvec; jb++) {
+                    const double qx = sqrt(p->bval[jb] / p->td[tidx]) *
+                                      (dx * p->bvec[jb * 3] + dy * p->bvec[jb * 3 + 1] + dz * p->bvec[jb * 3 + 2]);
+                    out->sigre[p->nbvec * tidx + jb] += s0 * cos(qx);
+                }
+            }
+        }
+    }
+}
+
+typedef void (*walk_fn)(const or_params*, int64_t, or_outputs*, double*, int32_t*, int32_t*,
+                        uint32_t*, double*);
+
+static int run_range(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
+                     or_trace* tr, walk_fn fn);
+
+int or_run_split(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
+                 or_trace* tr) {
+    int rc = check(p);
+    if (rc) return rc;
+    return run_range(p, w_begin, w_end, out, tr, walk_one_split);
+}
+
 int or_run(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
            or_trace* tr) {
     int rc = check(p);
     if (rc) return rc;
+    return run_range(p, w_begin, w_end, out, tr, walk_one);
+}
+
+static int run_range(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
+                     or_trace* tr, walk_fn fn) {
     double* phase = NULL;
     if (p->mode == OR_MODE_PGSE && p->ngrad > 0) {
         phase = (double*)malloc(sizeof(double) * (size_t)p->ngrad);
@@ -277,7 +447,7 @@ int or_run(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
             te = tr->events + r * p->tn;
             if (tr->pos) tp = tr->pos + r * p->tn * 3;
         }
-        walk_one(p, w, out, phase, ti, tv, te, tp);
+        fn(p, w, out, phase, ti, tv, te, tp);
     }
     free(phase);
     return 0;
@@ -304,8 +474,21 @@ static void add_outputs(const or_params* p, or_outputs* dst, const or_outputs* s
         for (int i = 0; i < p->ngrad; i++) dst->sig[i] += src->sig[i];
 }
 
+static int run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthreads,
+                        or_outputs* out, int split);
+
 int or_run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthreads,
                     or_outputs* out) {
+    return run_parallel(p, w_begin, w_end, nthreads, out, 0);
+}
+
+int or_run_split_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthreads,
+                          or_outputs* out) {
+    return run_parallel(p, w_begin, w_end, nthreads, out, 1);
+}
+
+static int run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthreads,
+                        or_outputs* out, int split) {
     int rc = check(p);
     if (rc) return rc;
     if (nthreads < 1) nthreads = 1;
@@ -330,7 +513,7 @@ int or_run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthr
     {
         int t = omp_get_thread_num(), nt = omp_get_num_threads();
         int64_t lo = w_begin + n * t / nt, hi = w_begin + n * (t + 1) / nt;
-        if (or_run(p, lo, hi, &priv[t], NULL) != 0) {
+        if ((split ? or_run_split(p, lo, hi, &priv[t], NULL) : or_run(p, lo, hi, &priv[t], NULL)) != 0) {
 #pragma omp atomic write
             err = 1;
         }
@@ -352,6 +535,16 @@ void or_stream_doubles(uint64_t seed, uint64_t walker, int n, double* out) {
     or_stream s;
     or_stream_init(&s, seed, walker);
     for (int i = 0; i < n; i++) out[i] = or_stream_double(&s);
+}
+
+void or_split_dir_uniforms(uint64_t seed, uint64_t walker, int nsteps, float* out) {
+    for (int i = 0; i < nsteps; i++) or_dir_uniforms(seed, walker, (uint32_t)i, &out[2 * i], &out[2 * i + 1]);
+}
+
+void or_split_domain_floats(uint64_t seed, uint64_t walker, uint32_t dom, int n, float* out) {
+    or_dstream s;
+    or_dstream_init(&s, seed, walker, dom);
+    for (int i = 0; i < n; i++) out[i] = or_dstream_float(&s);
 }
 
 void or_stream_floats(uint64_t seed, uint64_t walker, int n, float* out) {

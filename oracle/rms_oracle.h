@@ -85,10 +85,23 @@ int or_run(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
 int or_run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthreads,
                     or_outputs* out);
 
+/* FP64 replay of the engine's split-precision walk (RMS_PREC_SPLIT): the same
+ * algorithm and the same random streams (philox_stream.h, split domains),
+ * every quantity after the start position in FP64.  The start position is
+ * formed in FP32 exactly as the GPU forms it, so both runs start from the same
+ * point and differ only by the precision of the dynamics.  PGSE phases are
+ * accumulated per step as in the reference (main_PGSE.cu:340-346). */
+int or_run_split(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
+                 or_trace* trace);
+int or_run_split_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthreads,
+                          or_outputs* out);
+
 /* The project's stream, exposed for known-answer tests. */
 void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void or_stream_doubles(uint64_t seed, uint64_t walker, int n, double* out);
 void or_stream_floats(uint64_t seed, uint64_t walker, int n, float* out);
+void or_split_dir_uniforms(uint64_t seed, uint64_t walker, int nsteps, float* out);  /* [nsteps*2] */
+void or_split_domain_floats(uint64_t seed, uint64_t walker, uint32_t dom, int n, float* out);
 
 #ifdef __cplusplus
 }

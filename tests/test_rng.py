@@ -33,6 +33,14 @@ def test_streams_match_oracle(seed, walker):
     assert np.array_equal(engine.rng_floats(seed, walker, 257), pyoracle.stream_floats(seed, walker, 257))
 
 
+@pytest.mark.parametrize("seed,walker", [(0, 0), (99, 123456), (2**64 - 1, 2**39 + 1)])
+def test_split_streams_match_oracle(seed, walker):
+    assert np.array_equal(engine.rng_split(seed, walker, 0, 400), pyoracle.split_dir_uniforms(seed, walker, 200))
+    for dom in (1, 2):
+        assert np.array_equal(engine.rng_split(seed, walker, dom, 101),
+                              pyoracle.split_domain_floats(seed, walker, dom, 101))
+
+
 def test_uniform_maps_open_interval_and_moments():
     d = np.concatenate([engine.rng_doubles(3, w, 2000) for w in range(20)])
     f = np.concatenate([engine.rng_floats(3, w, 2000) for w in range(20)]).astype(np.float64)
