@@ -238,7 +238,8 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn)
-    w0, w1 = rank * per_gpu, (rank + 1) * per_gpu
+    from rms_b200 import shards
+    w0, w1 = shards.walker_shard(per_gpu, rank)
     sim = engine.Sim(lab, **sim_kw)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -305,6 +306,9 @@ def run_ours(args):
         sim.set_lattice(lab_pinned)
         one(3000 + i)
         out = sim.outputs()
+        if world > 1:
+            # the whole job's result: rank-order sum of the shards' accumulators
+            out = shards.gather_sum({k: v for k, v in out.items() if k != "td"}, device="cuda")
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     if world > 1:

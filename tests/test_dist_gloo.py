@@ -1,0 +1,69 @@
+"""Walker sharding across two ranks (gloo, CPU): each rank walks its shard
+and the FP64 accumulators are summed in rank order; the result equals the
+unsharded job (counts exactly, sums to 1e-12).  The walk itself is the
+oracle here, standing in for the GPU kernel on this CPU-only check of the
+rank logic (rms_b200.shards, used by bench.py)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import pyoracle
+from rms_b200 import geometry, shards
+
+
+def _job():
+    lab = geometry.axon_lattice(12, 12, 16, 0.1, seed=3, exterior=2, r0=0.4)
+    step, t2s, pij, td = pyoracle.reference_tables(2e-4, 0.1, [0, 2.0, 1.0], [80, 80, 40], 1000, 1000)
+    return pyoracle.Job(lab, dt=2e-4, tn=1000, npar=60, res=0.1, step=step, t2_steps=t2s, pij=pij,
+                        seed=5, td=td, bval=[1.0], bvec=[[1, 0, 0]])
+
+
+def _rank(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    job = _job()
+    w0, w1 = shards.split_range(job.npar, rank, world)
+    o = pyoracle.run_oracle(job, w0, w1)
+    fields = {k: o[k] for k in ("sig0", "dx2", "dx4", "sigre", "npar_count")}
+    tot = shards.gather_sum(fields)
+    if rank == 0:
+        q.put({k: v.copy() for k, v in tot.items()})
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def test_two_rank_shards_sum_to_the_whole_job():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    whole = pyoracle.run_oracle(_job())
+    assert np.array_equal(got["npar_count"], whole["npar_count"])
+    for k in ("sig0", "dx2", "dx4", "sigre"):
+        np.testing.assert_allclose(got[k], whole[k], rtol=1e-12, atol=1e-12 * np.abs(whole[k]).max())
+
+
+def test_shard_ranges_cover_the_job():
+    for npar, world in ((10, 3), (1, 2), (1000003, 8)):
+        rs = [shards.split_range(npar, r, world) for r in range(world)]
+        assert rs[0][0] == 0 and rs[-1][1] == npar
+        assert all(a[1] == b[0] for a, b in zip(rs, rs[1:]))
+    assert shards.walker_shard(100, 3) == (300, 400)
