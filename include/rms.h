@@ -193,6 +193,30 @@ int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out)
  * shape, hpc_code/lib/main.cu:499-504). */
 int rms_split_variant(int k, int* block, int* min_blocks_per_sm);
 
+/* ---- Walk without allocating device memory --------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library
+ * call cudaMalloc: applications whose device memory is all owned by their own
+ * allocator (a framework pool, a fixed pre-reserved budget), and code that
+ * must not hit cudaMalloc/cudaFree because they synchronise the whole device.
+ * Runs the SPLIT walk of `sim` (its configuration and tables; the sim itself is
+ * not changed) on device buffers the caller owns:
+ *   d_labels  [n1*n2*n3] uint8 lattice, n3 fastest, labels < nc (nc <= 4)
+ *   d_rows    [timepoints * W] doubles, W = 32 (PGSE) or 32 + 32*ceil(nbvec/32)
+ *             (narrow); row t holds sig0 at column 0, dx2 at 1-6, dx4 at 7-21,
+ *             compartment counts at 22.., sigRe at 32..
+ *   d_sig     [32*ceil(max(ngrad,1)/32)] doubles (PGSE; NULL for narrow)
+ * on opts->stream (NULL = the default stream), and returns after the walk
+ * finished.  All scratch lives in one fixed device array of
+ * RMS_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit; a job needing more scratch than that is refused with RMS_ERR_RANGE,
+ * and large jobs run on fewer warps than rms_sim_run uses.  The first call on
+ * each device looks up the array's device address: make it before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race:
+ * serialise them.  No memory is allocated, host or device. */
+#define RMS_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint8_t* d_labels,
+                        double* d_rows, double* d_sig);
+
 /* Library version string. */
 const char* rms_version(void);
 

@@ -31,7 +31,7 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_sim_write_dir",
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
-           "rms_split_variant", "rms_rng_split")
+           "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc")
 
 _DP = C.POINTER(C.c_double)
 
@@ -95,6 +95,7 @@ def lib():
         L.rms_rng_doubles.argtypes = [C.c_uint64, C.c_uint64, C.c_int, _DP]
         L.rms_rng_floats.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.POINTER(C.c_float)]
         L.rms_philox4x32_10.argtypes = [C.POINTER(C.c_uint32)] * 3
+        L.rms_sim_run_noalloc.argtypes = [C.c_void_p, C.POINTER(RunOpts), C.c_void_p, C.c_void_p, C.c_void_p]
         L.rms_rng_split.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.rms_split_variant.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         _lib = L
@@ -176,6 +177,17 @@ class Sim:
         opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION[precision], int(device), st,
                        int(trace_walkers), int(variant), int(w0), int(w1))
         _check(lib().rms_sim_run(self._h, C.byref(opts)))
+        return self
+
+    def run_noalloc(self, d_labels: int, d_rows: int, d_sig: int = 0, seed: int = 0, device: int = 0,
+                    stream=None, walker_range=None):
+        """The split walk on caller-owned device buffers (raw device addresses),
+        allocating nothing; see rms_sim_run_noalloc in include/rms.h."""
+        w0, w1 = walker_range if walker_range is not None else (0, 0)
+        st = None if stream is None else C.c_void_p(int(stream))
+        opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION["split"], int(device), st, 0, 0, int(w0), int(w1))
+        _check(lib().rms_sim_run_noalloc(self._h, C.byref(opts), C.c_void_p(int(d_labels)),
+                                         C.c_void_p(int(d_rows)), C.c_void_p(int(d_sig)) if d_sig else None))
         return self
 
     def field_size(self, name: str) -> int:
