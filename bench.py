@@ -327,12 +327,14 @@ def run_ours(args):
     except OSError:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
+    # DRAM bytes per launch from the ncu capture summarised in profiles/
+    # (measured per walker-step on a production-shaped case, scaled to this launch)
     traffic = None
-    try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "walk_traffic.json")))
-        traffic = prof.get(f"{args.workload}/{precision}")
-    except OSError:
-        pass
+    prof = os.path.join(ROOT, "profiles", f"walk_{precision}_kernel__{args.workload}.md")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            if ln.startswith("traffic_bytes_per_walker_step:"):
+                traffic = float(ln.split(":")[1]) * walker_steps
 
     if rank == 0:
         cpu = None
