@@ -180,7 +180,8 @@ int finalize_config(rms_sim* s) {
     }
     if (!(s->res > 0.0)) return set_error(RMS_ERR_RANGE, "voxel size must be > 0");
     if (s->n1 < 1 || s->n2 < 1 || s->n3 < 1) return set_error(RMS_ERR_RANGE, "lattice size must be >= 1");
-    if ((double)s->n1 * s->n2 * s->n3 >= 2147483648.0)
+    if ((double)s->n1 * s->n2 * s->n3 >= 2147483648.0 ||
+        ((double)s->n1 + 2) * ((double)s->n2 + 2) * ((double)s->n3 + 2) >= 4294967296.0)
         return set_error(RMS_ERR_RANGE, "lattice larger than 2^31 voxels");
     if ((int)s->diffusivity.size() != s->nc || (int)s->t2.size() != s->nc)
         return set_error(RMS_ERR_ARG, "diffusivity and T2 need Nc values");
@@ -327,7 +328,7 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
     RMS_CUDA(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
     int block = kCompatBlock;
     int per_sm;
-    const int lattice_bits = (prec == RMS_PREC_SPLIT && s->nc <= 4) ? 2 : 8;
+    const int lattice_bits = split_lattice_bits(s->nc);
     int variant = 0;
     if (prec == RMS_PREC_COMPAT) {
         per_sm = walk_compat_blocks_per_sm(s->nc, trace_n > 0);
@@ -359,10 +360,10 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
         d->packed_valid = false;
         s->lattice_dirty = false;
     }
-    if (lattice_bits == 2 && !d->packed_valid) {
-        const size_t nvox = s->labels.size();
-        RMS_CUDA(d->packed.ensure((nvox + 3) / 4));
-        int pe = pack_labels_2bit(d->labels.as<uint8_t>(), nvox, d->packed.as<uint8_t>(), st);
+    if (prec == RMS_PREC_SPLIT && !d->packed_valid) {
+        RMS_CUDA(d->packed.ensure(padded_lattice_bytes(s->n1, s->n2, s->n3, lattice_bits)));
+        int pe = pack_lattice_padded(d->labels.as<uint8_t>(), s->n1, s->n2, s->n3, lattice_bits,
+                                     d->packed.as<uint8_t>(), st);
         if (pe) return cuda_fail((cudaError_t)pe, "label packing");
         d->packed_valid = true;
     }
@@ -434,8 +435,7 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
 
     RMS_CUDA(cudaEventRecord(d->e0, st));
     int e = (prec == RMS_PREC_COMPAT) ? launch_walk_compat(a, grid, block, trace_n > 0, st)
-                                      : launch_walk_split(a, lattice_bits == 2 ? d->packed.as<uint8_t>() : a.labels,
-                                                          lattice_bits, variant, grid, st);
+                                      : launch_walk_split(a, d->packed.as<uint8_t>(), lattice_bits, variant, grid, st);
     if (e) return cuda_fail((cudaError_t)e, "walk kernel launch");
     RMS_CUDA(cudaEventRecord(d->e1, st));
     e = launch_reduce_slots(a.slots, nslots, row, d->out.as<double>(), st);

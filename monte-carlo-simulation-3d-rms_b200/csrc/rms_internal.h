@@ -65,8 +65,11 @@ int launch_walk_split(const WalkArgs& a, const uint8_t* lattice, int lattice_bit
 int split_variant_count();
 int split_variant_block(int variant);   // threads per block of a launch variant
 int split_variant_minb(int variant);    // its minimum resident blocks per SM
-// Pack one-byte labels (< 4) into 2 bits per voxel, voxel i in bits 2(i%4) of byte i/4.
-int pack_labels_2bit(const uint8_t* labels, size_t n, uint8_t* out, void* stream);
+// The split walk's lattice: (n1+2) x (n2+2) x (n3+2) with a wall-code border,
+// 2 bits per voxel when Nc <= 3 (wall 3), else one byte (wall 255).
+int split_lattice_bits(int nc);
+size_t padded_lattice_bytes(int n1, int n2, int n3, int bits);
+int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits, uint8_t* out, void* stream);
 int launch_reduce_slots(const double* slots, int nslots, size_t row, double* out, void* stream);
 // Resident blocks per SM of the walk kernels (occupancy API); -1 on error.
 int walk_compat_blocks_per_sm(int nc, bool trace);

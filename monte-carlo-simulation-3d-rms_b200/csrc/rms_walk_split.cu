@@ -6,17 +6,29 @@
 // walls, T2 weighting, moments and signal at the same records -- in the
 // arithmetic a B200 issues fastest:
 //
-//  - position = int32 voxel index + FP32 offset inside the voxel, so FP32
-//    keeps ~1e-7 voxel resolution anywhere in a 2048-voxel lattice; a walker
-//    that crosses or reflects at a face is put exactly on it (offset 0 or 1);
-//  - FP32 uniforms (one Philox4x32-10 block per two steps), hardware
-//    sine/cosine and reciprocal for the direction and face distances;
-//  - labels packed 2 bits per voxel when Nc <= 4 (a 256x256x2048 lattice is
-//    33.5 MB and stays in the 126 MB L2), else one byte per voxel;
+//  - position = voxel + FP32 offset inside it, carried per axis as d_a, the
+//    distance to the next face in the current direction of travel (0..1).
+//    The time to a face is one multiply, and after any face event -- a cross
+//    into the neighbour or a reflection -- the walker sits on that face with a
+//    whole voxel ahead: d = 1 exactly, so no drift accumulates;
+//  - the voxel is one linear index into a lattice padded with a one-voxel
+//    border that holds a wall code: a face step is `lin += stride`, and
+//    reaching a wall is a label like any other (rare branch); the integer
+//    part of the displacement, D = voxel - origin image, is carried per axis;
+//  - labels packed 2 bits per voxel when Nc <= 3 (wall = 3; a padded
+//    256x256x2048 lattice is 34 MB and stays in the 126 MB L2), else one byte
+//    per voxel (wall = 255);
+//  - FP32 uniforms, one Philox4x32-10 block per two steps; hardware
+//    sine/cosine and reciprocal for the direction and face times;
 //  - per-walker sums that grow over the walk (T2 exponent, PGSE displacement
 //    sums) are carried in FP32 for at most 32 steps and folded into FP64;
 //  - cross-walker sums: FP32 products per walker, warp reduce-scatter in
 //    FP64, per-warp FP64 rows, ordered FP64 reduction (rms_reduce.cu).
+//
+// Mirror walls: the reference mirrors the origin image at the end of a step
+// for each wall the step touched (main.cu:302-310).  A step shorter than a
+// voxel touches a wall at most once per axis and nothing else moves the
+// origin during the step, so the mirror is applied at the wall event itself.
 //
 // Random streams (philox.cuh): per walker, direction uniforms of steps 2k and
 // 2k+1 come from one Philox4x32-10 block indexed by k, so all lanes of a warp
@@ -40,10 +52,6 @@ constexpr SplitVariant kVariants[] = {
     {256, 1}, {256, 2}, {256, 3}, {256, 4}, {128, 4}, {128, 6}, {128, 8}, {512, 1}, {512, 2}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-__device__ __forceinline__ unsigned lin3(int i, int j, int k, int n2, int n3) {
-    return ((unsigned)i * (unsigned)n2 + (unsigned)j) * (unsigned)n3 + (unsigned)k;
-}
-
 template <int BITS>
 __device__ __forceinline__ int label_at(const uint8_t* __restrict__ lat, unsigned lin) {
     if (BITS == 2) {
@@ -54,12 +62,7 @@ __device__ __forceinline__ int label_at(const uint8_t* __restrict__ lat, unsigne
     }
 }
 
-// Distance along the ray to the face the walker moves towards, on one axis
-// (clamped at 0 for an offset a rounding step outside [0, 1]).
-__device__ __forceinline__ float face_dist(float f, float v, float inv_abs_v) {
-    const float d = (v > 0.0f) ? (1.0f - f) : f;
-    return (v == 0.0f) ? INFINITY : fmaxf(d, 0.0f) * inv_abs_v;
-}
+template <int BITS> __host__ __device__ constexpr int wall_code() { return BITS == 2 ? 3 : 255; }
 
 // Origin image after a mirror wall: x -> -x (lo) or x -> 2N - x (hi), on the
 // split form x = I + F, F in [0, 1).
@@ -87,6 +90,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         }
     }
     __syncthreads();
+    // A face into the same compartment is always crossed -- unless a caller's
+    // table says otherwise, or lets walkers into the null compartment 0.
+    bool same_certain = true;
+    for (int c = 1; c < a.nc; ++c)
+        same_certain = same_certain && (s_pij[c * NCMAX + c] > 0.999999f) && (s_pij[c * NCMAX] < 0.000001f);
 
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -97,9 +105,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     const bool pgse = (a.mode == 1);
     const bool mirror = (a.boundary == 0);
     const int n1 = a.n1, n2 = a.n2, n3 = a.n3;
-    const unsigned stride0 = (unsigned)n2 * (unsigned)n3, stride1 = (unsigned)n3;
+    // padded lattice strides
+    const int s1 = n3 + 2, s0 = (n2 + 2) * (n3 + 2);
     const float res = (float)a.res;
     const uint32_t key0 = (uint32_t)a.seed, key1 = (uint32_t)(a.seed >> 32);
+    constexpr int kWall = wall_code<BITS>();
     double* slot = a.slots + (size_t)warp_global * a.timepoints * a.nvals;
     double* sig_slot = pgse ? a.sig_slots + (size_t)warp_global * a.ngrad_pad : nullptr;
 
@@ -109,8 +119,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         const uint32_t wlo = (uint32_t)w, whi = (uint32_t)((uint64_t)w >> 32);
 
         // initial position: uniform in the labelled voxels (rejection sampling)
-        int g0 = 0, g1 = 0, g2 = 0;
         float f0 = 0.5f, f1 = 0.5f, f2 = 0.5f;
+        unsigned lin = 0;
         if (active) {
             DomainStream init;
             init.init(a.seed, (uint64_t)w, kDomInit);
@@ -119,18 +129,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 const float x0 = init.next() * (float)n1;
                 const float x1 = init.next() * (float)n2;
                 const float x2 = init.next() * (float)n3;
-                g0 = min((int)x0, n1 - 1); g1 = min((int)x1, n2 - 1); g2 = min((int)x2, n3 - 1);
+                const int g0 = min((int)x0, n1 - 1), g1 = min((int)x1, n2 - 1), g2 = min((int)x2, n3 - 1);
                 f0 = x0 - (float)g0; f1 = x1 - (float)g1; f2 = x2 - (float)g2;
-                if (label_at<BITS>(lat, lin3(g0, g1, g2, n2, n3)) != 0) break;
+                lin = (unsigned)(g0 + 1) * (unsigned)s0 + (unsigned)(g1 + 1) * (unsigned)s1 + (unsigned)(g2 + 1);
+                if (label_at<BITS>(lat, lin) != 0) break;
                 if (++tries >= kInitTryCap) { atomicOr(a.err, kErrInitCap); active = false; break; }
             }
         }
-        unsigned lin = lin3(g0, g1, g2, n2, n3);
         int ai = active ? label_at<BITS>(lat, lin) : 0;
         float cur_step = s_step[ai], cur_k = s_k[ai];
-        // origin image (I + F per axis); displacement = (g - I) + (f - F)
-        int I0 = g0, I1 = g1, I2 = g2;
-        float F0 = f0, F1 = f1, F2 = f2;
+        // displacement = D + (offset - Fm) per axis; offset = up ? 1 - d : d
+        int D0 = 0, D1 = 0, D2 = 0;
+        float Fm0 = f0, Fm1 = f1, Fm2 = f2;    // origin fractions (mirrored at walls)
+        float d0 = f0, d1 = f1, d2 = f2;       // as if travelling down
+        unsigned up = 0u;                      // bit a: travelling up along axis a
         DomainStream perm;
         perm.init(a.seed, (uint64_t)w, kDomPerm);
 
@@ -162,52 +174,69 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 // azimuth 2 pi (u2 - 1/2): uniform on [-pi, pi), within the
                 // hardware sine/cosine's accurate range
                 __sincosf(6.283185307179586f * (u2 - 0.5f), &sp, &cp);
-                float v0 = sz * cp, v1 = sz * sp, v2 = cz;
-                const float iv0 = __fdividef(1.0f, fabsf(v0));
-                const float iv1 = __fdividef(1.0f, fabsf(v1));
-                const float iv2 = __fdividef(1.0f, fabsf(v2));
+                const float v0 = sz * cp, v1 = sz * sp, v2 = cz;
+                const unsigned nu = (v0 > 0.0f ? 1u : 0u) | (v1 > 0.0f ? 2u : 0u) | (v2 > 0.0f ? 4u : 0u);
+                const unsigned turn = nu ^ up;
+                if (turn & 1u) d0 = 1.0f - d0;
+                if (turn & 2u) d1 = 1.0f - d1;
+                if (turn & 4u) d2 = 1.0f - d2;
+                up = nu;
+                const float av0 = fabsf(v0), av1 = fabsf(v1), av2 = fabsf(v2);
+                const float iv0 = __fdividef(1.0f, av0), iv1 = __fdividef(1.0f, av1), iv2 = __fdividef(1.0f, av2);
+                // signed lattice step along each axis in the direction of travel
+                int dl0 = (up & 1u) ? s0 : -s0;
+                int dl1 = (up & 2u) ? s1 : -s1;
+                int dl2 = (up & 4u) ? 1 : -1;
                 float rem = cur_step;        // path left in this step, voxels
-                unsigned flo = 0u, fhi = 0u;
                 for (int j = 0; j < a.nite; ++j) {
-                    const float t0 = face_dist(f0, v0, iv0);
-                    const float t1 = face_dist(f1, v1, iv1);
-                    const float t2 = face_dist(f2, v2, iv2);
-                    const float tmin = fminf(t0, fminf(t1, t2));
-                    if (rem < tmin) {
+                    const float t0 = d0 * iv0, t1 = d1 * iv1, t2 = d2 * iv2;
+                    const float tm = fminf(t0, fminf(t1, t2));
+                    if (rem < tm) {
                         // the step ends inside the voxel
-                        f0 = fmaf(rem, v0, f0); f1 = fmaf(rem, v1, f1); f2 = fmaf(rem, v2, f2);
+                        d0 = fmaf(-rem, av0, d0); d1 = fmaf(-rem, av1, d1); d2 = fmaf(-rem, av2, d2);
                         w32 = fmaf(rem, cur_k, w32);
                         rem = 0.0f;
                         break;
                     }
                     // onto the nearest face (lowest axis on ties, like the reference's scan)
-                    const int hit = (t0 == tmin) ? 0 : ((t1 == tmin) ? 1 : 2);
-                    f0 = fmaf(tmin, v0, f0); f1 = fmaf(tmin, v1, f1); f2 = fmaf(tmin, v2, f2);
-                    w32 = fmaf(tmin, cur_k, w32);
-                    rem -= tmin;
-                    const float vh = hit == 0 ? v0 : (hit == 1 ? v1 : v2);
-                    const bool up = vh > 0.0f;
-                    const float on_face = up ? 1.0f : 0.0f;
-                    if (hit == 0) f0 = on_face; else if (hit == 1) f1 = on_face; else f2 = on_face;
-                    const int gh = hit == 0 ? g0 : (hit == 1 ? g1 : g2);
-                    const int nh = hit == 0 ? n1 : (hit == 1 ? n2 : n3);
-                    const unsigned st_h = hit == 0 ? stride0 : (hit == 1 ? stride1 : 1u);
-                    int gj = up ? gh + 1 : gh - 1;
-                    unsigned lj = up ? lin + st_h : lin - st_h;
-                    const bool wall = (unsigned)gj >= (unsigned)nh;
-                    if (wall) {
-                        if (mirror) {
-                            if (up) fhi |= 1u << hit; else flo |= 1u << hit;
-                            if (hit == 0) v0 = -v0; else if (hit == 1) v1 = -v1; else v2 = -v2;
-                            if (!(rem > 0.0f)) break;
-                            continue;
+                    const int hit = (t0 == tm) ? 0 : ((t1 == tm) ? 1 : 2);
+                    const float tc = fmaxf(tm, 0.0f);
+                    d0 = fmaf(-tc, av0, d0); d1 = fmaf(-tc, av1, d1); d2 = fmaf(-tc, av2, d2);
+                    w32 = fmaf(tc, cur_k, w32);
+                    rem -= tc;
+                    const int dl = hit == 0 ? dl0 : (hit == 1 ? dl1 : dl2);
+                    unsigned lj = lin + (unsigned)dl;
+                    int aj = label_at<BITS>(lat, lj);
+                    bool cross;
+                    if (aj == ai && same_certain) {
+                        cross = true;
+                    } else {
+                        if (aj == kWall) {
+                            const bool hi = (up >> hit) & 1u;
+                            const int nh = hit == 0 ? n1 : (hit == 1 ? n2 : n3);
+                            if (mirror) {
+                                // mirror wall: reflect, and mirror the origin image
+                                const int g = hi ? nh - 1 : 0;
+                                if (hit == 0) { int I = g - D0; mirror_origin(I, Fm0, hi, nh); D0 = g - I; }
+                                else if (hit == 1) { int I = g - D1; mirror_origin(I, Fm1, hi, nh); D1 = g - I; }
+                                else { int I = g - D2; mirror_origin(I, Fm2, hi, nh); D2 = g - I; }
+                                aj = -1;   // reflect below
+                            } else {
+                                // periodic: the neighbour is on the far side; the
+                                // unfolded displacement just continues
+                                const int sh = hit == 0 ? s0 : (hit == 1 ? s1 : 1);
+                                lj = hi ? lin - (unsigned)(nh - 1) * (unsigned)sh
+                                        : lin + (unsigned)(nh - 1) * (unsigned)sh;
+                                aj = label_at<BITS>(lat, lj);
+                            }
                         }
-                        gj = up ? 0 : nh - 1;   // periodic neighbour
-                        lj = up ? lin - (unsigned)(nh - 1) * st_h : lin + (unsigned)(nh - 1) * st_h;
+                        if (aj < 0) {
+                            cross = false;
+                        } else {
+                            const float P = s_pij[ai * NCMAX + aj];
+                            cross = (P > 0.999999f) || (P >= 0.000001f && perm.next() < P);
+                        }
                     }
-                    const int aj = label_at<BITS>(lat, lj);
-                    const float P = s_pij[ai * NCMAX + aj];
-                    const bool cross = (P > 0.999999f) || (P >= 0.000001f && perm.next() < P);
                     if (cross) {
                         if (aj != ai) {
                             rem *= s_ratio[ai * NCMAX + aj];
@@ -216,36 +245,27 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                             ai = aj;
                         }
                         lin = lj;
-                        const float fin = up ? 0.0f : 1.0f;
-                        if (hit == 0) { g0 = gj; f0 = fin; }
-                        else if (hit == 1) { g1 = gj; f1 = fin; }
-                        else { g2 = gj; f2 = fin; }
-                        if (wall) {
-                            // periodic: shift the origin with the walker
-                            const int sh = up ? -nh : nh;
-                            if (hit == 0) I0 += sh; else if (hit == 1) I1 += sh; else I2 += sh;
-                        }
+                        const int du = ((up >> hit) & 1u) ? 1 : -1;
+                        if (hit == 0) D0 += du; else if (hit == 1) D1 += du; else D2 += du;
                     } else {
-                        if (hit == 0) v0 = -v0; else if (hit == 1) v1 = -v1; else v2 = -v2;
+                        up ^= 1u << hit;
+                        if (hit == 0) dl0 = -dl0; else if (hit == 1) dl1 = -dl1; else dl2 = -dl2;
                     }
+                    // on the face, a whole voxel ahead
+                    if (hit == 0) d0 = 1.0f; else if (hit == 1) d1 = 1.0f; else d2 = 1.0f;
                     if (!(rem > 0.0f)) break;
                 }
-                // mirror the origin for each wall hit this step (main.cu:302-310)
-                if (flo | fhi) {
-                    if (flo & 1u) mirror_origin(I0, F0, false, n1);
-                    if (fhi & 1u) mirror_origin(I0, F0, true, n1);
-                    if (flo & 2u) mirror_origin(I1, F1, false, n2);
-                    if (fhi & 2u) mirror_origin(I1, F1, true, n2);
-                    if (flo & 4u) mirror_origin(I2, F2, false, n3);
-                    if (fhi & 4u) mirror_origin(I2, F2, true, n3);
-                }
             }
+            // in-voxel offsets of the current position
+            const float o0 = (up & 1u) ? 1.0f - d0 : d0;
+            const float o1 = (up & 2u) ? 1.0f - d1 : d1;
+            const float o2 = (up & 4u) ? 1.0f - d2 : d2;
 
             if (pgse) {
                 // displacement sums (voxels) over the lobes
-                p0 += (float)(g0 - I0) + (f0 - F0);
-                p1 += (float)(g1 - I1) + (f1 - F1);
-                p2 += (float)(g2 - I2) + (f2 - F2);
+                p0 += (float)D0 + (o0 - Fm0);
+                p1 += (float)D1 + (o1 - Fm1);
+                p2 += (float)D2 + (o2 - Fm2);
                 const bool event = (i + 1 == next_ev);
                 if (event || (i & 31) == 31) {
                     P0 += (double)p0; P1 += (double)p1; P2 += (double)p2;
@@ -289,9 +309,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     w64 += (double)w32;
                     w32 = 0.0f;
                     const float s0 = active ? (float)exp(-w64) : 0.0f;
-                    const float dx = ((float)(g0 - I0) + (f0 - F0)) * res;
-                    const float dy = ((float)(g1 - I1) + (f1 - F1)) * res;
-                    const float dz = ((float)(g2 - I2) + (f2 - F2)) * res;
+                    const float dx = ((float)D0 + (o0 - Fm0)) * res;
+                    const float dy = ((float)D1 + (o1 - Fm1)) * res;
+                    const float dz = ((float)D2 + (o2 - Fm2)) * res;
                     const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
                     const float sxx = s0 * xx, syy = s0 * yy, szz = s0 * zz;
                     double* row = slot + (size_t)tidx * a.nvals;
@@ -338,14 +358,26 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     }
 }
 
-__global__ void pack2_kernel(const uint8_t* __restrict__ labels, size_t n, uint8_t* __restrict__ out) {
-    const size_t nb = (n + 3) / 4;
-    for (size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (size_t)gridDim.x * blockDim.x) {
+// Padded lattice: (n1+2) x (n2+2) x (n3+2), interior = the labels, border =
+// the wall code.  BITS = 2: voxel v in bits 2(v % 4) of byte v / 4.
+template <int BITS>
+__global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int n2, int n3,
+                                uint8_t* __restrict__ out, size_t nbytes) {
+    const size_t P3 = (size_t)n3 + 2, P2 = (size_t)n2 + 2;
+    const size_t nvox = ((size_t)n1 + 2) * P2 * P3;
+    constexpr int per = BITS == 2 ? 4 : 1;
+    for (size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x; b < nbytes; b += (size_t)gridDim.x * blockDim.x) {
         unsigned v = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const size_t i = 4 * b + k;
-            if (i < n) v |= (unsigned)(labels[i] & 3u) << (2 * k);
+        for (int k = 0; k < per; ++k) {
+            const size_t p = b * per + k;
+            const size_t pk = p % P3, pj = (p / P3) % P2, pi = p / (P3 * P2);
+            unsigned lab;
+            if (p >= nvox || pi == 0 || pi > (size_t)n1 || pj == 0 || pj > (size_t)n2 || pk == 0 || pk > (size_t)n3)
+                lab = (unsigned)wall_code<BITS>();
+            else
+                lab = labels[((pi - 1) * (size_t)n2 + (pj - 1)) * (size_t)n3 + (pk - 1)];
+            v |= (BITS == 2 ? (lab & 3u) : lab) << (BITS * k);
         }
         out[b] = (uint8_t)v;
     }
@@ -366,7 +398,7 @@ const void* kernel_ptr(int nc, int bits) {
 
 template <int BLOCK, int MINB>
 int launch_v(const WalkArgs& a, const uint8_t* lat, int bits, int grid, void* stream) {
-    if (bits == 2) return a.nc <= 4 ? launch_t<4, 2, BLOCK, MINB>(a, lat, grid, stream) : (int)cudaErrorInvalidValue;
+    if (bits == 2) return a.nc <= 3 ? launch_t<4, 2, BLOCK, MINB>(a, lat, grid, stream) : (int)cudaErrorInvalidValue;
     return a.nc <= 4 ? launch_t<4, 8, BLOCK, MINB>(a, lat, grid, stream)
                      : launch_t<8, 8, BLOCK, MINB>(a, lat, grid, stream);
 }
@@ -389,11 +421,19 @@ auto by_variant(int v, F&& f) {
 
 }  // namespace
 
-int pack_labels_2bit(const uint8_t* labels, size_t n, uint8_t* out, void* stream) {
-    const size_t nb = (n + 3) / 4;
-    size_t grid = (nb + 255) / 256;
-    if (grid > 8192) grid = 8192;
-    pack2_kernel<<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n, out);
+int split_lattice_bits(int nc) { return nc <= 3 ? 2 : 8; }
+
+size_t padded_lattice_bytes(int n1, int n2, int n3, int bits) {
+    const size_t nv = ((size_t)n1 + 2) * ((size_t)n2 + 2) * ((size_t)n3 + 2);
+    return bits == 2 ? (nv + 3) / 4 : nv;
+}
+
+int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits, uint8_t* out, void* stream) {
+    const size_t nbytes = padded_lattice_bytes(n1, n2, n3, bits);
+    size_t grid = (nbytes + 255) / 256;
+    if (grid > 16384) grid = 16384;
+    if (bits == 2) pad_pack_kernel<2><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
+    else pad_pack_kernel<8><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
     return (int)cudaGetLastError();
 }
 
