@@ -200,7 +200,7 @@ int rms_split_variant(int k, int* block, int* min_blocks_per_sm);
  * must not hit cudaMalloc/cudaFree because they synchronise the whole device.
  * Runs the SPLIT walk of `sim` (its configuration and tables; the sim itself is
  * not changed) on device buffers the caller owns:
- *   d_labels  [n1*n2*n3] uint8 lattice, n3 fastest, labels < nc (nc <= 3)
+ *   d_labels  [n1*n2*n3] uint8 lattice, n3 fastest, labels < nc (nc <= 7)
  *   d_rows    [timepoints * W] doubles, W = 32 (PGSE) or 32 + 32*ceil(nbvec/32)
  *             (narrow); row t holds sig0 at column 0, dx2 at 1-6, dx4 at 7-21,
  *             compartment counts at 22.., sigRe at 32..
@@ -213,7 +213,7 @@ int rms_split_variant(int k, int* block, int* min_blocks_per_sm);
  * each device looks up the array's device address: make it before any stream
  * capture.  Calls share the array, so calls that overlap on the GPU race:
  * serialise them.  No memory is allocated, host or device. */
-#define RMS_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+#define RMS_NOALLOC_SCRATCH_BYTES ((size_t)128 << 20)
 int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint8_t* d_labels,
                         double* d_rows, double* d_sig);
 

@@ -22,7 +22,7 @@ namespace {
 thread_local std::string g_last_error;
 
 constexpr int kCompatBlock = 128;
-constexpr int kSplitVariantDefault = 3;   // 256 threads, >= 4 blocks per SM (64 registers): fastest measured
+constexpr int kSplitVariantDefault = 0;   // 256 threads, >= 4 blocks per SM (64 registers): fastest measured
 constexpr int kMaxGrad = 1 << 16;
 
 // One device allocation that only grows.

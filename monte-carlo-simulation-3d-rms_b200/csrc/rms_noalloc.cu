@@ -17,8 +17,10 @@
 // (rms_walk_split.cu, rms_reduce.cu), launched on that scratch.  The grid is
 // sized so the per-warp rows fit in the scratch; a job whose fixed tables or
 // single block of rows do not fit is refused with RMS_ERR_RANGE.  The walk
-// reads a padded, packed copy of the caller's lattice (2 bits per voxel for
-// Nc <= 3), which is built in the scratch too: 34 MB for 256x256x2048.
+// reads the same padded, packed lattice as rms_sim_run (4 bits per voxel with
+// the free-flight flags, Nc <= 7), built in the scratch too: 68 MB for
+// 256x256x2048.  Same lattice, same kernel, same walkers: the results equal
+// rms_sim_run's up to the order of the final sums.
 //
 // Host code cannot use the array's name as a device address (in host code it
 // names a host-side stand-in).  The first call on each device, with that
@@ -42,7 +44,7 @@ namespace {
 
 constexpr size_t kScratchBytes = RMS_NOALLOC_SCRATCH_BYTES;
 constexpr int kMaxDevices = 64;
-constexpr int kVariant = 3;   // 256 threads, >= 4 resident blocks per SM
+constexpr int kVariant = 0;   // 256 threads, >= 4 resident blocks per SM
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -93,7 +95,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
                                    double* d_rows, double* d_sig) {
     if (!s || !o || !d_labels || !d_rows) return set_error(RMS_ERR_ARG, "null argument");
     if (s->mode == RMS_MODE_PGSE && !d_sig) return set_error(RMS_ERR_ARG, "PGSE needs the sig buffer");
-    if (s->nc > 3) return set_error(RMS_ERR_RANGE, "the no-allocation walk supports Nc <= 3");
+    if (s->nc > 7) return set_error(RMS_ERR_RANGE, "the no-allocation walk supports Nc <= 7");
     cudaError_t e = cudaSetDevice(o->device);
     if (e != cudaSuccess) return set_error(RMS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     unsigned char* base = nullptr;
@@ -113,7 +115,8 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     const int warps_per_block = block / 32;
 
     // fixed part of the scratch
-    const size_t lat_bytes = padded_lattice_bytes(s->n1, s->n2, s->n3, 2);
+    const int bits = split_lattice_bits(nc);
+    const size_t lat_bytes = padded_lattice_bytes(s->n1, s->n2, s->n3, bits);
     const size_t fixed = align256(lat_bytes) + align256(sizeof(int)) + align256(sizeof(double) * (2 * nc + nc * nc)) +
                          align256(sizeof(float) * (2 * nc + nc * nc)) + align256(sizeof(double) * s->qtab.size()) +
                          align256(sizeof(double) * s->bvec.size()) + align256(sizeof(double) * s->grad.size()) +
@@ -133,7 +136,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     int dev_sms = 0;
     e = cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, o->device);
     if (e != cudaSuccess) return set_error(RMS_ERR_CUDA, cudaGetErrorString(e));
-    const int per_sm = walk_split_blocks_per_sm(nc, 2, kVariant);
+    const int per_sm = walk_split_blocks_per_sm(nc, bits, kVariant);
     if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed");
     const int64_t ntiles = (w1 - w0 + 31) / 32;
     int64_t grid64 = std::min<int64_t>((int64_t)dev_sms * per_sm, (ntiles + warps_per_block - 1) / warps_per_block);
@@ -188,7 +191,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
          (e = cudaMemsetAsync(d_sigslots, 0, (size_t)nslots * ngrad_pad * sizeof(double), st)) != cudaSuccess))
         return set_error(RMS_ERR_CUDA, std::string("scratch clear: ") + cudaGetErrorString(e));
 
-    int pe = pack_lattice_padded(d_labels, s->n1, s->n2, s->n3, 2, d_lat, st);
+    int pe = pack_lattice_padded(d_labels, s->n1, s->n2, s->n3, bits, d_lat, st);
     if (pe) return set_error(RMS_ERR_CUDA, std::string("lattice packing: ") + cudaGetErrorString((cudaError_t)pe));
 
     WalkArgs a{};
@@ -211,7 +214,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     a.sig_slots = d_sigslots;
     a.err = d_err;
 
-    int ke = launch_walk_split(a, d_lat, 2, kVariant, grid, st);
+    int ke = launch_walk_split(a, d_lat, bits, kVariant, grid, st);
     if (ke) return set_error(RMS_ERR_CUDA, std::string("walk launch: ") + cudaGetErrorString((cudaError_t)ke));
     ke = launch_reduce_slots(d_slots, nslots, row, d_rows, st);
     if (!ke && s->mode == RMS_MODE_PGSE) ke = launch_reduce_slots(d_sigslots, nslots, (size_t)ngrad_pad, d_sig, st);

@@ -15,9 +15,16 @@
 //    border that holds a wall code: a face step is `lin += stride`, and
 //    reaching a wall is a label like any other (rare branch); the integer
 //    part of the displacement, D = voxel - origin image, is carried per axis;
-//  - labels packed 2 bits per voxel when Nc <= 3 (wall = 3; a padded
-//    256x256x2048 lattice is 34 MB and stays in the 126 MB L2), else one byte
-//    per voxel (wall = 255);
+//  - free flight: a voxel whose 26 neighbours all carry its label (and none
+//    is a wall) has a flag bit in the lattice; a step that starts there is
+//    shorter than a voxel, so it cannot meet a membrane or a wall and moves in
+//    one straight line -- a floor per axis instead of the face loop.  It is
+//    the face loop's own outcome (every face on the way is a same-label face,
+//    always crossed) with at most three crossings, within the nite = 4 cap;
+//  - labels packed 4 bits per voxel (3-bit label, wall = 7, plus the flag;
+//    a padded 256x256x2048 lattice is 68 MB and stays in the 126 MB L2), one
+//    byte for Nc = 8, or 2 bits without flags (wall = 3) for the
+//    no-allocation walk;
 //  - FP32 uniforms, one Philox4x32-10 block per two steps; hardware
 //    sine/cosine and reciprocal for the direction and face times;
 //  - per-walker sums that grow over the walk (T2 exponent, PGSE displacement
@@ -48,21 +55,28 @@ namespace {
 // number caps registers per thread at 65536 / (block * minb), trading spills
 // in the rare record path for more resident warps to hide gather latency.
 struct SplitVariant { int block, minb; };
-constexpr SplitVariant kVariants[] = {
-    {256, 1}, {256, 2}, {256, 3}, {256, 4}, {128, 4}, {128, 6}, {128, 8}, {512, 1}, {512, 2}};
+constexpr SplitVariant kVariants[] = {{256, 4}, {256, 3}, {256, 2}, {128, 8}, {512, 2}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+// Lattice cell: label in the low bits, free-flight flag in the top bit
+// (BITS = 4: 3 + 1 bits, two voxels per byte, voxel v in bits 4(v % 2);
+// BITS = 8: 7 + 1; BITS = 2: label only, voxel v in bits 2(v % 4)).
+template <int BITS>
+__device__ __forceinline__ unsigned cell_at(const uint8_t* __restrict__ lat, unsigned lin) {
+    if (BITS == 2) return (__ldg(lat + (lin >> 2)) >> ((lin & 3u) * 2u)) & 3u;
+    if (BITS == 4) return (__ldg(lat + (lin >> 1)) >> ((lin & 1u) * 4u)) & 15u;
+    return __ldg(lat + lin);
+}
+
+template <int BITS> __host__ __device__ constexpr unsigned label_mask() { return BITS == 2 ? 3u : (BITS == 4 ? 7u : 127u); }
+template <int BITS> __host__ __device__ constexpr unsigned flight_bit() { return BITS == 2 ? 0u : (BITS == 4 ? 8u : 128u); }
 
 template <int BITS>
 __device__ __forceinline__ int label_at(const uint8_t* __restrict__ lat, unsigned lin) {
-    if (BITS == 2) {
-        const unsigned byte = __ldg(lat + (lin >> 2));
-        return (int)((byte >> ((lin & 3u) * 2u)) & 3u);
-    } else {
-        return (int)__ldg(lat + lin);
-    }
+    return (int)(cell_at<BITS>(lat, lin) & label_mask<BITS>());
 }
 
-template <int BITS> __host__ __device__ constexpr int wall_code() { return BITS == 2 ? 3 : 255; }
+template <int BITS> __host__ __device__ constexpr int wall_code() { return (int)label_mask<BITS>(); }
 
 // Origin image after a mirror wall: x -> -x (lo) or x -> 2N - x (hi), on the
 // split form x = I + F, F in [0, 1).
@@ -95,6 +109,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     bool same_certain = true;
     for (int c = 1; c < a.nc; ++c)
         same_certain = same_certain && (s_pij[c * NCMAX + c] > 0.999999f) && (s_pij[c * NCMAX] < 0.000001f);
+    // free flight needs same-label faces always crossed and room for three
+    // crossings within the sub-segment cap
+    const bool flight = (BITS != 2) && same_certain && (a.nite >= 4);
 
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -176,6 +193,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 __sincosf(6.283185307179586f * (u2 - 0.5f), &sp, &cp);
                 const float v0 = sz * cp, v1 = sz * sp, v2 = cz;
                 const unsigned nu = (v0 > 0.0f ? 1u : 0u) | (v1 > 0.0f ? 2u : 0u) | (v2 > 0.0f ? 4u : 0u);
+                if (flight && (cell_at<BITS>(lat, lin) & flight_bit<BITS>())) {
+                    // free flight: straight line, at most one voxel per axis
+                    const float x0 = fmaf(cur_step, v0, (up & 1u) ? 1.0f - d0 : d0);
+                    const float x1 = fmaf(cur_step, v1, (up & 2u) ? 1.0f - d1 : d1);
+                    const float x2 = fmaf(cur_step, v2, (up & 4u) ? 1.0f - d2 : d2);
+                    const float k0 = floorf(x0), k1 = floorf(x1), k2 = floorf(x2);
+                    const int ik0 = (int)k0, ik1 = (int)k1, ik2 = (int)k2;
+                    const float o0n = x0 - k0, o1n = x1 - k1, o2n = x2 - k2;
+                    lin += (unsigned)(ik0 * s0 + ik1 * s1 + ik2);
+                    D0 += ik0; D1 += ik1; D2 += ik2;
+                    w32 = fmaf(cur_step, cur_k, w32);
+                    d0 = (nu & 1u) ? 1.0f - o0n : o0n;
+                    d1 = (nu & 2u) ? 1.0f - o1n : o1n;
+                    d2 = (nu & 4u) ? 1.0f - o2n : o2n;
+                    up = nu;
+                } else {
                 const unsigned turn = nu ^ up;
                 if (turn & 1u) d0 = 1.0f - d0;
                 if (turn & 2u) d1 = 1.0f - d1;
@@ -254,6 +287,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     // on the face, a whole voxel ahead
                     if (hit == 0) d0 = 1.0f; else if (hit == 1) d1 = 1.0f; else d2 = 1.0f;
                     if (!(rem > 0.0f)) break;
+                }
                 }
             }
             // in-voxel offsets of the current position
@@ -359,25 +393,40 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
 }
 
 // Padded lattice: (n1+2) x (n2+2) x (n3+2), interior = the labels, border =
-// the wall code.  BITS = 2: voxel v in bits 2(v % 4) of byte v / 4.
+// the wall code.  With BITS = 4 or 8 an interior voxel also gets the
+// free-flight flag when its 26 neighbours are interior and share its label.
 template <int BITS>
 __global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int n2, int n3,
                                 uint8_t* __restrict__ out, size_t nbytes) {
     const size_t P3 = (size_t)n3 + 2, P2 = (size_t)n2 + 2;
     const size_t nvox = ((size_t)n1 + 2) * P2 * P3;
-    constexpr int per = BITS == 2 ? 4 : 1;
+    constexpr int per = 8 / BITS;
     for (size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x; b < nbytes; b += (size_t)gridDim.x * blockDim.x) {
         unsigned v = 0;
 #pragma unroll
         for (int k = 0; k < per; ++k) {
             const size_t p = b * per + k;
             const size_t pk = p % P3, pj = (p / P3) % P2, pi = p / (P3 * P2);
-            unsigned lab;
-            if (p >= nvox || pi == 0 || pi > (size_t)n1 || pj == 0 || pj > (size_t)n2 || pk == 0 || pk > (size_t)n3)
-                lab = (unsigned)wall_code<BITS>();
-            else
-                lab = labels[((pi - 1) * (size_t)n2 + (pj - 1)) * (size_t)n3 + (pk - 1)];
-            v |= (BITS == 2 ? (lab & 3u) : lab) << (BITS * k);
+            unsigned cell;
+            if (p >= nvox || pi == 0 || pi > (size_t)n1 || pj == 0 || pj > (size_t)n2 || pk == 0 || pk > (size_t)n3) {
+                cell = (unsigned)wall_code<BITS>();
+            } else {
+                const long i = (long)pi - 1, j = (long)pj - 1, kk = (long)pk - 1;
+                const unsigned lab = labels[((size_t)i * n2 + j) * (size_t)n3 + kk];
+                cell = lab & label_mask<BITS>();
+                if (BITS != 2 && i >= 1 && i + 1 < n1 && j >= 1 && j + 1 < n2 && kk >= 1 && kk + 1 < n3) {
+                    bool same = true;
+                    for (int di = -1; di <= 1 && same; ++di)
+                        for (int dj = -1; dj <= 1 && same; ++dj)
+                            for (int dk = -1; dk <= 1; ++dk)
+                                if (labels[((size_t)(i + di) * n2 + (j + dj)) * (size_t)n3 + (kk + dk)] != lab) {
+                                    same = false;
+                                    break;
+                                }
+                    if (same) cell |= flight_bit<BITS>();
+                }
+            }
+            v |= cell << (BITS * k);
         }
         out[b] = (uint8_t)v;
     }
@@ -392,40 +441,36 @@ int launch_t(const WalkArgs& a, const uint8_t* lat, int grid, void* stream) {
 template <int BLOCK, int MINB>
 const void* kernel_ptr(int nc, int bits) {
     if (bits == 2) return (const void*)walk_split_kernel<4, 2, BLOCK, MINB>;
-    if (nc <= 4) return (const void*)walk_split_kernel<4, 8, BLOCK, MINB>;
+    if (bits == 4) return (const void*)walk_split_kernel<8, 4, BLOCK, MINB>;
     return (const void*)walk_split_kernel<8, 8, BLOCK, MINB>;
 }
 
 template <int BLOCK, int MINB>
 int launch_v(const WalkArgs& a, const uint8_t* lat, int bits, int grid, void* stream) {
     if (bits == 2) return a.nc <= 3 ? launch_t<4, 2, BLOCK, MINB>(a, lat, grid, stream) : (int)cudaErrorInvalidValue;
-    return a.nc <= 4 ? launch_t<4, 8, BLOCK, MINB>(a, lat, grid, stream)
-                     : launch_t<8, 8, BLOCK, MINB>(a, lat, grid, stream);
+    if (bits == 4) return a.nc <= 7 ? launch_t<8, 4, BLOCK, MINB>(a, lat, grid, stream) : (int)cudaErrorInvalidValue;
+    return launch_t<8, 8, BLOCK, MINB>(a, lat, grid, stream);
 }
 
 // Dispatch over the variant table (index v, 0-based).
 template <class F>
 auto by_variant(int v, F&& f) {
     switch (v) {
-        case 0: return f.template operator()<256, 1>();
-        case 1: return f.template operator()<256, 2>();
-        case 2: return f.template operator()<256, 3>();
-        case 3: return f.template operator()<256, 4>();
-        case 4: return f.template operator()<128, 4>();
-        case 5: return f.template operator()<128, 6>();
-        case 6: return f.template operator()<128, 8>();
-        case 7: return f.template operator()<512, 1>();
+        case 0: return f.template operator()<256, 4>();
+        case 1: return f.template operator()<256, 3>();
+        case 2: return f.template operator()<256, 2>();
+        case 3: return f.template operator()<128, 8>();
         default: return f.template operator()<512, 2>();
     }
 }
 
 }  // namespace
 
-int split_lattice_bits(int nc) { return nc <= 3 ? 2 : 8; }
+int split_lattice_bits(int nc) { return nc <= 7 ? 4 : 8; }
 
 size_t padded_lattice_bytes(int n1, int n2, int n3, int bits) {
     const size_t nv = ((size_t)n1 + 2) * ((size_t)n2 + 2) * ((size_t)n3 + 2);
-    return bits == 2 ? (nv + 3) / 4 : nv;
+    return (nv * (size_t)bits + 7) / 8;
 }
 
 int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits, uint8_t* out, void* stream) {
@@ -433,6 +478,7 @@ int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits,
     size_t grid = (nbytes + 255) / 256;
     if (grid > 16384) grid = 16384;
     if (bits == 2) pad_pack_kernel<2><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
+    else if (bits == 4) pad_pack_kernel<4><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
     else pad_pack_kernel<8><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
     return (int)cudaGetLastError();
 }

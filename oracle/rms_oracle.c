@@ -265,9 +265,26 @@ static void split_mirror_origin(double* xi, int hi, int n) {
     *xi = hi ? 2.0 * (double)n - *xi : -*xi;
 }
 
+/* Free flight of the split walk: the voxel's 26 neighbours all lie inside the
+ * lattice and carry its label. */
+static int homogeneous(const or_params* p, const int g[3]) {
+    if (g[0] < 1 || g[0] + 1 >= p->n1 || g[1] < 1 || g[1] + 1 >= p->n2 || g[2] < 1 || g[2] + 1 >= p->n3) return 0;
+    const uint8_t lab = p->labels[lin(p, g[0], g[1], g[2])];
+    for (int a = -1; a <= 1; a++)
+        for (int b = -1; b <= 1; b++)
+            for (int c = -1; c <= 1; c++)
+                if (p->labels[lin(p, g[0] + a, g[1] + b, g[2] + c)] != lab) return 0;
+    return 1;
+}
+
 static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, double* phase,
                            int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev, double* tr_pos) {
     const int Nc = p->nc;
+    /* free flight applies when same-label faces are always crossed, no walker
+     * can enter compartment 0, and three crossings fit the sub-segment cap */
+    int flight = p->nite >= 4;
+    for (int c = 1; c < Nc; c++)
+        if (!(p->pij[c * Nc + c] > 0.999999) || !(p->pij[c * Nc] < 0.000001)) flight = 0;
     const int Tstep = p->tn / p->timepoints;
     const int NPix[3] = {p->n1, p->n2, p->n3};
     const uint8_t* APix = p->labels;
@@ -302,7 +319,18 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
         double rem = p->step[ai];
         int flo = 0, fhi = 0, nev = 0;
         uint32_t ev = 0;
-        for (int j = 0; j < p->nite; j++) {
+        if (flight && homogeneous(p, g)) {
+            /* a straight line within the homogeneous neighbourhood */
+            for (int a = 0; a < 3; a++) {
+                const double x = f[a] + rem * v[a];
+                const double k = floor(x);
+                g[a] += (int)k;
+                f[a] = x - k;
+            }
+            wexp += rem / p->step[ai] / p->t2[ai];
+            rem = 0.0;
+        }
+        for (int j = 0; j < p->nite && rem > 0.0; j++) {
             double t[3], tmin;
             for (int a = 0; a < 3; a++) {
                 double d = (v[a] > 0.0) ? 1.0 - f[a] : f[a];

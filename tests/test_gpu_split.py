@@ -5,6 +5,12 @@ or_run_split): the same algorithm fed the same random streams, every quantity
 after the start position in FP64.  Bar (the engine's stated tolerance):
 D(t) within 0.5 % and K(t) within 2 % (absolute 0.02 where |K| < 1) of the
 replay, compartment counts conserved, signals within 2e-3 of S0.
+
+The FP32 and FP64 walks are the same walk until a face decision falls within
+the FP32 position error of a tie; such a walker then takes another branch and
+decorrelates (measured: 6 of 400 walkers within 2000 steps in the thin-axon
+lattice below, walker by walker).  The fourth moment feels those few walkers,
+so the comparison uses 16384 walkers.
 """
 import numpy as np
 import pytest
@@ -52,12 +58,13 @@ def test_split_vs_fp64_replay_permeable_narrow():
     rng = np.random.default_rng(3)
     bv = rng.normal(size=(6, 3)); bv /= np.linalg.norm(bv, axis=1, keepdims=True)
     b = np.array([0.5, 1, 1.5, 2, 2.5, 3.0])
-    sim, job = jobs(lattice3(), [0, 2.0, 1.0], [80, 80, 40], npar=4096, tn=2000, seed=17, bval=b, bvec=bv)
+    n = 16384
+    sim, job = jobs(lattice3(), [0, 2.0, 1.0], [80, 80, 40], npar=n, tn=2000, seed=17, bval=b, bvec=bv)
     got = sim.run(seed=17, precision="split").outputs()
     want = pyoracle.run_oracle(job, nthreads=8, split=True)
     check_dk(got, want, "narrow")
-    assert np.array_equal(got["npar_count"].sum(axis=1), np.full(1000, 4096.0))
-    assert np.abs(got["npar_count"] - want["npar_count"]).max() <= 0.01 * 4096
+    assert np.array_equal(got["npar_count"].sum(axis=1), np.full(1000, float(n)))
+    assert np.abs(got["npar_count"] - want["npar_count"]).max() <= 0.01 * n
     np.testing.assert_allclose(got["sig0"], want["sig0"], rtol=1e-5)
     S, Sw = got["sigre"] / got["sig0"][:, None], want["sigre"] / want["sig0"][:, None]
     assert np.abs(S - Sw).max() < 2e-3
@@ -69,7 +76,7 @@ def test_split_vs_fp64_replay_pgse_kappa_periodic():
     g = np.column_stack([rng.choice([0.1, 0.2], ng), rng.choice([0.05, 0.1], ng),
                          rng.uniform(0.5, 4, ng), rng.normal(size=(ng, 3))])
     g[:, 3:] /= np.linalg.norm(g[:, 3:], axis=1, keepdims=True)
-    sim, job = jobs(lattice3(5), [0, 2.0, 2.0], [80, 70, 50], npar=4096, tn=2000, seed=23, grad=g,
+    sim, job = jobs(lattice3(5), [0, 2.0, 2.0], [80, 70, 50], npar=16384, tn=2000, seed=23, grad=g,
                     boundary="periodic", permeation="kappa", kappa=0.05)
     got = sim.run(seed=23, precision="split").outputs()
     want = pyoracle.run_oracle(job, nthreads=8, split=True)
