@@ -1,7 +1,12 @@
 #!/usr/bin/env python
 """Walker-steps/s of the B200 random-walk engine (one JSON line on rank 0).
 
-Workload ``production`` (default): a 256 x 256 x 2048 label lattice at 0.1 um
+Workload ``batch`` (default; the batched form the metric names): 64 axons,
+lattices of log-uniform voxel counts between 64x64x256 and 256x256x2048,
+5e7 walkers per GPU in proportion to intra-axonal volume, D0 ~ U(1.5, 2.5)
+um^2/ms and kappa ~ U(0, 0.05) um/ms per axon, 20,000 steps, moments only,
+all walked by ONE persistent split-precision launch (rms_batch_run).
+Workload ``production``: a 256 x 256 x 2048 label lattice at 0.1 um
 (one undulating, caliber-varying axon, label 1, in extra-axonal space, label
 2), 1e7 walkers per GPU, 50,000 steps of dt = 2e-4 ms, D = 2 um^2/ms in both
 compartments, membrane permeability kappa = 0.01 um/ms, T2 = 80 / 60 ms, and
@@ -12,7 +17,8 @@ Workload ``single``: the 64 x 64 x 512 single-axon lattice (labels 0/1),
 10 steps.  Inputs are synthetic and seeded.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision split|compat] [--workload production|single]
+                  [--precision split|compat] [--workload batch|production|single]
+                  [--plain-ratio]
 
 ``value``: walker-steps/s of the whole job, lattice already resident on the
 GPU, timed with CUDA events on the launching stream (max over ranks).
@@ -57,6 +63,18 @@ def fib_directions(n: int) -> np.ndarray:
 
 def workload(name: str, world: int, walkers: int | None = None, tn: int | None = None):
     lab, sim_kw, per_gpu, cfg = _workload(name, world)
+    if isinstance(sim_kw, list):
+        if walkers:
+            scale = walkers / per_gpu
+            sim_kw = [dict(kw, npar=max(32, int(kw["npar"] * scale))) for kw in sim_kw]
+            per_gpu = sum(kw["npar"] for kw in sim_kw)
+            cfg["walkers_per_gpu"] = per_gpu
+            cfg["workload"] += f" [walkers/GPU overridden: {per_gpu}]"
+        if tn:
+            sim_kw = [dict(kw, tn=int(tn)) for kw in sim_kw]
+            cfg["steps_per_walk"] = int(tn)
+            cfg["workload"] += f" [steps overridden: {tn}]"
+        return lab, sim_kw, per_gpu, cfg
     if walkers:
         per_gpu = int(walkers)
         sim_kw["npar"] = per_gpu * world
@@ -88,6 +106,28 @@ def _workload(name: str, world: int):
                             "kappa=0.01 um/ms, T2 80/60 ms, PGSE 540 gradients",
                    lattice=[256, 256, 2048], walkers_per_gpu=per_gpu, steps_per_walk=50_000,
                    ngrad=len(rows), mode="pgse")
+    elif name == "batch":
+        # 64 axons, lattices of log-uniform voxel counts between 64x64x256 and
+        # 256x256x2048, walkers proportional to the intra-axonal volume (5e7 in
+        # all), D0 ~ U(1.5, 2.5) um^2/ms and kappa ~ U(0, 0.05) um/ms per axon
+        rng = np.random.default_rng(2)
+        shapes = geometry.batch_sizes(64, seed=0)
+        lattices = [geometry.axon_lattice(*shp, 0.1, seed=100 + k, exterior=2) for k, shp in enumerate(shapes)]
+        intra = np.array([max(1, int(np.count_nonzero(l == 1))) for l in lattices], dtype=np.float64)
+        total = 50_000_000
+        npar = np.maximum(32, np.round(total * intra / intra.sum()).astype(np.int64))
+        D0 = rng.uniform(1.5, 2.5, 64)
+        kap = rng.uniform(0.0, 0.05, 64)
+        sims_kw = [dict(dt=2e-4, tn=20_000, npar=int(npar[k]), res=0.1,
+                        diffusivity=[0.0, float(D0[k]), float(D0[k])], t2=[1e12, 1e12, 1e12],
+                        bval=[], bvec=np.zeros((0, 3)), permeation="kappa", kappa=float(kap[k]))
+                   for k in range(64)]
+        cfg = dict(workload="batch: 64 axons, lattices 64x64x256..256x256x2048 (log-uniform voxels), "
+                            "5e7 walkers/GPU in proportion to intra-axonal volume, D0~U(1.5,2.5), "
+                            "kappa~U(0,0.05), 20000 steps, moments only",
+                   axons=64, lattice_voxels=int(sum(l.size for l in lattices)),
+                   walkers_per_gpu=int(npar.sum()), steps_per_walk=20_000, mode="narrow (no b-table)")
+        return lattices, sims_kw, int(npar.sum()), cfg
     elif name == "single":
         lab = geometry.axon_lattice(64, 64, 512, 0.1, seed=0, exterior=0)
         per_gpu = 100_000
@@ -199,6 +239,10 @@ def run_reference_arm(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     lab, sim_kw, per_gpu, cfg = workload(args.workload, 1, args.walkers, args.tn)
+    if isinstance(lab, list):
+        # a batch: time the reference loop on the axon with the most walkers
+        k = int(np.argmax([kw["npar"] for kw in sim_kw]))
+        lab, sim_kw = lab[k], sim_kw[k]
     try:
         job, n, cores, kind = cpu_reference_rate(lab, sim_kw, target_s=6.0)
     except Exception as e:  # the build is missing on this machine
@@ -225,10 +269,95 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+class SingleJob:
+    """One simulation; rank r walks walker shard r of a world * per_gpu job."""
+
+    def __init__(self, lab, kw, per_gpu, rank, device, stream):
+        from rms_b200 import engine, shards
+        self.lab, self.kw = lab, kw
+        self.w0, self.w1 = shards.walker_shard(per_gpu, rank)
+        self.sim = engine.Sim(lab, **kw)
+        self.device, self.stream = device, stream
+        self.walker_steps = (self.w1 - self.w0) * kw["tn"]
+        self.launches_per_step = 2 + (1 if self.sim.mode == "pgse" else 0)
+        self.pinned = None
+
+    def run(self, seed, precision):
+        self.sim.run(seed=seed, precision=precision, device=self.device, stream=self.stream,
+                     walker_range=(self.w0, self.w1))
+
+    def walk_ms(self):
+        return self.sim.timing()[0]
+
+    def reload_inputs(self):
+        import torch
+        if self.pinned is None:
+            self.pinned = torch.from_numpy(np.ascontiguousarray(self.lab)).pin_memory().numpy()
+        self.sim.set_lattice(self.pinned)
+
+    def outputs(self):
+        return self.sim.outputs()
+
+    def input_bytes(self):
+        return int(self.lab.nbytes)
+
+    def cpu_case(self):
+        return self.lab, self.kw
+
+    def close(self):
+        self.sim.close()
+
+
+class BatchJob:
+    """Many axons walked by one launch (rms_batch_run); every rank walks its own
+    copy of the batch with its own seed (weak scaling)."""
+
+    def __init__(self, labs, kws, rank, device, stream):
+        from rms_b200 import engine
+        self.engine = engine
+        self.labs, self.kws = labs, kws
+        self.sims = [engine.Sim(l, **kw) for l, kw in zip(labs, kws)]
+        self.rank, self.device, self.stream = rank, device, stream
+        self.walker_steps = sum(kw["npar"] * kw["tn"] for kw in kws)
+        self.launches_per_step = 1 + len(self.sims)   # one walk + one ordered reduction per axon
+        self.pinned = None
+
+    def run(self, seed, precision):
+        self.engine.batch_run(self.sims, seed=seed + (self.rank << 40), precision=precision,
+                              device=self.device, stream=self.stream)
+
+    def walk_ms(self):
+        return self.sims[0].timing()[0]
+
+    def reload_inputs(self):
+        import torch
+        if self.pinned is None:
+            self.pinned = [torch.from_numpy(np.ascontiguousarray(l)).pin_memory().numpy() for l in self.labs]
+        for sim, lab in zip(self.sims, self.pinned):
+            sim.set_lattice(lab)
+
+    def outputs(self):
+        out = {}
+        for k, sim in enumerate(self.sims):
+            for f, v in sim.outputs().items():
+                out[f"{k}/{f}"] = v
+        return out
+
+    def input_bytes(self):
+        return int(sum(l.nbytes for l in self.labs))
+
+    def cpu_case(self):
+        k = int(np.argmax([kw["npar"] for kw in self.kws]))
+        return self.labs[k], self.kws[k]
+
+    def close(self):
+        for sim in self.sims:
+            sim.close()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from rms_b200 import engine
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -238,24 +367,30 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn)
-    from rms_b200 import shards
-    w0, w1 = shards.walker_shard(per_gpu, rank)
-    sim = engine.Sim(lab, **sim_kw)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
+    if isinstance(lab, list):
+        if world > 1:
+            sim_kw = [dict(kw, npar=kw["npar"] // world) for kw in sim_kw]
+        job = BatchJob(lab, sim_kw, rank, local, sh)
+    else:
+        job = SingleJob(lab, sim_kw, per_gpu, rank, local, sh)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     precision = args.precision
-
-    def one(seed):
-        sim.run(seed=seed, precision=precision, device=local, stream=sh, walker_range=(w0, w1))
 
     def barrier():
         if world > 1:
             dist.barrier()
 
+    def max_over_ranks(*vals):
+        if world == 1:
+            return vals
+        t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return tuple(float(x) for x in t)
+
     for i in range(args.warmup):
-        one(1000 + i)
-    launches_per_step = 2 + (1 if sim.mode == "pgse" else 0)
+        job.run(1000 + i, precision)
     walk_ms = []
     barrier()
     torch.cuda.synchronize()
@@ -264,62 +399,49 @@ def run_ours(args):
         e0.record(stream)
         for i in range(args.steps):
             flush.zero_()
-            one(2000 + i)
-            walk_ms.append(sim.timing()[0])
+            job.run(2000 + i, precision)
+            walk_ms.append(job.walk_ms())
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-    walk = float(np.mean(walk_ms))
-    if world > 1:
-        t = torch.tensor([ms, walk], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, walk = float(t[0]), float(t[1])
-    tn = sim_kw["tn"]
-    value = world * per_gpu * tn / (ms * 1e-3)
-    # the plain FP64 walk on the same workload, for the split / plain ratio
+    ms, walk = max_over_ranks(e0.elapsed_time(e1) / args.steps, float(np.mean(walk_ms)))
+    value = world * job.walker_steps / (ms * 1e-3)
+
+    # the plain FP64 walk on the same workload (one launch per axon), for the
+    # split / plain ratio
     plain = None
     if args.plain_ratio and precision == "split":
-        sim.run(seed=999, precision="compat", device=local, stream=sh, walker_range=(w0, w1))
+        job.run(999, "compat")
         torch.cuda.synchronize()
         e0.record(stream)
-        sim.run(seed=998, precision="compat", device=local, stream=sh, walker_range=(w0, w1))
+        job.run(998, "compat")
         e1.record(stream)
         torch.cuda.synchronize()
-        pms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([pms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            pms = float(t[0])
-        plain = {"value": world * per_gpu * tn / (pms * 1e-3), "ms_per_step": pms, "precision": "compat (FP64)",
-                 "steps": 1}
+        (pms,) = max_over_ranks(e0.elapsed_time(e1))
+        plain = {"value": world * job.walker_steps / (pms * 1e-3), "ms_per_step": pms,
+                 "precision": "compat (FP64), one launch per axon", "steps": 1}
 
-    # end to end through the public API: lattice from pinned host memory,
+    # end to end through the public API: lattices from pinned host memory,
     # results read back, every step
-    pinned = torch.from_numpy(np.ascontiguousarray(lab)).pin_memory()
-    lab_pinned = pinned.numpy()
     e2e_steps = max(1, min(args.steps, 3))
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for i in range(e2e_steps):
-        sim.set_lattice(lab_pinned)
-        one(3000 + i)
-        out = sim.outputs()
+        job.reload_inputs()
+        job.run(3000 + i, precision)
+        out = job.outputs()
         if world > 1:
             # the whole job's result: rank-order sum of the shards' accumulators
-            out = shards.gather_sum({k: v for k, v in out.items() if k != "td"}, device="cuda")
+            from rms_b200 import shards
+            out = shards.gather_sum({k: v for k, v in out.items() if not k.endswith("td")}, device="cuda")
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t[0])
+    (e2e_s,) = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
     d2h = int(sum(v.nbytes for v in out.values()))
-    h2d = int(lab.nbytes)
+    h2d = job.input_bytes()
 
     # roofline of the walk kernel (the dominant launch)
-    walker_steps = per_gpu * tn
+    walker_steps = job.walker_steps
     achieved_gbs = walker_steps * BYTES_PER_WALKER_STEP / (walk * 1e-3) / 1e9
     peaks = {}
     try:
@@ -328,7 +450,7 @@ def run_ours(args):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     # DRAM bytes per launch from the ncu capture summarised in profiles/
-    # (measured per walker-step on a production-shaped case, scaled to this launch)
+    # (measured per walker-step on a case of the same shape, scaled to this launch)
     traffic = None
     prof = os.path.join(ROOT, "profiles", f"walk_{precision}_kernel__{args.workload}.md")
     if os.path.exists(prof):
@@ -342,12 +464,13 @@ def run_ours(args):
             try:
                 sys.path.insert(0, os.path.join(ROOT, "oracle"))
                 import pyoracle
-                job, n, cores, kind = cpu_reference_rate(lab, sim_kw, target_s=15.0)
+                clab, ckw = job.cpu_case()
+                cjob, n, cores, kind = cpu_reference_rate(clab, ckw, target_s=15.0)
                 t0 = time.perf_counter()
-                pyoracle.run_reference_walkers(job, n, cores)
+                pyoracle.run_reference_walkers(cjob, n, cores)
                 el = time.perf_counter() - t0
-                cpu = {"value": n * job.tn / el, "unit": UNIT, "cores": cores, "kind": kind,
-                       "sample": f"walkers [0,{n}) x {job.tn} steps, reference propagate() "
+                cpu = {"value": n * cjob.tn / el, "unit": UNIT, "cores": cores, "kind": kind,
+                       "sample": f"walkers [0,{n}) x {cjob.tn} steps, reference propagate() "
                                  f"(oracle/_ref) on {cores} host threads, {el:.1f} s"}
             except Exception as e:
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
@@ -356,9 +479,9 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if precision == "compat" else "f32+i32 (f64 sums)",
-            "data": "synthetic (seeded axon lattice)",
+            "data": "synthetic (seeded axon lattices)",
             "config": dict(cfg, precision=precision, parallelism=f"walker shards x{world}",
-                           l2="flushed between steps (256 MiB write); lattice 134 MB > L2"),
+                           l2="flushed between steps (256 MiB write); lattices larger than L2"),
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak, "traffic": traffic,
                          "model": f"{BYTES_PER_WALKER_STEP} B/walker-step x {walker_steps:.3g} walker-steps "
@@ -367,14 +490,14 @@ def run_ours(args):
                       "ops_per_walker_step": OPS_PER_WALKER_STEP},
             "walk_ms": walk,
             "plain": plain,
-            "e2e": {"value": world * per_gpu * tn / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "e2e": {"value": world * walker_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": job.launches_per_step * args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
+    job.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -386,7 +509,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="split", choices=["split", "compat"])
-    ap.add_argument("--workload", default="production", choices=["production", "single"])
+    ap.add_argument("--workload", default="batch", choices=["production", "batch", "single"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--walkers", type=int, default=None, help="walkers per GPU (smaller case, e.g. for ncu)")
     ap.add_argument("--plain-ratio", action="store_true",

@@ -167,8 +167,15 @@ int rms_sim_write_dir(const rms_sim* sim, const char* dir);
  * main.cu:536-540. */
 int rms_sim_last_timing(const rms_sim* sim, double* walk_ms, double* run_ms);
 
-/* Run several simulations (e.g. one per axon) on one device back to back on
- * one stream.  Replaces: the serial per-axon loop of part1_demo3_simulation.m:83-92. */
+/* Run several simulations (e.g. one per axon) on one device.  Simulation k
+ * walks with seed + k * 0x9E3779B97F4A7C15, so it reproduces rms_sim_run of
+ * that simulation with that seed.  RMS_PREC_SPLIT walks all of them in ONE
+ * persistent launch (uneven lattices and walker counts share the grid); they
+ * must share TN, dt, timepoints, nite, walls and the b-table or gradient
+ * table (lattice, Nc, D, T2, permeation, res and NPar may differ).
+ * RMS_PREC_COMPAT runs them one after another.  opts->walker_begin/end are
+ * ignored (every simulation walks all its walkers).
+ * Replaces: the serial per-axon loop of part1_demo3_simulation.m:83-92. */
 int rms_batch_run(rms_sim* const* sims, int n, const rms_run_opts* opts);
 
 /* Thread-local message of the last failed call ("" if none). */

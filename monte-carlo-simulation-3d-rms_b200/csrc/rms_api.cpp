@@ -24,6 +24,7 @@ thread_local std::string g_last_error;
 constexpr int kCompatBlock = 128;
 constexpr int kSplitVariantDefault = 0;   // 256 threads, >= 4 blocks per SM (64 registers): fastest measured
 constexpr int kMaxGrad = 1 << 16;
+constexpr uint64_t kBatchSeedStep = 0x9E3779B97F4A7C15ull;   // seed of batch member k: seed + k * this
 
 // One device allocation that only grows.
 struct DevBuf {
@@ -70,7 +71,7 @@ struct rms_device_state {
     int device = -1;
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
-    DevBuf labels, packed, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
+    DevBuf labels, packed, axons, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
         ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos;
     HostPinned h_out;
     size_t labels_bytes = 0;
@@ -78,7 +79,7 @@ struct rms_device_state {
 
     ~rms_device_state() {
         if (device >= 0) cudaSetDevice(device);
-        for (DevBuf* b : {&labels, &packed, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
+        for (DevBuf* b : {&labels, &packed, &axons, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
                           &tr_vox, &tr_ev, &tr_pos})
             b->release();
@@ -167,6 +168,31 @@ void build_pgse_schedule(rms_sim* s) {
 }
 
 }  // namespace
+
+void fill_axon_desc(AxonDesc& x, const rms_sim* s, int64_t w0, int64_t w1, int64_t tile_begin, uint64_t seed,
+                    const uint8_t* lat) {
+    std::memset(&x, 0, sizeof x);
+    x.lat = lat;
+    x.n1 = s->n1; x.n2 = s->n2; x.n3 = s->n3; x.nc = s->nc;
+    x.s1 = s->n3 + 2;
+    x.s0 = (s->n2 + 2) * (s->n3 + 2);
+    x.walker_begin = w0; x.walker_end = w1;
+    x.tile_begin = tile_begin;
+    x.seed = seed;
+    x.res = (float)s->res;
+    bool same = true;
+    for (int c = 0; c < s->nc; ++c) {
+        x.step[c] = (float)s->step[c];
+        x.k[c] = s->step[c] > 0.0 ? (float)(1.0 / (s->step[c] * s->t2_steps[c])) : 0.0f;
+        for (int e = 0; e < s->nc; ++e) {
+            x.pij[c * kNcMax + e] = (float)s->pij[(size_t)c * s->nc + e];
+            x.ratio[c * kNcMax + e] = s->step[c] > 0.0 ? (float)(s->step[e] / s->step[c]) : 0.0f;
+        }
+        if (c >= 1) same = same && s->pij[(size_t)c * s->nc + c] > 0.999999 && s->pij[(size_t)c * s->nc] < 0.000001;
+    }
+    x.same_cross = same ? 1 : 0;
+    x.flight = (same && s->nite >= 4) ? 1 : 0;
+}
 
 int finalize_config(rms_sim* s) {
     std::ostringstream m;
@@ -304,55 +330,17 @@ cudaError_t upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
     return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
 }
 
-int run_one(rms_sim* s, const rms_run_opts* o) {
-    if (!s->have_lattice) return set_error(RMS_ERR_STATE, "no lattice: call rms_sim_set_lattice or load a run directory");
-    const int prec = o ? o->precision : RMS_PREC_COMPAT;
-    if (prec != RMS_PREC_COMPAT && prec != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "precision");
-    const int device = o ? o->device : 0;
-    int rc = ensure_device(s, device);
-    if (rc) return rc;
+// One simulation of a launch: its walker range and seed.
+struct LaunchJob {
+    rms_sim* s;
+    int64_t w0, w1;
+    uint64_t seed;
+};
+
+// Upload a simulation's lattice (when changed) and, for the split walk, its
+// padded packed copy; both live in the simulation's own device state.
+int prepare_lattice(rms_sim* s, cudaStream_t st, bool split, int bits) {
     rms_device_state* d = s->dev;
-    RMS_CUDA(cudaSetDevice(device));
-    cudaStream_t st = (o && o->stream) ? (cudaStream_t)o->stream : d->own;
-
-    int64_t w0 = o ? o->walker_begin : 0, w1 = o ? o->walker_end : 0;
-    if (w0 == 0 && w1 == 0) w1 = s->npar;
-    if (w0 < 0 || w1 > s->npar || w0 >= w1) return set_error(RMS_ERR_ARG, "walker range outside [0, NPar)");
-    int64_t trace_n = (o && o->trace_walkers > 0) ? o->trace_walkers : 0;
-    if (trace_n && prec != RMS_PREC_COMPAT) return set_error(RMS_ERR_ARG, "traces are recorded by the COMPAT walk only");
-    if (trace_n && w0 != 0) return set_error(RMS_ERR_ARG, "traces need walker_begin = 0");
-    trace_n = std::min<int64_t>(trace_n, w1);
-
-    // launch shape: persistent grid, warps stride over 32-walker tiles
-    int dev_sms = 0;
-    RMS_CUDA(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
-    int block = kCompatBlock;
-    int per_sm;
-    const int lattice_bits = split_lattice_bits(s->nc);
-    int variant = 0;
-    if (prec == RMS_PREC_COMPAT) {
-        per_sm = walk_compat_blocks_per_sm(s->nc, trace_n > 0);
-    } else {
-        variant = (o && o->variant > 0) ? o->variant - 1 : kSplitVariantDefault;
-        if (variant >= split_variant_count()) return set_error(RMS_ERR_ARG, "variant out of range");
-        block = split_variant_block(variant);
-        per_sm = walk_split_blocks_per_sm(s->nc, lattice_bits, variant);
-    }
-    if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
-    const int64_t ntiles = (w1 - w0 + 31) / 32;
-    const int64_t warps_per_block = block / 32;
-    int64_t grid64 = std::min<int64_t>((int64_t)dev_sms * per_sm, (ntiles + warps_per_block - 1) / warps_per_block);
-    const int grid = (int)std::max<int64_t>(grid64, 1);
-    const int nthr = grid * block;
-    const int nslots = nthr / 32;
-    const int T = s->timepoints;
-    const int nb = s->nbvec();
-    const int nvals = (s->mode == RMS_MODE_NARROW) ? kRowHead + ((nb + 31) / 32) * 32 : kRowHead;
-    const int ngrad = s->ngrad();
-    const int ngrad_pad = std::max(32, ((ngrad + 31) / 32) * 32);
-    const size_t row = (size_t)T * nvals;
-
-    // inputs
     if (s->lattice_dirty || d->labels_bytes != s->labels.size()) {
         RMS_CUDA(d->labels.ensure(s->labels.size()));
         RMS_CUDA(cudaMemcpyAsync(d->labels.p, s->labels.data(), s->labels.size(), cudaMemcpyHostToDevice, st));
@@ -360,23 +348,93 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
         d->packed_valid = false;
         s->lattice_dirty = false;
     }
-    if (prec == RMS_PREC_SPLIT && !d->packed_valid) {
-        RMS_CUDA(d->packed.ensure(padded_lattice_bytes(s->n1, s->n2, s->n3, lattice_bits)));
-        int pe = pack_lattice_padded(d->labels.as<uint8_t>(), s->n1, s->n2, s->n3, lattice_bits,
-                                     d->packed.as<uint8_t>(), st);
+    if (split && !d->packed_valid) {
+        RMS_CUDA(d->packed.ensure(padded_lattice_bytes(s->n1, s->n2, s->n3, bits)));
+        int pe = pack_lattice_padded(d->labels.as<uint8_t>(), s->n1, s->n2, s->n3, bits, d->packed.as<uint8_t>(), st);
         if (pe) return cuda_fail((cudaError_t)pe, "label packing");
         d->packed_valid = true;
+    }
+    return RMS_OK;
+}
+
+// Settings every simulation of one split launch must share (the signal
+// tables and the record schedule are the launch's).
+bool same_schedule(const rms_sim* a, const rms_sim* b) {
+    return a->mode == b->mode && a->tn == b->tn && a->dt == b->dt && a->timepoints == b->timepoints &&
+           a->tstep == b->tstep && a->nite == b->nite && a->boundary == b->boundary && a->bval == b->bval &&
+           a->bvec == b->bvec && a->grad == b->grad;
+}
+
+// Run one launch: COMPAT (one simulation) or SPLIT (one or more simulations,
+// "axons", walked by one persistent grid).  The first job's simulation owns
+// the launch's accumulators.
+int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
+    rms_sim* s = jobs[0].s;
+    const int prec = o ? o->precision : RMS_PREC_COMPAT;
+    if (prec != RMS_PREC_COMPAT && prec != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "precision");
+    if (prec == RMS_PREC_COMPAT && jobs.size() != 1) return set_error(RMS_ERR_ARG, "a COMPAT launch walks one simulation");
+    const int device = o ? o->device : 0;
+    for (LaunchJob& j : jobs) {
+        if (!j.s->have_lattice) return set_error(RMS_ERR_STATE, "no lattice: call rms_sim_set_lattice or load a run directory");
+        if (!same_schedule(s, j.s)) return set_error(RMS_ERR_ARG, "simulations of one launch need the same steps, records, walls and signal tables");
+        int rc = ensure_device(j.s, device);
+        if (rc) return rc;
+    }
+    rms_device_state* d = s->dev;
+    RMS_CUDA(cudaSetDevice(device));
+    cudaStream_t st = (o && o->stream) ? (cudaStream_t)o->stream : d->own;
+    const int naxons = (int)jobs.size();
+
+    int64_t trace_n = (o && o->trace_walkers > 0) ? o->trace_walkers : 0;
+    if (trace_n && prec != RMS_PREC_COMPAT) return set_error(RMS_ERR_ARG, "traces are recorded by the COMPAT walk only");
+    if (trace_n && jobs[0].w0 != 0) return set_error(RMS_ERR_ARG, "traces need walker_begin = 0");
+    trace_n = std::min<int64_t>(trace_n, jobs[0].w1);
+
+    // launch shape: persistent grid
+    int dev_sms = 0;
+    RMS_CUDA(cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device));
+    int block = kCompatBlock, per_sm, variant = 0, lattice_bits = 8;
+    int nc_max = 0;
+    for (LaunchJob& j : jobs) nc_max = std::max(nc_max, j.s->nc);
+    if (prec == RMS_PREC_COMPAT) {
+        per_sm = walk_compat_blocks_per_sm(s->nc, trace_n > 0);
+    } else {
+        lattice_bits = split_lattice_bits(nc_max);
+        variant = (o && o->variant > 0) ? o->variant - 1 : kSplitVariantDefault;
+        if (variant >= split_variant_count()) return set_error(RMS_ERR_ARG, "variant out of range");
+        block = split_variant_block(variant);
+        per_sm = walk_split_blocks_per_sm(nc_max, lattice_bits, variant);
+    }
+    if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
+    std::vector<int64_t> tile_begin(naxons + 1, 0);
+    for (int k = 0; k < naxons; ++k) tile_begin[k + 1] = tile_begin[k] + (jobs[k].w1 - jobs[k].w0 + 31) / 32;
+    const int64_t ntiles = tile_begin[naxons];
+    const int64_t warps_per_block = block / 32;
+    const int64_t grid64 = std::min<int64_t>((int64_t)dev_sms * per_sm, (ntiles + warps_per_block - 1) / warps_per_block);
+    const int grid = (int)std::max<int64_t>(grid64, 1);
+    const int nthr = grid * block;
+    const int nwarps = nthr / 32;
+    const int T = s->timepoints;
+    const int nb = s->nbvec();
+    const int nvals = (s->mode == RMS_MODE_NARROW) ? kRowHead + ((nb + 31) / 32) * 32 : kRowHead;
+    const int ngrad = s->ngrad();
+    const int ngrad_pad = std::max(32, ((ngrad + 31) / 32) * 32);
+    const size_t row = (size_t)T * nvals;
+
+    const int nseg = nwarps;   // one accumulator row set per warp
+    const bool multi = naxons > 1;
+
+    // inputs
+    std::vector<AxonDesc> axons;
+    for (LaunchJob& j : jobs) {
+        int rc = prepare_lattice(j.s, st, prec == RMS_PREC_SPLIT, lattice_bits);
+        if (rc) return rc;
     }
     std::vector<double> tables;
     tables.insert(tables.end(), s->step.begin(), s->step.end());
     tables.insert(tables.end(), s->t2_steps.begin(), s->t2_steps.end());
     tables.insert(tables.end(), s->pij.begin(), s->pij.end());
-    std::vector<float> tablesf;
-    for (double x : s->step) tablesf.push_back((float)x);
-    for (double x : s->t2_steps) tablesf.push_back((float)(1.0 / x));
-    for (double x : s->pij) tablesf.push_back((float)x);
     RMS_CUDA(upload(d->tables, tables, st));
-    RMS_CUDA(upload(d->tablesf, tablesf, st));
     RMS_CUDA(upload(d->qtab, s->qtab, st));
     RMS_CUDA(upload(d->bvec, s->bvec, st));
     RMS_CUDA(upload(d->grad, s->grad, st));
@@ -384,17 +442,26 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
     RMS_CUDA(upload(d->ev_step, s->ev_step, st));
     RMS_CUDA(upload(d->ev_pair, s->ev_pair, st));
     RMS_CUDA(upload(d->ev_coef, s->ev_coef, st));
+    if (prec == RMS_PREC_SPLIT) {
+        axons.resize(naxons);
+        for (int k = 0; k < naxons; ++k)
+            fill_axon_desc(axons[k], jobs[k].s, jobs[k].w0, jobs[k].w1, tile_begin[k], jobs[k].seed,
+                           jobs[k].s->dev->packed.as<uint8_t>());
+        RMS_CUDA(upload(d->axons, axons, st));
+    }
 
     // accumulators
-    RMS_CUDA(d->slots.ensure((size_t)nslots * row * sizeof(double)));
-    RMS_CUDA(cudaMemsetAsync(d->slots.p, 0, (size_t)nslots * row * sizeof(double), st));
-    RMS_CUDA(d->out.ensure(row * sizeof(double)));
+    RMS_CUDA(d->slots.ensure((size_t)nseg * row * sizeof(double)));
+    RMS_CUDA(cudaMemsetAsync(d->slots.p, 0, (size_t)nseg * row * sizeof(double), st));
+    RMS_CUDA(d->out.ensure((size_t)naxons * row * sizeof(double)));
+    if (multi) RMS_CUDA(cudaMemsetAsync(d->out.p, 0, (size_t)naxons * row * sizeof(double), st));
     RMS_CUDA(d->err.ensure(sizeof(int)));
     RMS_CUDA(cudaMemsetAsync(d->err.p, 0, sizeof(int), st));
     if (s->mode == RMS_MODE_PGSE) {
-        RMS_CUDA(d->sig_slots.ensure((size_t)nslots * ngrad_pad * sizeof(double)));
-        RMS_CUDA(cudaMemsetAsync(d->sig_slots.p, 0, (size_t)nslots * ngrad_pad * sizeof(double), st));
-        RMS_CUDA(d->out_sig.ensure((size_t)ngrad_pad * sizeof(double)));
+        RMS_CUDA(d->sig_slots.ensure((size_t)nseg * ngrad_pad * sizeof(double)));
+        RMS_CUDA(cudaMemsetAsync(d->sig_slots.p, 0, (size_t)nseg * ngrad_pad * sizeof(double), st));
+        RMS_CUDA(d->out_sig.ensure((size_t)naxons * ngrad_pad * sizeof(double)));
+        if (multi) RMS_CUDA(cudaMemsetAsync(d->out_sig.p, 0, (size_t)naxons * ngrad_pad * sizeof(double), st));
         RMS_CUDA(d->vscr.ensure(std::max<size_t>((size_t)s->npairs * 3 * nthr * sizeof(double), 16)));
     }
     if (trace_n) {
@@ -407,17 +474,14 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
     WalkArgs a{};
     a.labels = d->labels.as<uint8_t>();
     a.n1 = s->n1; a.n2 = s->n2; a.n3 = s->n3;
-    a.walker_begin = w0; a.walker_end = w1;
-    a.tn = s->tn; a.tstep = s->tstep; a.timepoints = T; a.nite = s->nite; a.nc = s->nc;
+    a.walker_begin = jobs[0].w0; a.walker_end = jobs[0].w1;
+    a.tn = s->tn; a.tstep = s->tstep; a.timepoints = T; a.nite = s->nite; a.nc = nc_max;
     a.boundary = s->boundary; a.mode = s->mode;
     a.res = s->res; a.dt = s->dt;
-    a.seed = o ? o->seed : 0;
+    a.seed = jobs[0].seed;
     a.step = d->tables.as<double>();
     a.t2 = a.step + s->nc;
     a.pij = a.t2 + s->nc;
-    a.stepf = d->tablesf.as<float>();
-    a.t2invf = a.stepf + s->nc;
-    a.pijf = a.t2invf + s->nc;
     a.nvals = nvals;
     a.slots = d->slots.as<double>();
     a.nbvec = nb;
@@ -429,31 +493,38 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
     a.vscr = d->vscr.as<double>();
     a.sig_slots = d->sig_slots.as<double>();
     a.err = d->err.as<int>();
+    a.axons = d->axons.as<AxonDesc>();
+    a.naxons = naxons;
+    a.ntiles = ntiles;
+    a.out_rows = d->out.as<double>();
+    a.out_sig = d->out_sig.as<double>();
+    if (!axons.empty()) a.axon0 = axons[0];
     a.trace_n = trace_n;
     a.tr_init = d->tr_init.as<int32_t>(); a.tr_vox = d->tr_vox.as<int32_t>(); a.tr_ev = d->tr_ev.as<uint32_t>();
     a.tr_pos = d->tr_pos.as<double>();
 
     RMS_CUDA(cudaEventRecord(d->e0, st));
     int e = (prec == RMS_PREC_COMPAT) ? launch_walk_compat(a, grid, block, trace_n > 0, st)
-                                      : launch_walk_split(a, d->packed.as<uint8_t>(), lattice_bits, variant, grid, st);
+                                      : launch_walk_split(a, lattice_bits, variant, grid, st);
     if (e) return cuda_fail((cudaError_t)e, "walk kernel launch");
     RMS_CUDA(cudaEventRecord(d->e1, st));
-    e = launch_reduce_slots(a.slots, nslots, row, d->out.as<double>(), st);
-    if (e) return cuda_fail((cudaError_t)e, "reduce launch");
-    if (s->mode == RMS_MODE_PGSE) {
-        e = launch_reduce_slots(a.sig_slots, nslots, (size_t)ngrad_pad, d->out_sig.as<double>(), st);
+    if (!multi) {
+        // one axon: the warps' rows summed in a fixed order (repeatable)
+        e = launch_reduce_slots(a.slots, nseg, row, d->out.as<double>(), st);
+        if (!e && s->mode == RMS_MODE_PGSE)
+            e = launch_reduce_slots(a.sig_slots, nseg, (size_t)ngrad_pad, d->out_sig.as<double>(), st);
         if (e) return cuda_fail((cudaError_t)e, "reduce launch");
     }
     RMS_CUDA(cudaEventRecord(d->e2, st));
 
-    // results back (one pinned staging buffer: row, then sig, then the error word)
-    const size_t host_bytes = (row + ngrad_pad + 1) * sizeof(double);
-    RMS_CUDA(d->h_out.ensure(host_bytes));
+    // results back (one pinned staging buffer: rows, then signals, then the error word)
+    const size_t nrow = (size_t)naxons * row, nsig = (size_t)naxons * ngrad_pad;
+    RMS_CUDA(d->h_out.ensure((nrow + nsig + 1) * sizeof(double)));
     double* h = static_cast<double*>(d->h_out.p);
-    RMS_CUDA(cudaMemcpyAsync(h, d->out.p, row * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RMS_CUDA(cudaMemcpyAsync(h, d->out.p, nrow * sizeof(double), cudaMemcpyDeviceToHost, st));
     if (s->mode == RMS_MODE_PGSE)
-        RMS_CUDA(cudaMemcpyAsync(h + row, d->out_sig.p, ngrad_pad * sizeof(double), cudaMemcpyDeviceToHost, st));
-    int* herr = reinterpret_cast<int*>(h + row + ngrad_pad);
+        RMS_CUDA(cudaMemcpyAsync(h + nrow, d->out_sig.p, nsig * sizeof(double), cudaMemcpyDeviceToHost, st));
+    int* herr = reinterpret_cast<int*>(h + nrow + nsig);
     RMS_CUDA(cudaMemcpyAsync(herr, d->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     if (trace_n) {
         s->tr_init.resize(trace_n);
@@ -470,34 +541,47 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
         return set_error(RMS_ERR_RANGE, "a walker found no labelled voxel within the rejection-sampling cap");
     if (*herr & kErrStep) return set_error(RMS_ERR_RANGE, "a step segment found no voxel face (step >= 1 voxel)");
 
-    float ms = 0.f;
-    RMS_CUDA(cudaEventElapsedTime(&ms, d->e0, d->e1));
-    s->walk_ms = ms;
-    RMS_CUDA(cudaEventElapsedTime(&ms, d->e0, d->e2));
-    s->run_ms = ms;
-    s->last_grid = grid;
-    s->last_block = block;
+    float ms_walk = 0.f, ms_run = 0.f;
+    RMS_CUDA(cudaEventElapsedTime(&ms_walk, d->e0, d->e1));
+    RMS_CUDA(cudaEventElapsedTime(&ms_run, d->e0, d->e2));
 
     // unpack record rows into the reference's field layouts
-    s->sig0.assign(T, 0.0);
-    s->dx2.assign((size_t)T * 6, 0.0);
-    s->dx4.assign((size_t)T * 15, 0.0);
-    s->npar_count.assign((size_t)T * s->nc, 0.0);
-    s->sigre.assign((size_t)T * nb, 0.0);
-    for (int t = 0; t < T; ++t) {
-        const double* r = h + (size_t)t * nvals;
-        s->sig0[t] = r[kColSig0];
-        for (int k = 0; k < 6; ++k) s->dx2[t * 6 + k] = r[kColDx2 + k];
-        for (int k = 0; k < 15; ++k) s->dx4[t * 15 + k] = r[kColDx4 + k];
-        for (int c = 0; c < s->nc; ++c) s->npar_count[t * s->nc + c] = r[kColCount + c];
-        if (s->mode == RMS_MODE_NARROW)
-            for (int j = 0; j < nb; ++j) s->sigre[(size_t)t * nb + j] = r[kRowHead + j];
+    for (int k = 0; k < naxons; ++k) {
+        rms_sim* sk = jobs[k].s;
+        const double* hk = h + (size_t)k * row;
+        const int nc = sk->nc;
+        sk->sig0.assign(T, 0.0);
+        sk->dx2.assign((size_t)T * 6, 0.0);
+        sk->dx4.assign((size_t)T * 15, 0.0);
+        sk->npar_count.assign((size_t)T * nc, 0.0);
+        sk->sigre.assign((size_t)T * nb, 0.0);
+        for (int t = 0; t < T; ++t) {
+            const double* r = hk + (size_t)t * nvals;
+            sk->sig0[t] = r[kColSig0];
+            for (int q = 0; q < 6; ++q) sk->dx2[t * 6 + q] = r[kColDx2 + q];
+            for (int q = 0; q < 15; ++q) sk->dx4[t * 15 + q] = r[kColDx4 + q];
+            for (int c = 0; c < nc; ++c) sk->npar_count[t * nc + c] = r[kColCount + c];
+            if (sk->mode == RMS_MODE_NARROW)
+                for (int q = 0; q < nb; ++q) sk->sigre[(size_t)t * nb + q] = r[kRowHead + q];
+        }
+        sk->sig.assign(sk->mode == RMS_MODE_PGSE ? ngrad : 0, 0.0);
+        for (int q = 0; q < (int)sk->sig.size(); ++q) sk->sig[q] = h[nrow + (size_t)k * ngrad_pad + q];
+        sk->trace_n = k == 0 ? trace_n : 0;
+        sk->walk_ms = ms_walk;
+        sk->run_ms = ms_run;
+        sk->last_grid = grid;
+        sk->last_block = block;
+        sk->have_results = true;
     }
-    s->sig.assign(s->mode == RMS_MODE_PGSE ? ngrad : 0, 0.0);
-    for (int j = 0; j < (int)s->sig.size(); ++j) s->sig[j] = h[row + j];
-    s->trace_n = trace_n;
-    s->have_results = true;
     return RMS_OK;
+}
+
+int run_one(rms_sim* s, const rms_run_opts* o) {
+    int64_t w0 = o ? o->walker_begin : 0, w1 = o ? o->walker_end : 0;
+    if (w0 == 0 && w1 == 0) w1 = s->npar;
+    if (w0 < 0 || w1 > s->npar || w0 >= w1) return set_error(RMS_ERR_ARG, "walker range outside [0, NPar)");
+    std::vector<LaunchJob> jobs{LaunchJob{s, w0, w1, o ? o->seed : 0}};
+    return run_launch(jobs, o);
 }
 
 bool field_size(const rms_sim* s, int field, size_t& n) {
@@ -613,15 +697,34 @@ int rms_sim_run(rms_sim* s, const rms_run_opts* opts) {
 
 int rms_batch_run(rms_sim* const* sims, int n, const rms_run_opts* opts) {
     if (!sims || n < 0) return set_error(RMS_ERR_ARG, "null argument");
-    for (int i = 0; i < n; ++i) {
-        int rc = rms_sim_run(sims[i], opts);
-        if (rc) {
-            std::ostringstream m;
-            m << "simulation " << i << ": " << g_last_error;
-            return set_error(rc, m.str());
+    for (int i = 0; i < n; ++i)
+        if (!sims[i]) return set_error(RMS_ERR_ARG, "null simulation in the batch");
+    if (n == 0) return RMS_OK;
+    const int prec = opts ? opts->precision : RMS_PREC_COMPAT;
+    const uint64_t seed = opts ? opts->seed : 0;
+    try {
+        if (prec == RMS_PREC_SPLIT) {
+            // one persistent launch over all simulations
+            std::vector<LaunchJob> jobs;
+            for (int i = 0; i < n; ++i)
+                jobs.push_back(LaunchJob{sims[i], 0, sims[i]->npar, seed + (uint64_t)i * kBatchSeedStep});
+            return run_launch(jobs, opts);
         }
+        for (int i = 0; i < n; ++i) {
+            rms_run_opts oi = opts ? *opts : rms_run_opts{};
+            oi.seed = seed + (uint64_t)i * kBatchSeedStep;
+            oi.walker_begin = oi.walker_end = 0;
+            int rc = run_one(sims[i], &oi);
+            if (rc) {
+                std::ostringstream m;
+                m << "simulation " << i << ": " << g_last_error;
+                return set_error(rc, m.str());
+            }
+        }
+        return RMS_OK;
+    } catch (const std::exception& e) {
+        return set_error(RMS_ERR_NOMEM, e.what());
     }
-    return RMS_OK;
 }
 
 int rms_sim_field_size(const rms_sim* s, int field, size_t* n) {

@@ -18,6 +18,25 @@ constexpr long long kInitTryCap = 1ll << 26;   // rejection-sampling attempts pe
 constexpr int kErrInitCap = 1;                  // a walker found no labelled voxel in kInitTryCap tries
 constexpr int kErrStep = 2;                     // a segment found no face (step >= 1 voxel)
 
+// One simulation ("axon") of a split-precision launch.  A launch walks the
+// tiles (32 walkers) of all its axons; axon k owns global tiles
+// [tile_begin, tile_begin + ceil((walker_end - walker_begin) / 32)).
+struct AxonDesc {
+    const uint8_t* lat;         // padded, packed lattice of this axon
+    int n1, n2, n3, nc;
+    int s0, s1;                 // padded lattice strides: (n2+2)(n3+2), n3+2
+    int64_t walker_begin, walker_end;   // walker ids (random streams) within the axon's job
+    int64_t tile_begin;
+    uint64_t seed;
+    float res;
+    int same_cross;             // same-label faces always crossed, compartment 0 never entered
+    int flight;                 // free flight allowed (same_cross and nite >= 4)
+    float step[kNcMax];         // step length, voxels
+    float k[kNcMax];            // T2 exponent per voxel of path
+    float pij[kNcMax * kNcMax]; // [a * kNcMax + b]
+    float ratio[kNcMax * kNcMax];   // step[b] / step[a]
+};
+
 // Arguments of the walk kernels (passed by value; pointers are device memory).
 struct WalkArgs {
     const uint8_t* labels;      // [n1*n2*n3], n3 fastest
@@ -49,6 +68,14 @@ struct WalkArgs {
     const float* t2invf;        // [nc] 1 / (T2 in steps)
     const float* pijf;          // [nc*nc]
     int* err;                   // device error word (kErr* bits), zeroed per run
+    // split launches: the axons and their tiles; with several axons each warp
+    // adds its rows into out_rows[axon][timepoints][nvals] / out_sig[axon][ngrad_pad]
+    const AxonDesc* axons;
+    int naxons;
+    int64_t ntiles;
+    double* out_rows;
+    double* out_sig;
+    AxonDesc axon0;             // the first axon, by value (read from kernel parameters)
     // traces (COMPAT)
     int64_t trace_n;
     int32_t* tr_init;
@@ -60,8 +87,9 @@ struct WalkArgs {
 // Launchers (rms_walk_*.cu, rms_reduce.cu).  All asynchronous on `stream`;
 // they return a cudaError_t value (0 = success).
 int launch_walk_compat(const WalkArgs& a, int grid, int block, bool trace, void* stream);
-int launch_walk_split(const WalkArgs& a, const uint8_t* lattice, int lattice_bits, int variant, int grid,
-                      void* stream);
+// Split walk over a.naxons axons (a.axons, a.ntiles, per-warp a.slots, and
+// a.out_rows/out_sig for several axons); lattice_bits: packed lattice format.
+int launch_walk_split(const WalkArgs& a, int lattice_bits, int variant, int grid, void* stream);
 int split_variant_count();
 int split_variant_block(int variant);   // threads per block of a launch variant
 int split_variant_minb(int variant);    // its minimum resident blocks per SM

@@ -117,7 +117,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     // fixed part of the scratch
     const int bits = split_lattice_bits(nc);
     const size_t lat_bytes = padded_lattice_bytes(s->n1, s->n2, s->n3, bits);
-    const size_t fixed = align256(lat_bytes) + align256(sizeof(int)) + align256(sizeof(double) * (2 * nc + nc * nc)) +
+    const size_t fixed = align256(lat_bytes) + align256(sizeof(AxonDesc)) + align256(sizeof(int)) + align256(sizeof(double) * (2 * nc + nc * nc)) +
                          align256(sizeof(float) * (2 * nc + nc * nc)) + align256(sizeof(double) * s->qtab.size()) +
                          align256(sizeof(double) * s->bvec.size()) + align256(sizeof(double) * s->grad.size()) +
                          align256(sizeof(int) * s->gpair.size()) + align256(sizeof(int) * s->ev_step.size()) +
@@ -146,6 +146,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
 
     Carve c{base};
     uint8_t* d_lat = c.take<uint8_t>(lat_bytes);
+    AxonDesc* d_axon = c.take<AxonDesc>(1);
     int* d_err = c.take<int>(1);
     double* d_tab = c.take<double>(2 * nc + nc * nc);
     float* d_tabf = c.take<float>(2 * nc + nc * nc);
@@ -184,6 +185,10 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
         (e = put(d_evp, s->ev_pair.data(), s->ev_pair.size(), st)) != cudaSuccess ||
         (e = put(d_evc, s->ev_coef.data(), s->ev_coef.size(), st)) != cudaSuccess)
         return set_error(RMS_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
+    AxonDesc axon;
+    fill_axon_desc(axon, s, w0, w1, 0, o->seed, d_lat);
+    if ((e = put(d_axon, &axon, 1, st)) != cudaSuccess)
+        return set_error(RMS_ERR_CUDA, std::string("axon upload: ") + cudaGetErrorString(e));
     // what must start at zero: error word and the accumulator rows
     if ((e = cudaMemsetAsync(d_err, 0, sizeof(int), st)) != cudaSuccess ||
         (e = cudaMemsetAsync(d_slots, 0, (size_t)nslots * row * sizeof(double), st)) != cudaSuccess ||
@@ -213,8 +218,12 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     a.vscr = d_vscr;
     a.sig_slots = d_sigslots;
     a.err = d_err;
+    a.axons = d_axon;
+    a.axon0 = axon;
+    a.naxons = 1;
+    a.ntiles = ntiles;
 
-    int ke = launch_walk_split(a, d_lat, bits, kVariant, grid, st);
+    int ke = launch_walk_split(a, bits, kVariant, grid, st);
     if (ke) return set_error(RMS_ERR_CUDA, std::string("walk launch: ") + cudaGetErrorString((cudaError_t)ke));
     ke = launch_reduce_slots(d_slots, nslots, row, d_rows, st);
     if (!ke && s->mode == RMS_MODE_PGSE) ke = launch_reduce_slots(d_sigslots, nslots, (size_t)ngrad_pad, d_sig, st);

@@ -60,6 +60,10 @@ struct rms_sim {
 };
 
 namespace rms {
+struct AxonDesc;
+// describe one simulation as an axon of a split launch (rms_internal.h)
+void fill_axon_desc(AxonDesc& x, const rms_sim* s, int64_t w0, int64_t w1, int64_t tile_begin, uint64_t seed,
+                    const uint8_t* lat);
 // error reporting (thread-local message behind rms_last_error)
 int set_error(int code, const std::string& msg);
 // derive tables and validate a filled-in configuration

@@ -30,7 +30,8 @@
 //  - per-walker sums that grow over the walk (T2 exponent, PGSE displacement
 //    sums) are carried in FP32 for at most 32 steps and folded into FP64;
 //  - cross-walker sums: FP32 products per walker, warp reduce-scatter in
-//    FP64, per-warp FP64 rows, ordered FP64 reduction (rms_reduce.cu).
+//    FP64, per-warp FP64 rows, then an ordered FP64 reduction (rms_reduce.cu)
+//    for one axon, or FP64 atomic adds into each axon's totals for several.
 //
 // Mirror walls: the reference mirrors the origin image at the end of a step
 // for each wall the step touched (main.cu:302-310).  A step shorter than a
@@ -86,53 +87,105 @@ __device__ __forceinline__ void mirror_origin(int& I, float& F, bool hi, int n) 
     else { I = base - I; }
 }
 
-template <int NCMAX, int BITS, int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs a, const uint8_t* __restrict__ lat) {
-    // per compartment: step (voxels), T2 exponent per voxel of path; per pair:
-    // Pij and the step-length ratio that rescales the rest of a step
-    __shared__ float s_step[NCMAX], s_k[NCMAX], s_pij[NCMAX * NCMAX], s_ratio[NCMAX * NCMAX];
-    for (int i = threadIdx.x; i < NCMAX * NCMAX; i += blockDim.x) {
-        const int r = i / NCMAX, c = i % NCMAX;
-        const bool in = r < a.nc && c < a.nc;
-        s_pij[i] = in ? a.pijf[r * a.nc + c] : 0.0f;
-        const float sr = (r < a.nc) ? a.stepf[r] : 0.0f, sc = (c < a.nc) ? a.stepf[c] : 0.0f;
-        s_ratio[i] = (in && sr > 0.0f) ? sc / sr : 0.0f;
-        if (i < NCMAX) {
-            const float st = (i < a.nc) ? a.stepf[i] : 0.0f;
-            s_step[i] = st;
-            s_k[i] = st > 0.0f ? (1.0f / st) * ((i < a.nc) ? a.t2invf[i] : 0.0f) : 0.0f;
+// Add a warp's accumulator rows (and PGSE signal row) into axon `axon`'s
+// totals and clear them (multi-axon launches; other warps add concurrently).
+__device__ __noinline__ void flush_rows(double* slot, double* sig_slot, double* out, double* os, size_t n,
+                                        int ngrad, int lane) {
+    for (size_t i = lane; i < n; i += 32) {
+        const double x = slot[i];
+        if (x != 0.0) {
+            atomicAdd(out + i, x);
+            slot[i] = 0.0;
         }
     }
-    __syncthreads();
-    // A face into the same compartment is always crossed -- unless a caller's
-    // table says otherwise, or lets walkers into the null compartment 0.
-    bool same_certain = true;
-    for (int c = 1; c < a.nc; ++c)
-        same_certain = same_certain && (s_pij[c * NCMAX + c] > 0.999999f) && (s_pij[c * NCMAX] < 0.000001f);
-    // free flight needs same-label faces always crossed and room for three
-    // crossings within the sub-segment cap
-    const bool flight = (BITS != 2) && same_certain && (a.nite >= 4);
+    if (os) {
+        for (int i = lane; i < ngrad; i += 32) {
+            const double x = sig_slot[i];
+            if (x != 0.0) {
+                atomicAdd(os + i, x);
+                sig_slot[i] = 0.0;
+            }
+        }
+    }
+}
+
+// ONE: the launch has one axon, whose scalars are read from the kernel
+// parameters (a.axon0) instead of being held in registers.
+template <int NCMAX, int BITS, int BLOCK, int MINB, bool ONE>
+__global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs a) {
+    // per warp, the current axon's tables: step (voxels), T2 exponent per voxel
+    // of path, Pij and the step-length ratio that rescales the rest of a step
+    constexpr int kTab = 2 * NCMAX + 2 * NCMAX * NCMAX;
+    __shared__ float s_tab[BLOCK / 32][kTab];
 
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthr = gridDim.x * blockDim.x;
     const int warp_global = gtid >> 5;
     const int nwarps = nthr >> 5;
-    const int64_t ntiles = (a.walker_end - a.walker_begin + 31) / 32;
+    float* tab = s_tab[threadIdx.x >> 5];
     const bool pgse = (a.mode == 1);
     const bool mirror = (a.boundary == 0);
-    const int n1 = a.n1, n2 = a.n2, n3 = a.n3;
-    // padded lattice strides
-    const int s1 = n3 + 2, s0 = (n2 + 2) * (n3 + 2);
-    const float res = (float)a.res;
-    const uint32_t key0 = (uint32_t)a.seed, key1 = (uint32_t)(a.seed >> 32);
     constexpr int kWall = wall_code<BITS>();
+
+    // Tiles are walked in strided order (warp w: tiles w, w + nwarps, ...), so at
+    // any moment the grid works on one narrow window of the tile list -- one or
+    // two axons, whose lattices then share the L2.  A one-axon launch keeps
+    // one accumulator row set per warp, summed in order afterwards.  A
+    // multi-axon launch keeps the warp's rows for its current axon and adds
+    // them into that axon's totals (FP64 atomics) when the warp moves on.
+    int ax = 0;          // current axon
+    int held = -1;       // axon whose records the warp's rows hold
+    int64_t next_tb = ONE ? INT64_MAX : ((a.naxons > 1) ? a.axons[1].tile_begin : INT64_MAX);
+    // a field of the current axon: kernel parameters for a one-axon launch,
+    // else the axon table (read where used, so it holds no registers)
+#define AXF(f) (ONE ? a.axon0.f : a.axons[ax].f)
     double* slot = a.slots + (size_t)warp_global * a.timepoints * a.nvals;
     double* sig_slot = pgse ? a.sig_slots + (size_t)warp_global * a.ngrad_pad : nullptr;
 
-    for (int64_t tile = warp_global; tile < ntiles; tile += nwarps) {
-        const int64_t w = a.walker_begin + tile * 32 + lane;
-        bool active = w < a.walker_end;
+    for (int64_t tile = warp_global; tile < a.ntiles; tile += nwarps) {
+        if (!ONE) {
+            while (tile >= next_tb) {
+                ++ax;
+                next_tb = (ax + 1 < a.naxons) ? a.axons[ax + 1].tile_begin : INT64_MAX;
+            }
+        }
+        if (held != ax) {
+            if (!ONE && held >= 0)
+                flush_rows(slot, sig_slot, a.out_rows + (size_t)held * a.timepoints * a.nvals,
+                           pgse ? a.out_sig + (size_t)held * a.ngrad_pad : nullptr,
+                           (size_t)a.timepoints * a.nvals, a.ngrad, lane);   // previous axon's records to its totals
+            held = ax;
+            // this axon's tables into the warp's shared memory
+            __syncwarp();
+            for (int i = lane; i < kTab; i += 32) {
+                float v;
+                if (i < NCMAX) v = AXF(step[i]);
+                else if (i < 2 * NCMAX) v = AXF(k[i - NCMAX]);
+                else if (i < 2 * NCMAX + NCMAX * NCMAX) {
+                    const int r = (i - 2 * NCMAX) / NCMAX, c = (i - 2 * NCMAX) % NCMAX;
+                    v = AXF(pij[r * kNcMax + c]);
+                } else {
+                    const int r = (i - 2 * NCMAX - NCMAX * NCMAX) / NCMAX, c = (i - 2 * NCMAX - NCMAX * NCMAX) % NCMAX;
+                    v = AXF(ratio[r * kNcMax + c]);
+                }
+                tab[i] = v;
+            }
+            __syncwarp();
+        }
+        const uint8_t* lat = AXF(lat);
+        const int s0 = AXF(s0), s1 = AXF(s1);
+        const uint64_t seed = AXF(seed);
+        const bool flight = (BITS != 2) && AXF(flight);
+        const bool same_certain = AXF(same_cross);
+        const float* t_step = tab;
+        const float* t_k = tab + NCMAX;
+        const float* t_pij = tab + 2 * NCMAX;
+        const float* t_ratio = tab + 2 * NCMAX + NCMAX * NCMAX;
+        const uint32_t key0 = (uint32_t)seed, key1 = (uint32_t)(seed >> 32);
+
+        const int64_t w = AXF(walker_begin) + (tile - (ONE ? 0 : AXF(tile_begin))) * 32 + lane;
+        bool active = w < AXF(walker_end);
         const uint32_t wlo = (uint32_t)w, whi = (uint32_t)((uint64_t)w >> 32);
 
         // initial position: uniform in the labelled voxels (rejection sampling)
@@ -140,9 +193,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         unsigned lin = 0;
         if (active) {
             DomainStream init;
-            init.init(a.seed, (uint64_t)w, kDomInit);
+            init.init(seed, (uint64_t)w, kDomInit);
             long long tries = 0;
             for (;;) {
+                const int n1 = AXF(n1), n2 = AXF(n2), n3 = AXF(n3);
                 const float x0 = init.next() * (float)n1;
                 const float x1 = init.next() * (float)n2;
                 const float x2 = init.next() * (float)n3;
@@ -154,14 +208,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
             }
         }
         int ai = active ? label_at<BITS>(lat, lin) : 0;
-        float cur_step = s_step[ai], cur_k = s_k[ai];
+        float cur_step = t_step[ai], cur_k = t_k[ai];
         // displacement = D + (offset - Fm) per axis; offset = up ? 1 - d : d
         int D0 = 0, D1 = 0, D2 = 0;
         float Fm0 = f0, Fm1 = f1, Fm2 = f2;    // origin fractions (mirrored at walls)
         float d0 = f0, d1 = f1, d2 = f2;       // as if travelling down
         unsigned up = 0u;                      // bit a: travelling up along axis a
         DomainStream perm;
-        perm.init(a.seed, (uint64_t)w, kDomPerm);
+        perm.init(seed, (uint64_t)w, kDomPerm);
 
         double w64 = 0.0;          // T2 exponent, folded
         float w32 = 0.0f;          // T2 exponent since the last fold
@@ -246,7 +300,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     } else {
                         if (aj == kWall) {
                             const bool hi = (up >> hit) & 1u;
-                            const int nh = hit == 0 ? n1 : (hit == 1 ? n2 : n3);
+                            const int nh = hit == 0 ? AXF(n1) : (hit == 1 ? AXF(n2) : AXF(n3));
                             if (mirror) {
                                 // mirror wall: reflect, and mirror the origin image
                                 const int g = hi ? nh - 1 : 0;
@@ -266,15 +320,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                         if (aj < 0) {
                             cross = false;
                         } else {
-                            const float P = s_pij[ai * NCMAX + aj];
+                            const float P = t_pij[ai * NCMAX + aj];
                             cross = (P > 0.999999f) || (P >= 0.000001f && perm.next() < P);
                         }
                     }
                     if (cross) {
                         if (aj != ai) {
-                            rem *= s_ratio[ai * NCMAX + aj];
-                            cur_step = s_step[aj];
-                            cur_k = s_k[aj];
+                            rem *= t_ratio[ai * NCMAX + aj];
+                            cur_step = t_step[aj];
+                            cur_k = t_k[aj];
                             ai = aj;
                         }
                         lin = lj;
@@ -343,6 +397,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     w64 += (double)w32;
                     w32 = 0.0f;
                     const float s0 = active ? (float)exp(-w64) : 0.0f;
+                    const float res = AXF(res);
                     const float dx = ((float)D0 + (o0 - Fm0)) * res;
                     const float dy = ((float)D1 + (o1 - Fm1)) * res;
                     const float dz = ((float)D2 + (o2 - Fm2)) * res;
@@ -390,7 +445,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
             }
         }
     }
+    if (!ONE && held >= 0)
+        flush_rows(slot, sig_slot, a.out_rows + (size_t)held * a.timepoints * a.nvals,
+                   pgse ? a.out_sig + (size_t)held * a.ngrad_pad : nullptr, (size_t)a.timepoints * a.nvals, a.ngrad,
+                   lane);
 }
+
+#undef AXF
 
 // Padded lattice: (n1+2) x (n2+2) x (n3+2), interior = the labels, border =
 // the wall code.  With BITS = 4 or 8 an interior voxel also gets the
@@ -433,23 +494,24 @@ __global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int 
 }
 
 template <int NCMAX, int BITS, int BLOCK, int MINB>
-int launch_t(const WalkArgs& a, const uint8_t* lat, int grid, void* stream) {
-    walk_split_kernel<NCMAX, BITS, BLOCK, MINB><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a, lat);
+int launch_t(const WalkArgs& a, int grid, void* stream) {
+    if (a.naxons == 1) walk_split_kernel<NCMAX, BITS, BLOCK, MINB, true><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a);
+    else walk_split_kernel<NCMAX, BITS, BLOCK, MINB, false><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a);
     return (int)cudaGetLastError();
 }
 
 template <int BLOCK, int MINB>
 const void* kernel_ptr(int nc, int bits) {
-    if (bits == 2) return (const void*)walk_split_kernel<4, 2, BLOCK, MINB>;
-    if (bits == 4) return (const void*)walk_split_kernel<8, 4, BLOCK, MINB>;
-    return (const void*)walk_split_kernel<8, 8, BLOCK, MINB>;
+    if (bits == 2) return (const void*)walk_split_kernel<4, 2, BLOCK, MINB, false>;
+    if (bits == 4) return (const void*)walk_split_kernel<8, 4, BLOCK, MINB, false>;
+    return (const void*)walk_split_kernel<8, 8, BLOCK, MINB, false>;
 }
 
 template <int BLOCK, int MINB>
-int launch_v(const WalkArgs& a, const uint8_t* lat, int bits, int grid, void* stream) {
-    if (bits == 2) return a.nc <= 3 ? launch_t<4, 2, BLOCK, MINB>(a, lat, grid, stream) : (int)cudaErrorInvalidValue;
-    if (bits == 4) return a.nc <= 7 ? launch_t<8, 4, BLOCK, MINB>(a, lat, grid, stream) : (int)cudaErrorInvalidValue;
-    return launch_t<8, 8, BLOCK, MINB>(a, lat, grid, stream);
+int launch_v(const WalkArgs& a, int bits, int grid, void* stream) {
+    if (bits == 2) return a.nc <= 3 ? launch_t<4, 2, BLOCK, MINB>(a, grid, stream) : (int)cudaErrorInvalidValue;
+    if (bits == 4) return a.nc <= 7 ? launch_t<8, 4, BLOCK, MINB>(a, grid, stream) : (int)cudaErrorInvalidValue;
+    return launch_t<8, 8, BLOCK, MINB>(a, grid, stream);
 }
 
 // Dispatch over the variant table (index v, 0-based).
@@ -487,10 +549,9 @@ int split_variant_count() { return kNumVariants; }
 int split_variant_block(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].block : -1; }
 int split_variant_minb(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[v].minb : -1; }
 
-int launch_walk_split(const WalkArgs& a, const uint8_t* lattice, int lattice_bits, int variant, int grid,
-                      void* stream) {
+int launch_walk_split(const WalkArgs& a, int lattice_bits, int variant, int grid, void* stream) {
     if (variant < 0 || variant >= kNumVariants) return (int)cudaErrorInvalidValue;
-    return by_variant(variant, [&]<int B, int M>() { return launch_v<B, M>(a, lattice, lattice_bits, grid, stream); });
+    return by_variant(variant, [&]<int B, int M>() { return launch_v<B, M>(a, lattice_bits, grid, stream); });
 }
 
 int walk_split_blocks_per_sm(int nc, int lattice_bits, int variant) {

@@ -1,0 +1,64 @@
+"""Batched runs (rms_batch_run): many axons with uneven lattices and walker
+counts walked by one persistent split launch.  Axon k uses seed + k * phi64
+(include/rms.h), so each must equal its own rms_sim_run with that seed --
+the same walkers, the same arithmetic: compartment counts equal, FP64 sums
+equal up to summation order."""
+import numpy as np
+import pytest
+
+from conftest import assert_fp64_close
+from rms_b200 import engine, geometry
+
+pytestmark = pytest.mark.gpu
+PHI64 = 0x9E3779B97F4A7C15
+
+
+def axon_sims(mode="narrow"):
+    rng = np.random.default_rng(11)
+    sims = []
+    shapes = [(16, 16, 40), (24, 20, 32), (12, 12, 64), (32, 32, 24), (20, 16, 16)]
+    for k, shp in enumerate(shapes):
+        lab = geometry.axon_lattice(*shp, 0.1, seed=k, exterior=2, r0=float(rng.uniform(0.4, 0.9)))
+        D1 = float(rng.uniform(1.5, 2.5))
+        kw = dict(dt=2e-4, tn=1000, npar=int(rng.integers(300, 5000)), res=0.1,
+                  diffusivity=[0, D1, 2.0], t2=[80, 80, 60], permeation="kappa",
+                  kappa=float(rng.uniform(0, 0.05)))
+        if mode == "pgse":
+            kw["grad"] = np.array([[0.1, 0.05, 2.0, 1, 0, 0], [0.15, 0.05, 3.0, 0, 0.6, 0.8]])
+        else:
+            kw["bval"], kw["bvec"] = [1.0, 2.0], [[1, 0, 0], [0, 0, 1]]
+        sims.append(engine.Sim(lab, **kw))
+    return sims
+
+
+@pytest.mark.parametrize("mode", ["narrow", "pgse"])
+def test_batch_equals_single_runs(mode):
+    sims = axon_sims(mode)
+    seed = 77
+    engine.batch_run(sims, seed=seed, precision="split")
+    batched = [s.outputs() for s in sims]
+    for k, s in enumerate(sims):
+        single = s.run(seed=(seed + k * PHI64) % (1 << 64), precision="split").outputs()
+        assert np.array_equal(batched[k]["npar_count"], single["npar_count"]), k
+        for f in ("sig0", "dx2", "dx4") + (("sig",) if mode == "pgse" else ("sigre",)):
+            assert_fp64_close(batched[k][f], single[f], 1e-9, f"axon {k} {f}")
+
+
+def test_batch_compat_is_serial_equivalent():
+    sims = axon_sims()[:2]
+    engine.batch_run(sims, seed=5, precision="compat")
+    b = [s.outputs() for s in sims]
+    for k, s in enumerate(sims):
+        one = s.run(seed=(5 + k * PHI64) % (1 << 64), precision="compat").outputs()
+        for f in one:
+            assert np.array_equal(b[k][f], one[f]), (k, f)
+
+
+def test_batch_rejects_mixed_schedules():
+    sims = axon_sims()[:2]
+    lab = np.ones((8, 8, 8), dtype=np.uint8)
+    other = engine.Sim(lab, dt=2e-4, tn=2000, npar=10, res=0.1, diffusivity=[0, 2.0], t2=[80, 80],
+                       bval=[1.0, 2.0], bvec=[[1, 0, 0], [0, 0, 1]])
+    with pytest.raises(engine.RmsError) as e:
+        engine.batch_run(sims + [other], seed=1, precision="split")
+    assert e.value.code == -1
