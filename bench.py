@@ -61,8 +61,15 @@ def fib_directions(n: int) -> np.ndarray:
     return np.column_stack([r * np.cos(phi), r * np.sin(phi), z])
 
 
-def workload(name: str, world: int, walkers: int | None = None, tn: int | None = None):
+def workload(name: str, world: int, walkers: int | None = None, tn: int | None = None,
+             timepoints: int | None = None):
     lab, sim_kw, per_gpu, cfg = _workload(name, world)
+    if timepoints:
+        if isinstance(sim_kw, list):
+            sim_kw = [dict(kw, timepoints=int(timepoints)) for kw in sim_kw]
+        else:
+            sim_kw["timepoints"] = int(timepoints)
+        cfg["workload"] += f" [timepoints overridden: {timepoints}]"
     if isinstance(sim_kw, list):
         if walkers:
             scale = walkers / per_gpu
@@ -224,10 +231,15 @@ def cpu_reference_rate(lab, sim_kw, target_s: float, nthreads: int | None = None
         # the reference build has fixed 1000 records and mirror walls: time its loop as is
         pass
     nthreads = nthreads or pyoracle.ref_max_threads()
-    n = max(nthreads, 2 * nthreads)
-    t0 = time.perf_counter()
-    pyoracle.run_reference_walkers(job, n, nthreads)
-    dt_probe = time.perf_counter() - t0
+    # probe with doubling walker counts until a probe lasts a second, then scale
+    n = 2 * nthreads
+    while True:
+        t0 = time.perf_counter()
+        pyoracle.run_reference_walkers(job, n, nthreads)
+        dt_probe = time.perf_counter() - t0
+        if dt_probe >= 1.0 or n >= job.npar:
+            break
+        n = min(job.npar, 2 * n)
     n = int(max(nthreads, min(job.npar, n * target_s / max(dt_probe, 1e-3))))
     return job, n, nthreads, kind
 
@@ -238,7 +250,7 @@ def run_reference_arm(args):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    lab, sim_kw, per_gpu, cfg = workload(args.workload, 1, args.walkers, args.tn)
+    lab, sim_kw, per_gpu, cfg = workload(args.workload, 1, args.walkers, args.tn, args.timepoints)
     if isinstance(lab, list):
         # a batch: time the reference loop on the axon with the most walkers
         k = int(np.argmax([kw["npar"] for kw in sim_kw]))
@@ -366,7 +378,7 @@ def run_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn)
+    lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn, args.timepoints)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
     if isinstance(lab, list):
@@ -515,6 +527,8 @@ def main():
     ap.add_argument("--plain-ratio", action="store_true",
                     help="also time one run of the plain FP64 walk on the same workload")
     ap.add_argument("--tn", type=int, default=None, help="steps per walk (smaller case, e.g. for ncu)")
+    ap.add_argument("--timepoints", type=int, default=None,
+                    help="records per walk (keep steps/record when shortening the walk)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
