@@ -39,6 +39,7 @@ extern "C" {
 /* Signal form: narrow-pulse b-table (main.cu) or rectangular PGSE (main_PGSE.cu). */
 #define RMS_MODE_NARROW 0
 #define RMS_MODE_PGSE 1
+#define RMS_MODE_WAVEFORM 2   /* general gradient waveforms on time bins (SPLIT walk only) */
 #define RMS_MODE_AUTO (-1)    /* rms_sim_load_dir: PGSE iff gradient_time.txt exists */
 
 /* Lattice walls: mirror (the reference, main.cu:249-265, 302-310) or periodic. */
@@ -81,6 +82,16 @@ typedef struct rms_config {
     /* PGSE (main_PGSE.cu:495-506) */
     int ngrad;
     const double* grad;        /* [ngrad*6]: Delta, delta, |g|, gx, gy, gz */
+    /* general waveforms (RMS_MODE_WAVEFORM; no reference counterpart): nwave
+     * waveforms, each piecewise constant on nbins equal time bins (TN must be
+     * a multiple of nbins); wave[(j*nbins + b)*3 + axis] = gamma*g in
+     * rad/(um ms).  Phase of walker and waveform j:
+     *   phi_j = dt * sum_b wave_j,b . X_b,  X_b = sum over the bin's steps of
+     *   the displacement (um) at the end of each step (the PGSE convention of
+     *   main_PGSE.cu:340-346). */
+    int nwave;
+    int nbins;
+    const double* wave;
     /* extensions; 0 selects the reference's value */
     int timepoints;            /* records; 0 -> 1000 (main.cu:35) */
     int nite;                  /* sub-segment cap per step; 0 -> 4 (main.cu:36) */
@@ -101,6 +112,9 @@ typedef struct rms_run_opts {
                                   k >= 1 = entry k of rms_split_variant() */
     int64_t walker_begin;      /* walk walkers [walker_begin, walker_end) of */
     int64_t walker_end;        /* the job; 0, 0 = all.  Lets ranks shard a job. */
+    float* traj_out;           /* RMS_MODE_WAVEFORM, SPLIT: optional DEVICE buffer
+                                  [walker - walker_begin][nbins][3] of the
+                                  per-bin displacement sums X_b (um) */
 } rms_run_opts;
 
 typedef struct rms_sim rms_sim;
@@ -118,6 +132,7 @@ typedef struct rms_sim rms_sim;
 #define RMS_FIELD_DIFFUSIVITY 7 /* [nc]           um^2/ms */
 #define RMS_FIELD_STEP 8        /* [nc]           step length in voxels */
 #define RMS_FIELD_PIJ 9         /* [nc*nc]        permeation probability a -> b */
+#define RMS_FIELD_SIGW 10       /* [nwave*2]      waveform signal: sum s0 cos phi, sum s0 sin phi */
 
 /* Build a simulation from a configuration (what main.cu:414-487 derives from
  * the text inputs).  Replaces: the input parsing + table set-up of

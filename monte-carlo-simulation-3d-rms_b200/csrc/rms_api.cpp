@@ -71,7 +71,7 @@ struct rms_device_state {
     int device = -1;
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
-    DevBuf labels, packed, axons, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
+    DevBuf labels, packed, axons, wavef, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
         ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos;
     HostPinned h_out;
     size_t labels_bytes = 0;
@@ -79,7 +79,7 @@ struct rms_device_state {
 
     ~rms_device_state() {
         if (device >= 0) cudaSetDevice(device);
-        for (DevBuf* b : {&labels, &packed, &axons, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
+        for (DevBuf* b : {&labels, &packed, &axons, &wavef, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
                           &tr_vox, &tr_ev, &tr_pos})
             b->release();
@@ -196,7 +196,8 @@ void fill_axon_desc(AxonDesc& x, const rms_sim* s, int64_t w0, int64_t w1, int64
 
 int finalize_config(rms_sim* s) {
     std::ostringstream m;
-    if (s->mode != RMS_MODE_NARROW && s->mode != RMS_MODE_PGSE) return set_error(RMS_ERR_ARG, "mode");
+    if (s->mode != RMS_MODE_NARROW && s->mode != RMS_MODE_PGSE && s->mode != RMS_MODE_WAVEFORM)
+        return set_error(RMS_ERR_ARG, "mode");
     if (!(s->dt > 0.0) || !std::isfinite(s->dt)) return set_error(RMS_ERR_RANGE, "dt must be > 0");
     if (s->tn < 1) return set_error(RMS_ERR_RANGE, "TN must be >= 1");
     if (s->npar < 1 || s->npar > (int64_t)1 << 40) return set_error(RMS_ERR_RANGE, "NPar out of range");
@@ -228,6 +229,13 @@ int finalize_config(rms_sim* s) {
     if ((int)s->bvec.size() != 3 * s->nbvec()) return set_error(RMS_ERR_ARG, "bvec needs 3 values per b-value");
     if (s->mode == RMS_MODE_PGSE && s->ngrad() > kMaxGrad) return set_error(RMS_ERR_RANGE, "Ngrad too large");
     if (s->grad.size() % 6) return set_error(RMS_ERR_ARG, "grad needs 6 values per gradient");
+    if (s->mode == RMS_MODE_WAVEFORM) {
+        if (s->nbins < 1 || s->tn % s->nbins) return set_error(RMS_ERR_RANGE, "waveforms need TN to be a multiple of nbins >= 1");
+        if (s->nwave < 1 || s->nwave > kMaxGrad) return set_error(RMS_ERR_RANGE, "nwave out of range");
+        if (s->wave.size() != (size_t)s->nwave * s->nbins * 3) return set_error(RMS_ERR_ARG, "wave needs nwave*nbins*3 values");
+        for (double x : s->wave)
+            if (!std::isfinite(x)) return set_error(RMS_ERR_RANGE, "waveform values must be finite");
+    }
 
     const int nc = s->nc;
     s->tstep = s->tn / s->timepoints;                       // main.cu:68
@@ -362,7 +370,7 @@ int prepare_lattice(rms_sim* s, cudaStream_t st, bool split, int bits) {
 bool same_schedule(const rms_sim* a, const rms_sim* b) {
     return a->mode == b->mode && a->tn == b->tn && a->dt == b->dt && a->timepoints == b->timepoints &&
            a->tstep == b->tstep && a->nite == b->nite && a->boundary == b->boundary && a->bval == b->bval &&
-           a->bvec == b->bvec && a->grad == b->grad;
+           a->bvec == b->bvec && a->grad == b->grad && a->nbins == b->nbins && a->wave == b->wave;
 }
 
 // Run one launch: COMPAT (one simulation) or SPLIT (one or more simulations,
@@ -373,6 +381,11 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     const int prec = o ? o->precision : RMS_PREC_COMPAT;
     if (prec != RMS_PREC_COMPAT && prec != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "precision");
     if (prec == RMS_PREC_COMPAT && jobs.size() != 1) return set_error(RMS_ERR_ARG, "a COMPAT launch walks one simulation");
+    if (prec == RMS_PREC_COMPAT && s->mode == RMS_MODE_WAVEFORM)
+        return set_error(RMS_ERR_ARG, "general waveforms are walked by the SPLIT walk");
+    float* traj = o ? o->traj_out : nullptr;
+    if (traj && (s->mode != RMS_MODE_WAVEFORM || prec != RMS_PREC_SPLIT || jobs.size() != 1))
+        return set_error(RMS_ERR_ARG, "trajectory output needs a one-simulation SPLIT run in waveform mode");
     const int device = o ? o->device : 0;
     for (LaunchJob& j : jobs) {
         if (!j.s->have_lattice) return set_error(RMS_ERR_STATE, "no lattice: call rms_sim_set_lattice or load a run directory");
@@ -417,7 +430,10 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     const int T = s->timepoints;
     const int nb = s->nbvec();
     const int nvals = (s->mode == RMS_MODE_NARROW) ? kRowHead + ((nb + 31) / 32) * 32 : kRowHead;
-    const int ngrad = s->ngrad();
+    const bool wavemode = s->mode == RMS_MODE_WAVEFORM;
+    const bool has_sig = s->mode != RMS_MODE_NARROW;
+    // signal row: PGSE, one value per gradient; waveforms, (cos, sin) per waveform
+    const int ngrad = wavemode ? 2 * s->nwave : s->ngrad();
     const int ngrad_pad = std::max(32, ((ngrad + 31) / 32) * 32);
     const size_t row = (size_t)T * nvals;
 
@@ -442,6 +458,15 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     RMS_CUDA(upload(d->ev_step, s->ev_step, st));
     RMS_CUDA(upload(d->ev_pair, s->ev_pair, st));
     RMS_CUDA(upload(d->ev_coef, s->ev_coef, st));
+    if (wavemode) {
+        // [bin][waveform][axis], scaled by dt: the phase per um of X_b
+        std::vector<double> wf((size_t)s->nbins * s->nwave * 3);
+        for (int j = 0; j < s->nwave; ++j)
+            for (int b = 0; b < s->nbins; ++b)
+                for (int x = 0; x < 3; ++x)
+                    wf[((size_t)b * s->nwave + j) * 3 + x] = s->wave[((size_t)j * s->nbins + b) * 3 + x] * s->dt;
+        RMS_CUDA(upload(d->wavef, wf, st));
+    }
     if (prec == RMS_PREC_SPLIT) {
         axons.resize(naxons);
         for (int k = 0; k < naxons; ++k)
@@ -457,12 +482,13 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     if (multi) RMS_CUDA(cudaMemsetAsync(d->out.p, 0, (size_t)naxons * row * sizeof(double), st));
     RMS_CUDA(d->err.ensure(sizeof(int)));
     RMS_CUDA(cudaMemsetAsync(d->err.p, 0, sizeof(int), st));
-    if (s->mode == RMS_MODE_PGSE) {
+    if (has_sig) {
         RMS_CUDA(d->sig_slots.ensure((size_t)nseg * ngrad_pad * sizeof(double)));
         RMS_CUDA(cudaMemsetAsync(d->sig_slots.p, 0, (size_t)nseg * ngrad_pad * sizeof(double), st));
         RMS_CUDA(d->out_sig.ensure((size_t)naxons * ngrad_pad * sizeof(double)));
         if (multi) RMS_CUDA(cudaMemsetAsync(d->out_sig.p, 0, (size_t)naxons * ngrad_pad * sizeof(double), st));
-        RMS_CUDA(d->vscr.ensure(std::max<size_t>((size_t)s->npairs * 3 * nthr * sizeof(double), 16)));
+        const size_t per_thread = wavemode ? (size_t)s->nwave : (size_t)s->npairs * 3;
+        RMS_CUDA(d->vscr.ensure(std::max<size_t>(per_thread * nthr * sizeof(double), 16)));
     }
     if (trace_n) {
         RMS_CUDA(d->tr_init.ensure((size_t)trace_n * sizeof(int32_t)));
@@ -496,6 +522,11 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     a.axons = d->axons.as<AxonDesc>();
     a.naxons = naxons;
     a.ntiles = ntiles;
+    a.nwave = wavemode ? s->nwave : 0;
+    a.nbins = wavemode ? s->nbins : 0;
+    a.bin_steps = wavemode ? s->tn / s->nbins : 0;
+    a.wave = d->wavef.as<double>();
+    a.traj = traj;
     a.out_rows = d->out.as<double>();
     a.out_sig = d->out_sig.as<double>();
     if (!axons.empty()) a.axon0 = axons[0];
@@ -511,7 +542,7 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     if (!multi) {
         // one axon: the warps' rows summed in a fixed order (repeatable)
         e = launch_reduce_slots(a.slots, nseg, row, d->out.as<double>(), st);
-        if (!e && s->mode == RMS_MODE_PGSE)
+        if (!e && has_sig)
             e = launch_reduce_slots(a.sig_slots, nseg, (size_t)ngrad_pad, d->out_sig.as<double>(), st);
         if (e) return cuda_fail((cudaError_t)e, "reduce launch");
     }
@@ -522,7 +553,7 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     RMS_CUDA(d->h_out.ensure((nrow + nsig + 1) * sizeof(double)));
     double* h = static_cast<double*>(d->h_out.p);
     RMS_CUDA(cudaMemcpyAsync(h, d->out.p, nrow * sizeof(double), cudaMemcpyDeviceToHost, st));
-    if (s->mode == RMS_MODE_PGSE)
+    if (has_sig)
         RMS_CUDA(cudaMemcpyAsync(h + nrow, d->out_sig.p, nsig * sizeof(double), cudaMemcpyDeviceToHost, st));
     int* herr = reinterpret_cast<int*>(h + nrow + nsig);
     RMS_CUDA(cudaMemcpyAsync(herr, d->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -566,6 +597,8 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
         }
         sk->sig.assign(sk->mode == RMS_MODE_PGSE ? ngrad : 0, 0.0);
         for (int q = 0; q < (int)sk->sig.size(); ++q) sk->sig[q] = h[nrow + (size_t)k * ngrad_pad + q];
+        sk->sigw.assign(wavemode ? ngrad : 0, 0.0);
+        for (int q = 0; q < (int)sk->sigw.size(); ++q) sk->sigw[q] = h[nrow + (size_t)k * ngrad_pad + q];
         sk->trace_n = k == 0 ? trace_n : 0;
         sk->walk_ms = ms_walk;
         sk->run_ms = ms_run;
@@ -597,6 +630,7 @@ bool field_size(const rms_sim* s, int field, size_t& n) {
         case RMS_FIELD_DIFFUSIVITY: n = s->nc; return true;
         case RMS_FIELD_STEP: n = s->nc; return true;
         case RMS_FIELD_PIJ: n = (size_t)s->nc * s->nc; return true;
+        case RMS_FIELD_SIGW: n = s->mode == RMS_MODE_WAVEFORM ? (size_t)2 * s->nwave : 0; return true;
         default: return false;
     }
 }
@@ -641,8 +675,13 @@ int rms_sim_create(const rms_config* cfg, rms_sim** out) {
     if (cfg->mode == RMS_MODE_NARROW) {
         ok = ok && cfg->nbvec >= 0 && copy(cfg->bval, cfg->nbvec, s->bval) &&
              copy(cfg->bvec, (size_t)cfg->nbvec * 3, s->bvec);
-    } else {
+    } else if (cfg->mode == RMS_MODE_PGSE) {
         ok = ok && cfg->ngrad >= 0 && copy(cfg->grad, (size_t)cfg->ngrad * 6, s->grad);
+    } else if (cfg->mode == RMS_MODE_WAVEFORM) {
+        ok = ok && cfg->nwave >= 0 && cfg->nbins >= 0 &&
+             copy(cfg->wave, (size_t)cfg->nwave * cfg->nbins * 3, s->wave);
+        s->nwave = cfg->nwave;
+        s->nbins = cfg->nbins;
     }
     if (cfg->permeation == RMS_PERM_TABLE) ok = ok && copy(cfg->pij, (size_t)nc * nc, s->pij_in);
     if (!ok) { delete s; return set_error(RMS_ERR_ARG, "missing array for a non-zero count"); }
@@ -760,6 +799,7 @@ int rms_sim_get(const rms_sim* s, int field, double* out, size_t n) {
         case RMS_FIELD_SIGRE: v = &s->sigre; break;
         case RMS_FIELD_SIG: v = &s->sig; break;
         case RMS_FIELD_NPAR_COUNT: v = &s->npar_count; break;
+        case RMS_FIELD_SIGW: v = &s->sigw; break;
     }
     std::copy(v->begin(), v->end(), out);
     return RMS_OK;

@@ -75,6 +75,12 @@ struct WalkArgs {
     int64_t ntiles;
     double* out_rows;
     double* out_sig;
+    // general waveforms: phase per um of a bin's displacement sum (waveform x
+    // dt), [bin][waveform][axis]; optional per-walker bin means out,
+    // [walker - walker_begin][bin][axis] in um
+    int nwave, nbins, bin_steps;
+    const double* wave;
+    float* traj;
     AxonDesc axon0;             // the first axon, by value (read from kernel parameters)
     // traces (COMPAT)
     int64_t trace_n;

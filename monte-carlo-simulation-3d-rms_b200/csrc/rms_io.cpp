@@ -188,7 +188,7 @@ int write_run_dir(const rms_sim* s, const char* dir) {
     int rc;
     std::ofstream fs0, fdx2, fdx4, fsig, fnp;
     if ((rc = open("sig0.txt", fs0)) || (rc = open("dx2.txt", fdx2)) || (rc = open("dx4.txt", fdx4)) ||
-        (rc = open(s->mode == RMS_MODE_NARROW ? "sigRe.txt" : "sig.txt", fsig)) ||
+        (rc = open(s->mode == RMS_MODE_NARROW ? "sigRe.txt" : (s->mode == RMS_MODE_PGSE ? "sig.txt" : "sigw.txt"), fsig)) ||
         (rc = open("NPar_count.txt", fnp)))
         return rc;
     fs0.precision(15);
@@ -219,6 +219,9 @@ int write_run_dir(const rms_sim* s, const char* dir) {
     }
     if (s->mode == RMS_MODE_PGSE) {                    // main_PGSE.cu:649-651
         for (int i = 0; i < s->ngrad(); i++) fsig << s->sig[i] << std::endl;
+    }
+    if (s->mode == RMS_MODE_WAVEFORM) {                // extension: one row "cos<TAB>sin" per waveform
+        for (int i = 0; i < s->nwave; i++) fsig << s->sigw[2 * i] << "\t" << s->sigw[2 * i + 1] << std::endl;
     }
     for (std::ofstream* f : {&fs0, &fdx2, &fdx4, &fsig, &fnp}) {
         f->close();

@@ -17,7 +17,8 @@ struct rms_sim {
     int nc = 0;
     double res = 0.0;
     int n1 = 0, n2 = 0, n3 = 0;
-    std::vector<double> diffusivity, t2, bval, bvec, grad, pij_in;
+    std::vector<double> diffusivity, t2, bval, bvec, grad, pij_in, wave;
+    int nwave = 0, nbins = 0;
     int timepoints = 1000, nite = 4, boundary = RMS_BOUNDARY_MIRROR,
         permeation = RMS_PERM_REFERENCE;
     double kappa = 0.0;
@@ -47,7 +48,7 @@ struct rms_sim {
 
     // results of the last run
     bool have_results = false;
-    std::vector<double> sig0, dx2, dx4, sigre, sig, npar_count;
+    std::vector<double> sig0, dx2, dx4, sigre, sig, sigw, npar_count;
     int64_t trace_n = 0;
     std::vector<int32_t> tr_init, tr_vox;
     std::vector<uint32_t> tr_ev;

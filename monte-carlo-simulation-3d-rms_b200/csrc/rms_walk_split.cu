@@ -109,6 +109,42 @@ __device__ __noinline__ void flush_rows(double* slot, double* sig_slot, double* 
     }
 }
 
+// General waveforms, at the end of bin `bin`: X (voxels) is the bin's
+// displacement sum; every waveform's phase gets wave_b . X res, and the bin's
+// mean displacement (um) goes to the trajectory output when one is given.
+__device__ __noinline__ void wave_bin(const double* __restrict__ wave, int nwave, int bin, double X0, double X1,
+                                      double X2, double res, double* ph, int nthr, float* traj, int64_t tw,
+                                      int nbins, int bin_steps) {
+    const double x0 = X0 * res, x1 = X1 * res, x2 = X2 * res;
+    const double* wv = wave + (size_t)bin * nwave * 3;
+    for (int j = 0; j < nwave; ++j) ph[(size_t)j * nthr] += wv[3 * j] * x0 + wv[3 * j + 1] * x1 + wv[3 * j + 2] * x2;
+    if (traj && tw >= 0) {
+        float* t = traj + ((size_t)tw * nbins + bin) * 3;
+        const double inv = 1.0 / (double)bin_steps;
+        t[0] = (float)(x0 * inv); t[1] = (float)(x1 * inv); t[2] = (float)(x2 * inv);
+    }
+}
+
+// General waveforms, after the last step: the warp's sums of s0 cos(phase) and
+// s0 sin(phase) per waveform, (cos, sin) pairs into the signal row.
+__device__ __noinline__ void wave_final(const double* ph, int nthr, int nwave, double s0, double* sig_slot,
+                                        int lane) {
+    for (int base = 0; base < 2 * nwave; base += 32) {
+        double mine = 0.0;
+        const int cnt = min(32, 2 * nwave - base);
+        for (int k = 0; k < cnt; k += 2) {
+            const int j = (base + k) >> 1;
+            double sn, cs;
+            sincos(ph[(size_t)j * nthr], &sn, &cs);
+            const double rc = warp_sum(s0 * cs);
+            const double rs = warp_sum(s0 * sn);
+            if (lane == k) mine = rc;
+            if (lane == k + 1) mine = rs;
+        }
+        if (lane < cnt) sig_slot[base + lane] += mine;
+    }
+}
+
 // ONE: the launch has one axon, whose scalars are read from the kernel
 // parameters (a.axon0) instead of being held in registers.
 template <int NCMAX, int BITS, int BLOCK, int MINB, bool ONE>
@@ -125,6 +161,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     const int nwarps = nthr >> 5;
     float* tab = s_tab[threadIdx.x >> 5];
     const bool pgse = (a.mode == 1);
+    const bool wave = (a.mode == 2);
+    const bool sums = pgse || wave;   // displacement sums over the walk
     const bool mirror = (a.boundary == 0);
     constexpr int kWall = wall_code<BITS>();
 
@@ -141,7 +179,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     // else the axon table (read where used, so it holds no registers)
 #define AXF(f) (ONE ? a.axon0.f : a.axons[ax].f)
     double* slot = a.slots + (size_t)warp_global * a.timepoints * a.nvals;
-    double* sig_slot = pgse ? a.sig_slots + (size_t)warp_global * a.ngrad_pad : nullptr;
+    double* sig_slot = sums ? a.sig_slots + (size_t)warp_global * a.ngrad_pad : nullptr;
 
     for (int64_t tile = warp_global; tile < a.ntiles; tile += nwarps) {
         if (!ONE) {
@@ -153,7 +191,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         if (held != ax) {
             if (!ONE && held >= 0)
                 flush_rows(slot, sig_slot, a.out_rows + (size_t)held * a.timepoints * a.nvals,
-                           pgse ? a.out_sig + (size_t)held * a.ngrad_pad : nullptr,
+                           sums ? a.out_sig + (size_t)held * a.ngrad_pad : nullptr,
                            (size_t)a.timepoints * a.nvals, a.ngrad, lane);   // previous axon's records to its totals
             held = ax;
             // this axon's tables into the warp's shared memory
@@ -219,12 +257,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
 
         double w64 = 0.0;          // T2 exponent, folded
         float w32 = 0.0f;          // T2 exponent since the last fold
-        double P0 = 0.0, P1 = 0.0, P2 = 0.0;   // PGSE displacement sums (voxels), folded
+        double P0 = 0.0, P1 = 0.0, P2 = 0.0;   // displacement sums (voxels), folded
         float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f;
-        int evi = 0;
-        int next_ev = (pgse && a.nevents > 0) ? a.ev_step[0] : -1;
-        if (pgse)
-            for (int k = 0; k < a.npairs * 3; ++k) a.vscr[(size_t)k * nthr + gtid] = 0.0;
+        int evi = 0;   // next PGSE event, or current waveform bin
+        int next_ev = pgse ? (a.nevents > 0 ? a.ev_step[0] : -1) : (wave ? a.bin_steps : -1);
+        if (sums)
+            for (int k = 0; k < (pgse ? a.npairs * 3 : a.nwave); ++k) a.vscr[(size_t)k * nthr + gtid] = 0.0;
         uint32_t spare_u1 = 0u, spare_u2 = 0u;
 
         for (int i = 0; i < a.tn; ++i) {
@@ -349,8 +387,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
             const float o1 = (up & 2u) ? 1.0f - d1 : d1;
             const float o2 = (up & 4u) ? 1.0f - d2 : d2;
 
-            if (pgse) {
-                // displacement sums (voxels) over the lobes
+            if (sums) {
+                // displacement sums (voxels): PGSE, prefix sums read at the
+                // lobe edges; waveforms, one sum per time bin
                 p0 += (float)D0 + (o0 - Fm0);
                 p1 += (float)D1 + (o1 - Fm1);
                 p2 += (float)D2 + (o2 - Fm2);
@@ -359,7 +398,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     P0 += (double)p0; P1 += (double)p1; P2 += (double)p2;
                     p0 = p1 = p2 = 0.0f;
                 }
-                if (event) {
+                if (event && wave) {
+                    wave_bin(a.wave, a.nwave, evi, P0, P1, P2, (double)AXF(res), a.vscr + gtid, nthr, a.traj,
+                             active ? w - AXF(walker_begin) : -1, a.nbins, a.bin_steps);
+                    P0 = P1 = P2 = 0.0;
+                    ++evi;
+                    next_ev += a.bin_steps;
+                } else if (event) {
                     do {
                         const double cf = a.ev_coef[evi];
                         double* vv = a.vscr + (size_t)(a.ev_pair[evi] * 3) * nthr + gtid;
@@ -370,7 +415,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     } while (evi < a.nevents && a.ev_step[evi] == i + 1);
                     next_ev = (evi < a.nevents) ? a.ev_step[evi] : -1;
                 }
-                if (i == a.tn - 1) {
+                if (i == a.tn - 1 && wave) {
+                    wave_final(a.vscr + gtid, nthr, a.nwave, active ? exp(-(w64 + (double)w32)) : 0.0, sig_slot, lane);
+                } else if (i == a.tn - 1) {
                     // final T2-weighted signal: phase_j = |g| (g_hat . V) res dt
                     const double s0 = active ? exp(-(w64 + (double)w32)) : 0.0;
                     const double scale = a.res * a.dt;
@@ -426,7 +473,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                         if (lane >= 16) r = rb;
                     }
                     row[lane] += r;
-                    if (!pgse) {
+                    if (!sums) {
                         for (int base = 0; base < a.nbvec; base += 32) {
                             double mine = 0.0;
                             const int cnt = min(32, a.nbvec - base);
@@ -447,7 +494,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     }
     if (!ONE && held >= 0)
         flush_rows(slot, sig_slot, a.out_rows + (size_t)held * a.timepoints * a.nvals,
-                   pgse ? a.out_sig + (size_t)held * a.ngrad_pad : nullptr, (size_t)a.timepoints * a.nvals, a.ngrad,
+                   sums ? a.out_sig + (size_t)held * a.ngrad_pad : nullptr, (size_t)a.timepoints * a.nvals, a.ngrad,
                    lane);
 }
 

@@ -16,12 +16,12 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "_build", "librms.so")
 CLI_PATH = os.path.join(PKG_DIR, "_build", "rms_main")
 
-MODE = {"narrow": 0, "pgse": 1, "auto": -1}
+MODE = {"narrow": 0, "pgse": 1, "waveform": 2, "auto": -1}
 BOUNDARY = {"mirror": 0, "periodic": 1}
 PERMEATION = {"reference": 0, "kappa": 1, "table": 2}
 PRECISION = {"compat": 0, "split": 1}
 FIELD = {"sig0": 0, "dx2": 1, "dx4": 2, "sigre": 3, "sig": 4, "npar_count": 5, "td": 6,
-         "diffusivity": 7, "step": 8, "pij": 9}
+         "diffusivity": 7, "step": 8, "pij": 9, "sigw": 10}
 ERRORS = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "RANGE", -5: "CUDA", -6: "NOMEM",
           -7: "STATE", -8: "TIMEOUT"}
 
@@ -49,6 +49,7 @@ class Config(C.Structure):
         ("diffusivity", _DP), ("t2", _DP),
         ("nbvec", C.c_int), ("bval", _DP), ("bvec", _DP),
         ("ngrad", C.c_int), ("grad", _DP),
+        ("nwave", C.c_int), ("nbins", C.c_int), ("wave", _DP),
         ("timepoints", C.c_int), ("nite", C.c_int), ("boundary", C.c_int),
         ("permeation", C.c_int), ("kappa", C.c_double), ("pij", _DP),
     ]
@@ -59,6 +60,7 @@ class RunOpts(C.Structure):
         ("seed", C.c_uint64), ("precision", C.c_int), ("device", C.c_int),
         ("stream", C.c_void_p), ("trace_walkers", C.c_int), ("variant", C.c_int),
         ("walker_begin", C.c_int64), ("walker_end", C.c_int64),
+        ("traj_out", C.c_void_p),
     ]
 
 
@@ -119,12 +121,20 @@ class Sim:
     """One simulation (an ``rms_sim``): configuration, lattice, results."""
 
     def __init__(self, labels=None, *, dt, tn, npar, res, diffusivity, t2, nc=None,
-                 shape=None, bval=None, bvec=None, grad=None, timepoints=0, nite=0,
+                 shape=None, bval=None, bvec=None, grad=None, wave=None, timepoints=0, nite=0,
                  boundary="mirror", permeation="reference", kappa=0.0, pij=None):
+        """``wave``: general waveforms, array [nwave, nbins, 3] (phase per um of
+        a bin's displacement sum, per ms: phase_j = dt sum_b wave[j, b] . X_b);
+        selects the waveform mode (SPLIT walk only)."""
         self._h = C.c_void_p()
         d = _arr(diffusivity)
         t2a = _arr(t2)
-        mode = "pgse" if grad is not None else "narrow"
+        mode = "waveform" if wave is not None else ("pgse" if grad is not None else "narrow")
+        wv = None
+        if wave is not None:
+            wv = np.ascontiguousarray(np.asarray(wave, dtype=np.float64))
+            if wv.ndim != 3 or wv.shape[2] != 3:
+                raise ValueError("wave must be [nwave, nbins, 3]")
         if labels is not None:
             labels = np.ascontiguousarray(labels, dtype=np.uint8)
             shape = labels.shape
@@ -135,11 +145,13 @@ class Sim:
         bvc = _arr(bvec if bvec is not None else [])
         gr = _arr(grad if grad is not None else [])
         pj = _arr(pij) if pij is not None else None
-        self._keep += [bv, bvc, gr, pj]
+        self._keep += [bv, bvc, gr, pj, wv]
         cfg = Config(MODE[mode], float(dt), int(tn), int(npar), int(nc or d.size), float(res),
                      int(shape[0]), int(shape[1]), int(shape[2]), _ptr(d), _ptr(t2a),
                      bv.size if mode == "narrow" else 0, _ptr(bv), _ptr(bvc),
                      gr.size // 6 if mode == "pgse" else 0, _ptr(gr),
+                     wv.shape[0] if wv is not None else 0, wv.shape[1] if wv is not None else 0,
+                     _ptr(wv.reshape(-1)) if wv is not None else None,
                      int(timepoints), int(nite), BOUNDARY[boundary], PERMEATION[permeation],
                      float(kappa), _ptr(pj))
         _check(lib().rms_sim_create(C.byref(cfg), C.byref(self._h)))
@@ -171,11 +183,14 @@ class Sim:
                                          *[int(x) for x in lab.shape]))
 
     def run(self, seed: int = 0, precision: str = "compat", device: int = 0, stream=None,
-            trace_walkers: int = 0, variant: int = 0, walker_range=None):
+            trace_walkers: int = 0, variant: int = 0, walker_range=None, traj_out: int = 0):
+        """``traj_out``: device address of a float32 [walkers, nbins, 3] buffer
+        for the bins' mean displacements (waveform mode, SPLIT)."""
         w0, w1 = walker_range if walker_range is not None else (0, 0)
         st = None if stream is None else C.c_void_p(int(stream))
         opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION[precision], int(device), st,
-                       int(trace_walkers), int(variant), int(w0), int(w1))
+                       int(trace_walkers), int(variant), int(w0), int(w1),
+                       C.c_void_p(int(traj_out)) if traj_out else None)
         _check(lib().rms_sim_run(self._h, C.byref(opts)))
         return self
 
@@ -209,8 +224,10 @@ class Sim:
         o["npar_count"] = self.get("npar_count").reshape(T, nc)
         if self.mode == "narrow":
             o["sigre"] = self.get("sigre").reshape(T, -1)
-        else:
+        elif self.mode == "pgse":
             o["sig"] = self.get("sig")
+        else:
+            o["sigw"] = self.get("sigw").reshape(-1, 2)
         return o
 
     def trace(self, nwalkers: int) -> dict:

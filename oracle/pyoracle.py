@@ -21,7 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "librmsref.so")
 
-MODE_NARROW, MODE_PGSE = 0, 1
+MODE_NARROW, MODE_PGSE, MODE_WAVEFORM = 0, 1, 2
 BOUNDARY_MIRROR, BOUNDARY_PERIODIC = 0, 1
 
 
@@ -34,18 +34,19 @@ class OrParams(C.Structure):
         ("pij", C.POINTER(C.c_double)), ("labels", C.POINTER(C.c_uint8)),
         ("nbvec", C.c_int), ("bval", C.POINTER(C.c_double)), ("bvec", C.POINTER(C.c_double)),
         ("td", C.POINTER(C.c_double)), ("ngrad", C.c_int), ("grad", C.POINTER(C.c_double)),
+        ("nwave", C.c_int), ("nbins", C.c_int), ("wave", C.POINTER(C.c_double)),
     ]
 
 
 class OrOutputs(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in
-                ("sig0", "dx2", "dx4", "sigre", "sig", "npar_count")]
+                ("sig0", "dx2", "dx4", "sigre", "sig", "npar_count", "sigw")]
 
 
 class OrTrace(C.Structure):
     _fields_ = [("w0", C.c_int64), ("nw", C.c_int64), ("init_voxel", C.POINTER(C.c_int32)),
                 ("voxel", C.POINTER(C.c_int32)), ("events", C.POINTER(C.c_uint32)),
-                ("pos", C.POINTER(C.c_double))]
+                ("pos", C.POINTER(C.c_double)), ("binmean", C.POINTER(C.c_double))]
 
 
 _lib = None
@@ -112,7 +113,7 @@ class Job:
 
     def __init__(self, labels, *, dt, tn, npar, res, step, t2_steps, pij, seed,
                  timepoints=1000, nite=4, boundary=BOUNDARY_MIRROR,
-                 bval=None, bvec=None, td=None, grad=None):
+                 bval=None, bvec=None, td=None, grad=None, wave=None):
         self.labels = np.ascontiguousarray(labels, dtype=np.uint8)
         self.n1, self.n2, self.n3 = self.labels.shape
         self.dt, self.tn, self.npar, self.res = float(dt), int(tn), int(npar), float(res)
@@ -122,7 +123,10 @@ class Job:
         self.nc = self.step.size
         self.seed = int(seed)
         self.timepoints, self.nite, self.boundary = int(timepoints), int(nite), int(boundary)
-        self.mode = MODE_PGSE if grad is not None else MODE_NARROW
+        self.mode = MODE_WAVEFORM if wave is not None else (MODE_PGSE if grad is not None else MODE_NARROW)
+        # general waveforms [nwave, nbins, 3] (split replay only)
+        self.wave = np.ascontiguousarray(wave if wave is not None else np.zeros((0, 0, 3)), dtype=np.float64)
+        self.nwave, self.nbins = (self.wave.shape[0], self.wave.shape[1]) if wave is not None else (0, 0)
         self.bval = np.ascontiguousarray(bval if bval is not None else np.zeros(0), dtype=np.float64)
         self.bvec = np.ascontiguousarray(bvec if bvec is not None else np.zeros(0), dtype=np.float64).reshape(-1)
         self.nbvec = self.bval.size if self.mode == MODE_NARROW else 0
@@ -140,17 +144,17 @@ class Job:
             _dp(self.step), _dp(self.t2), _dp(self.pij),
             self.labels.ctypes.data_as(C.POINTER(C.c_uint8)),
             self.nbvec, _dp(self.bval), _dp(self.bvec), _dp(self.td),
-            self.ngrad, _dp(self.grad))
+            self.ngrad, _dp(self.grad), self.nwave, self.nbins, _dp(self.wave))
 
     def empty_outputs(self):
         T = self.timepoints
         return dict(sig0=np.zeros(T), dx2=np.zeros((T, 6)), dx4=np.zeros((T, 15)),
                     sigre=np.zeros((T, max(self.nbvec, 0))), sig=np.zeros(self.ngrad),
-                    npar_count=np.zeros((T, self.nc)))
+                    npar_count=np.zeros((T, self.nc)), sigw=np.zeros((max(self.nwave, 0), 2)))
 
 
 def _out_struct(o):
-    return OrOutputs(*(_dp(o[k]) for k in ("sig0", "dx2", "dx4", "sigre", "sig", "npar_count")))
+    return OrOutputs(*(_dp(o[k]) for k in ("sig0", "dx2", "dx4", "sigre", "sig", "npar_count", "sigw")))
 
 
 def run_oracle(job: Job, w_begin: int = 0, w_end: Optional[int] = None, nthreads: int = 1,
@@ -174,11 +178,12 @@ def run_oracle(job: Job, w_begin: int = 0, w_end: Optional[int] = None, nthreads
         tr_vox = np.zeros((nw, job.tn), dtype=np.int32)
         tr_ev = np.zeros((nw, job.tn), dtype=np.uint32)
         tr_pos = np.zeros((nw, job.tn, 3))
+        tr_bin = np.zeros((nw, max(job.nbins, 1), 3))
         tr = OrTrace(w_begin, nw, tr_init.ctypes.data_as(C.POINTER(C.c_int32)),
                      tr_vox.ctypes.data_as(C.POINTER(C.c_int32)),
-                     tr_ev.ctypes.data_as(C.POINTER(C.c_uint32)), _dp(tr_pos))
+                     tr_ev.ctypes.data_as(C.POINTER(C.c_uint32)), _dp(tr_pos), _dp(tr_bin))
         rc = run1(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.byref(outs), C.byref(tr))
-        o["trace"] = dict(init_voxel=tr_init, voxel=tr_vox, events=tr_ev, pos=tr_pos)
+        o["trace"] = dict(init_voxel=tr_init, voxel=tr_vox, events=tr_ev, pos=tr_pos, binmean=tr_bin)
     elif nthreads > 1:
         rc = runp(C.byref(p), C.c_int64(w_begin), C.c_int64(w_end), C.c_int(nthreads), C.byref(outs))
     else:

@@ -30,6 +30,7 @@ static int check(const or_params* p) {
     if (p->n1 < 1 || p->n2 < 1 || p->n3 < 1) return -4;
     if (p->mode == OR_MODE_PGSE && p->ngrad < 0) return -5;
     if (p->mode == OR_MODE_NARROW && p->nbvec < 0) return -5;
+    if (p->mode == OR_MODE_WAVEFORM && (p->nwave < 1 || p->nbins < 1 || p->tn % p->nbins)) return -6;
     return 0;
 }
 
@@ -278,7 +279,8 @@ static int homogeneous(const or_params* p, const int g[3]) {
 }
 
 static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, double* phase,
-                           int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev, double* tr_pos) {
+                           int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev, double* tr_pos,
+                           double* tr_bin) {
     const int Nc = p->nc;
     /* free flight applies when same-label faces are always crossed, no walker
      * can enter compartment 0, and three crossings fit the sub-segment cap */
@@ -308,6 +310,8 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
     int ai = APix[lin(p, g[0], g[1], g[2])];
     if (tr_init) *tr_init = (int32_t)lin(p, g[0], g[1], g[2]);
     double wexp = 0.0;   /* T2 exponent */
+    double X[3] = {0.0, 0.0, 0.0};   /* waveform mode: the current bin's displacement sum (um) */
+    const int bin_steps = p->mode == OR_MODE_WAVEFORM ? p->tn / p->nbins : 0;
     for (int i = 0; i < p->tn; i++) {
         float u1f, u2f;
         or_dir_uniforms(p->seed, (uint64_t)w, (uint32_t)i, &u1f, &u2f);
@@ -411,6 +415,26 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
                 for (int jg = 0; jg < p->ngrad; jg++) out->sig[jg] += s0 * cos(phase[jg]);
             }
         }
+        if (p->mode == OR_MODE_WAVEFORM) {
+            X[0] += dx; X[1] += dy; X[2] += dz;
+            if ((i + 1) % bin_steps == 0) {
+                const int b = (i + 1) / bin_steps - 1;
+                for (int j = 0; j < p->nwave; j++) {
+                    const double* wv = p->wave + ((size_t)j * p->nbins + b) * 3;
+                    phase[j] += p->dt * (wv[0] * X[0] + wv[1] * X[1] + wv[2] * X[2]);
+                }
+                if (tr_bin)
+                    for (int a = 0; a < 3; a++) tr_bin[3 * b + a] = X[a] / (double)bin_steps;
+                X[0] = X[1] = X[2] = 0.0;
+            }
+            if (i == p->tn - 1) {
+                const double s0 = exp(-wexp);
+                for (int j = 0; j < p->nwave; j++) {
+                    out->sigw[2 * j] += s0 * cos(phase[j]);
+                    out->sigw[2 * j + 1] += s0 * sin(phase[j]);
+                }
+            }
+        }
         if ((i % Tstep) == 0) {
             const int tidx = i / Tstep;
             if (tidx >= p->timepoints) continue;
@@ -439,7 +463,7 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
 }
 
 typedef void (*walk_fn)(const or_params*, int64_t, or_outputs*, double*, int32_t*, int32_t*,
-                        uint32_t*, double*);
+                        uint32_t*, double*, double*);
 
 static int run_range(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
                      or_trace* tr, walk_fn fn);
@@ -451,31 +475,40 @@ int or_run_split(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs*
     return run_range(p, w_begin, w_end, out, tr, walk_one_split);
 }
 
+static void walk_one_ref(const or_params* p, int64_t w, or_outputs* out, double* phase, int32_t* ti,
+                         int32_t* tv, uint32_t* te, double* tp, double* tb) {
+    (void)tb;
+    walk_one(p, w, out, phase, ti, tv, te, tp);
+}
+
 int or_run(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
            or_trace* tr) {
     int rc = check(p);
     if (rc) return rc;
-    return run_range(p, w_begin, w_end, out, tr, walk_one);
+    if (p->mode == OR_MODE_WAVEFORM) return -6;   /* the reference's order has no waveform mode */
+    return run_range(p, w_begin, w_end, out, tr, walk_one_ref);
 }
 
 static int run_range(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
                      or_trace* tr, walk_fn fn) {
     double* phase = NULL;
-    if (p->mode == OR_MODE_PGSE && p->ngrad > 0) {
-        phase = (double*)malloc(sizeof(double) * (size_t)p->ngrad);
+    const int nph = p->mode == OR_MODE_PGSE ? p->ngrad : (p->mode == OR_MODE_WAVEFORM ? p->nwave : 0);
+    if (nph > 0) {
+        phase = (double*)malloc(sizeof(double) * (size_t)nph);
         if (!phase) return -10;
     }
     for (int64_t w = w_begin; w < w_end; ++w) {
-        if (phase) memset(phase, 0, sizeof(double) * (size_t)p->ngrad);
-        int32_t* ti = NULL; int32_t* tv = NULL; uint32_t* te = NULL; double* tp = NULL;
+        if (phase) memset(phase, 0, sizeof(double) * (size_t)nph);
+        int32_t* ti = NULL; int32_t* tv = NULL; uint32_t* te = NULL; double* tp = NULL; double* tb = NULL;
         if (tr && w >= tr->w0 && w < tr->w0 + tr->nw) {
             int64_t r = w - tr->w0;
             ti = tr->init_voxel + r;
             tv = tr->voxel + r * p->tn;
             te = tr->events + r * p->tn;
             if (tr->pos) tp = tr->pos + r * p->tn * 3;
+            if (tr->binmean && p->mode == OR_MODE_WAVEFORM) tb = tr->binmean + r * p->nbins * 3;
         }
-        fn(p, w, out, phase, ti, tv, te, tp);
+        fn(p, w, out, phase, ti, tv, te, tp, tb);
     }
     free(phase);
     return 0;
@@ -489,6 +522,7 @@ static void zero_outputs(const or_params* p, or_outputs* o) {
     if (p->mode == OR_MODE_NARROW && p->nbvec > 0)
         memset(o->sigre, 0, sizeof(double) * p->timepoints * p->nbvec);
     if (p->mode == OR_MODE_PGSE && p->ngrad > 0) memset(o->sig, 0, sizeof(double) * p->ngrad);
+    if (p->mode == OR_MODE_WAVEFORM) memset(o->sigw, 0, sizeof(double) * 2 * p->nwave);
 }
 
 static void add_outputs(const or_params* p, or_outputs* dst, const or_outputs* src) {
@@ -500,6 +534,8 @@ static void add_outputs(const or_params* p, or_outputs* dst, const or_outputs* s
         for (int i = 0; i < p->timepoints * p->nbvec; i++) dst->sigre[i] += src->sigre[i];
     if (p->mode == OR_MODE_PGSE)
         for (int i = 0; i < p->ngrad; i++) dst->sig[i] += src->sig[i];
+    if (p->mode == OR_MODE_WAVEFORM)
+        for (int i = 0; i < 2 * p->nwave; i++) dst->sigw[i] += src->sigw[i];
 }
 
 static int run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int nthreads,
@@ -522,7 +558,8 @@ static int run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int 
     if (nthreads < 1) nthreads = 1;
     size_t per = (size_t)p->timepoints * (1 + 6 + 15 + p->nc) +
                  (size_t)p->timepoints * (p->mode == OR_MODE_NARROW ? p->nbvec : 0) +
-                 (size_t)(p->mode == OR_MODE_PGSE ? p->ngrad : 0);
+                 (size_t)(p->mode == OR_MODE_PGSE ? p->ngrad : 0) +
+                 (size_t)(p->mode == OR_MODE_WAVEFORM ? 2 * p->nwave : 0);
     double* buf = (double*)calloc(per * (size_t)nthreads, sizeof(double));
     or_outputs* priv = (or_outputs*)calloc((size_t)nthreads, sizeof(or_outputs));
     if (!buf || !priv) { free(buf); free(priv); return -10; }
@@ -533,7 +570,8 @@ static int run_parallel(const or_params* p, int64_t w_begin, int64_t w_end, int 
         priv[t].dx4 = b; b += p->timepoints * 15;
         priv[t].npar_count = b; b += p->timepoints * p->nc;
         priv[t].sigre = b; if (p->mode == OR_MODE_NARROW) b += p->timepoints * p->nbvec;
-        priv[t].sig = b;
+        priv[t].sig = b; if (p->mode == OR_MODE_PGSE) b += p->ngrad;
+        priv[t].sigw = b;
     }
     int64_t n = w_end - w_begin;
     int err = 0;

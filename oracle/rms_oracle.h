@@ -22,6 +22,7 @@ extern "C" {
 
 #define OR_MODE_NARROW 0
 #define OR_MODE_PGSE 1
+#define OR_MODE_WAVEFORM 2   /* engine extension: general gradient waveforms */
 #define OR_BOUNDARY_MIRROR 0
 #define OR_BOUNDARY_PERIODIC 1
 
@@ -55,6 +56,10 @@ typedef struct or_params {
     /* PGSE */
     int ngrad;
     const double* grad;  /* [ngrad*6] Delta, delta, |g|, gx, gy, gz */
+    /* general waveforms (split replay only): phase_j = dt sum_b wave[j][b] . X_b,
+     * X_b = sum over bin b's steps of the displacement (um) after each step */
+    int nwave, nbins;
+    const double* wave;  /* [nwave*nbins*3] */
 } or_params;
 
 typedef struct or_outputs {
@@ -64,6 +69,7 @@ typedef struct or_outputs {
     double* sigre;       /* [timepoints*nbvec] narrow */
     double* sig;         /* [ngrad] PGSE */
     double* npar_count;  /* [timepoints*nc] */
+    double* sigw;        /* [nwave*2] waveform mode: sums of s0 cos(phase), s0 sin(phase) */
 } or_outputs;
 
 typedef struct or_trace {
@@ -73,6 +79,7 @@ typedef struct or_trace {
     int32_t* voxel;      /* [nw*tn] voxel after each step */
     uint32_t* events;    /* [nw*tn] event code of each step */
     double* pos;         /* [nw*tn*3] position (voxel units) after each step, or NULL */
+    double* binmean;     /* [nw*nbins*3] waveform mode: bin mean displacement (um), or NULL */
 } or_trace;
 
 /* Walk walkers [w_begin, w_end) in order, adding into *out (which the caller
