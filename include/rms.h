@@ -239,6 +239,29 @@ int rms_split_variant(int k, int* block, int* min_blocks_per_sm);
 int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint8_t* d_labels,
                         double* d_rows, double* d_sig);
 
+/* ---- Multi-waveform phase contraction -------------------------------------
+ * No counterpart in the reference (its only gradient form is the PGSE pair,
+ * hpc_code/lib/main_PGSE.cu:336-346, summed per step per gradient).  For
+ * walker positions sampled on time bins and many gradient waveforms:
+ *   d_pos   [nwalk][nbins][3] float, um (e.g. the trajectory output of a
+ *           RMS_MODE_WAVEFORM run: bin mean displacements)
+ *   d_wave  [nwave][nbins][3] float, phase per um of a bin's position
+ *           (gamma g times the bin's duration)
+ *   d_out   [nwave][2] double: sum over walkers of cos(phi), sin(phi),
+ *           phi[w][j] = sum_{b,axis} pos[w][b][axis] wave[j][b][axis]
+ * All three are device buffers on the current device; the call runs on
+ * `stream` and returns when the contraction has finished.  Methods:
+ * RMS_CONTRACT_FP32 (FP32 products and sums on the CUDA cores) and
+ * RMS_CONTRACT_BF16X3 (both operands split into BF16 hi + lo parts, three
+ * tensor-core products hi.hi + hi.lo + lo.hi summed in FP32; needs
+ * nbins % 4 == 0 and a 16-byte aligned d_pos).  Phases are reduced mod 2 pi in
+ * FP32 before the sine and cosine; the per-waveform sums are FP64.
+ * kernel_ms (optional, may be NULL) receives the kernel's device time. */
+#define RMS_CONTRACT_FP32 0
+#define RMS_CONTRACT_BF16X3 1
+int rms_contract_phases(const float* d_pos, int64_t nwalk, int nbins, const float* d_wave, int nwave, int method,
+                        double* d_out, void* stream, float* kernel_ms);
+
 /* Library version string. */
 const char* rms_version(void);
 

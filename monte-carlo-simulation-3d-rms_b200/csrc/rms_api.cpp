@@ -646,6 +646,19 @@ const char* rms_last_error(void) { return g_last_error.c_str(); }
 
 const char* rms_version(void) { return "rms_b200 0.1 (sm_100a)"; }
 
+int rms_contract_phases(const float* d_pos, int64_t nwalk, int nbins, const float* d_wave, int nwave, int method,
+                        double* d_out, void* stream, float* kernel_ms) {
+    const char* msg = nullptr;
+    const int rc = contract_phases(d_pos, nwalk, nbins, d_wave, nwave, method, d_out, stream, &msg, kernel_ms);
+    if (rc != RMS_OK) {
+        std::string m = std::string("contraction: ") + (msg ? msg : "failed");
+        const cudaError_t ce = cudaGetLastError();
+        if (rc == RMS_ERR_CUDA && ce != cudaSuccess) m += std::string(" (") + cudaGetErrorString(ce) + ")";
+        return set_error(rc, m);
+    }
+    return RMS_OK;
+}
+
 int rms_split_variant(int k, int* block, int* min_blocks_per_sm) {
     if (k < 1 || k > split_variant_count()) return set_error(RMS_ERR_ARG, "no such variant");
     if (block) *block = split_variant_block(k - 1);

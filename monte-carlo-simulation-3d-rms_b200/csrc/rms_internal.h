@@ -17,6 +17,7 @@ constexpr int kMaxTimepoints = 1 << 20;
 constexpr long long kInitTryCap = 1ll << 26;   // rejection-sampling attempts per walker
 constexpr int kErrInitCap = 1;                  // a walker found no labelled voxel in kInitTryCap tries
 constexpr int kErrStep = 2;                     // a segment found no face (step >= 1 voxel)
+constexpr int kErrTimeout = 4;                  // a bounded wait of a pipelined kernel ran out
 
 // One simulation ("axon") of a split-precision launch.  A launch walks the
 // tiles (32 walkers) of all its axons; axon k owns global tiles
@@ -110,5 +111,12 @@ int launch_reduce_slots(const double* slots, int nslots, size_t row, double* out
 int walk_compat_blocks_per_sm(int nc, bool trace);
 int walk_split_blocks_per_sm(int nc, int lattice_bits, int variant);
 const char* cuda_error_string(int code);
+
+// Multi-waveform phase contraction (rms_contract.cu): out[j] = (sum_w cos phi,
+// sum_w sin phi), phi[w][j] = sum_k pos[w][k] wave[j][k], K = 3 nbins.
+// method RMS_CONTRACT_FP32 or RMS_CONTRACT_BF16X3.  Returns an RMS_* status;
+// msg gets a reason on failure.
+int contract_phases(const float* d_pos, int64_t nwalk, int nbins, const float* d_wave, int nwave, int method,
+                    double* d_out, void* stream, const char** msg, float* kernel_ms);
 
 }  // namespace rms

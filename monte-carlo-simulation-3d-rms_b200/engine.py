@@ -31,7 +31,8 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_sim_write_dir",
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
-           "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc")
+           "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases")
+CONTRACT = {"fp32": 0, "bf16x3": 1}
 
 _DP = C.POINTER(C.c_double)
 
@@ -100,6 +101,8 @@ def lib():
         L.rms_sim_run_noalloc.argtypes = [C.c_void_p, C.POINTER(RunOpts), C.c_void_p, C.c_void_p, C.c_void_p]
         L.rms_rng_split.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.rms_split_variant.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.rms_contract_phases.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                          C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]
         _lib = L
     return _lib
 
@@ -273,6 +276,19 @@ def batch_run(sims, seed: int = 0, precision: str = "compat", device: int = 0, s
     st = None if stream is None else C.c_void_p(int(stream))
     opts = RunOpts(int(seed), PRECISION[precision], int(device), st, 0, 0, 0, 0)
     _check(lib().rms_batch_run(arr, len(sims), C.byref(opts)))
+
+
+def contract_phases(d_pos: int, nwalk: int, nbins: int, d_wave: int, nwave: int, d_out: int,
+                    method: str = "bf16x3", stream=None) -> float:
+    """Multi-waveform phase contraction on device buffers (raw device
+    addresses): d_pos float32 [nwalk, nbins, 3], d_wave float32
+    [nwave, nbins, 3], d_out float64 [nwave, 2] receives the sums of cos and
+    sin of phi = pos . wave.  Returns the kernel's device time (ms)."""
+    ms = C.c_float()
+    st = None if stream is None else C.c_void_p(int(stream))
+    _check(lib().rms_contract_phases(C.c_void_p(int(d_pos)), int(nwalk), int(nbins), C.c_void_p(int(d_wave)),
+                                     int(nwave), CONTRACT[method], C.c_void_p(int(d_out)), st, C.byref(ms)))
+    return ms.value
 
 
 def rng_doubles(seed: int, walker: int, n: int) -> np.ndarray:

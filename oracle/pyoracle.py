@@ -271,3 +271,19 @@ def run_reference_walkers(job: Job, nsample: int, nthreads: int):
 
 def ref_max_threads() -> int:
     return int(ref_lib().ref_max_threads())
+
+
+def contract_phases_fp64(pos, wave, chunk: int = 65536):
+    """FP64 restatement of the multi-waveform phase contraction
+    (rms_contract_phases): for float inputs pos [nwalk, nbins, 3] and
+    wave [nwave, nbins, 3], phi = pos . wave over (bin, axis) in float64, and
+    the per-waveform sums of cos(phi) and sin(phi), [nwave, 2].  Test
+    infrastructure: the checker of the GPU contraction."""
+    P = np.asarray(pos, dtype=np.float32).reshape(len(pos), -1).astype(np.float64)
+    W = np.asarray(wave, dtype=np.float32).reshape(len(wave), -1).astype(np.float64)
+    out = np.zeros((W.shape[0], 2))
+    for a in range(0, P.shape[0], chunk):
+        phi = P[a:a + chunk] @ W.T
+        out[:, 0] += np.cos(phi).sum(axis=0)
+        out[:, 1] += np.sin(phi).sum(axis=0)
+    return out
