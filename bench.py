@@ -17,7 +17,7 @@ Workload ``single``: the 64 x 64 x 512 single-axon lattice (labels 0/1),
 10 steps.  Inputs are synthetic and seeded.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision split|compat] [--workload batch|production|single]
+                  [--precision split|compat] [--workload batch|production|single|contraction]
                   [--plain-ratio]
 
 ``value``: walker-steps/s of the whole job, lattice already resident on the
@@ -514,6 +514,138 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+CONTRACT_METRIC = "walker-waveform phases/s of the multi-waveform phase contraction (signal mean(cos, sin))"
+
+
+def run_contraction(args):
+    """The multi-waveform phase contraction: positions of 1e7 walkers on 256
+    time bins x 3 axes (FP32, from the engine's own walk in waveform mode:
+    the 64x64x512 axon with label-2 exterior, kappa = 0.01 um/ms, 20480 steps
+    of dt = 5e-4 ms, bin means) contracted against 1024 seeded smooth random
+    waveforms with b in [0, 10] ms/um^2.  Times the BF16 hi/lo tensor-core
+    method (value) and the FP32 CUDA-core method, and states the signal error
+    of both against an FP64 evaluation on the first 65536 walkers, per b."""
+    import torch
+    from rms_b200 import engine, geometry, waveforms
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return   # one GPU: the positions of one walk fill 30.7 GB of its memory
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    nwalk = args.walkers or 10_000_000
+    nbins, nwave, per_bin, dt, D0 = 256, 1024, 80, 5e-4, 2.0
+    tn = nbins * per_bin
+    stream = torch.cuda.current_stream()
+    lab = geometry.axon_lattice(64, 64, 512, 0.1, seed=0, exterior=2)
+    dtb = dt * per_bin
+    w = waveforms.random_smooth(nwave, nbins, 1.0, seed=4)
+    b = np.linspace(0.0, 10.0, nwave)
+    w = waveforms.scale_to_b(w, dtb, np.maximum(b, 1e-9))
+    wave = np.ascontiguousarray((w * dtb).astype(np.float32))     # phase per um of a bin's position
+    # positions: the split walk's bin means (waveform mode, one zero waveform)
+    sim = engine.Sim(lab, dt=dt, tn=tn, npar=nwalk, res=0.1, diffusivity=[0.0, D0, D0], t2=[1e12] * 3,
+                     wave=np.zeros((1, nbins, 3)), timepoints=nbins, boundary="periodic",
+                     permeation="kappa", kappa=0.01)
+    pos = torch.empty((nwalk, nbins, 3), dtype=torch.float32, device="cuda")
+    sim.run(seed=5, precision="split", stream=stream.cuda_stream, traj_out=pos.data_ptr())
+    torch.cuda.synchronize()
+    d_wave = torch.from_numpy(wave).cuda()
+    out = torch.empty((nwave, 2), dtype=torch.float64, device="cuda")
+
+    def call(method, n=nwalk):
+        return engine.contract_phases(pos.data_ptr(), n, nbins, d_wave.data_ptr(), nwave, out.data_ptr(),
+                                      method=method, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        call("bf16x3")
+    torch.cuda.synchronize()
+    kms = []
+    with ClockSampler(0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            kms.append(call("bf16x3"))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    k_ms = float(np.mean(kms))
+    S_tc = out.cpu().numpy() / nwalk
+    f32_ms = call("fp32")
+    S_f32 = out.cpu().numpy() / nwalk
+    flops = 2.0 * nwalk * 3 * nbins * nwave
+
+    # end to end through the API: waveforms from pinned host memory, the
+    # signal read back; positions are the walk's device output
+    h_wave = torch.from_numpy(wave).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.steps, 3))):
+        d_wave.copy_(h_wave, non_blocking=True)
+        call("bf16x3")
+        sig = out.cpu()
+    e2e_s = (time.perf_counter() - t0) / max(1, min(args.steps, 3))
+
+    # signal error against FP64 on a sample, per b (bins of 1 ms/um^2)
+    ns = min(nwalk, 65536)
+    call("bf16x3", ns)
+    s_tc = out.cpu().numpy() / ns
+    call("fp32", ns)
+    s_f32 = out.cpu().numpy() / ns
+    P = pos[:ns].reshape(ns, -1).double().cpu().numpy()
+    phi = P @ wave.reshape(nwave, -1).astype(np.float64).T
+    s64 = np.stack([np.cos(phi).mean(0), np.sin(phi).mean(0)], axis=1)
+    errs = []
+    for lo in range(10):
+        m = (b >= lo) & (b < lo + 1) if lo < 9 else (b >= 9)
+        errs.append({"b": [lo, lo + 1], "bf16x3": float(np.abs(s_tc[m] - s64[m]).max()),
+                     "fp32": float(np.abs(s_f32[m] - s64[m]).max()),
+                     "S_mean": float(s64[m, 0].mean())})
+
+    # CPU: FP32 matmul + cos/sin in numpy on all host cores, a bounded sample
+    nc = 8192
+    Pc = pos[:nc].reshape(nc, -1).cpu().numpy()
+    Wc = wave.reshape(nwave, -1)
+    t0 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < 10.0:
+        ph = Pc @ Wc.T
+        np.cos(ph).sum(0), np.sin(ph).sum(0)
+        reps += 1
+    cpu_s = (time.perf_counter() - t0) / reps
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    achieved = flops / (k_ms * 1e-3) / 1e12
+    line = {
+        "metric": CONTRACT_METRIC, "value": nwalk * nwave / (ms * 1e-3), "unit": "phases/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16 hi/lo x3 (f32 accumulate, f64 sums)",
+        "data": "synthetic (seeded walk positions, seeded random waveforms)",
+        "config": {"workload": f"contraction: {nwalk} walkers x {nbins} bins x 3 axes (FP32 positions of the "
+                               f"engine's walk, {tn} steps) against {nwave} waveforms, b in [0, 10] ms/um^2",
+                   "walkers": nwalk, "nbins": nbins, "nwave": nwave, "K": 3 * nbins,
+                   "l2": "inputs (30.7 GB of positions) larger than L2", "parallelism": "1 GPU"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "model": f"2 M K N = {flops:.3g} algorithmic FLOP / contraction kernel {k_ms:.2f} ms "
+                              "(three BF16 products execute 3x that; peak: measured bf16_tflops, burst)"},
+        "kernel_ms": k_ms,
+        "fp32_cuda_cores": {"kernel_ms": f32_ms, "tflops": flops / (f32_ms * 1e-3) / 1e12,
+                            "max_abs_diff_vs_bf16x3": float(np.abs(S_f32 - S_tc).max())},
+        "signal_error_vs_fp64": {"sample_walkers": ns, "per_b": errs},
+        "e2e": {"value": nwalk * nwave / e2e_s, "unit": "phases/s", "h2d_bytes_per_step": int(wave.nbytes),
+                "d2h_bytes_per_step": int(sig.numel() * 8)},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+        "cpu_baseline": {"value": nc * nwave / cpu_s, "unit": "phases/s", "cores": os.cpu_count(),
+                         "kind": "port", "sample": f"numpy FP32 matmul + cos/sin, {nc} walkers x {nwave} "
+                                                   f"waveforms x K={3 * nbins}, {reps} reps in ~10 s"},
+    }
+    print(json.dumps(line), flush=True)
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -521,7 +653,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="split", choices=["split", "compat"])
-    ap.add_argument("--workload", default="batch", choices=["production", "batch", "single"])
+    ap.add_argument("--workload", default="batch", choices=["production", "batch", "single", "contraction"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--walkers", type=int, default=None, help="walkers per GPU (smaller case, e.g. for ncu)")
     ap.add_argument("--plain-ratio", action="store_true",
@@ -530,7 +662,13 @@ def main():
     ap.add_argument("--timepoints", type=int, default=None,
                     help="records per walk (keep steps/record when shortening the walk)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "contraction":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no waveform contraction "
+                                                                  "(its only gradient form is the PGSE pair)"}))
+        else:
+            run_contraction(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_ours(args)

@@ -22,12 +22,14 @@
 //    FP32 in tensor memory (the dropped A_lo B_lo term is below 2^-16 of each
 //    product).  tcgen05.mma kind::f16, M = 128 waveforms, N = 256 walkers,
 //    K = 16 per instruction, one CTA per SM:
-//      warp 8    TMA: FP32 position tiles (256 walkers x 32 k, 128B swizzle)
-//      warp 9    bulk copies of the pre-split waveform tiles
-//      warps 0-3 FP32 -> BF16 hi/lo into the MMA's canonical K-major layout
-//      warp 10   TMEM allocation, MMA issue (one thread), commits
-//      warps 4-7 epilogue: tcgen05.ld of 32-column slices, range reduction,
-//                sine/cosine, per-row sums; FP64 atomics into the totals
+//      warp 12    TMA: FP32 position tiles (256 walkers x 32 k, 128B swizzle),
+//                 3 stages
+//      warp 13    bulk copies of the pre-split waveform tiles, 4 stages
+//      warps 0-7  FP32 -> BF16 hi/lo into the MMA's canonical K-major layout,
+//                 2 stages
+//      warp 14    TMEM allocation, MMA issue (one thread), commits
+//      warps 8-11 epilogue: tcgen05.ld of 32-column slices, range reduction,
+//                 sine/cosine, per-row sums; FP64 atomics into the totals
 //    Two accumulators (2 x 256 of the 512 TMEM columns) let the epilogue of
 //    one tile overlap the MMAs of the next.  Work units (walker tile, waveform
 //    tile) are ordered waveform tile fastest, so the CTAs reading one walker
@@ -142,17 +144,20 @@ constexpr int kKc = 32;                         // k per pipeline chunk (FP32 el
 constexpr int kTileN = 256;                     // walkers per tile (MMA N)
 constexpr int kTileM = 128;                     // waveforms per tile (MMA M)
 constexpr int kXStages = 3;                     // FP32 position chunks in flight
-constexpr int kBStages = 2;                     // converted operand chunks
+constexpr int kBStages = 2;                     // converted position chunks
+constexpr int kGStages = 4;                     // waveform chunks (their copy is issued once an MMA frees one)
 constexpr uint32_t kXBytes = kTileN * kKc * 4;          // 32768
 constexpr uint32_t kXbBytes = kTileN * kKc * 2;         // one BF16 part: 16384
 constexpr uint32_t kGBytes = kTileM * kKc * 2;          // one BF16 part: 8192
 constexpr uint32_t kOffXa = 0;
 constexpr uint32_t kOffXb = kOffXa + kXStages * kXBytes;               // 98304
 constexpr uint32_t kOffG = kOffXb + kBStages * 2 * kXbBytes;           // 163840
-constexpr uint32_t kOffBar = kOffG + kBStages * 2 * kGBytes;           // 196608
+constexpr uint32_t kOffBar = kOffG + kGStages * 2 * kGBytes;           // 229376
 constexpr uint32_t kSmemUsed = kOffBar + 256;
 constexpr uint32_t kSmemBytes = kSmemUsed + 1024;                      // + alignment slack
-constexpr int kTcThreads = 352;
+constexpr int kConvThreads = 256;               // warps 0-7
+constexpr int kWarpEpi = 8, kWarpX = 12, kWarpG = 13, kWarpMma = 14;
+constexpr int kTcThreads = 480;
 constexpr uint32_t kTmemCols = 512;
 // canonical K-major layout without swizzle: 8 rows x 16 B core matrices; the
 // two core matrices of one K = 16 step are 128 B apart (LBO), 8-row groups
@@ -166,11 +171,12 @@ constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTi
                             ((uint32_t)(kTileM >> 4) << 24);
 
 // barrier indices (8 bytes each at kOffBar)
-enum : int { kBarXFull = 0, kBarXEmpty = 3, kBarGFull = 6, kBarConv = 8, kBarBEmpty = 10, kBarAccFull = 12,
-             kBarAccEmpty = 14, kBarFin = 16, kNumBars = 17 };
+enum : int { kBarXFull = 0, kBarXEmpty = 3, kBarGFull = 6, kBarGEmpty = 10, kBarConv = 14, kBarBEmpty = 16,
+             kBarAccFull = 18, kBarAccEmpty = 20, kBarFin = 22, kNumBars = 23 };
 constexpr uint32_t kOffTmemSlot = kOffBar + 8 * kNumBars;              // 4 bytes
 constexpr uint32_t kOffAbort = kOffTmemSlot + 4;
 static_assert(kOffAbort + 4 <= kSmemUsed, "barrier area");
+static_assert(kSmemBytes <= 232448, "227 KB of shared memory per block");
 
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
@@ -312,11 +318,14 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < kXStages; ++s) {
             mbar_init(bar(kBarXFull + s), 1);
-            mbar_init(bar(kBarXEmpty + s), 128);
+            mbar_init(bar(kBarXEmpty + s), kConvThreads);
+        }
+        for (int s = 0; s < kGStages; ++s) {
+            mbar_init(bar(kBarGFull + s), 1);
+            mbar_init(bar(kBarGEmpty + s), 1);
         }
         for (int s = 0; s < kBStages; ++s) {
-            mbar_init(bar(kBarGFull + s), 1);
-            mbar_init(bar(kBarConv + s), 128);
+            mbar_init(bar(kBarConv + s), kConvThreads);
             mbar_init(bar(kBarBEmpty + s), 1);
             mbar_init(bar(kBarAccFull + s), 1);
             mbar_init(bar(kBarAccEmpty + s), 128);
@@ -326,7 +335,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         fence_proxy_async();
     }
-    if (warp == 10) {
+    if (warp == kWarpMma) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(sbase + kOffTmemSlot), "r"(kTmemCols)
                      : "memory");
@@ -337,7 +346,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_after();
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kOffTmemSlot);
 
-    if (warp == 8) {
+    if (warp == kWarpX) {
         // position chunks: FP32 [256 walkers][32 k], 128-byte swizzle
         if (lane == 0) {
             int64_t i = 0;
@@ -356,7 +365,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             for (int64_t j = i > kXStages ? i - kXStages : 0; j < i; ++j)
                 mbar_wait(bar(kBarXFull + (int)(j % kXStages)), (uint32_t)((j / kXStages) & 1), abort_flag, err, false);
         }
-    } else if (warp == 9) {
+    } else if (warp == kWarpG) {
         // waveform chunks: pre-split BF16 hi/lo, 16 KB per (waveform tile, k chunk)
         if (lane == 0) {
             int64_t i = 0;
@@ -364,20 +373,20 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
                 const int mt = (int)(u % n_mtiles);
                 for (int kc = 0; kc < nk; ++kc, ++i) {
-                    const int s = (int)(i % kBStages);
-                    if (!(ok = mbar_wait(bar(kBarBEmpty + s), (uint32_t)((i / kBStages) & 1) ^ 1u, abort_flag, err, true)))
+                    const int s = (int)(i % kGStages);
+                    if (!(ok = mbar_wait(bar(kBarGEmpty + s), (uint32_t)((i / kGStages) & 1) ^ 1u, abort_flag, err, true)))
                         break;
                     mbar_arrive_tx(bar(kBarGFull + s), 2 * kGBytes);
                     bulk_load(sbase + kOffG + (uint32_t)s * 2 * kGBytes, gpack + ((size_t)mt * nk + kc) * (2 * kGBytes),
                               2 * kGBytes, bar(kBarGFull + s));
                 }
             }
-            for (int64_t j = i > kBStages ? i - kBStages : 0; j < i; ++j)
-                mbar_wait(bar(kBarGFull + (int)(j % kBStages)), (uint32_t)((j / kBStages) & 1), abort_flag, err, false);
+            for (int64_t j = i > kGStages ? i - kGStages : 0; j < i; ++j)
+                mbar_wait(bar(kBarGFull + (int)(j % kGStages)), (uint32_t)((j / kGStages) & 1), abort_flag, err, false);
         }
-    } else if (warp < 4) {
+    } else if (warp < kWarpEpi) {
         // converters: FP32 chunk -> BF16 hi and lo parts in the canonical layout
-        const int ct = threadIdx.x;   // 0 .. 127
+        const int ct = threadIdx.x;   // 0 .. kConvThreads - 1
         int64_t i = 0;
         bool ok = true;
         for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
@@ -389,9 +398,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 const uint8_t* xs = sm + kOffXa + (uint32_t)sx * kXBytes;
                 uint8_t* xh = sm + kOffXb + (uint32_t)sb * 2 * kXbBytes;
                 uint8_t* xl = xh + kXbBytes;
-#pragma unroll 4
-                for (int it = 0; it < (kTileN * kKc / 8) / 128; ++it) {   // 8 items per thread
-                    const int item = it * 128 + ct;
+#pragma unroll
+                for (int it = 0; it < (kTileN * kKc / 8) / kConvThreads; ++it) {   // 4 items per thread
+                    const int item = it * kConvThreads + ct;
                     const int n = item >> 2, g = item & 3;                 // walker row, 8-k group
                     const uint8_t* row = xs + n * (kKc * 4);
                     const int r7 = n & 7;                                  // 128B swizzle: chunk c at c ^ (row % 8)
@@ -411,7 +420,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 mbar_arrive(bar(kBarConv + sb));
             }
         }
-    } else if (warp == 10) {
+    } else if (warp == kWarpMma) {
         // MMA issue
         if (lane == 0) {
             int64_t i = 0, t = 0;
@@ -422,12 +431,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)buf * kTileN;
                 for (int kc = 0; kc < nk; ++kc, ++i) {
-                    const int sb = (int)(i % kBStages);
-                    const uint32_t ph = (uint32_t)((i / kBStages) & 1);
-                    if (!(ok = mbar_wait(bar(kBarConv + sb), ph, abort_flag, err, true))) break;
-                    if (!(ok = mbar_wait(bar(kBarGFull + sb), ph, abort_flag, err, true))) break;
+                    const int sb = (int)(i % kBStages), sg = (int)(i % kGStages);
+                    if (!(ok = mbar_wait(bar(kBarConv + sb), (uint32_t)((i / kBStages) & 1), abort_flag, err, true))) break;
+                    if (!(ok = mbar_wait(bar(kBarGFull + sg), (uint32_t)((i / kGStages) & 1), abort_flag, err, true))) break;
                     tc_fence_after();
-                    const uint32_t ga = sbase + kOffG + (uint32_t)sb * 2 * kGBytes;
+                    const uint32_t ga = sbase + kOffG + (uint32_t)sg * 2 * kGBytes;
                     const uint32_t xa = sbase + kOffXb + (uint32_t)sb * 2 * kXbBytes;
 #pragma unroll
                     for (int ks = 0; ks < kKc / 16; ++ks) {
@@ -439,6 +447,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                         umma_bf16(d, a_lo, b_hi, 1u);
                     }
                     umma_commit(bar(kBarBEmpty + sb));   // operands free when these MMAs are done
+                    umma_commit(bar(kBarGEmpty + sg));
                 }
                 if (ok) umma_commit(bar(kBarAccFull + buf));
             }
@@ -448,7 +457,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         }
     } else {
         // epilogue: warp q reads TMEM lanes 32q .. 32q + 31 (waveform rows)
-        const int q = warp - 4;
+        const int q = warp - kWarpEpi;   // = warp % 4, the lane quarter this warp may access
         int64_t t = 0;
         for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x, ++t) {
             const int buf = (int)(t & 1);
@@ -490,7 +499,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 10)
+    if (warp == kWarpMma)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
