@@ -239,6 +239,41 @@ int rms_split_variant(int k, int* block, int* min_blocks_per_sm);
 int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint8_t* d_labels,
                         double* d_rows, double* d_sig);
 
+/* ---- Adjoint of the waveform-mode signal ----------------------------------
+ * No counterpart in the reference.  For a RMS_MODE_WAVEFORM simulation (at
+ * most 16 waveforms, Nc <= 4, one diffusivity D shared by every labelled
+ * compartment) and upstream weights g_sigw[2j] = dL/dC_j, g_sigw[2j+1] =
+ * dL/dS_j of the signal sums C_j = sum_w s0 cos(phase_j), S_j = sum_w s0
+ * sin(phase_j) (RMS_FIELD_SIGW), computes the gradients of
+ * L = sum_j g_sigw[2j] C_j + g_sigw[2j+1] S_j for the same walkers and seed
+ * as rms_sim_run with opts (SPLIT precision):
+ *   d_wave[nwave*nbins*3]  dL/dwave, the layout of rms_config.wave; exact
+ *                          pathwise (the phase is linear in the waveform)
+ *   d_t2[c]                dL/dT2_c (ms), analytic through s0
+ *   d_kappa                dL/dkappa, score function of the permeation
+ *                          draws (RMS_PERM_KAPPA with kappa > 0, else 0)
+ *   d_diffusivity          dL/dD, pathwise through the step length with the
+ *                          event sequence fixed, plus the score through the
+ *                          kappa-mode permeation probability; the T2 weight's
+ *                          dependence on D (through residence times) is not
+ *                          included: it vanishes when T2 is equal across
+ *                          compartments.  With mirror walls the walk's
+ *                          displacement jumps when a walker meets a wall (the
+ *                          origin image is mirrored, main.cu:302-310), which
+ *                          this term does not see: use periodic walls
+ * Each walker is walked twice from its random streams (nothing stored).
+ * d_wave (caller-allocated host array) and sigw (optional, [nwave*2], the
+ * run's own signal sums) may be NULL. */
+typedef struct rms_adjoint_grads {
+    double* d_wave;
+    double d_diffusivity;
+    double d_kappa;
+    double d_t2[8];
+    double loss;
+    double* sigw;
+} rms_adjoint_grads;
+int rms_adjoint_run(rms_sim* sim, const rms_run_opts* opts, const double* g_sigw, rms_adjoint_grads* out);
+
 /* ---- Multi-waveform phase contraction -------------------------------------
  * No counterpart in the reference (its only gradient form is the PGSE pair,
  * hpc_code/lib/main_PGSE.cu:336-346, summed per step per gradient).  For

@@ -72,7 +72,7 @@ struct rms_device_state {
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     DevBuf labels, packed, axons, wavef, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
-        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos;
+        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave;
     HostPinned h_out;
     size_t labels_bytes = 0;
     bool packed_valid = false;
@@ -81,7 +81,7 @@ struct rms_device_state {
         if (device >= 0) cudaSetDevice(device);
         for (DevBuf* b : {&labels, &packed, &axons, &wavef, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
-                          &tr_vox, &tr_ev, &tr_pos})
+                          &tr_vox, &tr_ev, &tr_pos, &adj_g, &adj_sums, &adj_dwave})
             b->release();
         h_out.release();
         if (e0) cudaEventDestroy(e0);
@@ -617,6 +617,124 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
     return run_launch(jobs, o);
 }
 
+// Gradients of L = sum_j g_cos[j] C_j + g_sin[j] S_j for a waveform-mode
+// simulation, by the two-pass walk of rms_adjoint.cu.
+int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adjoint_grads* out) {
+    if (s->mode != RMS_MODE_WAVEFORM) return set_error(RMS_ERR_ARG, "the adjoint differentiates a waveform-mode simulation");
+    if (s->nwave > kAdjWaves) return set_error(RMS_ERR_RANGE, "the adjoint takes at most 16 waveforms per run");
+    if (s->nc > kAdjNc) return set_error(RMS_ERR_RANGE, "the adjoint supports Nc <= 4");
+    if (!s->have_lattice) return set_error(RMS_ERR_STATE, "no lattice: call rms_sim_set_lattice or load a run directory");
+    double D = 0.0;
+    for (int c = 1; c < s->nc; ++c) {
+        if (D == 0.0) D = s->diffusivity[c];
+        if (s->diffusivity[c] != D)
+            return set_error(RMS_ERR_ARG, "the adjoint needs one diffusivity for all labelled compartments");
+    }
+    if (!(D > 0.0)) return set_error(RMS_ERR_ARG, "the adjoint needs a positive diffusivity");
+    int64_t w0 = o ? o->walker_begin : 0, w1 = o ? o->walker_end : 0;
+    if (w0 == 0 && w1 == 0) w1 = s->npar;
+    if (w0 < 0 || w1 > s->npar || w0 >= w1) return set_error(RMS_ERR_ARG, "walker range outside [0, NPar)");
+    const int device = o ? o->device : 0;
+    int rc = ensure_device(s, device);
+    if (rc) return rc;
+    rms_device_state* d = s->dev;
+    RMS_CUDA(cudaSetDevice(device));
+    cudaStream_t st = (o && o->stream) ? (cudaStream_t)o->stream : d->own;
+    rc = prepare_lattice(s, st, true, 4);
+    if (rc) return rc;
+
+    AxonDesc x;
+    fill_axon_desc(x, s, w0, w1, 0, o ? o->seed : 0, d->packed.as<uint8_t>());
+    AdjArgs a{};
+    a.lat = x.lat;
+    a.n1 = x.n1; a.n2 = x.n2; a.n3 = x.n3; a.s0 = x.s0; a.s1 = x.s1;
+    a.walker_begin = w0; a.walker_end = w1;
+    a.ntiles = (w1 - w0 + 31) / 32;
+    a.seed = x.seed;
+    a.tn = s->tn; a.nbins = s->nbins; a.bin_steps = s->tn / s->nbins; a.nwave = s->nwave;
+    a.nite = s->nite; a.boundary = s->boundary;
+    a.res = x.res;
+    a.flight = x.flight; a.same_cross = x.same_cross;
+    for (int c = 0; c < kAdjNc; ++c) {
+        a.step[c] = c < s->nc ? x.step[c] : 0.0f;
+        a.kexp[c] = c < s->nc ? x.k[c] : 0.0f;
+        for (int e = 0; e < kAdjNc; ++e) {
+            a.pij[c * kAdjNc + e] = (c < s->nc && e < s->nc) ? x.pij[c * kNcMax + e] : 0.0f;
+            a.ratio[c * kAdjNc + e] = (c < s->nc && e < s->nc) ? x.ratio[c * kNcMax + e] : 0.0f;
+        }
+    }
+    std::vector<double> wf((size_t)s->nbins * s->nwave * 3);
+    for (int j = 0; j < s->nwave; ++j)
+        for (int b = 0; b < s->nbins; ++b)
+            for (int k = 0; k < 3; ++k)
+                wf[((size_t)b * s->nwave + j) * 3 + k] = s->wave[((size_t)j * s->nbins + b) * 3 + k] * s->dt;
+    RMS_CUDA(upload(d->wavef, wf, st));
+    std::vector<float> gup((size_t)2 * s->nwave);
+    for (int j = 0; j < 2 * s->nwave; ++j) gup[j] = (float)(g_sigw ? g_sigw[j] : 0.0);
+    RMS_CUDA(upload(d->adj_g, gup, st));
+    const size_t ndw = (size_t)s->nbins * s->nwave * 3;
+    RMS_CUDA(d->adj_sums.ensure(sizeof(double) * kAdjSums));
+    RMS_CUDA(cudaMemsetAsync(d->adj_sums.p, 0, sizeof(double) * kAdjSums, st));
+    RMS_CUDA(d->adj_dwave.ensure(sizeof(float) * ndw));
+    RMS_CUDA(cudaMemsetAsync(d->adj_dwave.p, 0, sizeof(float) * ndw, st));
+    RMS_CUDA(d->err.ensure(sizeof(int)));
+    RMS_CUDA(cudaMemsetAsync(d->err.p, 0, sizeof(int), st));
+    a.wave = d->wavef.as<double>();
+    a.gup = d->adj_g.as<float>();
+    a.sums = d->adj_sums.as<double>();
+    a.dwave = d->adj_dwave.as<float>();
+    a.err = d->err.as<int>();
+
+    int sms = 0;
+    RMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int per_sm = adjoint_blocks_per_sm();
+    if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
+    const int64_t wpb = kAdjBlock / 32;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (a.ntiles + wpb - 1) / wpb));
+    RMS_CUDA(cudaEventRecord(d->e0, st));
+    int e = launch_adjoint(a, grid, st);
+    if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch");
+    RMS_CUDA(cudaEventRecord(d->e1, st));
+    std::vector<double> sums(kAdjSums);
+    std::vector<float> dw(ndw);
+    int herr = 0;
+    RMS_CUDA(cudaMemcpyAsync(sums.data(), d->adj_sums.p, sizeof(double) * kAdjSums, cudaMemcpyDeviceToHost, st));
+    RMS_CUDA(cudaMemcpyAsync(dw.data(), d->adj_dwave.p, sizeof(float) * ndw, cudaMemcpyDeviceToHost, st));
+    RMS_CUDA(cudaMemcpyAsync(&herr, d->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RMS_CUDA(cudaStreamSynchronize(st));
+    if (herr & kErrInitCap)
+        return set_error(RMS_ERR_RANGE, "a walker found no labelled voxel within the rejection-sampling cap");
+    float ms = 0.f;
+    RMS_CUDA(cudaEventElapsedTime(&ms, d->e0, d->e1));
+    s->walk_ms = ms;
+    s->run_ms = ms;
+
+    // dL/dwave: phase_j = dt sum_b wave_j,b . X_b
+    if (out->d_wave)
+        for (int j = 0; j < s->nwave; ++j)
+            for (int b = 0; b < s->nbins; ++b)
+                for (int k = 0; k < 3; ++k)
+                    out->d_wave[((size_t)j * s->nbins + b) * 3 + k] =
+                        s->dt * (double)dw[((size_t)b * s->nwave + j) * 3 + k];
+    out->loss = sums[kAdjSumL];
+    // score of the permeation draws with the mean loss as baseline:
+    // sum_w (L_w - L/N) E_w (E[E_w] = 0 keeps it unbiased)
+    const double score = sums[kAdjSumLE] - sums[kAdjSumL] / (double)(w1 - w0) * sums[kAdjSumE];
+    // l = sqrt(6 D dt) / res: dl/dD = l / (2 D); in kappa mode P ~ kappa D^(-1/2)
+    const bool kap = s->permeation == RMS_PERM_KAPPA;
+    const double step = s->step[s->nc > 1 ? 1 : 0];
+    out->d_diffusivity = (sums[kAdjSumPath] * step / 2.0 - (kap ? score / 2.0 : 0.0)) / D;
+    out->d_kappa = (kap && s->kappa > 0.0) ? score / s->kappa : 0.0;
+    for (int c = 0; c < 8; ++c) out->d_t2[c] = 0.0;
+    for (int c = 0; c < s->nc; ++c) {
+        const double T2 = s->t2[c];
+        out->d_t2[c] = sums[kAdjSumLT + c] * s->dt / (T2 * T2);   // s0 = exp(-sum_c t_c / T2_c), t_c in ms
+    }
+    if (out->sigw)
+        for (int j = 0; j < 2 * s->nwave; ++j) out->sigw[j] = sums[kAdjSumSig + j];
+    return RMS_OK;
+}
+
 bool field_size(const rms_sim* s, int field, size_t& n) {
     const size_t T = s->timepoints;
     switch (field) {
@@ -736,6 +854,13 @@ int rms_sim_set_lattice(rms_sim* s, const uint8_t* labels, int n1, int n2, int n
     s->have_lattice = true;
     s->lattice_dirty = true;
     return RMS_OK;
+}
+
+int rms_adjoint_run(rms_sim* s, const rms_run_opts* opts, const double* g_sigw, rms_adjoint_grads* out) {
+    if (!s || !out) return set_error(RMS_ERR_ARG, "null argument");
+    if (opts && opts->precision != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "the adjoint walks the SPLIT walk");
+    if (opts && opts->traj_out) return set_error(RMS_ERR_ARG, "the adjoint writes no trajectory");
+    return run_adjoint(s, opts, g_sigw, out);
 }
 
 int rms_sim_run(rms_sim* s, const rms_run_opts* opts) {

@@ -112,6 +112,35 @@ int walk_compat_blocks_per_sm(int nc, bool trace);
 int walk_split_blocks_per_sm(int nc, int lattice_bits, int variant);
 const char* cuda_error_string(int code);
 
+// Adjoint of the waveform-mode split walk (rms_adjoint.cu): one axon, labels
+// below kAdjNc, at most kAdjWaves waveforms.
+constexpr int kAdjWaves = 16;
+constexpr int kAdjNc = 4;
+// sums[]: sum_w L_w, sum_w L_w E_w, sum_w sum_j a_jw dphi_jw, sum_w L_w t_wc
+// (steps, per compartment), sum_w E_w, then the signal sums (cos, sin) per
+// waveform
+constexpr int kAdjSumL = 0, kAdjSumLE = 1, kAdjSumPath = 2, kAdjSumLT = 3, kAdjSumE = 3 + kAdjNc,
+              kAdjSumSig = 4 + kAdjNc;
+constexpr int kAdjSums = kAdjSumSig + 2 * kAdjWaves;
+struct AdjArgs {
+    const uint8_t* lat;          // padded 4-bit lattice with free-flight flags
+    int n1, n2, n3, s0, s1;
+    int64_t walker_begin, walker_end, ntiles;
+    uint64_t seed;
+    int tn, nbins, bin_steps, nwave, nite, boundary;
+    float res;
+    int flight, same_cross;
+    float step[kAdjNc], kexp[kAdjNc], pij[kAdjNc * kAdjNc], ratio[kAdjNc * kAdjNc];
+    const double* wave;          // [bin][waveform][axis], x dt
+    const float* gup;            // [waveform][2]: dL/d(sum cos), dL/d(sum sin)
+    double* sums;                // [kAdjSums]
+    float* dwave;                // [bin][waveform][axis]: sum_w a_jw X_wb (um)
+    int* err;
+};
+int launch_adjoint(const AdjArgs& a, int grid, void* stream);
+int adjoint_blocks_per_sm();
+constexpr int kAdjBlock = 128;
+
 // Multi-waveform phase contraction (rms_contract.cu): out[j] = (sum_w cos phi,
 // sum_w sin phi), phi[w][j] = sum_k pos[w][k] wave[j][k], K = 3 nbins.
 // method RMS_CONTRACT_FP32 or RMS_CONTRACT_BF16X3.  Returns an RMS_* status;

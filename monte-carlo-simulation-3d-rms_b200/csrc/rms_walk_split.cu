@@ -47,6 +47,7 @@
 
 #include "philox.cuh"
 #include "rms_internal.h"
+#include "split_lattice.cuh"
 #include "warp_reduce.cuh"
 
 namespace rms {
@@ -58,34 +59,6 @@ namespace {
 struct SplitVariant { int block, minb; };
 constexpr SplitVariant kVariants[] = {{256, 4}, {256, 3}, {256, 2}, {128, 8}, {512, 2}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
-
-// Lattice cell: label in the low bits, free-flight flag in the top bit
-// (BITS = 4: 3 + 1 bits, two voxels per byte, voxel v in bits 4(v % 2);
-// BITS = 8: 7 + 1; BITS = 2: label only, voxel v in bits 2(v % 4)).
-template <int BITS>
-__device__ __forceinline__ unsigned cell_at(const uint8_t* __restrict__ lat, unsigned lin) {
-    if (BITS == 2) return (__ldg(lat + (lin >> 2)) >> ((lin & 3u) * 2u)) & 3u;
-    if (BITS == 4) return (__ldg(lat + (lin >> 1)) >> ((lin & 1u) * 4u)) & 15u;
-    return __ldg(lat + lin);
-}
-
-template <int BITS> __host__ __device__ constexpr unsigned label_mask() { return BITS == 2 ? 3u : (BITS == 4 ? 7u : 127u); }
-template <int BITS> __host__ __device__ constexpr unsigned flight_bit() { return BITS == 2 ? 0u : (BITS == 4 ? 8u : 128u); }
-
-template <int BITS>
-__device__ __forceinline__ int label_at(const uint8_t* __restrict__ lat, unsigned lin) {
-    return (int)(cell_at<BITS>(lat, lin) & label_mask<BITS>());
-}
-
-template <int BITS> __host__ __device__ constexpr int wall_code() { return (int)label_mask<BITS>(); }
-
-// Origin image after a mirror wall: x -> -x (lo) or x -> 2N - x (hi), on the
-// split form x = I + F, F in [0, 1).
-__device__ __forceinline__ void mirror_origin(int& I, float& F, bool hi, int n) {
-    const int base = hi ? 2 * n : 0;
-    if (F > 0.0f) { I = base - I - 1; F = 1.0f - F; }
-    else { I = base - I; }
-}
 
 // Add a warp's accumulator rows (and PGSE signal row) into axon `axon`'s
 // totals and clear them (multi-axon launches; other warps add concurrently).

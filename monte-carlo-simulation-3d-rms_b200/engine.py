@@ -31,7 +31,8 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_sim_write_dir",
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
-           "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases")
+           "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases",
+           "rms_adjoint_run")
 CONTRACT = {"fp32": 0, "bf16x3": 1}
 
 _DP = C.POINTER(C.c_double)
@@ -63,6 +64,11 @@ class RunOpts(C.Structure):
         ("walker_begin", C.c_int64), ("walker_end", C.c_int64),
         ("traj_out", C.c_void_p),
     ]
+
+
+class AdjointGrads(C.Structure):
+    _fields_ = [("d_wave", _DP), ("d_diffusivity", C.c_double), ("d_kappa", C.c_double),
+                ("d_t2", C.c_double * 8), ("loss", C.c_double), ("sigw", _DP)]
 
 
 _lib = None
@@ -101,6 +107,7 @@ def lib():
         L.rms_sim_run_noalloc.argtypes = [C.c_void_p, C.POINTER(RunOpts), C.c_void_p, C.c_void_p, C.c_void_p]
         L.rms_rng_split.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.rms_split_variant.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.rms_adjoint_run.argtypes = [C.c_void_p, C.POINTER(RunOpts), _DP, C.POINTER(AdjointGrads)]
         L.rms_contract_phases.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                           C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]
         _lib = L
@@ -149,6 +156,7 @@ class Sim:
         gr = _arr(grad if grad is not None else [])
         pj = _arr(pij) if pij is not None else None
         self._keep += [bv, bvc, gr, pj, wv]
+        self.wave_shape = wv.shape if wv is not None else None
         cfg = Config(MODE[mode], float(dt), int(tn), int(npar), int(nc or d.size), float(res),
                      int(shape[0]), int(shape[1]), int(shape[2]), _ptr(d), _ptr(t2a),
                      bv.size if mode == "narrow" else 0, _ptr(bv), _ptr(bvc),
@@ -169,6 +177,7 @@ class Sim:
         self = cls.__new__(cls)
         self._h = C.c_void_p()
         self._keep = []
+        self.wave_shape = None
         _check(lib().rms_sim_load_dir(path.encode(), MODE[mode], C.byref(self._h)))
         if mode == "auto":
             mode = "pgse" if os.path.exists(os.path.join(path, "gradient_time.txt")) else "narrow"
@@ -207,6 +216,26 @@ class Sim:
         _check(lib().rms_sim_run_noalloc(self._h, C.byref(opts), C.c_void_p(int(d_labels)),
                                          C.c_void_p(int(d_rows)), C.c_void_p(int(d_sig)) if d_sig else None))
         return self
+
+    def adjoint(self, g_sigw, seed: int = 0, device: int = 0, stream=None, walker_range=None) -> dict:
+        """Gradients of L = sum_j g_sigw[j, 0] C_j + g_sigw[j, 1] S_j (the
+        waveform-mode signal sums) for the walk ``run(seed, "split")`` makes;
+        see rms_adjoint_run in include/rms.h."""
+        if self.wave_shape is None:
+            raise ValueError("the adjoint needs a waveform-mode simulation")
+        nw, nb, _ = self.wave_shape
+        g = _arr(g_sigw)
+        if g.size != 2 * nw:
+            raise ValueError("g_sigw must hold (cos, sin) weights per waveform")
+        w0, w1 = walker_range if walker_range is not None else (0, 0)
+        st = None if stream is None else C.c_void_p(int(stream))
+        opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION["split"], int(device), st, 0, 0, int(w0), int(w1), None)
+        dwave = np.zeros(nw * nb * 3)
+        sigw = np.zeros(2 * nw)
+        out = AdjointGrads(_ptr(dwave), 0.0, 0.0, (C.c_double * 8)(), 0.0, _ptr(sigw))
+        _check(lib().rms_adjoint_run(self._h, C.byref(opts), _ptr(g), C.byref(out)))
+        return dict(d_wave=dwave.reshape(nw, nb, 3), d_diffusivity=out.d_diffusivity, d_kappa=out.d_kappa,
+                    d_t2=np.array(out.d_t2[:]), loss=out.loss, sigw=sigw.reshape(nw, 2))
 
     def field_size(self, name: str) -> int:
         n = C.c_size_t()
