@@ -17,7 +17,7 @@ Workload ``single``: the 64 x 64 x 512 single-axon lattice (labels 0/1),
 10 steps.  Inputs are synthetic and seeded.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision split|compat] [--workload batch|production|single|contraction]
+                  [--precision split|compat] [--workload batch|production|single|contraction|adjoint]
                   [--plain-ratio]
 
 ``value``: walker-steps/s of the whole job, lattice already resident on the
@@ -514,6 +514,95 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+ADJOINT_METRIC = "walker-steps/s of the adjoint (both passes) of the waveform-mode signal"
+
+
+def run_adjoint_bench(args):
+    """Gradients of the waveform signal: the 64x64x512 single-axon lattice
+    with a label-2 exterior (periodic walls), 1e6 walkers, dt = 2e-4 ms, 5000
+    steps, one smooth random gradient waveform of 1000 bins x 3 axes
+    (|gamma g| <= 0.0214 rad/(um ms), i.e. 80 mT/m) turned to 16 directions,
+    D = 2 um^2/ms, kappa = 0.02 um/ms, T2 = 80 / 60 ms.  Times the forward walk
+    and the adjoint, and checks every gradient against a central finite
+    difference with common random numbers (h = 1e-3 relative)."""
+    import torch
+    from rms_b200 import engine, geometry, waveforms
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    npar = args.walkers or 1_000_000
+    dt, tn, nb, nw = 2e-4, 5000, 1000, 16
+    lab = geometry.axon_lattice(64, 64, 512, 0.1, seed=0, exterior=2)
+    g = waveforms.random_smooth(1, nb, 0.0214, seed=3)[0]
+    rng = np.random.default_rng(1)
+    R = np.stack([np.linalg.qr(rng.normal(size=(3, 3)))[0] for _ in range(nw)])
+    W = rng.normal(size=(nw, 2))
+    par = dict(D=2.0, kappa=0.02, t2=np.array([1e6, 80.0, 60.0]))
+
+    def sim(gg, D, kappa, t2):
+        return engine.Sim(lab, dt=dt, tn=tn, npar=npar, res=0.1, diffusivity=[0.0, D, D], t2=list(t2),
+                          wave=np.einsum("jab,nb->jna", R, gg), timepoints=1000, boundary="periodic",
+                          permeation="kappa", kappa=kappa)
+
+    def loss(gg=g, D=par["D"], kappa=par["kappa"], t2=par["t2"]):
+        s_ = sim(gg, D, kappa, t2)
+        s_.run(seed=9, precision="split")
+        v = float((s_.get("sigw").reshape(-1, 2) * W).sum() / npar)
+        s_.close()
+        return v
+
+    s0 = sim(g, **par)
+    for _ in range(args.warmup):
+        s0.run(seed=9, precision="split")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s0.run(seed=9, precision="split")
+    fwd_s = time.perf_counter() - t0
+    fwd_ms = s0.timing()[0]
+    t0 = time.perf_counter()
+    r = s0.adjoint(W.reshape(-1) / npar, seed=9)
+    adj_s = time.perf_counter() - t0
+    adj_ms = s0.timing()[0]
+    dg = np.einsum("jab,jna->nb", R, r["d_wave"])      # chain rule through the rotations
+    h = 1e-3
+    d = np.random.default_rng(4).normal(size=g.shape) * np.abs(g).max()
+    checks = {}
+    fd_dir = (loss(gg=g + h * d) - loss(gg=g - h * d)) / (2 * h)
+    checks["waveform (random direction)"] = (float((dg * d).sum()), fd_dir)
+    for c in (1, 2):
+        t2p, t2m = par["t2"].copy(), par["t2"].copy()
+        t2p[c] *= 1 + h
+        t2m[c] *= 1 - h
+        checks[f"T2[{c}]"] = (float(r["d_t2"][c]), (loss(t2=t2p) - loss(t2=t2m)) / (2 * h * par["t2"][c]))
+    checks["D"] = (r["d_diffusivity"], (loss(D=2.0 * (1 + h)) - loss(D=2.0 * (1 - h))) / (2 * h * 2.0))
+    checks["kappa"] = (r["d_kappa"], (loss(kappa=0.02 * (1 + h)) - loss(kappa=0.02 * (1 - h))) / (2 * h * 0.02))
+    out = {k: {"adjoint": a, "finite_difference": f, "rel_err": abs(a / f - 1) if f else None}
+           for k, (a, f) in checks.items()}
+    # D and kappa act through discontinuous events (crossing decisions, face
+    # hits at voxel corners): the h = 1e-3 difference is dominated by those
+    # jumps, so a least-squares slope over +-5 % (7 points, same seed) is
+    # reported beside it
+    for k, x0, f in (("D", 2.0, lambda x: loss(D=x)), ("kappa", 0.02, lambda x: loss(kappa=x))):
+        xs = x0 * (1 + 0.05 * np.linspace(-1, 1, 7))
+        sl = float(np.polyfit(xs, [f(x) for x in xs], 1)[0])
+        out[k]["slope_5pct"] = sl
+        out[k]["rel_err_vs_slope"] = abs(out[k]["adjoint"] / sl - 1) if sl else None
+    ws = npar * tn * 2
+    line = {
+        "metric": ADJOINT_METRIC, "value": ws / (adj_ms * 1e-3), "unit": "walker-steps/s", "n_gpus": 1, "steps": 1,
+        "warmup": args.warmup, "ms_per_step": adj_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+i32 (f64 sums)", "data": "synthetic (seeded axon lattice and waveform)",
+        "config": {"workload": f"adjoint: 64x64x512 axon + label-2 exterior, {npar} walkers, {tn} steps, "
+                               f"waveform {nb} bins x 3 turned to {nw} directions, periodic walls",
+                   "walkers": npar, "steps_per_walk": tn, "nbins": nb, "nwave": nw, "parallelism": "1 GPU"},
+        "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
+        "e2e": {"value": ws / adj_s, "unit": "walker-steps/s", "h2d_bytes_per_step": int(lab.nbytes),
+                "d2h_bytes_per_step": int(r["d_wave"].nbytes)},
+        "gradient_checks": out, "loss": r["loss"], "gpu_launches": 1,
+    }
+    print(json.dumps(line), flush=True)
+
+
 CONTRACT_METRIC = "walker-waveform phases/s of the multi-waveform phase contraction (signal mean(cos, sin))"
 
 
@@ -653,7 +742,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="split", choices=["split", "compat"])
-    ap.add_argument("--workload", default="batch", choices=["production", "batch", "single", "contraction"])
+    ap.add_argument("--workload", default="batch", choices=["production", "batch", "single", "contraction", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--walkers", type=int, default=None, help="walkers per GPU (smaller case, e.g. for ncu)")
     ap.add_argument("--plain-ratio", action="store_true",
@@ -662,7 +751,12 @@ def main():
     ap.add_argument("--timepoints", type=int, default=None,
                     help="records per walk (keep steps/record when shortening the walk)")
     args = ap.parse_args()
-    if args.workload == "contraction":
+    if args.workload == "adjoint":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint"}))
+        else:
+            run_adjoint_bench(args)
+    elif args.workload == "contraction":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no waveform contraction "
                                                                   "(its only gradient form is the PGSE pair)"}))
