@@ -333,10 +333,18 @@ class BatchJob:
         self.walker_steps = sum(kw["npar"] * kw["tn"] for kw in kws)
         self.launches_per_step = 1 + len(self.sims)   # one walk + one ordered reduction per axon
         self.pinned = None
+        self.variant, self.variant_ms = 0, None
+
+    def tune(self, precision):
+        """Pick the split walk's launch variant for this batch (rms_autotune)."""
+        if precision == "split":
+            self.variant, self.variant_ms = self.engine.autotune(self.sims, seed=1, device=self.device,
+                                                                  stream=self.stream)
 
     def run(self, seed, precision):
         self.engine.batch_run(self.sims, seed=seed + (self.rank << 40), precision=precision,
-                              device=self.device, stream=self.stream)
+                              device=self.device, stream=self.stream,
+                              variant=self.variant if precision == "split" else 0)
 
     def walk_ms(self):
         return self.sims[0].timing()[0]
@@ -401,6 +409,8 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return tuple(float(x) for x in t)
 
+    if hasattr(job, "tune"):
+        job.tune(precision)   # outside the timed region
     for i in range(args.warmup):
         job.run(1000 + i, precision)
     walk_ms = []
@@ -493,7 +503,10 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f64" if precision == "compat" else "f32+i32 (f64 sums)",
             "data": "synthetic (seeded axon lattices)",
             "config": dict(cfg, precision=precision, parallelism=f"walker shards x{world}",
-                           l2="flushed between steps (256 MiB write); lattices larger than L2"),
+                           l2="flushed between steps (256 MiB write); lattices larger than L2",
+                           **({"launch_variant": int(job.variant),
+                               "autotune_walk_ms": [round(float(x), 2) for x in job.variant_ms]}
+                              if getattr(job, "variant_ms", None) is not None else {})),
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
                          "frac": achieved_gbs / peak, "traffic": traffic,
                          "model": f"{BYTES_PER_WALKER_STEP} B/walker-step x {walker_steps:.3g} walker-steps "

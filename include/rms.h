@@ -209,6 +209,17 @@ int rms_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
  * position draws, domain 2 the partial-permeation draws.  A test hook. */
 int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out);
 
+/* Autotuner of the SPLIT walk's launch variant for a batch (n >= 1 sims, as
+ * rms_batch_run would walk them with opts): every variant walks the same
+ * subset of each simulation's walkers (about four waves of the GPU), the
+ * fastest walk kernel wins; *variant receives its number (pass it as
+ * rms_run_opts.variant), variant_ms (optional, one per variant) the times.
+ * Results are cached per device, lattice encoding, Nc, axon count and size
+ * class, so later calls return at once.  The simulations' results are
+ * overwritten by the tuning runs.  No reference counterpart (the reference
+ * launches one fixed shape, hpc_code/lib/main.cu:499-504). */
+int rms_autotune(rms_sim* const* sims, int n, const rms_run_opts* opts, int* variant, double* variant_ms);
+
 /* Launch variants of the SPLIT walk (block size x minimum resident blocks per
  * SM).  rms_split_variant(k, ...) describes entry k >= 1; returns RMS_ERR_ARG
  * past the end.  No reference counterpart (the reference launches one fixed

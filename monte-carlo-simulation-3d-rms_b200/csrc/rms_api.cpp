@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <sstream>
 #include <tuple>
 
@@ -609,6 +610,79 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     return RMS_OK;
 }
 
+// Launch-variant autotuner: each variant walks the same subset of every
+// simulation's walkers (the first fraction f of each, f chosen so the subset
+// fills about four waves of the widest variant), one untimed launch first;
+// the fastest walk kernel wins.  Results are cached per (device, lattice
+// encoding, Nc, axon count, log2 of the lattice voxels, log2 of the steps).
+struct TuneKey {
+    int device, bits, nc, naxons, vox_log2, tn_log2, mode;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(device, bits, nc, naxons, vox_log2, tn_log2, mode) <
+               std::tie(o.device, o.bits, o.nc, o.naxons, o.vox_log2, o.tn_log2, o.mode);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, std::vector<double>>> g_tune;
+
+int autotune(rms_sim* const* sims, int n, const rms_run_opts* opts, int* variant, double* variant_ms) {
+    const int device = opts ? opts->device : 0;
+    int nc_max = 0;
+    double vox = 0.0;
+    int64_t total = 0;
+    for (int i = 0; i < n; ++i) {
+        nc_max = std::max(nc_max, sims[i]->nc);
+        vox += (double)sims[i]->n1 * sims[i]->n2 * sims[i]->n3;
+        total += sims[i]->npar;
+    }
+    const TuneKey key{device, split_lattice_bits(nc_max), nc_max, n, (int)std::log2(std::max(vox, 1.0)),
+                      (int)std::log2((double)std::max(sims[0]->tn, 1)), sims[0]->mode};
+    const int nv = split_variant_count();
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            *variant = it->second.first;
+            if (variant_ms)
+                for (int v = 0; v < nv; ++v) variant_ms[v] = it->second.second[v];
+            return RMS_OK;
+        }
+    }
+    int sms = 0;
+    RMS_CUDA(cudaSetDevice(device));
+    RMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const double want = 4.0 * sms * 4 * 256;     // four waves of 256 x 4 blocks per SM
+    const double f = std::min(1.0, want / (double)std::max<int64_t>(total, 1));
+    std::vector<LaunchJob> jobs;
+    const uint64_t seed = opts ? opts->seed : 0;
+    for (int i = 0; i < n; ++i) {
+        const int64_t m = std::max<int64_t>(std::min<int64_t>(32, sims[i]->npar), (int64_t)std::ceil(f * sims[i]->npar));
+        jobs.push_back(LaunchJob{sims[i], 0, std::min<int64_t>(m, sims[i]->npar), seed + (uint64_t)i * kBatchSeedStep});
+    }
+    rms_run_opts o = opts ? *opts : rms_run_opts{};
+    o.precision = RMS_PREC_SPLIT;
+    o.trace_walkers = 0;
+    o.traj_out = nullptr;
+    std::vector<double> ms(nv, 0.0);
+    int best = 0;
+    for (int v = -1; v < nv; ++v) {
+        o.variant = (v < 0 ? 0 : v) + 1;
+        int rc = run_launch(jobs, &o);
+        if (rc) return rc;
+        if (v < 0) continue;                     // warm-up launch
+        ms[v] = jobs[0].s->walk_ms;
+        if (ms[v] < ms[best]) best = v;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = {best + 1, ms};
+    }
+    *variant = best + 1;
+    if (variant_ms)
+        for (int v = 0; v < nv; ++v) variant_ms[v] = ms[v];
+    return RMS_OK;
+}
+
 int run_one(rms_sim* s, const rms_run_opts* o) {
     int64_t w0 = o ? o->walker_begin : 0, w1 = o ? o->walker_end : 0;
     if (w0 == 0 && w1 == 0) w1 = s->npar;
@@ -867,6 +941,17 @@ int rms_sim_run(rms_sim* s, const rms_run_opts* opts) {
     if (!s) return set_error(RMS_ERR_ARG, "null sim");
     try {
         return run_one(s, opts);
+    } catch (const std::exception& e) {
+        return set_error(RMS_ERR_NOMEM, e.what());
+    }
+}
+
+int rms_autotune(rms_sim* const* sims, int n, const rms_run_opts* opts, int* variant, double* variant_ms) {
+    if (!sims || n < 1 || !variant) return set_error(RMS_ERR_ARG, "null argument");
+    for (int i = 0; i < n; ++i)
+        if (!sims[i]) return set_error(RMS_ERR_ARG, "null simulation in the batch");
+    try {
+        return autotune(sims, n, opts, variant, variant_ms);
     } catch (const std::exception& e) {
         return set_error(RMS_ERR_NOMEM, e.what());
     }

@@ -32,7 +32,7 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
            "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases",
-           "rms_adjoint_run")
+           "rms_adjoint_run", "rms_autotune")
 CONTRACT = {"fp32": 0, "bf16x3": 1}
 
 _DP = C.POINTER(C.c_double)
@@ -107,6 +107,7 @@ def lib():
         L.rms_sim_run_noalloc.argtypes = [C.c_void_p, C.POINTER(RunOpts), C.c_void_p, C.c_void_p, C.c_void_p]
         L.rms_rng_split.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.rms_split_variant.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.rms_autotune.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_int), _DP]
         L.rms_adjoint_run.argtypes = [C.c_void_p, C.POINTER(RunOpts), _DP, C.POINTER(AdjointGrads)]
         L.rms_contract_phases.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                           C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]
@@ -300,10 +301,10 @@ class Sim:
         self.close()
 
 
-def batch_run(sims, seed: int = 0, precision: str = "compat", device: int = 0, stream=None):
+def batch_run(sims, seed: int = 0, precision: str = "compat", device: int = 0, stream=None, variant: int = 0):
     arr = (C.c_void_p * len(sims))(*[s._h.value for s in sims])
     st = None if stream is None else C.c_void_p(int(stream))
-    opts = RunOpts(int(seed), PRECISION[precision], int(device), st, 0, 0, 0, 0)
+    opts = RunOpts(int(seed), PRECISION[precision], int(device), st, 0, int(variant), 0, 0, None)
     _check(lib().rms_batch_run(arr, len(sims), C.byref(opts)))
 
 
@@ -318,6 +319,18 @@ def contract_phases(d_pos: int, nwalk: int, nbins: int, d_wave: int, nwave: int,
     _check(lib().rms_contract_phases(C.c_void_p(int(d_pos)), int(nwalk), int(nbins), C.c_void_p(int(d_wave)),
                                      int(nwave), CONTRACT[method], C.c_void_p(int(d_out)), st, C.byref(ms)))
     return ms.value
+
+
+def autotune(sims, seed: int = 0, device: int = 0, stream=None):
+    """(variant, [walk ms per variant]) of the SPLIT walk for this batch; pass
+    the variant to run()/batch_run().  Cached per job class."""
+    arr = (C.c_void_p * len(sims))(*[s._h.value for s in sims])
+    st = None if stream is None else C.c_void_p(int(stream))
+    opts = RunOpts(int(seed), PRECISION["split"], int(device), st, 0, 0, 0, 0, None)
+    v = C.c_int()
+    ms = np.zeros(len(split_variants()))
+    _check(lib().rms_autotune(arr, len(sims), C.byref(opts), C.byref(v), _ptr(ms)))
+    return v.value, ms
 
 
 def rng_doubles(seed: int, walker: int, n: int) -> np.ndarray:

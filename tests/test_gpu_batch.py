@@ -62,3 +62,23 @@ def test_batch_rejects_mixed_schedules():
     with pytest.raises(engine.RmsError) as e:
         engine.batch_run(sims + [other], seed=1, precision="split")
     assert e.value.code == -1
+
+
+def test_autotune_picks_a_variant_and_caches_it():
+    import time
+    sims = axon_sims()
+    v, ms = engine.autotune(sims, seed=3)
+    nv = len(engine.split_variants())
+    assert 1 <= v <= nv and ms.shape == (nv,) and np.all(ms > 0)
+    assert ms[v - 1] == ms.min()
+    t0 = time.perf_counter()
+    v2, ms2 = engine.autotune(sims, seed=3)
+    assert v2 == v and np.array_equal(ms, ms2) and time.perf_counter() - t0 < 0.05   # cached
+    # the variant changes the launch shape only: the same walkers, the same counts
+    engine.batch_run(sims, seed=5, precision="split", variant=v)
+    tuned = [s.outputs() for s in sims]
+    engine.batch_run(sims, seed=5, precision="split", variant=1)
+    for s, o in zip(sims, tuned):
+        p = s.outputs()
+        np.testing.assert_array_equal(p["npar_count"], o["npar_count"])
+        assert_fp64_close(p["dx2"], o["dx2"], 1e-9, "dx2")
