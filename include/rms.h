@@ -209,6 +209,23 @@ int rms_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
  * position draws, domain 2 the partial-permeation draws.  A test hook. */
 int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out);
 
+/* A batch launch captured once as a CUDA graph and replayed with new seeds.
+ * rms_batch_graph_create plans the SPLIT launch of rms_batch_run(sims, n,
+ * opts) (uploads the tables, sizes the buffers) and captures its device work
+ * -- axon table from pinned memory, accumulators cleared, the persistent walk,
+ * the reduction, results to pinned memory -- on opts->stream (or the first
+ * simulation's own stream); rms_graph_run(g, seed) replays it with member k's
+ * seed = seed + k * 0x9E3779B97F4A7C15 (as rms_batch_run), waits, and unpacks
+ * the results into the simulations (rms_sim_get as usual).  The graph refers
+ * to the simulations' device buffers: it stays valid while the simulations
+ * exist and no other call gives them a new lattice or larger buffers;
+ * rms_graph_run checks both and returns RMS_ERR_STATE otherwise.  Destroy the
+ * graph before its simulations.  No reference counterpart. */
+typedef struct rms_graph rms_graph;
+int rms_batch_graph_create(rms_sim* const* sims, int n, const rms_run_opts* opts, rms_graph** graph);
+int rms_graph_run(rms_graph* graph, uint64_t seed);
+void rms_graph_destroy(rms_graph* graph);
+
 /* Autotuner of the SPLIT walk's launch variant for a batch (n >= 1 sims, as
  * rms_batch_run would walk them with opts): every variant walks the same
  * subset of each simulation's walkers (about four waves of the GPU), the

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <sstream>
 #include <tuple>
@@ -74,7 +75,7 @@ struct rms_device_state {
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     DevBuf labels, packed, axons, wavef, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
         ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave;
-    HostPinned h_out;
+    HostPinned h_out, h_axons;
     size_t labels_bytes = 0;
     bool packed_valid = false;
 
@@ -85,6 +86,7 @@ struct rms_device_state {
                           &tr_vox, &tr_ev, &tr_pos, &adj_g, &adj_sums, &adj_dwave})
             b->release();
         h_out.release();
+        h_axons.release();
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
         if (e2) cudaEventDestroy(e2);
@@ -374,10 +376,26 @@ bool same_schedule(const rms_sim* a, const rms_sim* b) {
            a->bvec == b->bvec && a->grad == b->grad && a->nbins == b->nbins && a->wave == b->wave;
 }
 
+// One launch, in three parts: plan (validate, shape, allocate, upload the
+// tables), enqueue (device work only: accumulators cleared, axon table, walk,
+// reduction, results to pinned host memory -- what a CUDA graph captures),
+// finish (wait, check the error word, unpack into the simulations).
+struct LaunchPlan {
+    WalkArgs a{};
+    rms_device_state* d = nullptr;
+    cudaStream_t st = nullptr;
+    int prec = 0, grid = 0, block = 0, variant = 0, bits = 8, naxons = 0, T = 0, nb = 0, ngrad = 0,
+        ngrad_pad = 0, nvals = 0, nseg = 0;
+    size_t row = 0, nrow = 0, nsig = 0;
+    bool multi = false, has_sig = false, wavemode = false;
+    int64_t trace_n = 0;
+    std::vector<AxonDesc> axons;
+};
+
 // Run one launch: COMPAT (one simulation) or SPLIT (one or more simulations,
 // "axons", walked by one persistent grid).  The first job's simulation owns
 // the launch's accumulators.
-int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
+int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan& p) {
     rms_sim* s = jobs[0].s;
     const int prec = o ? o->precision : RMS_PREC_COMPAT;
     if (prec != RMS_PREC_COMPAT && prec != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "precision");
@@ -442,7 +460,6 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     const bool multi = naxons > 1;
 
     // inputs
-    std::vector<AxonDesc> axons;
     for (LaunchJob& j : jobs) {
         int rc = prepare_lattice(j.s, st, prec == RMS_PREC_SPLIT, lattice_bits);
         if (rc) return rc;
@@ -469,25 +486,20 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
         RMS_CUDA(upload(d->wavef, wf, st));
     }
     if (prec == RMS_PREC_SPLIT) {
-        axons.resize(naxons);
+        p.axons.resize(naxons);
         for (int k = 0; k < naxons; ++k)
-            fill_axon_desc(axons[k], jobs[k].s, jobs[k].w0, jobs[k].w1, tile_begin[k], jobs[k].seed,
+            fill_axon_desc(p.axons[k], jobs[k].s, jobs[k].w0, jobs[k].w1, tile_begin[k], jobs[k].seed,
                            jobs[k].s->dev->packed.as<uint8_t>());
-        RMS_CUDA(upload(d->axons, axons, st));
+        RMS_CUDA(d->axons.ensure(sizeof(AxonDesc) * naxons));
     }
 
     // accumulators
     RMS_CUDA(d->slots.ensure((size_t)nseg * row * sizeof(double)));
-    RMS_CUDA(cudaMemsetAsync(d->slots.p, 0, (size_t)nseg * row * sizeof(double), st));
     RMS_CUDA(d->out.ensure((size_t)naxons * row * sizeof(double)));
-    if (multi) RMS_CUDA(cudaMemsetAsync(d->out.p, 0, (size_t)naxons * row * sizeof(double), st));
     RMS_CUDA(d->err.ensure(sizeof(int)));
-    RMS_CUDA(cudaMemsetAsync(d->err.p, 0, sizeof(int), st));
     if (has_sig) {
         RMS_CUDA(d->sig_slots.ensure((size_t)nseg * ngrad_pad * sizeof(double)));
-        RMS_CUDA(cudaMemsetAsync(d->sig_slots.p, 0, (size_t)nseg * ngrad_pad * sizeof(double), st));
         RMS_CUDA(d->out_sig.ensure((size_t)naxons * ngrad_pad * sizeof(double)));
-        if (multi) RMS_CUDA(cudaMemsetAsync(d->out_sig.p, 0, (size_t)naxons * ngrad_pad * sizeof(double), st));
         const size_t per_thread = wavemode ? (size_t)s->nwave : (size_t)s->npairs * 3;
         RMS_CUDA(d->vscr.ensure(std::max<size_t>(per_thread * nthr * sizeof(double), 16)));
     }
@@ -497,8 +509,12 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
         RMS_CUDA(d->tr_ev.ensure((size_t)trace_n * s->tn * sizeof(uint32_t)));
         RMS_CUDA(d->tr_pos.ensure((size_t)trace_n * s->tn * 3 * sizeof(double)));
     }
+    const size_t nrow = (size_t)naxons * row, nsig = (size_t)naxons * ngrad_pad;
+    RMS_CUDA(d->h_out.ensure((nrow + nsig + 1) * sizeof(double)));
+    if (prec == RMS_PREC_SPLIT) RMS_CUDA(d->h_axons.ensure(sizeof(AxonDesc) * naxons));
 
-    WalkArgs a{};
+    WalkArgs& a = p.a;
+    a = WalkArgs{};
     a.labels = d->labels.as<uint8_t>();
     a.n1 = s->n1; a.n2 = s->n2; a.n3 = s->n3;
     a.walker_begin = jobs[0].w0; a.walker_end = jobs[0].w1;
@@ -530,57 +546,92 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
     a.traj = traj;
     a.out_rows = d->out.as<double>();
     a.out_sig = d->out_sig.as<double>();
-    if (!axons.empty()) a.axon0 = axons[0];
+    if (!p.axons.empty()) a.axon0 = p.axons[0];
     a.trace_n = trace_n;
     a.tr_init = d->tr_init.as<int32_t>(); a.tr_vox = d->tr_vox.as<int32_t>(); a.tr_ev = d->tr_ev.as<uint32_t>();
     a.tr_pos = d->tr_pos.as<double>();
 
-    RMS_CUDA(cudaEventRecord(d->e0, st));
-    int e = (prec == RMS_PREC_COMPAT) ? launch_walk_compat(a, grid, block, trace_n > 0, st)
-                                      : launch_walk_split(a, lattice_bits, variant, grid, st);
+    p.d = d; p.st = st; p.prec = prec; p.grid = grid; p.block = block; p.variant = variant; p.bits = lattice_bits;
+    p.naxons = naxons; p.T = T; p.nb = nb; p.ngrad = ngrad; p.ngrad_pad = ngrad_pad; p.nvals = nvals; p.nseg = nseg;
+    p.row = row; p.nrow = nrow; p.nsig = nsig; p.multi = multi; p.has_sig = has_sig; p.wavemode = wavemode;
+    p.trace_n = trace_n;
+    return RMS_OK;
+}
+
+// Device work of one launch, all asynchronous on p.st.  The axon table comes
+// from the pinned host copy (which the caller fills); `events` brackets the
+// walk and the reduction with the timing events (not inside a graph).
+int enqueue_launch(LaunchPlan& p, rms_sim* s, bool events) {
+    rms_device_state* d = p.d;
+    cudaStream_t st = p.st;
+    const WalkArgs& a = p.a;
+    if (p.prec == RMS_PREC_SPLIT)
+        RMS_CUDA(cudaMemcpyAsync(d->axons.p, d->h_axons.p, sizeof(AxonDesc) * p.naxons, cudaMemcpyHostToDevice, st));
+    RMS_CUDA(cudaMemsetAsync(d->slots.p, 0, (size_t)p.nseg * p.row * sizeof(double), st));
+    if (p.multi) RMS_CUDA(cudaMemsetAsync(d->out.p, 0, p.nrow * sizeof(double), st));
+    RMS_CUDA(cudaMemsetAsync(d->err.p, 0, sizeof(int), st));
+    if (p.has_sig) {
+        RMS_CUDA(cudaMemsetAsync(d->sig_slots.p, 0, (size_t)p.nseg * p.ngrad_pad * sizeof(double), st));
+        if (p.multi) RMS_CUDA(cudaMemsetAsync(d->out_sig.p, 0, p.nsig * sizeof(double), st));
+    }
+    if (events) RMS_CUDA(cudaEventRecord(d->e0, st));
+    int e = (p.prec == RMS_PREC_COMPAT) ? launch_walk_compat(a, p.grid, p.block, p.trace_n > 0, st)
+                                        : launch_walk_split(a, p.bits, p.variant, p.grid, st);
     if (e) return cuda_fail((cudaError_t)e, "walk kernel launch");
-    RMS_CUDA(cudaEventRecord(d->e1, st));
-    if (!multi) {
+    if (events) RMS_CUDA(cudaEventRecord(d->e1, st));
+    if (!p.multi) {
         // one axon: the warps' rows summed in a fixed order (repeatable)
-        e = launch_reduce_slots(a.slots, nseg, row, d->out.as<double>(), st);
-        if (!e && has_sig)
-            e = launch_reduce_slots(a.sig_slots, nseg, (size_t)ngrad_pad, d->out_sig.as<double>(), st);
+        e = launch_reduce_slots(a.slots, p.nseg, p.row, d->out.as<double>(), st);
+        if (!e && p.has_sig)
+            e = launch_reduce_slots(a.sig_slots, p.nseg, (size_t)p.ngrad_pad, d->out_sig.as<double>(), st);
         if (e) return cuda_fail((cudaError_t)e, "reduce launch");
     }
-    RMS_CUDA(cudaEventRecord(d->e2, st));
+    if (events) RMS_CUDA(cudaEventRecord(d->e2, st));
 
     // results back (one pinned staging buffer: rows, then signals, then the error word)
-    const size_t nrow = (size_t)naxons * row, nsig = (size_t)naxons * ngrad_pad;
-    RMS_CUDA(d->h_out.ensure((nrow + nsig + 1) * sizeof(double)));
     double* h = static_cast<double*>(d->h_out.p);
-    RMS_CUDA(cudaMemcpyAsync(h, d->out.p, nrow * sizeof(double), cudaMemcpyDeviceToHost, st));
-    if (has_sig)
-        RMS_CUDA(cudaMemcpyAsync(h + nrow, d->out_sig.p, nsig * sizeof(double), cudaMemcpyDeviceToHost, st));
-    int* herr = reinterpret_cast<int*>(h + nrow + nsig);
+    RMS_CUDA(cudaMemcpyAsync(h, d->out.p, p.nrow * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (p.has_sig)
+        RMS_CUDA(cudaMemcpyAsync(h + p.nrow, d->out_sig.p, p.nsig * sizeof(double), cudaMemcpyDeviceToHost, st));
+    int* herr = reinterpret_cast<int*>(h + p.nrow + p.nsig);
     RMS_CUDA(cudaMemcpyAsync(herr, d->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (trace_n) {
-        s->tr_init.resize(trace_n);
-        s->tr_vox.resize((size_t)trace_n * s->tn);
-        s->tr_ev.resize((size_t)trace_n * s->tn);
-        s->tr_pos.resize((size_t)trace_n * s->tn * 3);
-        RMS_CUDA(cudaMemcpyAsync(s->tr_init.data(), d->tr_init.p, trace_n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    if (p.trace_n) {
+        const size_t tn = (size_t)s->tn, n = (size_t)p.trace_n;
+        s->tr_init.resize(n);
+        s->tr_vox.resize(n * tn);
+        s->tr_ev.resize(n * tn);
+        s->tr_pos.resize(n * tn * 3);
+        RMS_CUDA(cudaMemcpyAsync(s->tr_init.data(), d->tr_init.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         RMS_CUDA(cudaMemcpyAsync(s->tr_vox.data(), d->tr_vox.p, s->tr_vox.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         RMS_CUDA(cudaMemcpyAsync(s->tr_ev.data(), d->tr_ev.p, s->tr_ev.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         RMS_CUDA(cudaMemcpyAsync(s->tr_pos.data(), d->tr_pos.p, s->tr_pos.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
-    RMS_CUDA(cudaStreamSynchronize(st));
-    if (*herr & kErrInitCap)
+    return RMS_OK;
+}
+
+int finish_launch(std::vector<LaunchJob>& jobs, LaunchPlan& p, bool events) {
+    rms_device_state* d = p.d;
+    RMS_CUDA(cudaStreamSynchronize(p.st));
+    const double* h = static_cast<const double*>(d->h_out.p);
+    const int herr = *reinterpret_cast<const int*>(h + p.nrow + p.nsig);
+    if (herr & kErrInitCap)
         return set_error(RMS_ERR_RANGE, "a walker found no labelled voxel within the rejection-sampling cap");
-    if (*herr & kErrStep) return set_error(RMS_ERR_RANGE, "a step segment found no voxel face (step >= 1 voxel)");
+    if (herr & kErrStep) return set_error(RMS_ERR_RANGE, "a step segment found no voxel face (step >= 1 voxel)");
 
     float ms_walk = 0.f, ms_run = 0.f;
-    RMS_CUDA(cudaEventElapsedTime(&ms_walk, d->e0, d->e1));
-    RMS_CUDA(cudaEventElapsedTime(&ms_run, d->e0, d->e2));
+    if (events) {
+        RMS_CUDA(cudaEventElapsedTime(&ms_walk, d->e0, d->e1));
+        RMS_CUDA(cudaEventElapsedTime(&ms_run, d->e0, d->e2));
+    } else {
+        RMS_CUDA(cudaEventElapsedTime(&ms_walk, d->e0, d->e1));
+        ms_run = ms_walk;
+    }
 
     // unpack record rows into the reference's field layouts
-    for (int k = 0; k < naxons; ++k) {
+    const int T = p.T, nb = p.nb, ngrad = p.ngrad;
+    for (int k = 0; k < p.naxons; ++k) {
         rms_sim* sk = jobs[k].s;
-        const double* hk = h + (size_t)k * row;
+        const double* hk = h + (size_t)k * p.row;
         const int nc = sk->nc;
         sk->sig0.assign(T, 0.0);
         sk->dx2.assign((size_t)T * 6, 0.0);
@@ -588,7 +639,7 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
         sk->npar_count.assign((size_t)T * nc, 0.0);
         sk->sigre.assign((size_t)T * nb, 0.0);
         for (int t = 0; t < T; ++t) {
-            const double* r = hk + (size_t)t * nvals;
+            const double* r = hk + (size_t)t * p.nvals;
             sk->sig0[t] = r[kColSig0];
             for (int q = 0; q < 6; ++q) sk->dx2[t * 6 + q] = r[kColDx2 + q];
             for (int q = 0; q < 15; ++q) sk->dx4[t * 15 + q] = r[kColDx4 + q];
@@ -597,17 +648,103 @@ int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
                 for (int q = 0; q < nb; ++q) sk->sigre[(size_t)t * nb + q] = r[kRowHead + q];
         }
         sk->sig.assign(sk->mode == RMS_MODE_PGSE ? ngrad : 0, 0.0);
-        for (int q = 0; q < (int)sk->sig.size(); ++q) sk->sig[q] = h[nrow + (size_t)k * ngrad_pad + q];
-        sk->sigw.assign(wavemode ? ngrad : 0, 0.0);
-        for (int q = 0; q < (int)sk->sigw.size(); ++q) sk->sigw[q] = h[nrow + (size_t)k * ngrad_pad + q];
-        sk->trace_n = k == 0 ? trace_n : 0;
+        for (int q = 0; q < (int)sk->sig.size(); ++q) sk->sig[q] = h[p.nrow + (size_t)k * p.ngrad_pad + q];
+        sk->sigw.assign(p.wavemode ? ngrad : 0, 0.0);
+        for (int q = 0; q < (int)sk->sigw.size(); ++q) sk->sigw[q] = h[p.nrow + (size_t)k * p.ngrad_pad + q];
+        sk->trace_n = k == 0 ? p.trace_n : 0;
         sk->walk_ms = ms_walk;
         sk->run_ms = ms_run;
-        sk->last_grid = grid;
-        sk->last_block = block;
+        sk->last_grid = p.grid;
+        sk->last_block = p.block;
         sk->have_results = true;
     }
     return RMS_OK;
+}
+
+int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
+    LaunchPlan p;
+    int rc = plan_launch(jobs, o, p);
+    if (rc) return rc;
+    if (p.prec == RMS_PREC_SPLIT)
+        std::memcpy(p.d->h_axons.p, p.axons.data(), sizeof(AxonDesc) * p.naxons);
+    rc = enqueue_launch(p, jobs[0].s, true);
+    if (rc) return rc;
+    return finish_launch(jobs, p, true);
+}
+
+}  // namespace
+}  // namespace rms
+
+// A captured batch launch (rms_batch_graph_create): the plan, the simulations
+// it walks, and the device buffers the graph refers to.
+struct rms_graph {
+    std::vector<rms::LaunchJob> jobs;
+    rms::LaunchPlan plan;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> buffers;
+    int device = 0;
+    ~rms_graph() {
+        cudaSetDevice(device);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace rms {
+namespace {
+
+std::vector<const void*> graph_buffers(const rms_graph* g) {
+    const rms_device_state* d = g->plan.d;
+    std::vector<const void*> v{d->axons.p, d->slots.p, d->out.p, d->err.p, d->sig_slots.p, d->out_sig.p,
+                               d->vscr.p, d->tables.p, d->qtab.p, d->bvec.p, d->grad.p, d->gpair.p,
+                               d->ev_step.p, d->ev_pair.p, d->ev_coef.p, d->wavef.p, d->h_out.p, d->h_axons.p};
+    for (const LaunchJob& j : g->jobs) v.push_back(j.s->dev ? j.s->dev->packed.p : nullptr);
+    return v;
+}
+
+int graph_create(rms_sim* const* sims, int n, const rms_run_opts* o, rms_graph** out) {
+    if (!o || o->precision != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "a graph captures the SPLIT walk");
+    if (o->trace_walkers > 0 || o->traj_out) return set_error(RMS_ERR_ARG, "a graph records no traces or trajectories");
+    std::unique_ptr<rms_graph> g(new rms_graph());
+    g->device = o->device;
+    for (int i = 0; i < n; ++i) g->jobs.push_back(LaunchJob{sims[i], 0, sims[i]->npar, o->seed + (uint64_t)i * kBatchSeedStep});
+    rms_run_opts oo = *o;
+    int rc = plan_launch(g->jobs, &oo, g->plan);
+    if (rc) return rc;
+    LaunchPlan& p = g->plan;
+    if (!o->stream) p.st = p.d->own;   // capture needs a stream other than the legacy default stream
+    std::memcpy(p.d->h_axons.p, p.axons.data(), sizeof(AxonDesc) * p.naxons);
+    RMS_CUDA(cudaStreamBeginCapture(p.st, cudaStreamCaptureModeThreadLocal));
+    rc = enqueue_launch(p, g->jobs[0].s, false);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(p.st, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ec != cudaSuccess) return cuda_fail(ec, "stream capture of the batch launch");
+    g->graph = graph;
+    RMS_CUDA(cudaGraphInstantiate(&g->exec, graph, 0));
+    g->buffers = graph_buffers(g.get());
+    *out = g.release();
+    return RMS_OK;
+}
+
+int graph_run(rms_graph* g, uint64_t seed) {
+    for (const LaunchJob& j : g->jobs)
+        if (j.s->lattice_dirty || !j.s->dev || !j.s->dev->packed_valid)
+            return set_error(RMS_ERR_STATE, "a simulation of the graph has a new lattice: create the graph again");
+    if (graph_buffers(g) != g->buffers)
+        return set_error(RMS_ERR_STATE, "the graph's device buffers were reallocated by another run: create the graph again");
+    LaunchPlan& p = g->plan;
+    RMS_CUDA(cudaSetDevice(g->device));
+    for (int k = 0; k < p.naxons; ++k) p.axons[k].seed = seed + (uint64_t)k * kBatchSeedStep;
+    std::memcpy(p.d->h_axons.p, p.axons.data(), sizeof(AxonDesc) * p.naxons);
+    RMS_CUDA(cudaEventRecord(p.d->e0, p.st));
+    RMS_CUDA(cudaGraphLaunch(g->exec, p.st));
+    RMS_CUDA(cudaEventRecord(p.d->e1, p.st));
+    return finish_launch(g->jobs, p, false);
 }
 
 // Launch-variant autotuner: each variant walks the same subset of every
@@ -945,6 +1082,29 @@ int rms_sim_run(rms_sim* s, const rms_run_opts* opts) {
         return set_error(RMS_ERR_NOMEM, e.what());
     }
 }
+
+int rms_batch_graph_create(rms_sim* const* sims, int n, const rms_run_opts* opts, rms_graph** out) {
+    if (!sims || n < 1 || !out) return set_error(RMS_ERR_ARG, "null argument");
+    for (int i = 0; i < n; ++i)
+        if (!sims[i]) return set_error(RMS_ERR_ARG, "null simulation in the batch");
+    *out = nullptr;
+    try {
+        return graph_create(sims, n, opts, out);
+    } catch (const std::exception& e) {
+        return set_error(RMS_ERR_NOMEM, e.what());
+    }
+}
+
+int rms_graph_run(rms_graph* g, uint64_t seed) {
+    if (!g) return set_error(RMS_ERR_ARG, "null graph");
+    try {
+        return graph_run(g, seed);
+    } catch (const std::exception& e) {
+        return set_error(RMS_ERR_NOMEM, e.what());
+    }
+}
+
+void rms_graph_destroy(rms_graph* g) { delete g; }
 
 int rms_autotune(rms_sim* const* sims, int n, const rms_run_opts* opts, int* variant, double* variant_ms) {
     if (!sims || n < 1 || !variant) return set_error(RMS_ERR_ARG, "null argument");

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         }
         const uint8_t* lat = AXF(lat);
         const int s0 = AXF(s0), s1 = AXF(s1);
-        const uint64_t seed = AXF(seed);
+        const uint64_t seed = a.axons[ONE ? 0 : ax].seed;   // device table: a replayed launch may change it
         const bool flight = (BITS != 2) && AXF(flight);
         const bool same_certain = AXF(same_cross);
         const float* t_step = tab;

@@ -32,7 +32,7 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
            "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases",
-           "rms_adjoint_run", "rms_autotune")
+           "rms_adjoint_run", "rms_autotune", "rms_batch_graph_create", "rms_graph_run", "rms_graph_destroy")
 CONTRACT = {"fp32": 0, "bf16x3": 1}
 
 _DP = C.POINTER(C.c_double)
@@ -85,7 +85,7 @@ def lib():
         L.rms_last_error.restype = C.c_char_p
         L.rms_version.restype = C.c_char_p
         for name in EXPORTS:
-            if name not in ("rms_last_error", "rms_version", "rms_sim_destroy"):
+            if name not in ("rms_last_error", "rms_version", "rms_sim_destroy", "rms_graph_destroy"):
                 getattr(L, name).restype = C.c_int
         L.rms_sim_destroy.restype = None
         L.rms_sim_create.argtypes = [C.POINTER(Config), C.POINTER(C.c_void_p)]
@@ -107,6 +107,10 @@ def lib():
         L.rms_sim_run_noalloc.argtypes = [C.c_void_p, C.POINTER(RunOpts), C.c_void_p, C.c_void_p, C.c_void_p]
         L.rms_rng_split.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_float)]
         L.rms_split_variant.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.rms_batch_graph_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_void_p)]
+        L.rms_graph_run.argtypes = [C.c_void_p, C.c_uint64]
+        L.rms_graph_destroy.argtypes = [C.c_void_p]
+        L.rms_graph_destroy.restype = None
         L.rms_autotune.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_int), _DP]
         L.rms_adjoint_run.argtypes = [C.c_void_p, C.POINTER(RunOpts), _DP, C.POINTER(AdjointGrads)]
         L.rms_contract_phases.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_int,
@@ -319,6 +323,33 @@ def contract_phases(d_pos: int, nwalk: int, nbins: int, d_wave: int, nwave: int,
     _check(lib().rms_contract_phases(C.c_void_p(int(d_pos)), int(nwalk), int(nbins), C.c_void_p(int(d_wave)),
                                      int(nwave), CONTRACT[method], C.c_void_p(int(d_out)), st, C.byref(ms)))
     return ms.value
+
+
+class Graph:
+    """A batch launch captured as a CUDA graph (rms_batch_graph_create) and
+    replayed per seed (rms_graph_run); results land in the simulations."""
+
+    def __init__(self, sims, seed: int = 0, device: int = 0, stream=None, variant: int = 0):
+        self._h = C.c_void_p()
+        self.sims = list(sims)
+        arr = (C.c_void_p * len(sims))(*[s._h.value for s in sims])
+        st = None if stream is None else C.c_void_p(int(stream))
+        opts = RunOpts(int(seed), PRECISION["split"], int(device), st, 0, int(variant), 0, 0, None)
+        _check(lib().rms_batch_graph_create(arr, len(sims), C.byref(opts), C.byref(self._h)))
+
+    def run(self, seed: int):
+        _check(lib().rms_graph_run(self._h, int(seed) & ((1 << 64) - 1)))
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().rms_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def autotune(sims, seed: int = 0, device: int = 0, stream=None):

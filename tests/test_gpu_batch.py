@@ -82,3 +82,23 @@ def test_autotune_picks_a_variant_and_caches_it():
         p = s.outputs()
         np.testing.assert_array_equal(p["npar_count"], o["npar_count"])
         assert_fp64_close(p["dx2"], o["dx2"], 1e-9, "dx2")
+
+
+def test_graph_replays_equal_batch_runs():
+    sims = axon_sims("pgse")
+    g = engine.Graph(sims, seed=0)
+    for seed in (21, 22):
+        g.run(seed)
+        replay = [s.outputs() for s in sims]
+        engine.batch_run(sims, seed=seed, precision="split")
+        for s, o in zip(sims, replay):
+            p = s.outputs()
+            np.testing.assert_array_equal(p["npar_count"], o["npar_count"])
+            assert_fp64_close(p["dx2"], o["dx2"], 1e-9, "dx2")
+            np.testing.assert_allclose(p["sig"], o["sig"], rtol=1e-9, atol=1e-9)
+    assert not np.array_equal(replay[0]["dx2"], sims[0].outputs()["dx2"] * 0)
+    # a new lattice invalidates the captured launch
+    sims[1].set_lattice(geometry.axon_lattice(24, 20, 32, 0.1, seed=9, exterior=2, r0=0.5))
+    with pytest.raises(engine.RmsError):
+        g.run(23)
+    g.close()
