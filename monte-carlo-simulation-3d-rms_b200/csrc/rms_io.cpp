@@ -122,6 +122,34 @@ int parse_lattice_text(const std::string& path, size_t n, std::vector<uint8_t>& 
     return RMS_OK;
 }
 
+// fiber.bin (engine extension): the same labels as fiber.txt, one byte per
+// voxel, i outer, k fastest, nothing else -- read as it lies instead of
+// parsed (a 256x256x2048 lattice is 134 M integers of text).
+int read_lattice_binary(const std::string& path, size_t n, std::vector<uint8_t>& out, int nc) {
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return set_error(RMS_ERR_IO, "cannot open " + path);
+    std::fseek(f, 0, SEEK_END);
+    const long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (size < 0 || (size_t)size != n) {
+        std::fclose(f);
+        std::ostringstream m;
+        m << path << ": " << size << " bytes; the lattice has " << n << " voxels (one byte each)";
+        return set_error(RMS_ERR_FORMAT, m.str());
+    }
+    out.assign(n, 0);
+    const size_t got = std::fread(out.data(), 1, n, f);
+    std::fclose(f);
+    if (got != n) return set_error(RMS_ERR_IO, path + ": short read");
+    for (size_t i = 0; i < n; ++i)
+        if (out[i] >= nc) {
+            std::ostringstream m;
+            m << path << ": label " << (int)out[i] << " at voxel " << i << " is not below Nc";
+            return set_error(RMS_ERR_RANGE, m.str());
+        }
+    return RMS_OK;
+}
+
 int load_run_dir(const char* dir, int mode, rms_sim* s) {
     const std::string grad_path = join(dir, "gradient_time.txt");
     if (mode == RMS_MODE_AUTO) mode = exists(grad_path) ? RMS_MODE_PGSE : RMS_MODE_NARROW;
@@ -170,7 +198,12 @@ int load_run_dir(const char* dir, int mode, rms_sim* s) {
     }
     if ((rc = finalize_config(s))) return rc;
     const size_t nvox = (size_t)s->n1 * s->n2 * s->n3;
-    if ((rc = parse_lattice_text(join(dir, "fiber.txt"), nvox, s->labels, s->nc))) return rc;
+    const std::string bin = join(dir, "fiber.bin");
+    if (exists(bin)) {
+        if ((rc = read_lattice_binary(bin, nvox, s->labels, s->nc))) return rc;
+    } else if ((rc = parse_lattice_text(join(dir, "fiber.txt"), nvox, s->labels, s->nc))) {
+        return rc;
+    }
     s->have_lattice = true;
     s->lattice_dirty = true;
     return RMS_OK;

@@ -40,14 +40,22 @@ def write_lattice(path: str, labels: np.ndarray) -> None:
             f.write("".join(digits[s:s + step].tolist()))
 
 
+def write_lattice_binary(path: str, labels: np.ndarray) -> None:
+    """fiber.bin: the labels of fiber.txt as raw bytes, i outer, k fastest
+    (engine extension; the engine reads it in place of fiber.txt)."""
+    np.ascontiguousarray(labels, dtype=np.uint8).reshape(-1).tofile(path)
+
+
 def write_inputs(target: str, labels: np.ndarray, *, dt: float, tn: int, npar: int,
-                 res: float, diffusivity, t2, bval=None, bvec=None, grad=None) -> None:
+                 res: float, diffusivity, t2, bval=None, bvec=None, grad=None,
+                 lattice: str = "txt") -> None:
     """Write one run directory.
 
     Narrow-pulse form when ``bval``/``bvec`` are given (setupRMS.m:16-69);
     PGSE form when ``grad`` (Ngrad x 6: Delta, delta, |g|, gx, gy, gz) is
     given (main_PGSE.cu:440-445, 495-506).  Units: ms, um, um^2/ms,
-    rad/(um ms) for |g|.
+    rad/(um ms) for |g|.  ``lattice``: "txt" (fiber.txt, what the reference
+    reads), "bin" (fiber.bin only) or "both".
     """
     os.makedirs(target, exist_ok=True)
     labels = np.asarray(labels)
@@ -62,7 +70,12 @@ def write_inputs(target: str, labels: np.ndarray, *, dt: float, tn: int, npar: i
     pgse = grad is not None
     if pgse == (bval is not None):
         raise ValueError("give either bval/bvec (narrow pulse) or grad (PGSE)")
-    write_lattice(os.path.join(target, "fiber.txt"), labels)
+    if lattice not in ("txt", "bin", "both"):
+        raise ValueError("lattice must be 'txt', 'bin' or 'both'")
+    if lattice in ("txt", "both"):
+        write_lattice(os.path.join(target, "fiber.txt"), labels)
+    if lattice in ("bin", "both"):
+        write_lattice_binary(os.path.join(target, "fiber.bin"), labels)
     lines = [_fmt_e(dt), _fmt_u(tn), _fmt_u(npar)]
     if not pgse:
         bv = np.atleast_1d(np.asarray(bval, dtype=np.float64))

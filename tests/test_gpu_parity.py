@@ -199,3 +199,20 @@ def test_cli_drop_in(tmp_path):
     got = runio.read_outputs(d)
     assert np.array_equal(got.npar_count, want.npar_count)
     assert_fp64_close(got.sig, want.sig, RTOL, "sig")
+
+
+def test_cli_binary_lattice_gives_the_reference_outputs(tmp_path):
+    """fiber.bin (raw bytes) in place of fiber.txt: the same walk, the same
+    reference output files."""
+    d = unpack_golden("narrow_3comp", str(tmp_path / "run"), inputs_only=True)
+    want = runio.read_outputs(unpack_golden("narrow_3comp", str(tmp_path / "want")))
+    vals = np.array(open(os.path.join(d, "fiber.txt")).read().split(), dtype=np.uint8)
+    os.remove(os.path.join(d, "fiber.txt"))
+    runio.write_lattice_binary(os.path.join(d, "fiber.bin"), vals)
+    r = subprocess.run([engine.CLI_PATH, "--seed", str(golden_seed("narrow_3comp"))], cwd=d,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = runio.read_outputs(d)
+    assert np.array_equal(got.npar_count, want.npar_count)
+    assert_fp64_close(got.sigre, want.sigre, RTOL, "sigRe")
+    assert_fp64_close(got.dx4, want.dx4, RTOL, "dx4")

@@ -139,3 +139,34 @@ def test_run_without_gpu_fails_loudly():
     with pytest.raises(engine.RmsError) as e:
         s.run(seed=1)
     assert e.value.code == -5
+
+
+def test_binary_lattice_is_read_in_place_of_text(tmp_path):
+    from rms_b200 import runio
+    d = unpack_golden("narrow_3comp", str(tmp_path / "a"), inputs_only=True)
+    vals = np.array(open(os.path.join(d, "fiber.txt")).read().split(), dtype=np.uint8)
+    runio.write_lattice_binary(os.path.join(d, "fiber.bin"), vals)
+    # fiber.bin wins: a broken fiber.txt beside it is not read
+    open(os.path.join(d, "fiber.txt"), "w").write("0 0 0")
+    engine.Sim.from_dir(d)
+    # wrong size and labels >= Nc are refused
+    vals[:-1].tofile(os.path.join(d, "fiber.bin"))
+    with pytest.raises(engine.RmsError) as e:
+        engine.Sim.from_dir(d)
+    assert e.value.code == -3
+    bad = vals.copy()
+    bad[7] = 200
+    bad.tofile(os.path.join(d, "fiber.bin"))
+    with pytest.raises(engine.RmsError) as e:
+        engine.Sim.from_dir(d)
+    assert e.value.code == -4
+
+
+def test_write_inputs_binary_lattice(tmp_path):
+    from rms_b200 import geometry, runio
+    lab = geometry.axon_lattice(8, 8, 12, 0.1, seed=1, exterior=2)
+    runio.write_inputs(str(tmp_path), lab, dt=2e-4, tn=1000, npar=10, res=0.1, diffusivity=[0, 2, 2],
+                       t2=[80, 80, 60], bval=[1.0], bvec=[[1, 0, 0]], lattice="bin")
+    assert not os.path.exists(os.path.join(tmp_path, "fiber.txt"))
+    assert np.array_equal(np.fromfile(os.path.join(tmp_path, "fiber.bin"), dtype=np.uint8), lab.reshape(-1))
+    engine.Sim.from_dir(str(tmp_path))
