@@ -209,6 +209,17 @@ int rms_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
  * position draws, domain 2 the partial-permeation draws.  A test hook. */
 int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out);
 
+/* Cumulants of a finished run, the formulas analysis/readRMS.m applies to the
+ * output files (:44-45 normalisation by sig0 with the tensor multiplicities,
+ * :96-103 D = <x^2>/(2t), K = <x^4>/<x^2>^2 - 3) along ndir unit directions
+ * dirs[ndir*3] (NULL: x, y, z): D[t*ndir + q], K[t*ndir + q] for the
+ * timepoints t.  rms_combine_cumulants combines per-axon D, K ([axon][t][dir])
+ * with volume fractions f[axon] as part1_demo4_analysis.m:88-90 does:
+ * D = sum f D_i, K = 3 (sum f D_i^2 - D^2) / D^2 + sum f D_i^2 K_i / D^2. */
+int rms_sim_cumulants(const rms_sim* sim, const double* dirs, int ndir, double* D, double* K);
+int rms_combine_cumulants(int naxons, int T, int ndir, const double* f, const double* D_axons,
+                          const double* K_axons, double* D, double* K);
+
 /* A batch launch captured once as a CUDA graph and replayed with new seeds.
  * rms_batch_graph_create plans the SPLIT launch of rms_batch_run(sims, n,
  * opts) (uploads the tables, sizes the buffers) and captures its device work

@@ -1083,6 +1083,59 @@ int rms_sim_run(rms_sim* s, const rms_run_opts* opts) {
     }
 }
 
+int rms_sim_cumulants(const rms_sim* s, const double* dirs, int ndir, double* D, double* K) {
+    if (!s || !D || !K) return set_error(RMS_ERR_ARG, "null argument");
+    if (!s->have_results) return set_error(RMS_ERR_STATE, "no results: run the simulation first");
+    static const double axes[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if (!dirs) {
+        dirs = axes;
+        ndir = 3;
+    }
+    if (ndir < 1) return set_error(RMS_ERR_ARG, "ndir must be >= 1");
+    // readRMS.m:13-18: tensor multiplicities and index lists of dx2 / dx4
+    static const double dcnt[6] = {1, 2, 2, 1, 2, 1};
+    static const double wcnt[15] = {1, 4, 4, 6, 12, 6, 4, 12, 12, 4, 1, 4, 6, 4, 1};
+    static const int dind[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+    static const int wind[15][4] = {{0, 0, 0, 0}, {0, 0, 0, 1}, {0, 0, 0, 2}, {0, 0, 1, 1}, {0, 0, 1, 2},
+                                    {0, 0, 2, 2}, {0, 1, 1, 1}, {0, 1, 1, 2}, {0, 1, 2, 2}, {0, 2, 2, 2},
+                                    {1, 1, 1, 1}, {1, 1, 1, 2}, {1, 1, 2, 2}, {1, 2, 2, 2}, {2, 2, 2, 2}};
+    const int T = s->timepoints;
+    for (int q = 0; q < ndir; ++q) {
+        const double* n = dirs + 3 * q;
+        double n2[6], n4[15];
+        for (int i = 0; i < 6; ++i) n2[i] = n[dind[i][0]] * n[dind[i][1]];
+        for (int i = 0; i < 15; ++i) n4[i] = n[wind[i][0]] * n[wind[i][1]] * n[wind[i][2]] * n[wind[i][3]];
+        for (int t = 0; t < T; ++t) {
+            // readRMS.m:44-45 (normalise by sig0 with multiplicities), :96-103 (D, K)
+            double x2 = 0.0, x4 = 0.0;
+            for (int i = 0; i < 6; ++i) x2 += s->dx2[(size_t)t * 6 + i] * dcnt[i] / s->sig0[t] * n2[i];
+            for (int i = 0; i < 15; ++i) x4 += s->dx4[(size_t)t * 15 + i] * wcnt[i] / s->sig0[t] * n4[i];
+            D[(size_t)t * ndir + q] = x2 / 2.0 / s->td[t];
+            K[(size_t)t * ndir + q] = x4 / (x2 * x2) - 3.0;
+        }
+    }
+    return RMS_OK;
+}
+
+int rms_combine_cumulants(int naxons, int T, int ndir, const double* f, const double* Din, const double* Kin,
+                          double* D, double* K) {
+    if (naxons < 1 || T < 1 || ndir < 1 || !f || !Din || !Kin || !D || !K) return set_error(RMS_ERR_ARG, "bad argument");
+    const size_t m = (size_t)T * ndir;
+    for (size_t i = 0; i < m; ++i) {
+        // part1_demo4_analysis.m:88-90
+        double d = 0.0, d2 = 0.0, d2k = 0.0;
+        for (int a = 0; a < naxons; ++a) {
+            const double di = Din[(size_t)a * m + i];
+            d += f[a] * di;
+            d2 += f[a] * di * di;
+            d2k += f[a] * di * di * Kin[(size_t)a * m + i];
+        }
+        D[i] = d;
+        K[i] = 3.0 * (d2 - d * d) / (d * d) + d2k / (d * d);
+    }
+    return RMS_OK;
+}
+
 int rms_batch_graph_create(rms_sim* const* sims, int n, const rms_run_opts* opts, rms_graph** out) {
     if (!sims || n < 1 || !out) return set_error(RMS_ERR_ARG, "null argument");
     for (int i = 0; i < n; ++i)

@@ -32,7 +32,8 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
            "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases",
-           "rms_adjoint_run", "rms_autotune", "rms_batch_graph_create", "rms_graph_run", "rms_graph_destroy")
+           "rms_adjoint_run", "rms_autotune", "rms_batch_graph_create", "rms_graph_run", "rms_graph_destroy",
+           "rms_sim_cumulants", "rms_combine_cumulants")
 CONTRACT = {"fp32": 0, "bf16x3": 1}
 
 _DP = C.POINTER(C.c_double)
@@ -111,6 +112,8 @@ def lib():
         L.rms_graph_run.argtypes = [C.c_void_p, C.c_uint64]
         L.rms_graph_destroy.argtypes = [C.c_void_p]
         L.rms_graph_destroy.restype = None
+        L.rms_sim_cumulants.argtypes = [C.c_void_p, _DP, C.c_int, _DP, _DP]
+        L.rms_combine_cumulants.argtypes = [C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP]
         L.rms_autotune.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_int), _DP]
         L.rms_adjoint_run.argtypes = [C.c_void_p, C.POINTER(RunOpts), _DP, C.POINTER(AdjointGrads)]
         L.rms_contract_phases.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_int,
@@ -242,6 +245,16 @@ class Sim:
         return dict(d_wave=dwave.reshape(nw, nb, 3), d_diffusivity=out.d_diffusivity, d_kappa=out.d_kappa,
                     d_t2=np.array(out.d_t2[:]), loss=out.loss, sigw=sigw.reshape(nw, 2))
 
+    def cumulants(self, dirs=None):
+        """(D, K), [timepoints, ndir], along unit directions dirs [ndir, 3]
+        (default x, y, z); readRMS.m's formulas, computed in the library."""
+        d = None if dirs is None else _arr(dirs)
+        ndir = 3 if d is None else d.size // 3
+        T = self.field_size("sig0")
+        D, K = np.zeros(T * ndir), np.zeros(T * ndir)
+        _check(lib().rms_sim_cumulants(self._h, _ptr(d) if d is not None else None, ndir, _ptr(D), _ptr(K)))
+        return D.reshape(T, ndir), K.reshape(T, ndir)
+
     def field_size(self, name: str) -> int:
         n = C.c_size_t()
         _check(lib().rms_sim_field_size(self._h, FIELD[name], C.byref(n)))
@@ -323,6 +336,16 @@ def contract_phases(d_pos: int, nwalk: int, nbins: int, d_wave: int, nwave: int,
     _check(lib().rms_contract_phases(C.c_void_p(int(d_pos)), int(nwalk), int(nbins), C.c_void_p(int(d_wave)),
                                      int(nwave), CONTRACT[method], C.c_void_p(int(d_out)), st, C.byref(ms)))
     return ms.value
+
+
+def combine_cumulants(f, Ds, Ks):
+    """Volume-weighted D, K of several axons (part1_demo4_analysis.m:88-90):
+    f [naxons], Ds/Ks [naxons, T, ndir] -> (D, K) [T, ndir]."""
+    Ds, Ks = np.asarray(Ds, dtype=np.float64), np.asarray(Ks, dtype=np.float64)
+    na, T, nd = Ds.shape
+    D, K = np.zeros(T * nd), np.zeros(T * nd)
+    _check(lib().rms_combine_cumulants(na, T, nd, _ptr(_arr(f)), _ptr(_arr(Ds)), _ptr(_arr(Ks)), _ptr(D), _ptr(K)))
+    return D.reshape(T, nd), K.reshape(T, nd)
 
 
 class Graph:

@@ -96,3 +96,21 @@ def test_parallel_planes(precision):
     assert abs(D[300:, 1:].mean() / 2.0 - 1) < 0.02          # parallel: free
     late = slice(800, None)
     np.testing.assert_allclose(D[late, 0], a * a / (12 * t[late]), rtol=0.08)
+
+
+def test_library_cumulants_match_the_readrms_restatement():
+    from rms_b200 import analysis
+    lab = np.ones((20, 20, 20), dtype=np.uint8)
+    sim = engine.Sim(lab, dt=2e-4, tn=2000, npar=20000, res=0.1, diffusivity=[0, 2.0], t2=[1e6, 1e6],
+                     bval=[], bvec=np.zeros((0, 3)), boundary="periodic")
+    o = sim.run(seed=3, precision="split").outputs()
+    D, K = sim.cumulants()
+    Dw, Kw = analysis.axis_dk(o["sig0"], o["dx2"], o["dx4"], o["td"])
+    np.testing.assert_allclose(D[1:], Dw[1:], rtol=1e-12)
+    np.testing.assert_allclose(K[5:], Kw[5:], rtol=1e-9, atol=1e-12)
+    n = np.array([[0.6, 0.8, 0.0], [0.0, 0.6, 0.8]])
+    Dn, Kn = sim.cumulants(n)
+    dx2t, dx4t = analysis.normalized_moments(o["sig0"], o["dx2"], o["dx4"])
+    Kr, Dr = analysis.akc_mom(dx2t, dx4t, o["td"], n)
+    np.testing.assert_allclose(Dn[1:], Dr[1:], rtol=1e-12)
+    np.testing.assert_allclose(abs(Dn[-1] / 2.0 - 1).max(), 0, atol=0.02)

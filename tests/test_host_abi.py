@@ -170,3 +170,21 @@ def test_write_inputs_binary_lattice(tmp_path):
     assert not os.path.exists(os.path.join(tmp_path, "fiber.txt"))
     assert np.array_equal(np.fromfile(os.path.join(tmp_path, "fiber.bin"), dtype=np.uint8), lab.reshape(-1))
     engine.Sim.from_dir(str(tmp_path))
+
+
+def test_combine_cumulants_matches_the_demo_formula():
+    rng = np.random.default_rng(0)
+    na, T, nd = 5, 40, 3
+    f = rng.dirichlet(np.ones(na))
+    Ds = rng.uniform(0.5, 2.0, (na, T, nd))
+    Ks = rng.uniform(-0.5, 2.0, (na, T, nd))
+    D, K = engine.combine_cumulants(f, Ds, Ks)
+    # part1_demo4_analysis.m:88-90
+    Dw = np.einsum("a,atd->td", f, Ds)
+    Kw = 3 * (np.einsum("a,atd->td", f, Ds ** 2) - Dw ** 2) / Dw ** 2 + np.einsum("a,atd->td", f, Ds ** 2 * Ks) / Dw ** 2
+    np.testing.assert_allclose(D, Dw, rtol=1e-14)
+    np.testing.assert_allclose(K, Kw, rtol=1e-12)
+    # one axon: D and K pass through
+    D1, K1 = engine.combine_cumulants([1.0], Ds[:1], Ks[:1])
+    np.testing.assert_allclose(D1, Ds[0], rtol=1e-15)
+    np.testing.assert_allclose(K1, Ks[0], rtol=1e-12, atol=1e-14)
