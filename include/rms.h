@@ -209,6 +209,16 @@ int rms_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
  * position draws, domain 2 the partial-permeation draws.  A test hook. */
 int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out);
 
+/* Lattice of one tube along z built on the GPU: voxel (i, j, k) gets
+ * `inside` when ((i+0.5) res - cx[k])^2 + ((j+0.5) res - cy[k])^2 < r2[k],
+ * else `outside` (per-slice radius^2 and centre, um, n3 values each: the
+ * caliber variation and undulation of an axon, analysis/visualizeaxon.m:28-67).
+ * Every operation is rounded on its own, so the lattice equals one built on
+ * the host in FP64 from the same tables.  Replaces the sim's lattice (a host
+ * copy is kept, as with rms_sim_set_lattice). */
+int rms_sim_set_tube_lattice(rms_sim* sim, const double* r2, const double* cx, const double* cy, int inside,
+                             int outside, int device);
+
 /* Cumulants of a finished run, the formulas analysis/readRMS.m applies to the
  * output files (:44-45 normalisation by sig0 with the tensor multiplicities,
  * :96-103 D = <x^2>/(2t), K = <x^4>/<x^2>^2 - 3) along ndir unit directions

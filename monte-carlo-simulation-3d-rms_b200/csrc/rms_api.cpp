@@ -1083,6 +1083,46 @@ int rms_sim_run(rms_sim* s, const rms_run_opts* opts) {
     }
 }
 
+int rms_sim_set_tube_lattice(rms_sim* s, const double* r2, const double* cx, const double* cy, int inside,
+                             int outside, int device) {
+    if (!s || !r2 || !cx || !cy) return set_error(RMS_ERR_ARG, "null argument");
+    if (inside < 0 || inside >= s->nc || outside < 0 || outside >= s->nc)
+        return set_error(RMS_ERR_RANGE, "labels must be below Nc");
+    if (inside == 0 && outside == 0) return set_error(RMS_ERR_RANGE, "a lattice needs labelled voxels");
+    try {
+        int rc = ensure_device(s, device);
+        if (rc) return rc;
+        rms_device_state* d = s->dev;
+        RMS_CUDA(cudaSetDevice(device));
+        cudaStream_t st = d->own;
+        const size_t nvox = (size_t)s->n1 * s->n2 * s->n3;
+        std::vector<double> tab;
+        tab.insert(tab.end(), r2, r2 + s->n3);
+        tab.insert(tab.end(), cx, cx + s->n3);
+        tab.insert(tab.end(), cy, cy + s->n3);
+        RMS_CUDA(upload(d->tables, tab, st));
+        RMS_CUDA(d->labels.ensure(nvox));
+        const double* t = d->tables.as<double>();
+        int e = build_tube_lattice(d->labels.as<uint8_t>(), s->n1, s->n2, s->n3, s->res, t, t + s->n3, t + 2 * s->n3,
+                                   (uint8_t)inside, (uint8_t)outside, st);
+        if (e) return cuda_fail((cudaError_t)e, "lattice kernel launch");
+        s->labels.resize(nvox);
+        RMS_CUDA(cudaMemcpyAsync(s->labels.data(), d->labels.p, nvox, cudaMemcpyDeviceToHost, st));
+        RMS_CUDA(cudaStreamSynchronize(st));
+        size_t nonzero = 0;
+        for (size_t i = 0; i < nvox; ++i) nonzero += s->labels[i] != 0;
+        if (nonzero == 0) return set_error(RMS_ERR_RANGE, "the lattice has no labelled voxel");
+        // the device already holds these labels; the packed form is rebuilt at the next run
+        s->have_lattice = true;
+        s->lattice_dirty = false;
+        d->labels_bytes = nvox;
+        d->packed_valid = false;
+        return RMS_OK;
+    } catch (const std::exception& ex) {
+        return set_error(RMS_ERR_NOMEM, ex.what());
+    }
+}
+
 int rms_sim_cumulants(const rms_sim* s, const double* dirs, int ndir, double* D, double* K) {
     if (!s || !D || !K) return set_error(RMS_ERR_ARG, "null argument");
     if (!s->have_results) return set_error(RMS_ERR_STATE, "no results: run the simulation first");

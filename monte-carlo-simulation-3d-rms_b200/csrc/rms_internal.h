@@ -112,6 +112,10 @@ int walk_compat_blocks_per_sm(int nc, bool trace);
 int walk_split_blocks_per_sm(int nc, int lattice_bits, int variant);
 const char* cuda_error_string(int code);
 
+// A tube lattice on the device (rms_geometry.cu).
+int build_tube_lattice(uint8_t* d_out, int n1, int n2, int n3, double res, const double* d_r2, const double* d_cx,
+                       const double* d_cy, uint8_t inside, uint8_t outside, void* stream);
+
 // Adjoint of the waveform-mode split walk (rms_adjoint.cu): one axon, labels
 // below kAdjNc, at most kAdjWaves waveforms.
 constexpr int kAdjWaves = 16;

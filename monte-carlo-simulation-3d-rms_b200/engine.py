@@ -33,7 +33,7 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
            "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases",
            "rms_adjoint_run", "rms_autotune", "rms_batch_graph_create", "rms_graph_run", "rms_graph_destroy",
-           "rms_sim_cumulants", "rms_combine_cumulants")
+           "rms_sim_cumulants", "rms_combine_cumulants", "rms_sim_set_tube_lattice")
 CONTRACT = {"fp32": 0, "bf16x3": 1}
 
 _DP = C.POINTER(C.c_double)
@@ -112,6 +112,7 @@ def lib():
         L.rms_graph_run.argtypes = [C.c_void_p, C.c_uint64]
         L.rms_graph_destroy.argtypes = [C.c_void_p]
         L.rms_graph_destroy.restype = None
+        L.rms_sim_set_tube_lattice.argtypes = [C.c_void_p, _DP, _DP, _DP, C.c_int, C.c_int, C.c_int]
         L.rms_sim_cumulants.argtypes = [C.c_void_p, _DP, C.c_int, _DP, _DP]
         L.rms_combine_cumulants.argtypes = [C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP]
         L.rms_autotune.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_int), _DP]
@@ -201,6 +202,13 @@ class Sim:
             raise ValueError("labels must be 3-D")
         _check(lib().rms_sim_set_lattice(self._h, lab.ctypes.data_as(C.POINTER(C.c_uint8)),
                                          *[int(x) for x in lab.shape]))
+
+    def set_tube_lattice(self, r2, cx, cy, inside: int = 1, outside: int = 0, device: int = 0):
+        """Build the lattice on the GPU from per-slice tables (geometry.axon_slices)."""
+        a, b, c = _arr(r2), _arr(cx), _arr(cy)
+        if not (a.size == b.size == c.size == self.shape[2]):
+            raise ValueError("one radius^2 and centre per z slice")
+        _check(lib().rms_sim_set_tube_lattice(self._h, _ptr(a), _ptr(b), _ptr(c), int(inside), int(outside), int(device)))
 
     def run(self, seed: int = 0, precision: str = "compat", device: int = 0, stream=None,
             trace_walkers: int = 0, variant: int = 0, walker_range=None, traj_out: int = 0):

@@ -49,11 +49,11 @@ def draw_shape(rng: np.random.Generator, r0: float = 1.0, und_amp: float = 0.5,
     return AxonShape(r0, a, lam, phi, und_amp, und_lam, psi)
 
 
-def axon_lattice(n1: int, n2: int, n3: int, res: float = 0.1, seed: int = 0,
-                 exterior: int = 0, r0: float = 1.0, shape: AxonShape | None = None
-                 ) -> np.ndarray:
-    """uint8 lattice (n1, n2, n3) of one undulating, caliber-varying axon
-    along z, centred in the x-y box."""
+def axon_slices(n1: int, n2: int, n3: int, res: float = 0.1, seed: int = 0, r0: float = 1.0,
+                shape: AxonShape | None = None):
+    """Per-slice (radius^2, centre x, centre y), um, of the axon along z: the
+    tables both the host builder below and the GPU builder
+    (Sim.set_tube_lattice, rms_sim_set_tube_lattice) fill voxels from."""
     if shape is None:
         shape = draw_shape(np.random.default_rng(seed), r0=r0)
     z = (np.arange(n3) + 0.5) * res
@@ -61,13 +61,25 @@ def axon_lattice(n1: int, n2: int, n3: int, res: float = 0.1, seed: int = 0,
     ang = 2.0 * np.pi * z / shape.und_lam + shape.psi
     cx = 0.5 * n1 * res + shape.und_amp * np.cos(ang)
     cy = 0.5 * n2 * res + shape.und_amp * np.sin(ang)
+    return r ** 2, cx, cy
+
+
+def axon_lattice(n1: int, n2: int, n3: int, res: float = 0.1, seed: int = 0,
+                 exterior: int = 0, r0: float = 1.0, shape: AxonShape | None = None
+                 ) -> np.ndarray:
+    """uint8 lattice (n1, n2, n3) of one undulating, caliber-varying axon
+    along z, centred in the x-y box (built on the host; Sim.set_tube_lattice
+    builds the same lattice on the GPU)."""
+    r2, cx, cy = axon_slices(n1, n2, n3, res, seed, r0, shape)
     x = (np.arange(n1) + 0.5) * res
     y = (np.arange(n2) + 0.5) * res
     out = np.full((n1, n2, n3), exterior, dtype=np.uint8)
     # slab by slab over z keeps peak memory at one x-y plane of floats
     for k in range(n3):
-        d2 = (x[:, None] - cx[k]) ** 2 + (y[None, :] - cy[k]) ** 2
-        out[:, :, k][d2 < r[k] ** 2] = 1
+        dx = x[:, None] - cx[k]
+        dy = y[None, :] - cy[k]
+        d2 = dx * dx + dy * dy
+        out[:, :, k][d2 < r2[k]] = 1
     return out
 
 
