@@ -99,7 +99,21 @@ typedef struct rms_config {
     int permeation;            /* RMS_PERM_* */
     double kappa;              /* um/ms, RMS_PERM_KAPPA */
     const double* pij;         /* [nc*nc], RMS_PERM_TABLE */
+    int membrane_rule;         /* RMS_RULE_*: what a membrane does to a walker it
+                                  turns back (SPLIT walk; COMPAT reflects) */
 } rms_config;
+
+/* Membrane rules.  REFLECT: elastic reflection at the membrane (the
+ * reference simulator, main.cu:274-300).  REJECT: the whole step is
+ * cancelled and the walker stays where it was for that step ("rejection
+ * sampling", analysis/interaction.m:302-345).  LEAP: the step is cancelled and
+ * taken again in a new direction (drawn from the partial-permeation stream)
+ * until it stays clear, at most 64 tries, then the walker stays ("equal-step-
+ * length random leap", interaction.m:256-300).  Mirror domain walls reflect
+ * under every rule. */
+#define RMS_RULE_REFLECT 0
+#define RMS_RULE_REJECT 1
+#define RMS_RULE_LEAP 2
 
 typedef struct rms_run_opts {
     uint64_t seed;             /* RNG seed (the reference reads /dev/random) */

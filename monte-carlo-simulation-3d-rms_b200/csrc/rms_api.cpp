@@ -201,6 +201,7 @@ int finalize_config(rms_sim* s) {
     std::ostringstream m;
     if (s->mode != RMS_MODE_NARROW && s->mode != RMS_MODE_PGSE && s->mode != RMS_MODE_WAVEFORM)
         return set_error(RMS_ERR_ARG, "mode");
+    if (s->rule < RMS_RULE_REFLECT || s->rule > RMS_RULE_LEAP) return set_error(RMS_ERR_ARG, "membrane rule");
     if (!(s->dt > 0.0) || !std::isfinite(s->dt)) return set_error(RMS_ERR_RANGE, "dt must be > 0");
     if (s->tn < 1) return set_error(RMS_ERR_RANGE, "TN must be >= 1");
     if (s->npar < 1 || s->npar > (int64_t)1 << 40) return set_error(RMS_ERR_RANGE, "NPar out of range");
@@ -373,7 +374,8 @@ int prepare_lattice(rms_sim* s, cudaStream_t st, bool split, int bits) {
 bool same_schedule(const rms_sim* a, const rms_sim* b) {
     return a->mode == b->mode && a->tn == b->tn && a->dt == b->dt && a->timepoints == b->timepoints &&
            a->tstep == b->tstep && a->nite == b->nite && a->boundary == b->boundary && a->bval == b->bval &&
-           a->bvec == b->bvec && a->grad == b->grad && a->nbins == b->nbins && a->wave == b->wave;
+           a->bvec == b->bvec && a->grad == b->grad && a->nbins == b->nbins && a->wave == b->wave &&
+           a->rule == b->rule;
 }
 
 // One launch, in three parts: plan (validate, shape, allocate, upload the
@@ -402,6 +404,8 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     if (prec == RMS_PREC_COMPAT && jobs.size() != 1) return set_error(RMS_ERR_ARG, "a COMPAT launch walks one simulation");
     if (prec == RMS_PREC_COMPAT && s->mode == RMS_MODE_WAVEFORM)
         return set_error(RMS_ERR_ARG, "general waveforms are walked by the SPLIT walk");
+    if (prec == RMS_PREC_COMPAT && s->rule != RMS_RULE_REFLECT)
+        return set_error(RMS_ERR_ARG, "the COMPAT walk reflects at membranes (the reference's rule); other rules walk SPLIT");
     float* traj = o ? o->traj_out : nullptr;
     if (traj && (s->mode != RMS_MODE_WAVEFORM || prec != RMS_PREC_SPLIT || jobs.size() != 1))
         return set_error(RMS_ERR_ARG, "trajectory output needs a one-simulation SPLIT run in waveform mode");
@@ -433,6 +437,7 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     } else {
         lattice_bits = split_lattice_bits(nc_max);
         variant = (o && o->variant > 0) ? o->variant - 1 : kSplitVariantDefault;
+        if (s->rule != RMS_RULE_REFLECT) variant = 0;   // the rules are built for the first variant
         if (variant >= split_variant_count()) return set_error(RMS_ERR_ARG, "variant out of range");
         block = split_variant_block(variant);
         per_sm = walk_split_blocks_per_sm(nc_max, lattice_bits, variant);
@@ -522,6 +527,7 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     a.boundary = s->boundary; a.mode = s->mode;
     a.res = s->res; a.dt = s->dt;
     a.seed = jobs[0].seed;
+    a.rule = s->rule;
     a.step = d->tables.as<double>();
     a.t2 = a.step + s->nc;
     a.pij = a.t2 + s->nc;
@@ -832,6 +838,7 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
 // simulation, by the two-pass walk of rms_adjoint.cu.
 int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adjoint_grads* out) {
     if (s->mode != RMS_MODE_WAVEFORM) return set_error(RMS_ERR_ARG, "the adjoint differentiates a waveform-mode simulation");
+    if (s->rule != RMS_RULE_REFLECT) return set_error(RMS_ERR_ARG, "the adjoint walks with reflecting membranes");
     if (s->nwave > kAdjWaves) return set_error(RMS_ERR_RANGE, "the adjoint takes at most 16 waveforms per run");
     if (s->nc > kAdjNc) return set_error(RMS_ERR_RANGE, "the adjoint supports Nc <= 4");
     if (!s->have_lattice) return set_error(RMS_ERR_STATE, "no lattice: call rms_sim_set_lattice or load a run directory");
@@ -1032,6 +1039,7 @@ int rms_sim_create(const rms_config* cfg, rms_sim** out) {
     s->boundary = cfg->boundary;
     s->permeation = cfg->permeation;
     s->kappa = cfg->kappa;
+    s->rule = cfg->membrane_rule;
     int rc = finalize_config(s);
     if (rc) { delete s; return rc; }
     *out = s;

@@ -80,6 +80,7 @@ struct WalkArgs {
     // dt), [bin][waveform][axis]; optional per-walker bin means out,
     // [walker - walker_begin][bin][axis] in um
     int nwave, nbins, bin_steps;
+    int rule;                   // membrane rule: 0 reflect, 1 reject (stay), 2 leap (redraw)
     const double* wave;
     float* traj;
     AxonDesc axon0;             // the first axon, by value (read from kernel parameters)

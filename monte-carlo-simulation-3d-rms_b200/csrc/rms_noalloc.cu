@@ -95,6 +95,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
                                    double* d_rows, double* d_sig) {
     if (!s || !o || !d_labels || !d_rows) return set_error(RMS_ERR_ARG, "null argument");
     if (s->mode == RMS_MODE_WAVEFORM) return set_error(RMS_ERR_ARG, "the no-allocation walk records narrow-pulse and PGSE runs");
+    if (s->rule != RMS_RULE_REFLECT) return set_error(RMS_ERR_ARG, "the no-allocation walk reflects at membranes");
     if (o->traj_out) return set_error(RMS_ERR_ARG, "the no-allocation walk writes no trajectory");
     if (s->mode == RMS_MODE_PGSE && !d_sig) return set_error(RMS_ERR_ARG, "PGSE needs the sig buffer");
     if (s->nc > 7) return set_error(RMS_ERR_RANGE, "the no-allocation walk supports Nc <= 7");

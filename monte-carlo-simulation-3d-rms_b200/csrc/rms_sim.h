@@ -22,6 +22,7 @@ struct rms_sim {
     int timepoints = 1000, nite = 4, boundary = RMS_BOUNDARY_MIRROR,
         permeation = RMS_PERM_REFERENCE;
     double kappa = 0.0;
+    int rule = 0;              // RMS_RULE_*
 
     // derived tables (main.cu:433-458, 484-487)
     int tstep = 1;

@@ -57,6 +57,7 @@ namespace {
 // number caps registers per thread at 65536 / (block * minb), trading spills
 // in the rare record path for more resident warps to hide gather latency.
 struct SplitVariant { int block, minb; };
+constexpr int kLeapCap = 64;   // equal-step-length leap: tries per step before staying put
 constexpr SplitVariant kVariants[] = {{256, 4}, {256, 3}, {256, 2}, {128, 8}, {512, 2}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -120,7 +121,7 @@ __device__ __noinline__ void wave_final(const double* ph, int nthr, int nwave, d
 
 // ONE: the launch has one axon, whose scalars are read from the kernel
 // parameters (a.axon0) instead of being held in registers.
-template <int NCMAX, int BITS, int BLOCK, int MINB, bool ONE>
+template <int NCMAX, int BITS, int BLOCK, int MINB, bool ONE, int RULE = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs a) {
     // per warp, the current axon's tables: step (voxels), T2 exponent per voxel
     // of path, Pij and the step-length ratio that rescales the rest of a step
@@ -248,7 +249,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 r1 = spare_u1; r2 = spare_u2;
             }
             if (active) {
-                const float u1 = u32_to_float(r1), u2 = u32_to_float(r2);
+                float u1 = u32_to_float(r1), u2 = u32_to_float(r2);
+                // RULE != 0: the step's start, restored when a membrane turns the step back
+                unsigned sv_lin = lin, sv_up = up;
+                float sv_d0 = d0, sv_d1 = d1, sv_d2 = d2, sv_w32 = w32, sv_F0 = Fm0, sv_F1 = Fm1, sv_F2 = Fm2;
+                float sv_step = cur_step, sv_k = cur_k;
+                int sv_D0 = D0, sv_D1 = D1, sv_D2 = D2, sv_ai = ai;
+                for (int attempt = 0;; ++attempt) {
+                bool turned_back = false;
                 const float cz = 1.0f - 2.0f * u1;
                 const float s2 = u1 * (1.0f - u1);
                 const float sz = 2.0f * s2 * rsqrtf(s2);
@@ -333,6 +341,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                         } else {
                             const float P = t_pij[ai * NCMAX + aj];
                             cross = (P > 0.999999f) || (P >= 0.000001f && perm.next() < P);
+                            if (RULE != 0 && !cross) {
+                                turned_back = true;   // a membrane sends the walker back: the rule decides
+                                break;
+                            }
                         }
                     }
                     if (cross) {
@@ -353,6 +365,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     if (hit == 0) d0 = 1.0f; else if (hit == 1) d1 = 1.0f; else d2 = 1.0f;
                     if (!(rem > 0.0f)) break;
                 }
+                }
+                if (RULE == 0 || !turned_back) break;
+                // the step is taken back (interaction.m:256-345): rejection
+                // sampling stays put for the step; the equal-step-length leap
+                // redraws the direction (partial-permeation stream) and walks
+                // the step again, up to kLeapCap tries, then stays
+                lin = sv_lin; up = sv_up; d0 = sv_d0; d1 = sv_d1; d2 = sv_d2; w32 = sv_w32;
+                Fm0 = sv_F0; Fm1 = sv_F1; Fm2 = sv_F2; D0 = sv_D0; D1 = sv_D1; D2 = sv_D2;
+                ai = sv_ai; cur_step = sv_step; cur_k = sv_k;
+                if (RULE == 1 || attempt + 1 >= kLeapCap) {
+                    w32 = fmaf(cur_step, cur_k, w32);   // the step's time passes in place
+                    break;
+                }
+                u1 = perm.next();
+                u2 = perm.next();
                 }
             }
             // in-voxel offsets of the current position
@@ -520,6 +547,16 @@ int launch_t(const WalkArgs& a, int grid, void* stream) {
     return (int)cudaGetLastError();
 }
 
+// The alternative membrane rules (rejection sampling, equal-step-length
+// leap): first launch variant, one-axon and batch forms.
+template <int NCMAX, int BITS, int RULE>
+int launch_rule(const WalkArgs& a, int grid, void* stream) {
+    constexpr int B = kVariants[0].block, M = kVariants[0].minb;
+    if (a.naxons == 1) walk_split_kernel<NCMAX, BITS, B, M, true, RULE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
+    else walk_split_kernel<NCMAX, BITS, B, M, false, RULE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
+    return (int)cudaGetLastError();
+}
+
 template <int BLOCK, int MINB>
 const void* kernel_ptr(int nc, int bits) {
     if (bits == 2) return (const void*)walk_split_kernel<4, 2, BLOCK, MINB, false>;
@@ -571,6 +608,12 @@ int split_variant_minb(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[
 
 int launch_walk_split(const WalkArgs& a, int lattice_bits, int variant, int grid, void* stream) {
     if (variant < 0 || variant >= kNumVariants) return (int)cudaErrorInvalidValue;
+    if (a.rule != 0) {
+        if (variant != 0 || lattice_bits == 2) return (int)cudaErrorInvalidValue;
+        if (lattice_bits == 4)
+            return a.rule == 1 ? launch_rule<8, 4, 1>(a, grid, stream) : launch_rule<8, 4, 2>(a, grid, stream);
+        return a.rule == 1 ? launch_rule<8, 8, 1>(a, grid, stream) : launch_rule<8, 8, 2>(a, grid, stream);
+    }
     return by_variant(variant, [&]<int B, int M>() { return launch_v<B, M>(a, lattice_bits, grid, stream); });
 }
 

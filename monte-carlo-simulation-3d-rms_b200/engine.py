@@ -55,7 +55,11 @@ class Config(C.Structure):
         ("nwave", C.c_int), ("nbins", C.c_int), ("wave", _DP),
         ("timepoints", C.c_int), ("nite", C.c_int), ("boundary", C.c_int),
         ("permeation", C.c_int), ("kappa", C.c_double), ("pij", _DP),
+        ("membrane_rule", C.c_int),
     ]
+
+
+RULE = {"reflect": 0, "reject": 1, "leap": 2}
 
 
 class RunOpts(C.Structure):
@@ -141,7 +145,7 @@ class Sim:
 
     def __init__(self, labels=None, *, dt, tn, npar, res, diffusivity, t2, nc=None,
                  shape=None, bval=None, bvec=None, grad=None, wave=None, timepoints=0, nite=0,
-                 boundary="mirror", permeation="reference", kappa=0.0, pij=None):
+                 boundary="mirror", permeation="reference", kappa=0.0, pij=None, rule="reflect"):
         """``wave``: general waveforms, array [nwave, nbins, 3] (phase per um of
         a bin's displacement sum, per ms: phase_j = dt sum_b wave[j, b] . X_b);
         selects the waveform mode (SPLIT walk only)."""
@@ -173,7 +177,7 @@ class Sim:
                      wv.shape[0] if wv is not None else 0, wv.shape[1] if wv is not None else 0,
                      _ptr(wv.reshape(-1)) if wv is not None else None,
                      int(timepoints), int(nite), BOUNDARY[boundary], PERMEATION[permeation],
-                     float(kappa), _ptr(pj))
+                     float(kappa), _ptr(pj), RULE[rule])
         _check(lib().rms_sim_create(C.byref(cfg), C.byref(self._h)))
         self.mode = mode
         self.shape = tuple(int(x) for x in shape)

@@ -315,14 +315,22 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
     for (int i = 0; i < p->tn; i++) {
         float u1f, u2f;
         or_dir_uniforms(p->seed, (uint64_t)w, (uint32_t)i, &u1f, &u2f);
-        const double u1 = u1f, u2 = u2f;
+        double u1 = u1f, u2 = u2f;
+        /* rule != reflect: the step's start, restored when a membrane turns it back */
+        const int sg[3] = {g[0], g[1], g[2]}, sai = ai;
+        const double sf[3] = {f[0], f[1], f[2]}, sxi[3] = {xi[0], xi[1], xi[2]}, swexp = wexp;
+        double rem;
+        int flo, fhi, nev;
+        uint32_t ev;
+        for (int attempt = 0;; attempt++) {
+        int turned = 0;
         const double cz = 1.0 - 2.0 * u1;
         const double sz = 2.0 * sqrt(u1 * (1.0 - u1));
         const double phi = 6.283185307179586 * (u2 - 0.5);
         double v[3] = {sz * cos(phi), sz * sin(phi), cz};
-        double rem = p->step[ai];
-        int flo = 0, fhi = 0, nev = 0;
-        uint32_t ev = 0;
+        rem = p->step[ai];
+        flo = 0; fhi = 0; nev = 0;
+        ev = 0;
         if (flight && homogeneous(p, g)) {
             /* a straight line within the homogeneous neighbourhood */
             for (int a = 0; a < 3; a++) {
@@ -369,6 +377,10 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
             const int aj = APix[lin(p, gn[0], gn[1], gn[2])];
             const double P = p->pij[ai * Nc + aj];
             const int cross = (P > 0.999999) || (P >= 0.000001 && (double)or_dstream_float(&perm) < P);
+            if (p->rule != OR_RULE_REFLECT && !cross) {
+                turned = 1;   /* the rule decides, after the loop */
+                break;
+            }
             if (cross) {
                 if (aj != ai) {
                     rem *= p->step[aj] / p->step[ai];
@@ -387,6 +399,23 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
                 ev |= (OR_EV_REFLECT << 2 | (uint32_t)hit) << (4 * nev++);
             }
             if (!(rem > 0.0)) break;
+        }
+        if (p->rule == OR_RULE_REFLECT || !turned) break;
+        /* taken back: rejection stays put for the step; the equal-step-length
+         * leap redraws the direction from the permeation stream and walks the
+         * step again, at most 64 tries (analysis/interaction.m:256-345) */
+        for (int a = 0; a < 3; a++) { g[a] = sg[a]; f[a] = sf[a]; xi[a] = sxi[a]; }
+        ai = sai;
+        wexp = swexp;
+        if (p->rule == OR_RULE_REJECT || attempt + 1 >= 64) {
+            wexp += 1.0 / p->t2[ai];
+            rem = 0.0;
+            flo = fhi = nev = 0;
+            ev = 0;
+            break;
+        }
+        u1 = (double)or_dstream_float(&perm);
+        u2 = (double)or_dstream_float(&perm);
         }
         if (rem > 0.0) ev |= 1u << 31;
         ev |= (uint32_t)nev << 28;
@@ -486,6 +515,7 @@ int or_run(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs* out,
     int rc = check(p);
     if (rc) return rc;
     if (p->mode == OR_MODE_WAVEFORM) return -6;   /* the reference's order has no waveform mode */
+    if (p->rule != OR_RULE_REFLECT) return -7;    /* nor other membrane rules */
     return run_range(p, w_begin, w_end, out, tr, walk_one_ref);
 }
 

@@ -60,7 +60,14 @@ typedef struct or_params {
      * X_b = sum over bin b's steps of the displacement (um) after each step */
     int nwave, nbins;
     const double* wave;  /* [nwave*nbins*3] */
+    /* membrane rule of the split replay: reflect (the reference), reject
+     * (stay for the step) or leap (redraw the direction), interaction.m */
+    int rule;
 } or_params;
+
+#define OR_RULE_REFLECT 0
+#define OR_RULE_REJECT 1
+#define OR_RULE_LEAP 2
 
 typedef struct or_outputs {
     double* sig0;        /* [timepoints] */
