@@ -501,7 +501,7 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     // accumulators
     RMS_CUDA(d->slots.ensure((size_t)nseg * row * sizeof(double)));
     RMS_CUDA(d->out.ensure((size_t)naxons * row * sizeof(double)));
-    RMS_CUDA(d->err.ensure(sizeof(int)));
+    RMS_CUDA(d->err.ensure(16));   // error word, then the multi-axon tile counter at byte 8
     if (has_sig) {
         RMS_CUDA(d->sig_slots.ensure((size_t)nseg * ngrad_pad * sizeof(double)));
         RMS_CUDA(d->out_sig.ensure((size_t)naxons * ngrad_pad * sizeof(double)));
@@ -542,6 +542,7 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     a.vscr = d->vscr.as<double>();
     a.sig_slots = d->sig_slots.as<double>();
     a.err = d->err.as<int>();
+    a.tile_ctr = reinterpret_cast<unsigned long long*>(static_cast<char*>(d->err.p) + 8);
     a.axons = d->axons.as<AxonDesc>();
     a.naxons = naxons;
     a.ntiles = ntiles;
@@ -575,7 +576,7 @@ int enqueue_launch(LaunchPlan& p, rms_sim* s, bool events) {
         RMS_CUDA(cudaMemcpyAsync(d->axons.p, d->h_axons.p, sizeof(AxonDesc) * p.naxons, cudaMemcpyHostToDevice, st));
     RMS_CUDA(cudaMemsetAsync(d->slots.p, 0, (size_t)p.nseg * p.row * sizeof(double), st));
     if (p.multi) RMS_CUDA(cudaMemsetAsync(d->out.p, 0, p.nrow * sizeof(double), st));
-    RMS_CUDA(cudaMemsetAsync(d->err.p, 0, sizeof(int), st));
+    RMS_CUDA(cudaMemsetAsync(d->err.p, 0, 16, st));
     if (p.has_sig) {
         RMS_CUDA(cudaMemsetAsync(d->sig_slots.p, 0, (size_t)p.nseg * p.ngrad_pad * sizeof(double), st));
         if (p.multi) RMS_CUDA(cudaMemsetAsync(d->out_sig.p, 0, p.nsig * sizeof(double), st));

@@ -69,6 +69,7 @@ struct WalkArgs {
     const float* t2invf;        // [nc] 1 / (T2 in steps)
     const float* pijf;          // [nc*nc]
     int* err;                   // device error word (kErr* bits), zeroed per run
+    unsigned long long* tile_ctr;   // multi-axon launches: next tile to hand out, zeroed per run
     // split launches: the axons and their tiles; with several axons each warp
     // adds its rows into out_rows[axon][timepoints][nvals] / out_sig[axon][ngrad_pad]
     const AxonDesc* axons;

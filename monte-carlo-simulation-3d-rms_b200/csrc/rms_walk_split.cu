@@ -155,7 +155,17 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     double* slot = a.slots + (size_t)warp_global * a.timepoints * a.nvals;
     double* sig_slot = sums ? a.sig_slots + (size_t)warp_global * a.ngrad_pad : nullptr;
 
-    for (int64_t tile = warp_global; tile < a.ntiles; tile += nwarps) {
+    // One axon: tiles in strided order (warp w: w, w + nwarps, ...), so each
+    // warp's rows, reduced in a fixed order, are the same every run.  Several
+    // axons: a queue (one counter per launch) hands out tiles in order, so the
+    // tiles in flight stay one narrow window of the list -- one or two axons,
+    // whose lattices then share the L2 -- however far warps drift apart.
+    auto claim = [&]() -> int64_t {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(a.tile_ctr, 1ull);
+        return (int64_t)__shfl_sync(0xffffffffu, t, 0);
+    };
+    for (int64_t tile = ONE ? warp_global : claim(); tile < a.ntiles; tile = ONE ? tile + nwarps : claim()) {
         if (!ONE) {
             while (tile >= next_tb) {
                 ++ax;
