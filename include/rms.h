@@ -127,8 +127,14 @@ typedef struct rms_run_opts {
     int64_t walker_begin;      /* walk walkers [walker_begin, walker_end) of */
     int64_t walker_end;        /* the job; 0, 0 = all.  Lets ranks shard a job. */
     float* traj_out;           /* RMS_MODE_WAVEFORM, SPLIT: optional DEVICE buffer
-                                  [walker - walker_begin][nbins][3] of the
-                                  per-bin displacement sums X_b (um) */
+                                  [walker - walker_begin][nbins][3] of each
+                                  bin's mean displacement X_b / steps (um) */
+    int traj_split;            /* nonzero: traj_out receives the means split into
+                                  BF16 pairs, x = hi + lo: n*nbins*3 hi parts
+                                  ([walker][nbins][3], n = walker_end -
+                                  walker_begin), then n*nbins*3 lo parts -- the
+                                  same bytes as the FP32 form; the input of
+                                  RMS_CONTRACT_BF16X3_PRESPLIT */
 } rms_run_opts;
 
 typedef struct rms_sim rms_sim;
@@ -357,6 +363,10 @@ int rms_adjoint_run(rms_sim* sim, const rms_run_opts* opts, const double* g_sigw
  * kernel_ms (optional, may be NULL) receives the kernel's device time. */
 #define RMS_CONTRACT_FP32 0
 #define RMS_CONTRACT_BF16X3 1
+/* d_pos holds the BF16 pairs a waveform walk wrote with traj_split (hi parts
+ * then lo parts); the tensor cores read them as they lie (TMA), no FP32 ->
+ * BF16 conversion in the contraction.  Needs nbins % 8 == 0. */
+#define RMS_CONTRACT_BF16X3_PRESPLIT 2
 int rms_contract_phases(const float* d_pos, int64_t nwalk, int nbins, const float* d_wave, int nwave, int method,
                         double* d_out, void* stream, float* kernel_ms);
 

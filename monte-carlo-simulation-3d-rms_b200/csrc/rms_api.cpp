@@ -551,6 +551,8 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     a.bin_steps = wavemode ? s->tn / s->nbins : 0;
     a.wave = d->wavef.as<double>();
     a.traj = traj;
+    a.traj_split = (o && o->traj_split) ? 1 : 0;
+    a.traj_n = jobs[0].w1 - jobs[0].w0;
     a.out_rows = d->out.as<double>();
     a.out_sig = d->out_sig.as<double>();
     if (!p.axons.empty()) a.axon0 = p.axons[0];

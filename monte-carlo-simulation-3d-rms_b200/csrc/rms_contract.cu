@@ -38,6 +38,7 @@
 //    walker tile run at the same time and share it in L2.  Every wait is bounded
 //    (4 s of global time); a wait that runs out sets an error bit, the CTA
 //    drains its copies and MMAs, frees its tensor memory and returns.
+#include <cuda.h>   // CUtensorMap and the encoder's signature (fetched through cudaGetDriverEntryPoint)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -246,6 +247,12 @@ __device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile i
     }
 }
 
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
@@ -559,8 +566,219 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
+// Positions already split by the walk (RMS_CONTRACT_BF16X3_PRESPLIT): the same
+// pipeline with one TMA warp for the positions in place of the converters.
+constexpr int kPsWarpX = 0, kPsWarpG = 1, kPsWarpMma = 2, kPsWarpEpi = 4;
+constexpr int kPsThreads = 256;
+
+__global__ void __launch_bounds__(kPsThreads, 1)
+    contract_presplit_kernel(const __grid_constant__ CUtensorMap xhi, const __grid_constant__ CUtensorMap xlo,
+                             const uint8_t* __restrict__ gpack, int64_t nwalk,
+                       int nwave, int nk, int n_mpairs, int64_t nunits, double* __restrict__ out, int* err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + kOffAbort);
+    auto bar = [&](int i) { return sbase + kOffBar + 8u * (uint32_t)i; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kGStages; ++s) {
+            mbar_init(bar(kBarGFull + s), 1);
+            mbar_init(bar(kBarGEmpty + s), 1);
+        }
+        for (int s = 0; s < kBStages; ++s) {
+            mbar_init(bar(kBarConv + s), 1);   // position chunk landed (TMA)
+            mbar_init(bar(kBarBEmpty + s), 1);
+        }
+        for (int s = 0; s < 2; ++s) {
+            mbar_init(bar(kBarAccFull + s), 1);
+            mbar_init(bar(kBarAccEmpty + s), 128);
+        }
+        mbar_init(bar(kBarFin), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        fence_proxy_async();
+    }
+    if (warp == kPsWarpMma) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(sbase + kOffTmemSlot), "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kOffTmemSlot);
+
+    if (warp == kPsWarpG) {
+        // waveform chunks: pre-split BF16 hi/lo, 32 KB per (waveform tile, k
+        // chunk); per position chunk, tile 2 pair then tile 2 pair + 1
+        if (lane == 0) {
+            int64_t j = 0;
+            bool ok = true;
+            for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                const int mp = (int)(u % n_mpairs);
+                for (int kc = 0; kc < nk && ok; ++kc) {
+                    for (int a = 0; a < 2; ++a, ++j) {
+                        const int s = (int)(j % kGStages);
+                        if (!(ok = mbar_wait(bar(kBarGEmpty + s), (uint32_t)((j / kGStages) & 1) ^ 1u, abort_flag, err,
+                                             true)))
+                            break;
+                        mbar_arrive_tx(bar(kBarGFull + s), 2 * kGBytes);
+                        bulk_load(sbase + kOffG + (uint32_t)s * 2 * kGBytes,
+                                  gpack + ((size_t)(2 * mp + a) * nk + kc) * (2 * kGBytes), 2 * kGBytes,
+                                  bar(kBarGFull + s));
+                    }
+                }
+            }
+            // drain: the last copies issued have landed (or land within the limit)
+            for (int64_t jj = j > kGStages ? j - kGStages : 0; jj < j; ++jj)
+                mbar_wait(bar(kBarGFull + (int)(jj % kGStages)), (uint32_t)((jj / kGStages) & 1), abort_flag, err, false);
+        }
+    } else if (warp == kPsWarpX) {
+        // position chunks: BF16 hi and lo tiles (256 walkers x 64 k), 128-byte
+        // swizzle -- the MMA's operand layout, as the walk wrote them
+        if (lane == 0) {
+            int64_t i = 0;
+            bool ok = true;
+            for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                const int y = (int)((u / n_mpairs) * kTileN);
+                for (int kc = 0; kc < nk; ++kc, ++i) {
+                    const int sb = (int)(i % kBStages);
+                    if (!(ok = mbar_wait(bar(kBarBEmpty + sb), (uint32_t)((i / kBStages) & 1) ^ 1u, abort_flag, err, true)))
+                        break;
+                    const uint32_t dst = sbase + kOffXb + (uint32_t)sb * 2 * kXbBytes;
+                    mbar_arrive_tx(bar(kBarConv + sb), 2 * kXbBytes);
+                    tma_load_2d(dst, &xhi, kc * kKc, y, bar(kBarConv + sb));
+                    tma_load_2d(dst + kXbBytes, &xlo, kc * kKc, y, bar(kBarConv + sb));
+                }
+            }
+            for (int64_t jj = i > kBStages ? i - kBStages : 0; jj < i; ++jj)
+                mbar_wait(bar(kBarConv + (int)(jj % kBStages)), (uint32_t)((jj / kBStages) & 1), abort_flag, err, false);
+        }
+    } else if (warp == kPsWarpMma) {
+        // MMA issue
+        if (lane == 0) {
+            int64_t i = 0, j = 0, t = 0;
+            bool ok = true;
+            for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++t) {
+                for (int kc = 0; kc < nk && ok; ++kc, ++i) {
+                    const int sb = (int)(i % kBStages);
+                    if (!(ok = mbar_wait(bar(kBarConv + sb), (uint32_t)((i / kBStages) & 1), abort_flag, err, true))) break;
+                    const uint32_t xa = sbase + kOffXb + (uint32_t)sb * 2 * kXbBytes;
+                    for (int a = 0; a < 2; ++a, ++j) {
+                        if (kc == 0) {
+                            // the epilogue has read this tile's accumulator of the previous unit
+                            if (!(ok = mbar_wait(bar(kBarAccEmpty + a), (uint32_t)(t & 1) ^ 1u, abort_flag, err, true)))
+                                break;
+                        }
+                        const int sg = (int)(j % kGStages);
+                        if (!(ok = mbar_wait(bar(kBarGFull + sg), (uint32_t)((j / kGStages) & 1), abort_flag, err, true)))
+                            break;
+                        tc_fence_after();
+                        const uint32_t ga = sbase + kOffG + (uint32_t)sg * 2 * kGBytes;
+                        const uint32_t d = tmem + (uint32_t)a * kTileN;
+#pragma unroll
+                        for (int ks = 0; ks < kKc / 16; ++ks) {
+                            const uint32_t dk = (uint32_t)ks * 32;        // K = 16 BF16 = 32 B into the rows
+                            const uint64_t a_hi = smem_desc(ga + dk), a_lo = smem_desc(ga + kGBytes + dk);
+                            const uint64_t b_hi = smem_desc(xa + dk), b_lo = smem_desc(xa + kXbBytes + dk);
+                            umma_bf16(d, a_hi, b_hi, (kc > 0 || ks > 0) ? 1u : 0u);
+                            umma_bf16(d, a_hi, b_lo, 1u);
+                            umma_bf16(d, a_lo, b_hi, 1u);
+                        }
+                        umma_commit(bar(kBarGEmpty + sg));   // this waveform chunk is free when these are done
+                        if (kc == nk - 1) umma_commit(bar(kBarAccFull + a));
+                    }
+                    if (ok) umma_commit(bar(kBarBEmpty + sb));   // the position chunk too
+                }
+            }
+            // every MMA issued has completed before the tensor memory is freed
+            umma_commit(bar(kBarFin));
+            mbar_wait(bar(kBarFin), 0, abort_flag, err, false);
+        }
+    } else if (warp >= kPsWarpEpi) {
+        // epilogue: warp q reads TMEM lanes 32q .. 32q + 31 (waveform rows)
+        const int q = warp - kPsWarpEpi;   // = warp % 4, the lane quarter this warp may access
+        int64_t t = 0;
+        bool ok = true;
+        for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++t) {
+            const int mp = (int)(u % n_mpairs);
+            const int64_t n0 = (u / n_mpairs) * kTileN;
+            for (int a = 0; a < 2; ++a) {
+                if (!(ok = mbar_wait(bar(kBarAccFull + a), (uint32_t)(t & 1), abort_flag, err, true))) break;
+                __syncwarp();   // tcgen05.ld is warp-wide
+                tc_fence_after();
+                const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)a * kTileN;
+                double CS = 0.0, SN = 0.0;
+#pragma unroll 1
+                for (int c = 0; c < kTileN / 32; ++c) {
+                    uint32_t r[32];
+                    tmem_ld32(taddr + (uint32_t)c * 32, r);
+                    const int64_t nb = n0 + c * 32;
+                    // full slices branch-free (32 independent chains the
+                    // scheduler can interleave); the last slice masked
+                    const int nvalid = (nwalk - nb >= 32) ? 32 : (int)(nwalk - nb);
+                    float cs[4] = {0.f, 0.f, 0.f, 0.f}, sn[4] = {0.f, 0.f, 0.f, 0.f};
+                    if (nvalid == 32) {
+#pragma unroll
+                        for (int e = 0; e < 32; ++e) {
+                            float s, co;
+                            sincos_reduced(__uint_as_float(r[e]), &s, &co);
+                            cs[e & 3] += co;
+                            sn[e & 3] += s;
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 32; ++e) {
+                            float s, co;
+                            sincos_reduced(__uint_as_float(r[e]), &s, &co);
+                            const float m = e < nvalid ? 1.0f : 0.0f;
+                            cs[e & 3] = fmaf(m, co, cs[e & 3]);
+                            sn[e & 3] = fmaf(m, s, sn[e & 3]);
+                        }
+                    }
+                    CS += (double)((cs[0] + cs[1]) + (cs[2] + cs[3]));
+                    SN += (double)((sn[0] + sn[1]) + (sn[2] + sn[3]));
+                }
+                tc_fence_before();
+                mbar_arrive(bar(kBarAccEmpty + a));
+                const int jw = (2 * mp + a) * kTileM + q * 32 + lane;
+                if (jw < nwave) {
+                    atomicAdd(out + 2 * jw, CS);
+                    atomicAdd(out + 2 * jw + 1, SN);
+                }
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == kPsWarpMma)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
 // ----------------------------------------------------------------------------
 // host side
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
 
 // per-device workspace: packed waveforms and the error word
 struct Workspace {
@@ -581,7 +799,8 @@ int contract_phases(const float* d_pos, int64_t nwalk, int nbins, const float* d
     if (!d_pos || !d_wave || !d_out) return fail(RMS_ERR_ARG, "null buffer");
     if (nwalk < 1 || nbins < 1 || nwave < 1) return fail(RMS_ERR_ARG, "empty contraction");
     if (nbins > (1 << 20) || nwave > (1 << 24)) return fail(RMS_ERR_RANGE, "nbins or nwave too large");
-    if (method != RMS_CONTRACT_FP32 && method != RMS_CONTRACT_BF16X3) return fail(RMS_ERR_ARG, "method");
+    if (method != RMS_CONTRACT_FP32 && method != RMS_CONTRACT_BF16X3 && method != RMS_CONTRACT_BF16X3_PRESPLIT)
+        return fail(RMS_ERR_ARG, "method");
     const int K = 3 * nbins;
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
@@ -612,7 +831,9 @@ int contract_phases(const float* d_pos, int64_t nwalk, int nbins, const float* d
         if (cudaGetLastError() != cudaSuccess) return fail(RMS_ERR_CUDA, "FP32 contraction launch");
         if (cudaStreamSynchronize(st) != cudaSuccess) return fail(RMS_ERR_CUDA, "FP32 contraction");
     } else {
+        const bool presplit = method == RMS_CONTRACT_BF16X3_PRESPLIT;
         if (nbins % 4) return fail(RMS_ERR_ARG, "the tensor-core contraction needs nbins % 4 == 0 (16-byte rows)");
+        if (presplit && nbins % 8) return fail(RMS_ERR_ARG, "pre-split positions need nbins % 8 == 0 (16-byte BF16 rows)");
         if (reinterpret_cast<uintptr_t>(d_pos) % 16) return fail(RMS_ERR_ARG, "positions must be 16-byte aligned");
         const int nk = (K + kKc - 1) / kKc;
         const int n_mpairs = (nwave + 2 * kTileM - 1) / (2 * kTileM);
@@ -643,13 +864,37 @@ int contract_phases(const float* d_pos, int64_t nwalk, int nbins, const float* d
         std::call_once(attr_once, [] {
             attr_err = cudaFuncSetAttribute(contract_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)kSmemBytes);
+            if (attr_err == cudaSuccess)
+                attr_err = cudaFuncSetAttribute(contract_presplit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)kSmemBytes);
         });
         if (attr_err != cudaSuccess) return fail(RMS_ERR_CUDA, "shared memory attribute");
+        CUtensorMap mhi, mlo;
+        if (presplit) {
+            EncodeTiledFn enc = encode_fn();
+            if (!enc) return fail(RMS_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+            if (nwalk > 0x7fffffffll) return fail(RMS_ERR_RANGE, "too many walkers for one tensor map");
+            const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)nwalk};
+            const cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+            const cuuint32_t box[2] = {(cuuint32_t)kKc, (cuuint32_t)kTileN};
+            const cuuint32_t estr[2] = {1, 1};
+            uint8_t* hi = reinterpret_cast<uint8_t*>(const_cast<float*>(d_pos));
+            uint8_t* lo = hi + (size_t)nwalk * K * 2;
+            for (int m = 0; m < 2; ++m)
+                if (enc(m ? &mlo : &mhi, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, m ? lo : hi, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                    return fail(RMS_ERR_CUDA, "tensor map of the positions");
+        }
         const int64_t nunits = (int64_t)n_mpairs * ((nwalk + kTileN - 1) / kTileN);
         const int grid = (int)std::min<int64_t>(nunits, sms);
         if (ev.a) cudaEventRecord(ev.a, st);
-        contract_tc_kernel<<<grid, kTcThreads, kSmemBytes, st>>>(d_pos, K, gpack, nwalk, nwave, nk, n_mpairs, nunits,
-                                                                 d_out, d_err);
+        if (presplit)
+            contract_presplit_kernel<<<grid, kPsThreads, kSmemBytes, st>>>(mhi, mlo, gpack, nwalk, nwave, nk, n_mpairs,
+                                                                           nunits, d_out, d_err);
+        else
+            contract_tc_kernel<<<grid, kTcThreads, kSmemBytes, st>>>(d_pos, K, gpack, nwalk, nwave, nk, n_mpairs,
+                                                                     nunits, d_out, d_err);
         if (ev.b) cudaEventRecord(ev.b, st);
         if (cudaGetLastError() != cudaSuccess) return fail(RMS_ERR_CUDA, "tensor-core contraction launch");
         int herr = 0;

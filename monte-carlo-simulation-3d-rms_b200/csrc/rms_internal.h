@@ -84,6 +84,8 @@ struct WalkArgs {
     int rule;                   // membrane rule: 0 reflect, 1 reject (stay), 2 leap (redraw)
     const double* wave;
     float* traj;
+    int traj_split;             // traj holds BF16 hi parts, then lo parts (per walker, bin, axis)
+    int64_t traj_n;             // walkers in the trajectory buffer
     AxonDesc axon0;             // the first axon, by value (read from kernel parameters)
     // traces (COMPAT)
     int64_t trace_n;

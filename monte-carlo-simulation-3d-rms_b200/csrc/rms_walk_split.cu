@@ -42,6 +42,7 @@
 // 2k+1 come from one Philox4x32-10 block indexed by k, so all lanes of a warp
 // generate in lock step; start positions and partial-permeation draws read
 // their own sequential counter domains.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -88,14 +89,27 @@ __device__ __noinline__ void flush_rows(double* slot, double* sig_slot, double* 
 // mean displacement (um) goes to the trajectory output when one is given.
 __device__ __noinline__ void wave_bin(const double* __restrict__ wave, int nwave, int bin, double X0, double X1,
                                       double X2, double res, double* ph, int nthr, float* traj, int64_t tw,
-                                      int nbins, int bin_steps) {
+                                      int nbins, int bin_steps, int split, int64_t traj_n) {
     const double x0 = X0 * res, x1 = X1 * res, x2 = X2 * res;
     const double* wv = wave + (size_t)bin * nwave * 3;
     for (int j = 0; j < nwave; ++j) ph[(size_t)j * nthr] += wv[3 * j] * x0 + wv[3 * j + 1] * x1 + wv[3 * j + 2] * x2;
     if (traj && tw >= 0) {
-        float* t = traj + ((size_t)tw * nbins + bin) * 3;
         const double inv = 1.0 / (double)bin_steps;
-        t[0] = (float)(x0 * inv); t[1] = (float)(x1 * inv); t[2] = (float)(x2 * inv);
+        const float m[3] = {(float)(x0 * inv), (float)(x1 * inv), (float)(x2 * inv)};
+        const size_t at = ((size_t)tw * nbins + bin) * 3;
+        if (split) {
+            // BF16 pairs, hi = bf16(x), lo = bf16(x - hi): the operands of the
+            // tensor-core contraction, split once here
+            __nv_bfloat16* hi = reinterpret_cast<__nv_bfloat16*>(traj);
+            __nv_bfloat16* lo = hi + (size_t)traj_n * nbins * 3;
+            for (int k = 0; k < 3; ++k) {
+                const __nv_bfloat16 h = __float2bfloat16_rn(m[k]);
+                hi[at + k] = h;
+                lo[at + k] = __float2bfloat16_rn(m[k] - __bfloat162float(h));
+            }
+        } else {
+            traj[at] = m[0]; traj[at + 1] = m[1]; traj[at + 2] = m[2];
+        }
     }
 }
 
@@ -410,7 +424,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 }
                 if (event && wave) {
                     wave_bin(a.wave, a.nwave, evi, P0, P1, P2, (double)AXF(res), a.vscr + gtid, nthr, a.traj,
-                             active ? w - AXF(walker_begin) : -1, a.nbins, a.bin_steps);
+                             active ? w - AXF(walker_begin) : -1, a.nbins, a.bin_steps, a.traj_split, a.traj_n);
                     P0 = P1 = P2 = 0.0;
                     ++evi;
                     next_ev += a.bin_steps;

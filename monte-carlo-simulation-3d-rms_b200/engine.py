@@ -34,7 +34,7 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases",
            "rms_adjoint_run", "rms_autotune", "rms_batch_graph_create", "rms_graph_run", "rms_graph_destroy",
            "rms_sim_cumulants", "rms_combine_cumulants", "rms_sim_set_tube_lattice")
-CONTRACT = {"fp32": 0, "bf16x3": 1}
+CONTRACT = {"fp32": 0, "bf16x3": 1, "bf16x3_presplit": 2}
 
 _DP = C.POINTER(C.c_double)
 
@@ -67,7 +67,7 @@ class RunOpts(C.Structure):
         ("seed", C.c_uint64), ("precision", C.c_int), ("device", C.c_int),
         ("stream", C.c_void_p), ("trace_walkers", C.c_int), ("variant", C.c_int),
         ("walker_begin", C.c_int64), ("walker_end", C.c_int64),
-        ("traj_out", C.c_void_p),
+        ("traj_out", C.c_void_p), ("traj_split", C.c_int),
     ]
 
 
@@ -215,14 +215,17 @@ class Sim:
         _check(lib().rms_sim_set_tube_lattice(self._h, _ptr(a), _ptr(b), _ptr(c), int(inside), int(outside), int(device)))
 
     def run(self, seed: int = 0, precision: str = "compat", device: int = 0, stream=None,
-            trace_walkers: int = 0, variant: int = 0, walker_range=None, traj_out: int = 0):
+            trace_walkers: int = 0, variant: int = 0, walker_range=None, traj_out: int = 0,
+            traj_split: bool = False):
         """``traj_out``: device address of a float32 [walkers, nbins, 3] buffer
-        for the bins' mean displacements (waveform mode, SPLIT)."""
+        for the bins' mean displacements (waveform mode, SPLIT); with
+        ``traj_split`` the same bytes hold BF16 hi parts then lo parts (the
+        input of contract_phases(method="bf16x3_presplit"))."""
         w0, w1 = walker_range if walker_range is not None else (0, 0)
         st = None if stream is None else C.c_void_p(int(stream))
         opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION[precision], int(device), st,
                        int(trace_walkers), int(variant), int(w0), int(w1),
-                       C.c_void_p(int(traj_out)) if traj_out else None)
+                       C.c_void_p(int(traj_out)) if traj_out else None, 1 if traj_split else 0)
         _check(lib().rms_sim_run(self._h, C.byref(opts)))
         return self
 

@@ -77,3 +77,41 @@ def test_contraction_methods_agree_and_errors():
     np.testing.assert_allclose(got / 300, pyoracle.contract_phases_fp64(pos5, wave5) / 300, atol=2e-5)
     with pytest.raises(engine.RmsError):
         run(pos5, wave5, "bf16x3")        # tensor path: nbins % 4 == 0
+
+
+def test_presplit_positions_from_the_walk():
+    """The walk writes the bin means as BF16 pairs (traj_split); the contraction
+    reading them through TMA equals the one converting the FP32 means of the
+    same walk, bit for bit (the same BF16 operands), and FP64 within 1e-4."""
+    import torch
+    from rms_b200 import geometry
+    nb, nw, n = 64, 200, 5000
+    dt, tn = 5e-4, 1280
+    lab = geometry.axon_lattice(20, 20, 40, 0.1, seed=3, exterior=2, r0=0.5)
+    dtb = dt * tn / nb
+    w = waveforms.scale_to_b(waveforms.random_smooth(nw, nb, 1.0, seed=2), dtb, np.linspace(0.1, 8.0, nw))
+    wave = np.ascontiguousarray((w * dtb).astype(np.float32))
+    kw = dict(dt=dt, tn=tn, npar=n, res=0.1, diffusivity=[0, 2.0, 2.0], t2=[1e6, 80, 60], wave=np.zeros((1, nb, 3)),
+              timepoints=nb, boundary="periodic")
+    f32 = torch.empty((n, nb, 3), dtype=torch.float32, device="cuda")
+    split = torch.empty((n, nb, 3), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    engine.Sim(lab, **kw).run(seed=4, precision="split", traj_out=f32.data_ptr())
+    engine.Sim(lab, **kw).run(seed=4, precision="split", traj_out=split.data_ptr(), traj_split=True)
+    d_wave = torch.from_numpy(wave).cuda()
+    outs = {}
+    for name, buf, method in (("f32", f32, "bf16x3"), ("split", split, "bf16x3_presplit")):
+        out = torch.full((nw, 2), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        engine.contract_phases(buf.data_ptr(), n, nb, d_wave.data_ptr(), nw, out.data_ptr(), method=method)
+        outs[name] = out.cpu().numpy()
+    np.testing.assert_array_equal(outs["split"], outs["f32"])
+    want = pyoracle.contract_phases_fp64(f32.cpu().numpy(), wave)
+    assert np.abs(outs["split"] - want).max() / n < 1e-4
+    # the pairs sum to the FP32 means to BF16 hi/lo precision
+    raw = split.view(torch.int16).cpu().numpy().reshape(-1)
+    m = n * nb * 3
+    hi = (raw[:m].astype(np.uint32) << 16).view(np.float32)
+    lo = (raw[m:2 * m].astype(np.uint32) << 16).view(np.float32)
+    x = f32.cpu().numpy().reshape(-1)
+    assert np.abs(hi + lo - x).max() <= 2 ** -16 * np.abs(x).max()
