@@ -1,0 +1,63 @@
+"""Edge cases on the GPU: one walker, walker counts around a warp tile, a
+one-voxel periodic lattice, one step per record, a one-member batch, and a
+contraction of one walker against one waveform."""
+import numpy as np
+import pytest
+
+import pyoracle
+from conftest import assert_fp64_close
+from rms_b200 import engine, geometry, waveforms
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("npar", [1, 31, 33])
+def test_walker_counts_around_a_tile_match_the_oracle(npar):
+    lab = geometry.axon_lattice(12, 12, 16, 0.1, seed=1, exterior=2, r0=0.4)
+    D, T2 = [0.0, 2.0, 1.0], [80.0, 80.0, 40.0]
+    sim = engine.Sim(lab, dt=2e-4, tn=200, npar=npar, res=0.1, diffusivity=D, t2=T2, bval=[1.0], bvec=[[1, 0, 0]],
+                     timepoints=200)
+    got = sim.run(seed=3, precision="compat").outputs()
+    step, t2s, pij, td = pyoracle.reference_tables(2e-4, 0.1, D, T2, 200, 200)
+    job = pyoracle.Job(lab, dt=2e-4, tn=200, npar=npar, res=0.1, step=step, t2_steps=t2s, pij=pij, seed=3, td=td,
+                       timepoints=200, bval=[1.0], bvec=[[1, 0, 0]])
+    want = pyoracle.run_oracle(job)
+    assert np.array_equal(got["npar_count"], want["npar_count"])
+    assert_fp64_close(got["dx2"], want["dx2"], 1e-9, "dx2")
+    split = sim.run(seed=3, precision="split").outputs()
+    assert np.array_equal(split["npar_count"].sum(axis=1), np.full(200, float(npar)))
+
+
+def test_one_voxel_periodic_lattice_is_free_diffusion():
+    sim = engine.Sim(np.ones((1, 1, 1), dtype=np.uint8), dt=2e-4, tn=4000, npar=8192, res=0.1,
+                     diffusivity=[0.0, 2.0], t2=[1e6, 1e6], bval=[], bvec=np.zeros((0, 3)), timepoints=100,
+                     boundary="periodic")
+    for prec in ("compat", "split"):
+        o = sim.run(seed=5, precision=prec).outputs()
+        D, _ = sim.cumulants()
+        assert np.abs(D[-1] / 2.0 - 1).max() < 0.05, (prec, D[-1])
+        assert np.array_equal(o["npar_count"][:, 1], np.full(100, 8192.0))
+
+
+def test_one_member_batch_equals_a_single_run():
+    lab = geometry.axon_lattice(16, 16, 24, 0.1, seed=2, exterior=2)
+    kw = dict(dt=2e-4, tn=500, npar=3000, res=0.1, diffusivity=[0, 2.0, 2.0], t2=[80, 80, 60], bval=[],
+              bvec=np.zeros((0, 3)), timepoints=100, permeation="kappa", kappa=0.02)
+    a = engine.Sim(lab, **kw)
+    engine.batch_run([a], seed=9, precision="split")
+    b = engine.Sim(lab, **kw).run(seed=9, precision="split")
+    np.testing.assert_array_equal(a.get("npar_count"), b.get("npar_count"))
+    assert_fp64_close(a.get("dx2").reshape(100, 6), b.get("dx2").reshape(100, 6), 1e-12, "dx2")
+
+
+def test_contraction_of_one_walker_and_one_waveform():
+    import torch
+    pos = np.random.default_rng(0).normal(size=(1, 8, 3)).astype(np.float32)
+    wave = np.random.default_rng(1).normal(size=(1, 8, 3)).astype(np.float32)
+    want = pyoracle.contract_phases_fp64(pos, wave)
+    for method, tol in (("fp32", 1e-6), ("bf16x3", 5e-5)):
+        d_pos, d_wave = torch.from_numpy(pos).cuda(), torch.from_numpy(wave).cuda()
+        out = torch.zeros((1, 2), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        engine.contract_phases(d_pos.data_ptr(), 1, 8, d_wave.data_ptr(), 1, out.data_ptr(), method=method)
+        assert np.abs(out.cpu().numpy() - want).max() < tol, method
