@@ -14,9 +14,13 @@
 // form is the PGSE pair (hpc_code/lib/main_PGSE.cu:336-346), accumulated per
 // step per gradient.
 //
-// Two methods:
+// Three methods:
 //  - FP32 on the CUDA cores (contract_f32_kernel): register-tiled, 128
 //    waveforms x 128 walkers per block;
+//  - positions already split into BF16 pairs by the walk
+//    (contract_presplit_kernel): the pipeline below with one TMA warp in
+//    place of the converters (two tensor maps, hi and lo, 128-byte swizzle:
+//    the tiles land in the MMA's operand layout as they are);
 //  - BF16 hi/lo on the tensor cores (contract_tc_kernel): x = x_hi + x_lo with
 //    both parts BF16, phi = A_hi B_hi + A_hi B_lo + A_lo B_hi accumulated in
 //    FP32 in tensor memory (the dropped A_lo B_lo term is below 2^-16 of each
