@@ -397,7 +397,7 @@ struct LaunchPlan {
 // Run one launch: COMPAT (one simulation) or SPLIT (one or more simulations,
 // "axons", walked by one persistent grid).  The first job's simulation owns
 // the launch's accumulators.
-int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan& p) {
+int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan& p, bool table_form = false) {
     rms_sim* s = jobs[0].s;
     const int prec = o ? o->precision : RMS_PREC_COMPAT;
     if (prec != RMS_PREC_COMPAT && prec != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "precision");
@@ -462,7 +462,10 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     const size_t row = (size_t)T * nvals;
 
     const int nseg = nwarps;   // one accumulator row set per warp
-    const bool multi = naxons > 1;
+    // several axons, or a launch a graph replays with new seeds: the table
+    // form (axon fields and seeds from device memory, rows added into the
+    // axon totals); one axon otherwise reads its fields from kernel parameters
+    const bool multi = naxons > 1 || table_form;
 
     // inputs
     for (LaunchJob& j : jobs) {
@@ -528,6 +531,7 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     a.res = s->res; a.dt = s->dt;
     a.seed = jobs[0].seed;
     a.rule = s->rule;
+    a.table_form = multi ? 1 : 0;
     a.step = d->tables.as<double>();
     a.t2 = a.step + s->nc;
     a.pij = a.t2 + s->nc;
@@ -719,7 +723,7 @@ int graph_create(rms_sim* const* sims, int n, const rms_run_opts* o, rms_graph**
     g->device = o->device;
     for (int i = 0; i < n; ++i) g->jobs.push_back(LaunchJob{sims[i], 0, sims[i]->npar, o->seed + (uint64_t)i * kBatchSeedStep});
     rms_run_opts oo = *o;
-    int rc = plan_launch(g->jobs, &oo, g->plan);
+    int rc = plan_launch(g->jobs, &oo, g->plan, true);
     if (rc) return rc;
     LaunchPlan& p = g->plan;
     if (!o->stream) p.st = p.d->own;   // capture needs a stream other than the legacy default stream

@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         }
         const uint8_t* lat = AXF(lat);
         const int s0 = AXF(s0), s1 = AXF(s1);
-        const uint64_t seed = a.axons[ONE ? 0 : ax].seed;   // device table: a replayed launch may change it
+        const uint64_t seed = AXF(seed);   // a graph captures the table form, whose seed a replay rewrites
         const bool flight = (BITS != 2) && AXF(flight);
         const bool same_certain = AXF(same_cross);
         const float* t_step = tab;
@@ -566,7 +566,7 @@ __global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int 
 
 template <int NCMAX, int BITS, int BLOCK, int MINB>
 int launch_t(const WalkArgs& a, int grid, void* stream) {
-    if (a.naxons == 1) walk_split_kernel<NCMAX, BITS, BLOCK, MINB, true><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a);
+    if (a.naxons == 1 && !a.table_form) walk_split_kernel<NCMAX, BITS, BLOCK, MINB, true><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a);
     else walk_split_kernel<NCMAX, BITS, BLOCK, MINB, false><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a);
     return (int)cudaGetLastError();
 }
@@ -576,7 +576,7 @@ int launch_t(const WalkArgs& a, int grid, void* stream) {
 template <int NCMAX, int BITS, int RULE>
 int launch_rule(const WalkArgs& a, int grid, void* stream) {
     constexpr int B = kVariants[0].block, M = kVariants[0].minb;
-    if (a.naxons == 1) walk_split_kernel<NCMAX, BITS, B, M, true, RULE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
+    if (a.naxons == 1 && !a.table_form) walk_split_kernel<NCMAX, BITS, B, M, true, RULE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
     else walk_split_kernel<NCMAX, BITS, B, M, false, RULE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
     return (int)cudaGetLastError();
 }

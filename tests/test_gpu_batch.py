@@ -102,3 +102,17 @@ def test_graph_replays_equal_batch_runs():
     with pytest.raises(engine.RmsError):
         g.run(23)
     g.close()
+
+
+def test_one_simulation_graph_equals_a_plain_run():
+    # a graph of one simulation walks it in the table form (seeds from device
+    # memory); the walkers and their draws are those of rms_sim_run
+    sims = axon_sims()[:1]
+    g = engine.Graph(sims, seed=0)
+    g.run(31)
+    o = sims[0].outputs()
+    sims[0].run(seed=31, precision="split")
+    p = sims[0].outputs()
+    np.testing.assert_array_equal(p["npar_count"], o["npar_count"])
+    assert_fp64_close(p["dx2"], o["dx2"], 1e-9, "dx2")
+    g.close()
