@@ -437,7 +437,7 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     } else {
         lattice_bits = split_lattice_bits(nc_max);
         variant = (o && o->variant > 0) ? o->variant - 1 : kSplitVariantDefault;
-        if (s->rule != RMS_RULE_REFLECT) variant = 0;   // the rules are built for the first variant
+        if (!split_variant_walks(variant, s->mode, s->rule)) variant = 0;   // waveforms and rules: first variant
         if (variant >= split_variant_count()) return set_error(RMS_ERR_ARG, "variant out of range");
         block = split_variant_block(variant);
         per_sm = walk_split_blocks_per_sm(nc_max, lattice_bits, variant);
@@ -816,6 +816,10 @@ int autotune(rms_sim* const* sims, int n, const rms_run_opts* opts, int* variant
     std::vector<double> ms(nv, 0.0);
     int best = 0;
     for (int v = -1; v < nv; ++v) {
+        if (v >= 0 && !split_variant_walks(v, sims[0]->mode, sims[0]->rule)) {
+            ms[v] = INFINITY;                    // built for the first variant only
+            continue;
+        }
         o.variant = (v < 0 ? 0 : v) + 1;
         int rc = run_launch(jobs, &o);
         if (rc) return rc;

@@ -103,6 +103,7 @@ int launch_walk_compat(const WalkArgs& a, int grid, int block, bool trace, void*
 // a.out_rows/out_sig for several axons); lattice_bits: packed lattice format.
 int launch_walk_split(const WalkArgs& a, int lattice_bits, int variant, int grid, void* stream);
 int split_variant_count();
+bool split_variant_walks(int variant, int mode, int rule);   // variants past the first: narrow/PGSE, reflecting
 int split_variant_block(int variant);   // threads per block of a launch variant
 int split_variant_minb(int variant);    // its minimum resident blocks per SM
 // The split walk's lattice: (n1+2) x (n2+2) x (n3+2) with a wall-code border;

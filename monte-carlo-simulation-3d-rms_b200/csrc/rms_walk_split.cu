@@ -135,7 +135,7 @@ __device__ __noinline__ void wave_final(const double* ph, int nthr, int nwave, d
 
 // ONE: the launch has one axon, whose scalars are read from the kernel
 // parameters (a.axon0) instead of being held in registers.
-template <int NCMAX, int BITS, int BLOCK, int MINB, bool ONE, int RULE = 0>
+template <int NCMAX, int BITS, int BLOCK, int MINB, bool ONE, int RULE = 0, int MODE = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs a) {
     // per warp, the current axon's tables: step (voxels), T2 exponent per voxel
     // of path, Pij and the step-length ratio that rescales the rest of a step
@@ -148,9 +148,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     const int warp_global = gtid >> 5;
     const int nwarps = nthr >> 5;
     float* tab = s_tab[threadIdx.x >> 5];
-    const bool pgse = (a.mode == 1);
-    const bool wave = (a.mode == 2);
-    const bool sums = pgse || wave;   // displacement sums over the walk
+    // the signal mode is compiled in: a walk carries no code of the others
+    constexpr bool pgse = (MODE == 1);
+    constexpr bool wave = (MODE == 2);
+    constexpr bool sums = pgse || wave;   // displacement sums over the walk
     const bool mirror = (a.boundary == 0);
     constexpr int kWall = wall_code<BITS>();
 
@@ -564,35 +565,54 @@ __global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int 
     }
 }
 
-template <int NCMAX, int BITS, int BLOCK, int MINB>
-int launch_t(const WalkArgs& a, int grid, void* stream) {
-    if (a.naxons == 1 && !a.table_form) walk_split_kernel<NCMAX, BITS, BLOCK, MINB, true><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a);
-    else walk_split_kernel<NCMAX, BITS, BLOCK, MINB, false><<<grid, BLOCK, 0, (cudaStream_t)stream>>>(a);
+template <int NCMAX, int BITS, int B, int M, int MODE, int RULE>
+int launch_k(const WalkArgs& a, int grid, void* stream) {
+    if (a.naxons == 1 && !a.table_form)
+        walk_split_kernel<NCMAX, BITS, B, M, true, RULE, MODE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
+    else
+        walk_split_kernel<NCMAX, BITS, B, M, false, RULE, MODE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
     return (int)cudaGetLastError();
 }
 
-// The alternative membrane rules (rejection sampling, equal-step-length
-// leap): first launch variant, one-axon and batch forms.
-template <int NCMAX, int BITS, int RULE>
-int launch_rule(const WalkArgs& a, int grid, void* stream) {
+// Launch variants 2.. walk narrow-pulse and PGSE jobs with reflecting
+// membranes; the first variant also walks waveforms and the alternative
+// membrane rules (rejection sampling, equal-step-length leap).
+template <int NCMAX, int BITS, int B, int M>
+int launch_modes(const WalkArgs& a, int grid, void* stream) {
+    if (a.rule != 0) return (int)cudaErrorInvalidValue;
+    if (a.mode == 0) return launch_k<NCMAX, BITS, B, M, 0, 0>(a, grid, stream);
+    if (a.mode == 1) return launch_k<NCMAX, BITS, B, M, 1, 0>(a, grid, stream);
+    return (int)cudaErrorInvalidValue;
+}
+
+template <int NCMAX, int BITS>
+int launch_first(const WalkArgs& a, int grid, void* stream) {
     constexpr int B = kVariants[0].block, M = kVariants[0].minb;
-    if (a.naxons == 1 && !a.table_form) walk_split_kernel<NCMAX, BITS, B, M, true, RULE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
-    else walk_split_kernel<NCMAX, BITS, B, M, false, RULE><<<grid, B, 0, (cudaStream_t)stream>>>(a);
-    return (int)cudaGetLastError();
+    switch (a.mode * 3 + a.rule) {
+        case 0: return launch_k<NCMAX, BITS, B, M, 0, 0>(a, grid, stream);
+        case 1: return launch_k<NCMAX, BITS, B, M, 0, 1>(a, grid, stream);
+        case 2: return launch_k<NCMAX, BITS, B, M, 0, 2>(a, grid, stream);
+        case 3: return launch_k<NCMAX, BITS, B, M, 1, 0>(a, grid, stream);
+        case 4: return launch_k<NCMAX, BITS, B, M, 1, 1>(a, grid, stream);
+        case 5: return launch_k<NCMAX, BITS, B, M, 1, 2>(a, grid, stream);
+        case 6: return launch_k<NCMAX, BITS, B, M, 2, 0>(a, grid, stream);
+        case 7: return launch_k<NCMAX, BITS, B, M, 2, 1>(a, grid, stream);
+        case 8: return launch_k<NCMAX, BITS, B, M, 2, 2>(a, grid, stream);
+        default: return (int)cudaErrorInvalidValue;
+    }
 }
 
 template <int BLOCK, int MINB>
-const void* kernel_ptr(int nc, int bits) {
-    if (bits == 2) return (const void*)walk_split_kernel<4, 2, BLOCK, MINB, false>;
+const void* kernel_ptr(int bits) {
     if (bits == 4) return (const void*)walk_split_kernel<8, 4, BLOCK, MINB, false>;
     return (const void*)walk_split_kernel<8, 8, BLOCK, MINB, false>;
 }
 
 template <int BLOCK, int MINB>
 int launch_v(const WalkArgs& a, int bits, int grid, void* stream) {
-    if (bits == 2) return a.nc <= 3 ? launch_t<4, 2, BLOCK, MINB>(a, grid, stream) : (int)cudaErrorInvalidValue;
-    if (bits == 4) return a.nc <= 7 ? launch_t<8, 4, BLOCK, MINB>(a, grid, stream) : (int)cudaErrorInvalidValue;
-    return launch_t<8, 8, BLOCK, MINB>(a, grid, stream);
+    if (bits == 4) return a.nc <= 7 ? launch_modes<8, 4, BLOCK, MINB>(a, grid, stream) : (int)cudaErrorInvalidValue;
+    if (bits == 8) return launch_modes<8, 8, BLOCK, MINB>(a, grid, stream);
+    return (int)cudaErrorInvalidValue;
 }
 
 // Dispatch over the variant table (index v, 0-based).
@@ -632,18 +652,20 @@ int split_variant_minb(int v) { return (v >= 0 && v < kNumVariants) ? kVariants[
 
 int launch_walk_split(const WalkArgs& a, int lattice_bits, int variant, int grid, void* stream) {
     if (variant < 0 || variant >= kNumVariants) return (int)cudaErrorInvalidValue;
-    if (a.rule != 0) {
-        if (variant != 0 || lattice_bits == 2) return (int)cudaErrorInvalidValue;
-        if (lattice_bits == 4)
-            return a.rule == 1 ? launch_rule<8, 4, 1>(a, grid, stream) : launch_rule<8, 4, 2>(a, grid, stream);
-        return a.rule == 1 ? launch_rule<8, 8, 1>(a, grid, stream) : launch_rule<8, 8, 2>(a, grid, stream);
+    if (a.mode < 0 || a.mode > 2 || a.rule < 0 || a.rule > 2) return (int)cudaErrorInvalidValue;
+    if (variant == 0) {
+        if (lattice_bits == 4) return a.nc <= 7 ? launch_first<8, 4>(a, grid, stream) : (int)cudaErrorInvalidValue;
+        if (lattice_bits == 8) return launch_first<8, 8>(a, grid, stream);
+        return (int)cudaErrorInvalidValue;
     }
     return by_variant(variant, [&]<int B, int M>() { return launch_v<B, M>(a, lattice_bits, grid, stream); });
 }
 
+bool split_variant_walks(int variant, int mode, int rule) { return variant == 0 || (mode != 2 && rule == 0); }
+
 int walk_split_blocks_per_sm(int nc, int lattice_bits, int variant) {
     if (variant < 0 || variant >= kNumVariants) return -1;
-    const void* k = by_variant(variant, [&]<int B, int M>() { return kernel_ptr<B, M>(nc, lattice_bits); });
+    const void* k = by_variant(variant, [&]<int B, int M>() { return kernel_ptr<B, M>(lattice_bits); });
     int n = 0;
     const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kVariants[variant].block, 0);
     return e == cudaSuccess ? n : -1;
