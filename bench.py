@@ -291,8 +291,14 @@ class SingleJob:
         self.sim = engine.Sim(lab, **kw)
         self.device, self.stream = device, stream
         self.walker_steps = (self.w1 - self.w0) * kw["tn"]
-        self.launches_per_step = 2 + (1 if self.sim.mode == "pgse" else 0)
+        self.launches_per_step = 1
         self.pinned = None
+
+    def tune(self, precision):
+        # SPLIT: the walk kernel alone (rows added into the totals);
+        # COMPAT: the walk, then the ordered reduce of the rows (and of the signals)
+        if precision == "compat":
+            self.launches_per_step = 2 + (1 if self.sim.mode == "pgse" else 0)
 
     def run(self, seed, precision):
         self.sim.run(seed=seed, precision=precision, device=self.device, stream=self.stream,

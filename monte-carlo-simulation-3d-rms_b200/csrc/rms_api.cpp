@@ -397,7 +397,7 @@ struct LaunchPlan {
 // Run one launch: COMPAT (one simulation) or SPLIT (one or more simulations,
 // "axons", walked by one persistent grid).  The first job's simulation owns
 // the launch's accumulators.
-int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan& p, bool table_form = false) {
+int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan& p) {
     rms_sim* s = jobs[0].s;
     const int prec = o ? o->precision : RMS_PREC_COMPAT;
     if (prec != RMS_PREC_COMPAT && prec != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "precision");
@@ -462,10 +462,12 @@ int plan_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o, LaunchPlan&
     const size_t row = (size_t)T * nvals;
 
     const int nseg = nwarps;   // one accumulator row set per warp
-    // several axons, or a launch a graph replays with new seeds: the table
-    // form (axon fields and seeds from device memory, rows added into the
-    // axon totals); one axon otherwise reads its fields from kernel parameters
-    const bool multi = naxons > 1 || table_form;
+    // The SPLIT walk runs in the table form (axon fields and seeds from device
+    // memory, tiles from a queue, each warp's rows added into the axon totals
+    // with FP64 atomics): for one axon too, where it is 1.3x faster than the
+    // form reading kernel parameters (fewer registers), at the price of sums
+    // repeatable only up to their order.  COMPAT: per-warp rows, ordered sum.
+    const bool multi = prec == RMS_PREC_SPLIT;
 
     // inputs
     for (LaunchJob& j : jobs) {
@@ -593,7 +595,7 @@ int enqueue_launch(LaunchPlan& p, rms_sim* s, bool events) {
     if (e) return cuda_fail((cudaError_t)e, "walk kernel launch");
     if (events) RMS_CUDA(cudaEventRecord(d->e1, st));
     if (!p.multi) {
-        // one axon: the warps' rows summed in a fixed order (repeatable)
+        // COMPAT: the warps' rows summed in a fixed order (repeatable)
         e = launch_reduce_slots(a.slots, p.nseg, p.row, d->out.as<double>(), st);
         if (!e && p.has_sig)
             e = launch_reduce_slots(a.sig_slots, p.nseg, (size_t)p.ngrad_pad, d->out_sig.as<double>(), st);
@@ -723,7 +725,7 @@ int graph_create(rms_sim* const* sims, int n, const rms_run_opts* o, rms_graph**
     g->device = o->device;
     for (int i = 0; i < n; ++i) g->jobs.push_back(LaunchJob{sims[i], 0, sims[i]->npar, o->seed + (uint64_t)i * kBatchSeedStep});
     rms_run_opts oo = *o;
-    int rc = plan_launch(g->jobs, &oo, g->plan, true);
+    int rc = plan_launch(g->jobs, &oo, g->plan);
     if (rc) return rc;
     LaunchPlan& p = g->plan;
     if (!o->stream) p.st = p.d->own;   // capture needs a stream other than the legacy default stream

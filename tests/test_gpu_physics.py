@@ -129,6 +129,6 @@ def test_gpu_tube_lattice_equals_the_host_builder():
         ref = engine.Sim(host, dt=2e-4, tn=1000, npar=2000, res=0.1, diffusivity=[0, 2.0, 2.0],
                          t2=[80, 80, 60], bval=[], bvec=np.zeros((0, 3)))
         b = ref.run(seed=1, precision="split").outputs()
-        # the same lattice: the same walk, bit for bit
-        np.testing.assert_array_equal(a["dx2"], b["dx2"])
+        # the same lattice: the same walk (FP64 totals up to their summation order)
+        np.testing.assert_allclose(a["dx2"], b["dx2"], rtol=1e-12, atol=1e-300)
         np.testing.assert_array_equal(a["npar_count"], b["npar_count"])
