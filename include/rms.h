@@ -250,6 +250,39 @@ int rms_sim_cumulants(const rms_sim* sim, const double* dirs, int ndir, double* 
 int rms_combine_cumulants(int naxons, int T, int ndir, const double* f, const double* D_axons,
                           const double* K_axons, double* D, double* K);
 
+/* DKI fits of a signal table (host functions; no simulation needed).
+ * sig[T*m]: signal per timepoint and measurement, normalised as the readers do
+ * (narrow pulses: |sigRe| / sig0, readRMS.m:47-48; PGSE: |sig|,
+ * readRMS_pgse.m:56); bvec[m*3] gradient directions, bval[m] b-values.
+ *
+ * rms_dki_shell (readRMS.m:51-78; readRMS_pgse.m:60-89 with intercept = 1):
+ * per unique direction (exact row equality) the least-squares fit of
+ * log(S + eps) against [1] -b, b^2/6, ..., b^nb/6 (nb = number of distinct
+ * b-values), D = first slope, K = second / D^2; then <x^2> = 2 D td[t] and
+ * <x^4> = (K + 3) <x^2>^2 per direction, fitted over the directions by the 6
+ * second-order and 15 fourth-order tensor elements: dt[t*21 + 0..5], [6..20].
+ * rms_dki_lls (readRMS.m:80-91): log(S + eps) fitted by the 21 DKI terms
+ * -b D_cnt g_i g_j and b^2/6 W_cnt g_i g_j g_k g_l (unit directions):
+ * dt[t*21 + 0..20] (the reference returns the transpose, [21][T]).
+ * Each least-squares solve is MATLAB's backslash: QR with column pivoting,
+ * and for a rank-deficient system (the intercept form always is: a direction
+ * has one more column than distinct b-values; fewer than 15 directions; one
+ * b-shell) its basic solution, where MATLAB also prints a warning.  Fewer
+ * than two distinct b-values is RMS_ERR_ARG (the reference indexes past X).
+ *
+ * rms_akc_shell (readRMS.m:105-112): D and K along ndir directions from a
+ * shell fit: x2 = dt[0..5].n2, x4 = dt[6..20].n4, D = x2/(2 td), K = x4/x2^2 - 3.
+ * rms_akc_lls (readRMS.m:114-117, whose DKI.akc is an external MATLAB class
+ * the reference does not ship): the DKI signal model
+ * ln S = -b D(n) + b^2 D(n)^2 K(n)/6 read off the LLS coefficients,
+ * D(n) = sum D_cnt dt_ij n_i n_j, K(n) = sum W_cnt dt_ijkl n_i n_j n_k n_l / D(n)^2.
+ * Outputs D[t*ndir + q], K[t*ndir + q]. */
+int rms_dki_shell(int T, int m, const double* sig, const double* bvec, const double* bval, const double* td,
+                  int intercept, double* dt);
+int rms_dki_lls(int T, int m, const double* sig, const double* bvec, const double* bval, double* dt);
+int rms_akc_shell(int T, const double* dt, int ndir, const double* dirs, const double* td, double* D, double* K);
+int rms_akc_lls(int T, const double* dt, int ndir, const double* dirs, double* D, double* K);
+
 /* A batch launch captured once as a CUDA graph and replayed with new seeds.
  * rms_batch_graph_create plans the SPLIT launch of rms_batch_run(sims, n,
  * opts) (uploads the tables, sizes the buffers) and captures its device work

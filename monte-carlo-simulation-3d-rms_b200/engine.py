@@ -33,7 +33,8 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
            "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases",
            "rms_adjoint_run", "rms_autotune", "rms_batch_graph_create", "rms_graph_run", "rms_graph_destroy",
-           "rms_sim_cumulants", "rms_combine_cumulants", "rms_sim_set_tube_lattice")
+           "rms_sim_cumulants", "rms_combine_cumulants", "rms_sim_set_tube_lattice",
+           "rms_dki_shell", "rms_dki_lls", "rms_akc_shell", "rms_akc_lls")
 CONTRACT = {"fp32": 0, "bf16x3": 1, "bf16x3_presplit": 2}
 
 _DP = C.POINTER(C.c_double)
@@ -119,6 +120,10 @@ def lib():
         L.rms_sim_set_tube_lattice.argtypes = [C.c_void_p, _DP, _DP, _DP, C.c_int, C.c_int, C.c_int]
         L.rms_sim_cumulants.argtypes = [C.c_void_p, _DP, C.c_int, _DP, _DP]
         L.rms_combine_cumulants.argtypes = [C.c_int, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP]
+        L.rms_dki_shell.argtypes = [C.c_int, C.c_int, _DP, _DP, _DP, _DP, C.c_int, _DP]
+        L.rms_dki_lls.argtypes = [C.c_int, C.c_int, _DP, _DP, _DP, _DP]
+        L.rms_akc_shell.argtypes = [C.c_int, _DP, C.c_int, _DP, _DP, _DP, _DP]
+        L.rms_akc_lls.argtypes = [C.c_int, _DP, C.c_int, _DP, _DP, _DP]
         L.rms_autotune.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_int), _DP]
         L.rms_adjoint_run.argtypes = [C.c_void_p, C.POINTER(RunOpts), _DP, C.POINTER(AdjointGrads)]
         L.rms_contract_phases.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_int,
@@ -361,6 +366,58 @@ def combine_cumulants(f, Ds, Ks):
     D, K = np.zeros(T * nd), np.zeros(T * nd)
     _check(lib().rms_combine_cumulants(na, T, nd, _ptr(_arr(f)), _ptr(_arr(Ds)), _ptr(_arr(Ks)), _ptr(D), _ptr(K)))
     return D.reshape(T, nd), K.reshape(T, nd)
+
+
+def _signal_table(sig, bvec, bval):
+    sig = np.atleast_2d(np.asarray(sig, dtype=np.float64))
+    bvec = _arr(bvec)
+    bval = _arr(bval)
+    T, m = sig.shape
+    if bvec.size != 3 * m or bval.size != m:
+        raise ValueError("sig [T, m] needs bvec [m, 3] and bval [m]")
+    return np.ascontiguousarray(sig), bvec, bval, T, m
+
+
+def dki_shell(sig, bvec, bval, td, intercept=False):
+    """Shell-wise DKI fit (readRMS.m:51-78; intercept=True: readRMS_pgse.m:60-89)
+    of sig [T, m] (e.g. analysis.narrow_signal): dt [T, 21], the 6 <x^2> and 15
+    <x^4> tensor elements per timepoint (rms_dki_shell)."""
+    sig, bvec, bval, T, m = _signal_table(sig, bvec, bval)
+    tdv = _arr(td)
+    if tdv.size != T:
+        raise ValueError("td needs one value per timepoint")
+    dt = np.zeros(T * 21)
+    _check(lib().rms_dki_shell(T, m, _ptr(sig), _ptr(bvec), _ptr(bval), _ptr(tdv), int(bool(intercept)), _ptr(dt)))
+    return dt.reshape(T, 21)
+
+
+def dki_lls(sig, bvec, bval):
+    """Linear least-squares DKI fit (readRMS.m:80-91) of sig [T, m]: the 21
+    coefficients per timepoint, dt [T, 21] (rms_dki_lls)."""
+    sig, bvec, bval, T, m = _signal_table(sig, bvec, bval)
+    dt = np.zeros(T * 21)
+    _check(lib().rms_dki_lls(T, m, _ptr(sig), _ptr(bvec), _ptr(bval), _ptr(dt)))
+    return dt.reshape(T, 21)
+
+
+def akc_shell(dt, dirs, td):
+    """(K, D) [T, ndir] along dirs [ndir, 3] from a shell fit (readRMS.m:105-112)."""
+    dt = np.ascontiguousarray(np.atleast_2d(np.asarray(dt, dtype=np.float64)))
+    d, tdv = _arr(dirs), _arr(td)
+    T, nd = dt.shape[0], d.size // 3
+    D, K = np.zeros(T * nd), np.zeros(T * nd)
+    _check(lib().rms_akc_shell(T, _ptr(dt), nd, _ptr(d), _ptr(tdv), _ptr(D), _ptr(K)))
+    return K.reshape(T, nd), D.reshape(T, nd)
+
+
+def akc_lls(dt, dirs):
+    """(K, D) [T, ndir] along dirs [ndir, 3] from an LLS fit (the DKI signal model)."""
+    dt = np.ascontiguousarray(np.atleast_2d(np.asarray(dt, dtype=np.float64)))
+    d = _arr(dirs)
+    T, nd = dt.shape[0], d.size // 3
+    D, K = np.zeros(T * nd), np.zeros(T * nd)
+    _check(lib().rms_akc_lls(T, _ptr(dt), nd, _ptr(d), _ptr(D), _ptr(K)))
+    return K.reshape(T, nd), D.reshape(T, nd)
 
 
 class Graph:
