@@ -244,6 +244,71 @@ def cpu_reference_rate(lab, sim_kw, target_s: float, nthreads: int | None = None
     return job, n, nthreads, kind
 
 
+def run_reference_cuda(args):
+    """The reference's own CUDA program beside this engine's drop-in, process
+    against process on the same run directory: main.cu built unchanged for
+    sm_100a (oracle/_ref/main_cuda) and rms_main (split and compat precision).
+    Workload: the 64x64x512 single-axon lattice in the reference's file
+    contract (mirror walls, 1000 records, b = 1 and 2 ms/um^2 along x and z),
+    1e5 walkers x 5000 steps.  Each process is timed by the wall clock: both
+    read fiber.txt, create a CUDA context, walk, and write the output files.
+    D(t) and K(t) along x and z at the last record come from each one's
+    output files (readRMS.m formulas); the reference seeds cuRAND from
+    /dev/random, so they agree within Monte-Carlo error, not bit for bit."""
+    import shutil
+    import subprocess
+    import tempfile
+    from rms_b200 import analysis, geometry, runio
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    exe = os.path.join(ROOT, "oracle", "_ref", "main_cuda")
+    ours = os.path.join(ROOT, "monte-carlo-simulation-3d-rms_b200", "_build", "rms_main")
+    if not (os.path.exists(exe) and os.path.exists(ours)):
+        print(json.dumps({"impl": "reference-cuda", "unavailable": "oracle/_ref/main_cuda or rms_main not built"}))
+        return
+    npar, tn = args.walkers or 100_000, args.tn or 5_000
+    lab = geometry.axon_lattice(64, 64, 512, 0.1, seed=0, exterior=0)
+    kw = dict(dt=2e-4, tn=tn, npar=npar, res=0.1, diffusivity=[0.0, 2.0], t2=[1e12, 1e12],
+              bval=[1.0, 2.0], bvec=[[1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
+    top = tempfile.mkdtemp(prefix="rms_refcuda_")
+    runs = {}
+    try:
+        for name, cmd in (("reference main.cu", [exe]),
+                          ("rms_main split", [ours, "--precision", "split", "--seed", "7"]),
+                          ("rms_main compat", [ours, "--precision", "compat", "--seed", "7"])):
+            d = os.path.join(top, name.replace(" ", "_").replace(".", "_"))
+            runio.write_inputs(d, lab, **kw)
+            t0 = time.perf_counter()
+            try:
+                r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=600)
+            except subprocess.TimeoutExpired:
+                runs[name] = {"error": "timed out after 600 s"}
+                continue
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                runs[name] = {"error": f"exit {r.returncode}: {(r.stderr or r.stdout)[-300:]}"}
+                continue
+            sig0 = np.loadtxt(os.path.join(d, "sig0.txt"))
+            dx2 = np.loadtxt(os.path.join(d, "dx2.txt"))
+            dx4 = np.loadtxt(os.path.join(d, "dx4.txt"))
+            td = np.loadtxt(os.path.join(d, "diff_time.txt"))
+            D, K = analysis.axis_dk(sig0, dx2, dx4, td)
+            runs[name] = {"wall_s": wall, "walker_steps_per_s": npar * tn / wall,
+                          "D_x": float(D[-1, 0]), "D_z": float(D[-1, 2]),
+                          "K_x": float(K[-1, 0]), "K_z": float(K[-1, 2]),
+                          "stdout_tail": r.stdout.strip().splitlines()[-1:]}
+    finally:
+        shutil.rmtree(top, ignore_errors=True)
+    ref = runs.get("reference main.cu", {})
+    line = {"metric": METRIC, "value": ref.get("walker_steps_per_s"), "unit": UNIT, "n_gpus": 1,
+            "higher_is_better": True, "impl": "reference-cuda", "data": "synthetic (seeded)",
+            "config": {"workload": f"64x64x512 axon (mirror walls, 1000 records, 2 b-values), {npar} walkers, "
+                                   f"{tn} steps: the reference's CUDA program and rms_main on the same run "
+                                   "directory, wall time per process (text I/O and context creation included)"},
+            "runs": runs}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -795,7 +860,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--precision", default="split", choices=["split", "compat"])
     ap.add_argument("--workload", default="batch", choices=["production", "batch", "single", "contraction", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -819,6 +884,8 @@ def main():
             run_contraction(args)
     elif args.impl == "reference":
         run_reference_arm(args)
+    elif args.impl == "reference-cuda":
+        run_reference_cuda(args)
     else:
         run_ours(args)
 
