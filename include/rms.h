@@ -61,7 +61,12 @@ extern "C" {
  *  COMPAT: FP64 positions, FP64 uniforms, the reference's operation order;
  *          per-walker voxel/event sequences equal the CPU oracle's.
  *  SPLIT:  int32 voxel index + FP32 in-voxel offset, FP32 uniforms, FP64
- *          cross-walker sums; statistically equal to COMPAT. */
+ *          cross-walker sums; statistically equal to COMPAT.
+ *  Repeatability: COMPAT sums each record's per-warp rows in a fixed order,
+ *  so a rerun with the same seed is identical bit for bit; SPLIT adds the
+ *  warps' rows into the totals with FP64 atomics, so a rerun has the same
+ *  walkers and compartment counts and equal sums up to their order (about
+ *  1e-15 relative). */
 #define RMS_PREC_COMPAT 0
 #define RMS_PREC_SPLIT 1
 
