@@ -93,6 +93,44 @@ def test_lattice_validation():
     assert e.value.code == -1
 
 
+def test_lattice_check_reports_the_first_bad_voxel():
+    # the check scans in 255-voxel blocks: bad labels on and around block edges
+    s = small_sim()
+    n = 12 * 12 * 16
+    for first in (0, 254, 255, 256, 509, 510, n - 1):
+        lab = np.ones(n, dtype=np.uint8)
+        lab[first] = 5
+        if first + 7 < n:
+            lab[first + 7] = 3
+        with pytest.raises(engine.RmsError) as e:
+            s.set_lattice(lab.reshape(12, 12, 16))
+        assert e.value.code == -4 and f"label 5 at voxel {first} " in str(e.value), str(e.value)
+    # one labelled voxel is enough; labels Nc - 1 are accepted
+    lab = np.zeros(n, dtype=np.uint8)
+    lab[300] = 2
+    s.set_lattice(lab.reshape(12, 12, 16))
+
+
+def test_large_lattice_check_spans_the_threads():
+    # above 32 MB the scan and the copy are split across host threads: a bad
+    # label in the last range is still found, and the first one is reported
+    shape = (64, 64, 16384 + 64)   # 67 MB: two ranges
+    s = engine.Sim(None, shape=shape, dt=2e-4, tn=1000, npar=32, res=0.1, diffusivity=[0, 2.0],
+                   t2=[80, 80], bval=[1.0], bvec=[[1, 0, 0]])
+    lab = np.ones(shape, dtype=np.uint8)
+    s.set_lattice(lab)
+    flat = lab.reshape(-1)
+    last = flat.size - 3
+    flat[last] = 2
+    with pytest.raises(engine.RmsError) as e:
+        s.set_lattice(lab)
+    assert f"label 2 at voxel {last} " in str(e.value)
+    flat[1000] = 7
+    with pytest.raises(engine.RmsError) as e:
+        s.set_lattice(lab)
+    assert "label 7 at voxel 1000 " in str(e.value)
+
+
 def test_results_before_run_are_an_error():
     s = small_sim()
     with pytest.raises(engine.RmsError) as e:
