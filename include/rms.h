@@ -158,6 +158,11 @@ typedef struct rms_sim rms_sim;
 #define RMS_FIELD_STEP 8        /* [nc]           step length in voxels */
 #define RMS_FIELD_PIJ 9         /* [nc*nc]        permeation probability a -> b */
 #define RMS_FIELD_SIGW 10       /* [nwave*2]      waveform signal: sum s0 cos phi, sum s0 sin phi */
+/* Gradient tables as configured, available without a run: */
+#define RMS_FIELD_BVAL 11       /* [nbvec]        bval.txt, ms/um^2 (narrow pulses; main.cu:469-474) */
+#define RMS_FIELD_BVEC 12       /* [nbvec*3]      bvec.txt rows (narrow pulses; main.cu:477-482) */
+#define RMS_FIELD_GRAD 13       /* [ngrad*6]      gradient_time.txt rows: Delta delta |g| gx gy gz
+                                                   (PGSE; main_PGSE.cu:501-506) */
 
 /* Build a simulation from a configuration (what main.cu:414-487 derives from
  * the text inputs).  Replaces: the input parsing + table set-up of

@@ -1027,6 +1027,9 @@ bool field_size(const rms_sim* s, int field, size_t& n) {
         case RMS_FIELD_STEP: n = s->nc; return true;
         case RMS_FIELD_PIJ: n = (size_t)s->nc * s->nc; return true;
         case RMS_FIELD_SIGW: n = s->mode == RMS_MODE_WAVEFORM ? (size_t)2 * s->nwave : 0; return true;
+        case RMS_FIELD_BVAL: n = s->mode == RMS_MODE_NARROW ? (size_t)s->nbvec() : 0; return true;
+        case RMS_FIELD_BVEC: n = s->mode == RMS_MODE_NARROW ? (size_t)3 * s->nbvec() : 0; return true;
+        case RMS_FIELD_GRAD: n = s->mode == RMS_MODE_PGSE ? (size_t)6 * s->ngrad() : 0; return true;
         default: return false;
     }
 }
@@ -1333,8 +1336,11 @@ int rms_sim_get(const rms_sim* s, int field, double* out, size_t n) {
     if (field == RMS_FIELD_DIFFUSIVITY) table = &s->diffusivity;
     if (field == RMS_FIELD_STEP) table = &s->step;
     if (field == RMS_FIELD_PIJ) table = &s->pij;
+    if (field == RMS_FIELD_BVAL) table = &s->bval;
+    if (field == RMS_FIELD_BVEC) table = &s->bvec;
+    if (field == RMS_FIELD_GRAD) table = &s->grad;
     if (table) {
-        std::copy(table->begin(), table->end(), out);
+        std::copy(table->begin(), table->begin() + want, out);
         return RMS_OK;
     }
     if (!s->have_results) return set_error(RMS_ERR_STATE, "no results: run the simulation first");

@@ -21,7 +21,7 @@ BOUNDARY = {"mirror": 0, "periodic": 1}
 PERMEATION = {"reference": 0, "kappa": 1, "table": 2}
 PRECISION = {"compat": 0, "split": 1}
 FIELD = {"sig0": 0, "dx2": 1, "dx4": 2, "sigre": 3, "sig": 4, "npar_count": 5, "td": 6,
-         "diffusivity": 7, "step": 8, "pij": 9, "sigw": 10}
+         "diffusivity": 7, "step": 8, "pij": 9, "sigw": 10, "bval": 11, "bvec": 12, "grad": 13}
 ERRORS = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "RANGE", -5: "CUDA", -6: "NOMEM",
           -7: "STATE", -8: "TIMEOUT"}
 
@@ -274,6 +274,41 @@ class Sim:
         D, K = np.zeros(T * ndir), np.zeros(T * ndir)
         _check(lib().rms_sim_cumulants(self._h, _ptr(d) if d is not None else None, ndir, _ptr(D), _ptr(K)))
         return D.reshape(T, ndir), K.reshape(T, ndir)
+
+    def signal_table(self):
+        """(sig, bvec [m, 3], bval [m]) of the last run, formed as the MATLAB
+        readers form them: narrow pulses |sigRe| / sig0 [T, m] against bval.txt
+        and bvec.txt (readRMS.m:38-48); PGSE |sig| [1, m] (the walker sum, not
+        normalised, as readRMS_pgse.m:56 reads it) against
+        b = |g|^2 delta^2 (Delta - delta/3) and the gradient directions
+        (readRMS_pgse.m:48-53)."""
+        from . import analysis
+        o = self.outputs()
+        if self.mode == "narrow":
+            return analysis.narrow_signal(o["sig0"], o["sigre"]), self.get("bvec").reshape(-1, 3), self.get("bval")
+        if self.mode == "pgse":
+            g = self.get("grad").reshape(-1, 6)
+            return np.abs(o["sig"]).reshape(1, -1), g[:, 3:6], analysis.pgse_bval(g)
+        raise ValueError("signal tables exist for narrow-pulse and PGSE runs")
+
+    def dki_shell(self, td=None):
+        """Shell-wise DKI fit of the last run, dt [T, 21] (rms_dki_shell):
+        narrow pulses as readRMS.m's dki_shell (td: the run's diffusion times);
+        PGSE as readRMS_pgse.m's, with the intercept column that absorbs the
+        walker count, for the diffusion time td of its one row (required)."""
+        sig, bvec, bval = self.signal_table()
+        if self.mode == "pgse":
+            if td is None:
+                raise ValueError("a PGSE table has one row: give its diffusion time td")
+            return dki_shell(sig, bvec, bval, np.atleast_1d(td), intercept=True)
+        return dki_shell(sig, bvec, bval, self.get("td") if td is None else td)
+
+    def dki_lls(self):
+        """Linear least-squares DKI fit of the last narrow-pulse run, dt [T, 21]
+        (readRMS.m's dki_lls, rms_dki_lls)."""
+        if self.mode != "narrow":
+            raise ValueError("the LLS fit reads a normalised signal: narrow-pulse runs (or call dki_lls)")
+        return dki_lls(*self.signal_table())
 
     def field_size(self, name: str) -> int:
         n = C.c_size_t()

@@ -167,3 +167,52 @@ def test_narrow_signal_normalises_by_sig0():
     sig0 = np.array([1.0, 0.5])
     sigre = np.array([[0.5, -0.25], [0.25, 0.125]])
     np.testing.assert_array_equal(analysis.narrow_signal(sig0, sigre), [[0.5, 0.25], [0.5, 0.25]])
+
+
+def test_gradient_tables_are_readable_without_a_run():
+    lab = np.ones((8, 8, 8), dtype=np.uint8)
+    bvec, bval = table(ndirs=20, bvals=(1.0, 2.0))
+    s = engine.Sim(lab, dt=2e-4, tn=1000, npar=32, res=0.1, diffusivity=[0, 2.0], t2=[80, 80],
+                   bval=bval, bvec=bvec)
+    np.testing.assert_array_equal(s.get("bval"), bval)
+    np.testing.assert_array_equal(s.get("bvec").reshape(-1, 3), bvec)
+    assert s.field_size("grad") == 0
+    grad = np.array([[20.0, 4.0, 0.05, 1, 0, 0], [30.0, 4.0, 0.04, 0, 0.6, 0.8]])
+    p = engine.Sim(lab, dt=2e-4, tn=1000, npar=32, res=0.1, diffusivity=[0, 2.0], t2=[80, 80], grad=grad)
+    np.testing.assert_array_equal(p.get("grad").reshape(-1, 6), grad)
+    assert p.field_size("bval") == 0 and p.field_size("bvec") == 0
+
+
+def test_sim_fits_read_the_run_as_the_matlab_readers_do():
+    """Sim.dki_shell / dki_lls form the signal table as readRMS.m (narrow) and
+    readRMS_pgse.m (PGSE) do; the run's outputs are stood in for here."""
+    lab = np.ones((8, 8, 8), dtype=np.uint8)
+    d6, w = model(9)
+    bvec, bval = table(ndirs=20, bvals=(1.0, 2.0, 3.0))
+    T = 4
+    td = np.array([5.0, 10.0, 15.0, 20.0])
+    sig0 = np.array([1e4, 0.9e4, 0.8e4, 0.7e4])
+    S = model_signal(d6, w, bvec, bval, T)
+    s = engine.Sim(lab, dt=2e-4, tn=1000, npar=32, res=0.1, diffusivity=[0, 2.0], t2=[80, 80],
+                   bval=bval, bvec=bvec)
+    s.outputs = lambda: dict(sig0=sig0, sigre=-S * sig0[:, None], td=td)
+    s.get = (lambda get: (lambda name: td if name == "td" else get(name)))(s.get)
+    np.testing.assert_allclose(s.dki_shell(), engine.dki_shell(S, bvec, bval, td), rtol=1e-12)
+    np.testing.assert_allclose(s.dki_lls(), engine.dki_lls(S, bvec, bval), rtol=1e-12)
+    # PGSE: |sig| as summed over walkers, b from the gradient rows, intercept fit
+    from rms_b200 import analysis
+    dirs = np.repeat(fib_dirs(20), 4, axis=0)
+    Delta = np.tile([20.0, 20.0, 30.0, 30.0], 20)
+    bv = np.tile([1.0, 2.0, 1.0, 2.0], 20)
+    g = analysis.pgse_gradient_for_b(bv, Delta, 4.0)
+    grad = np.column_stack([Delta, np.full(bv.size, 4.0), g, dirs])
+    p = engine.Sim(lab, dt=2e-4, tn=1000, npar=32, res=0.1, diffusivity=[0, 2.0], t2=[80, 80], grad=grad)
+    sums = 5e3 * model_signal(d6, w, dirs, bv, 1)[0]
+    p.outputs = lambda: dict(sig=sums)
+    got = p.dki_shell(td=20.0)
+    want = engine.dki_shell(sums[None, :], dirs, analysis.pgse_bval(grad), [20.0], intercept=True)
+    np.testing.assert_allclose(got, want, rtol=1e-12)
+    with pytest.raises(ValueError):
+        p.dki_shell()
+    with pytest.raises(ValueError):
+        p.dki_lls()
