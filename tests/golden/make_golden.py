@@ -6,6 +6,12 @@ written by the REFERENCE PROGRAM ITSELF -- hpc_code/lib/main.cu or
 main_PGSE.cu compiled for the host through oracle/ref_shim (oracle/_ref),
 seed pinned.  Files are stored gzip-compressed.
 
+The realistic case takes its lattice (the first axon of the mitochondria
+family, hpc_code/input/I_realistic_axon_mitochondria/fiber.mat) and every
+6th row of its b-table (hpc_code/btable/btable_5shell_90ndir_b1000.mat) from
+the reference checkout, with the compartment parameters its own demo uses for
+that family (part1_demo3_simulation.m: D = [0 2 2/15], T2 = [80 80 20]).
+
 Needs the reference checkout (to build oracle/_ref); run from the repo root:
     make -C oracle && python tests/golden/make_golden.py
 """
@@ -27,6 +33,7 @@ import pyoracle  # noqa: E402
 from rms_b200 import geometry, runio  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("RMS_REFERENCE", "/root/reference")
 
 
 def lattice(seed: int) -> np.ndarray:
@@ -55,14 +62,40 @@ CASES = {
               [0.25, 0.2, 1.0, 0, 0.6, 0.8], [0.30, 0.15, 2.5, 0.48, 0.6, 0.64],
               [0.35, 0.1, 1.5, 1, 0, 0], [0.40, 0.1, 1.5, 0, 0, 1]],
     ),
+    "realistic_mito_1": dict(
+        seed=31337, tn=2000, npar=64, dt=2e-4, res=0.1,
+        diffusivity=[0.0, 2.0, 2.0 / 15.0], t2=[80.0, 80.0, 20.0],
+        lattice="realistic", btable="reference",
+    ),
 }
+
+
+def realistic_lattice() -> np.ndarray:
+    """The first axon of the reference's mitochondria family: 100 x 100 x 180
+    voxels of 0.1 um, labels 0 (outside), 1 (axon), 2 (mitochondria)."""
+    from scipy.io import loadmat
+    m = loadmat(os.path.join(REF, "hpc_code", "input", "I_realistic_axon_mitochondria", "fiber.mat"))
+    return np.ascontiguousarray(m["fiber"][0, 0]["shape"], dtype=np.uint8)
+
+
+def reference_btable():
+    """Every 6th row of the reference's 5-shell, 90-direction b-table."""
+    from scipy.io import loadmat
+    m = loadmat(os.path.join(REF, "hpc_code", "btable", "btable_5shell_90ndir_b1000.mat"))
+    return m["bval"].ravel()[::6].tolist(), m["bvec"][::6].tolist()
 
 
 def main():
     if not pyoracle.ref_available():
         sys.exit("oracle/_ref/librmsref.so is missing: run make -C oracle with the reference present")
+    only = set(sys.argv[1:])
     for name, c in CASES.items():
-        lab = lattice(1)
+        if only and name not in only:
+            continue
+        lab = realistic_lattice() if c.get("lattice") == "realistic" else lattice(1)
+        if c.get("btable") == "reference":
+            c = dict(c)
+            c["bval"], c["bvec"] = reference_btable()
         tmp = tempfile.mkdtemp()
         kw = dict(dt=c["dt"], tn=c["tn"], npar=c["npar"], res=c["res"],
                   diffusivity=c["diffusivity"], t2=c["t2"])

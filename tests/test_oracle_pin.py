@@ -3,7 +3,9 @@ walk) to the reference itself.
 
 1. Against the golden run directories: output files written by the reference
    program (hpc_code/lib/main.cu, main_PGSE.cu compiled for the host through
-   oracle/ref_shim), regenerated by tests/golden/make_golden.py.
+   oracle/ref_shim), regenerated by tests/golden/make_golden.py -- including
+   one of the reference's own realistic lattices (an axon with mitochondria,
+   0.2 % of the box labelled: ~480 rejection-sampling tries per walker).
 2. Against the reference host build directly (oracle/_ref), bit for bit, on
    fresh random jobs -- skipped when that build is absent.
 """
@@ -45,7 +47,7 @@ def fmt15(a):
     return np.array(["%.15g" % x for x in np.asarray(a).ravel()])
 
 
-@pytest.mark.parametrize("case", ["narrow_3comp", "pgse_3comp"])
+@pytest.mark.parametrize("case", ["narrow_3comp", "pgse_3comp", "realistic_mito_1"])
 def test_oracle_reproduces_reference_outputs(case, tmp_path):
     d = unpack_golden(case, str(tmp_path))
     job = job_from_dir(d, golden_seed(case))
