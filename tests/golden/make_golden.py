@@ -6,11 +6,14 @@ written by the REFERENCE PROGRAM ITSELF -- hpc_code/lib/main.cu or
 main_PGSE.cu compiled for the host through oracle/ref_shim (oracle/_ref),
 seed pinned.  Files are stored gzip-compressed.
 
-The realistic case takes its lattice (the first axon of the mitochondria
-family, hpc_code/input/I_realistic_axon_mitochondria/fiber.mat) and every
-6th row of its b-table (hpc_code/btable/btable_5shell_90ndir_b1000.mat) from
-the reference checkout, with the compartment parameters its own demo uses for
-that family (part1_demo3_simulation.m: D = [0 2 2/15], T2 = [80 80 20]).
+The realistic cases take their lattices from the reference checkout: the
+first axon of the mitochondria family (hpc_code/input/
+I_realistic_axon_mitochondria/fiber.mat) with every 6th row of the b-table
+hpc_code/btable/btable_5shell_90ndir_b1000.mat and the compartment
+parameters the reference's demo uses for that family
+(part1_demo3_simulation.m: D = [0 2 2/15], T2 = [80 80 20]); and the first
+axon of the undulation family (hpc_code/input/IV_undulation/fiber.mat) under
+a PGSE table, walked by main_PGSE.cu.
 
 Needs the reference checkout (to build oracle/_ref); run from the repo root:
     make -C oracle && python tests/golden/make_golden.py
@@ -67,14 +70,23 @@ CASES = {
         diffusivity=[0.0, 2.0, 2.0 / 15.0], t2=[80.0, 80.0, 20.0],
         lattice="realistic", btable="reference",
     ),
+    "realistic_undulation_pgse": dict(
+        seed=4242, tn=2000, npar=64, dt=2e-4, res=0.1,
+        diffusivity=[0.0, 2.0, 2.0], t2=[80.0, 80.0, 80.0],
+        # Delta, delta, |g|, gx, gy, gz: along the axon (z), across it, oblique
+        grad=[[0.20, 0.10, 3.0, 0, 0, 1], [0.20, 0.10, 3.0, 1, 0, 0], [0.20, 0.10, 3.0, 0, 1, 0],
+              [0.30, 0.05, 4.0, 0.48, 0.6, 0.64], [0.35, 0.05, 2.0, 0, 0.6, 0.8]],
+        lattice="undulation",
+    ),
 }
 
 
-def realistic_lattice() -> np.ndarray:
-    """The first axon of the reference's mitochondria family: 100 x 100 x 180
-    voxels of 0.1 um, labels 0 (outside), 1 (axon), 2 (mitochondria)."""
+def realistic_lattice(family: str = "I_realistic_axon_mitochondria") -> np.ndarray:
+    """The first axon of one of the reference's lattice families: 100 x 100 x
+    180 voxels of 0.1 um, labels 0 (outside), 1 (axon) and, in the
+    mitochondria family, 2 (mitochondria)."""
     from scipy.io import loadmat
-    m = loadmat(os.path.join(REF, "hpc_code", "input", "I_realistic_axon_mitochondria", "fiber.mat"))
+    m = loadmat(os.path.join(REF, "hpc_code", "input", family, "fiber.mat"))
     return np.ascontiguousarray(m["fiber"][0, 0]["shape"], dtype=np.uint8)
 
 
@@ -92,7 +104,12 @@ def main():
     for name, c in CASES.items():
         if only and name not in only:
             continue
-        lab = realistic_lattice() if c.get("lattice") == "realistic" else lattice(1)
+        if c.get("lattice") == "realistic":
+            lab = realistic_lattice()
+        elif c.get("lattice") == "undulation":
+            lab = realistic_lattice("IV_undulation")
+        else:
+            lab = lattice(1)
         if c.get("btable") == "reference":
             c = dict(c)
             c["bval"], c["bvec"] = reference_btable()

@@ -47,7 +47,7 @@ def fmt15(a):
     return np.array(["%.15g" % x for x in np.asarray(a).ravel()])
 
 
-@pytest.mark.parametrize("case", ["narrow_3comp", "pgse_3comp", "realistic_mito_1"])
+@pytest.mark.parametrize("case", ["narrow_3comp", "pgse_3comp", "realistic_mito_1", "realistic_undulation_pgse"])
 def test_oracle_reproduces_reference_outputs(case, tmp_path):
     d = unpack_golden(case, str(tmp_path))
     job = job_from_dir(d, golden_seed(case))
