@@ -4,7 +4,9 @@ Writers produce the input files the reference's ``./main_cuda`` reads, in the
 layout its MATLAB writer uses (analysis/setupRMS.m:16-69); the PGSE inputs,
 for which the reference ships no writer, follow the reader in
 hpc_code/lib/main_PGSE.cu:440-445, 495-506.  Readers load the output files
-the simulator writes (hpc_code/lib/main.cu:550-615, main_PGSE.cu:596-669).
+the simulator writes (hpc_code/lib/main.cu:550-615, main_PGSE.cu:596-669), and
+the reference's MATLAB geometry and b-table files (hpc_code/input/*/fiber.mat,
+hpc_code/btable/*.mat).
 """
 from __future__ import annotations
 
@@ -144,3 +146,39 @@ def read_outputs(root: str) -> RunOutputs:
     if os.path.exists(p_sig):
         out.sig = _load(p_sig)
     return out
+
+
+# ---- the reference's MATLAB data files (MAT v5) ----
+
+def read_fiber_mat(path: str) -> list:
+    """The lattices of a geometry file in the reference's layout
+    (hpc_code/input/*/fiber.mat, read by part1_demo3_simulation.m:28-31): a
+    struct array ``fiber`` whose elements hold ``shape`` (a uint8 label
+    lattice, [NPix1, NPix2, NPix3]) and ``voxel_size`` (um).  Returns a list of
+    (labels, voxel_size), labels C-contiguous uint8 in the engine's layout (k
+    fastest, as fiber.txt is written)."""
+    from scipy.io import loadmat
+    m = loadmat(path)
+    if "fiber" not in m:
+        raise ValueError(f"{path}: no 'fiber' variable")
+    fib = m["fiber"].ravel()
+    out = []
+    for f in fib:
+        lab = np.ascontiguousarray(np.asarray(f["shape"]), dtype=np.uint8)
+        if lab.ndim != 3:
+            raise ValueError(f"{path}: a fiber shape is not a 3-D lattice")
+        out.append((lab, float(np.asarray(f["voxel_size"]).ravel()[0])))
+    return out
+
+
+def read_btable_mat(path: str):
+    """A b-table in the reference's layout (hpc_code/btable/*.mat, read by
+    part1_demo3_simulation.m:35-37): ``bval`` [Nbvec] (ms/um^2) and ``bvec``
+    [Nbvec, 3].  Returns (bval, bvec) as float64 arrays."""
+    from scipy.io import loadmat
+    m = loadmat(path)
+    bval = np.asarray(m["bval"], dtype=np.float64).ravel()
+    bvec = np.asarray(m["bvec"], dtype=np.float64).reshape(-1, 3)
+    if bvec.shape[0] != bval.size:
+        raise ValueError(f"{path}: bval and bvec disagree in length")
+    return bval, bvec
