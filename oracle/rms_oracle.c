@@ -278,9 +278,22 @@ static int homogeneous(const or_params* p, const int g[3]) {
     return 1;
 }
 
-static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, double* phase,
-                           int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev, double* tr_pos,
-                           double* tr_bin) {
+/* Adjoint bookkeeping of one walker (or_adjoint_split; the GPU kernel's
+ * pass-1 quantities, restated in FP64): the tangent of the displacement with
+ * respect to the step length l with the event sequence frozen (gains the step
+ * direction each step, flips its component at every reflection, membrane or
+ * mirror wall), its bin sums folded into dphi, the permeation score
+ * E = sum over Bernoulli crossings of (1[crossed] - Pij), the path per
+ * compartment (voxels), the final T2 exponent and each bin's displacement sum. */
+typedef struct {
+    double T[3], B[3], E, tc[8], wexp;
+    double* dphi;   /* [nwave] */
+    double* xbin;   /* [nbins*3], um */
+} or_adj;
+
+static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, double* phase,
+                            int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev, double* tr_pos,
+                            double* tr_bin, or_adj* adj) {
     const int Nc = p->nc;
     /* free flight applies when same-label faces are always crossed, no walker
      * can enter compartment 0, and three crossings fit the sub-segment cap */
@@ -328,6 +341,7 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
         const double sz = 2.0 * sqrt(u1 * (1.0 - u1));
         const double phi = 6.283185307179586 * (u2 - 0.5);
         double v[3] = {sz * cos(phi), sz * sin(phi), cz};
+        if (adj) for (int a = 0; a < 3; a++) adj->T[a] += v[a];
         rem = p->step[ai];
         flo = 0; fhi = 0; nev = 0;
         ev = 0;
@@ -340,6 +354,7 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
                 f[a] = x - k;
             }
             wexp += rem / p->step[ai] / p->t2[ai];
+            if (adj) adj->tc[ai] += rem;
             rem = 0.0;
         }
         for (int j = 0; j < p->nite && rem > 0.0; j++) {
@@ -353,12 +368,14 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
             if (rem < tmin) {
                 for (int a = 0; a < 3; a++) f[a] += rem * v[a];
                 wexp += rem / p->step[ai] / p->t2[ai];
+                if (adj) adj->tc[ai] += rem;
                 rem = 0.0;
                 break;
             }
             const int hit = (t[0] == tmin) ? 0 : ((t[1] == tmin) ? 1 : 2);
             for (int a = 0; a < 3; a++) f[a] += tmin * v[a];
             wexp += tmin / p->step[ai] / p->t2[ai];
+            if (adj) adj->tc[ai] += tmin;
             rem -= tmin;
             const int up = v[hit] > 0.0;
             f[hit] = up ? 1.0 : 0.0;
@@ -367,6 +384,7 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
             if (wall && p->boundary == OR_BOUNDARY_MIRROR) {
                 if (up) fhi |= 1 << hit; else flo |= 1 << hit;
                 v[hit] = -v[hit];
+                if (adj) adj->T[hit] = -adj->T[hit];
                 ev |= (OR_EV_MIRROR << 2 | (uint32_t)hit) << (4 * nev++);
                 if (!(rem > 0.0)) break;
                 continue;
@@ -377,6 +395,7 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
             const int aj = APix[lin(p, gn[0], gn[1], gn[2])];
             const double P = p->pij[ai * Nc + aj];
             const int cross = (P > 0.999999) || (P >= 0.000001 && (double)or_dstream_float(&perm) < P);
+            if (adj && !(P > 0.999999) && P >= 0.000001) adj->E += (cross ? 1.0 : 0.0) - P;
             if (p->rule != OR_RULE_REFLECT && !cross) {
                 turned = 1;   /* the rule decides, after the loop */
                 break;
@@ -396,6 +415,7 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
                 }
             } else {
                 v[hit] = -v[hit];
+                if (adj) adj->T[hit] = -adj->T[hit];
                 ev |= (OR_EV_REFLECT << 2 | (uint32_t)hit) << (4 * nev++);
             }
             if (!(rem > 0.0)) break;
@@ -446,11 +466,18 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
         }
         if (p->mode == OR_MODE_WAVEFORM) {
             X[0] += dx; X[1] += dy; X[2] += dz;
+            if (adj) for (int a = 0; a < 3; a++) adj->B[a] += adj->T[a];
             if ((i + 1) % bin_steps == 0) {
                 const int b = (i + 1) / bin_steps - 1;
                 for (int j = 0; j < p->nwave; j++) {
                     const double* wv = p->wave + ((size_t)j * p->nbins + b) * 3;
                     phase[j] += p->dt * (wv[0] * X[0] + wv[1] * X[1] + wv[2] * X[2]);
+                    if (adj)
+                        adj->dphi[j] += p->dt * (wv[0] * adj->B[0] + wv[1] * adj->B[1] + wv[2] * adj->B[2]) * p->res;
+                }
+                if (adj) {
+                    for (int a = 0; a < 3; a++) adj->xbin[3 * b + a] = X[a];
+                    adj->B[0] = adj->B[1] = adj->B[2] = 0.0;
                 }
                 if (tr_bin)
                     for (int a = 0; a < 3; a++) tr_bin[3 * b + a] = X[a] / (double)bin_steps;
@@ -489,6 +516,13 @@ static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, doubl
             }
         }
     }
+    if (adj) adj->wexp = wexp;
+}
+
+static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, double* phase,
+                           int32_t* tr_init, int32_t* tr_vox, uint32_t* tr_ev, double* tr_pos,
+                           double* tr_bin) {
+    walk_split_core(p, w, out, phase, tr_init, tr_vox, tr_ev, tr_pos, tr_bin, NULL);
 }
 
 typedef void (*walk_fn)(const or_params*, int64_t, or_outputs*, double*, int32_t*, int32_t*,
@@ -502,6 +536,61 @@ int or_run_split(const or_params* p, int64_t w_begin, int64_t w_end, or_outputs*
     int rc = check(p);
     if (rc) return rc;
     return run_range(p, w_begin, w_end, out, tr, walk_one_split);
+}
+
+int or_adjoint_split(const or_params* p, const double* gup, int64_t w_begin, int64_t w_end, double* sums,
+                     double* dwave) {
+    int rc = check(p);
+    if (rc) return rc;
+    if (p->mode != OR_MODE_WAVEFORM || p->rule != OR_RULE_REFLECT || p->nc > 8) return -6;
+    const int nw = p->nwave, nb = p->nbins, nc = p->nc;
+    double* phase = (double*)calloc((size_t)nw, sizeof(double));
+    double* dphi = (double*)calloc((size_t)nw, sizeof(double));
+    double* xbin = (double*)calloc((size_t)nb * 3, sizeof(double));
+    or_outputs scratch;
+    double* sbuf = (double*)calloc((size_t)p->timepoints * (1 + 6 + 15 + nc) + 2 * (size_t)nw + 1, sizeof(double));
+    if (!phase || !dphi || !xbin || !sbuf) {
+        free(phase); free(dphi); free(xbin); free(sbuf);
+        return -10;
+    }
+    scratch.sig0 = sbuf;
+    scratch.dx2 = scratch.sig0 + p->timepoints;
+    scratch.dx4 = scratch.dx2 + 6 * p->timepoints;
+    scratch.npar_count = scratch.dx4 + 15 * p->timepoints;
+    scratch.sigw = scratch.npar_count + (size_t)nc * p->timepoints;
+    scratch.sigre = NULL;
+    scratch.sig = NULL;
+    for (int64_t w = w_begin; w < w_end; ++w) {
+        or_adj adj;
+        memset(&adj, 0, sizeof adj);
+        memset(phase, 0, sizeof(double) * (size_t)nw);
+        memset(dphi, 0, sizeof(double) * (size_t)nw);
+        adj.dphi = dphi;
+        adj.xbin = xbin;
+        walk_split_core(p, w, &scratch, phase, NULL, NULL, NULL, NULL, NULL, &adj);
+        /* this walker's loss L_w = s0 sum_j (gC_j cos phi_j + gS_j sin phi_j)
+         * and a_j = dL_w / dphi_j */
+        const double s0 = exp(-adj.wexp);
+        double Lw = 0.0, G = 0.0;
+        for (int j = 0; j < nw; j++) {
+            const double c = cos(phase[j]), sn = sin(phase[j]);
+            const double a = s0 * (gup[2 * j + 1] * c - gup[2 * j] * sn);
+            Lw += s0 * (gup[2 * j] * c + gup[2 * j + 1] * sn);
+            G += a * dphi[j];
+            sums[4 + nc + 2 * j] += s0 * c;
+            sums[4 + nc + 2 * j + 1] += s0 * sn;
+            for (int b = 0; b < nb; b++)
+                for (int k = 0; k < 3; k++) dwave[((size_t)b * nw + j) * 3 + k] += a * xbin[3 * b + k];
+        }
+        sums[0] += Lw;
+        sums[1] += Lw * adj.E;
+        sums[2] += G;
+        sums[3] += adj.E;
+        for (int c = 0; c < nc; c++)
+            if (p->step[c] > 0.0) sums[4 + c] += Lw * adj.tc[c] / p->step[c];
+    }
+    free(phase); free(dphi); free(xbin); free(sbuf);
+    return 0;
 }
 
 static void walk_one_ref(const or_params* p, int64_t w, or_outputs* out, double* phase, int32_t* ti,

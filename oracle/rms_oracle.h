@@ -111,6 +111,20 @@ int or_run_split_parallel(const or_params* p, int64_t w_begin, int64_t w_end, in
                           or_outputs* out);
 
 /* The project's stream, exposed for known-answer tests. */
+/* The adjoint of the split walk in waveform mode (reflecting membranes), FP64:
+ * per walker the tangent of the displacement with respect to the step length
+ * with the event sequence frozen, the permeation score, the path per
+ * compartment and the bin displacement sums, folded with the upstream weights
+ * gup[2*nwave] (gC_j, gS_j) into walker sums:
+ *   sums[0] = sum L_w, sums[1] = sum L_w E_w, sums[2] = sum_w sum_j a_jw dphi_jw,
+ *   sums[3] = sum E_w, sums[4+c] = sum L_w t_wc / step_c (c < nc),
+ *   sums[4+nc+2j], [4+nc+2j+1] = sum s0 cos phi_j, sum s0 sin phi_j;
+ *   dwave[(b*nwave + j)*3 + k] += sum a_jw X_wbk (um).
+ * The same sums as the GPU adjoint kernel (csrc/rms_adjoint.cu); the caller
+ * zeroes them.  Returns -6 for other modes or rules. */
+int or_adjoint_split(const or_params* p, const double* gup, int64_t w_begin, int64_t w_end, double* sums,
+                     double* dwave);
+
 void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void or_stream_doubles(uint64_t seed, uint64_t walker, int n, double* out);
 void or_stream_floats(uint64_t seed, uint64_t walker, int n, float* out);
