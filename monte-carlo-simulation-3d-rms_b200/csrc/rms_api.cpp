@@ -8,7 +8,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -723,15 +726,48 @@ int finish_launch(std::vector<LaunchJob>& jobs, LaunchPlan& p, bool events) {
     return RMS_OK;
 }
 
+// RMS_TRACE set (and not "0"): every launch prints one line to stderr with its
+// phases -- plan (validation, shape, uploads), enqueue, finish (wait, error
+// word, unpack) on the host clock, and the walk / walk+reduce kernel times the
+// launch's events measured.  Read once per process.
+bool trace_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("RMS_TRACE");
+        return v && *v && std::strcmp(v, "0") != 0;
+    }();
+    return on;
+}
+
 int run_launch(std::vector<LaunchJob>& jobs, const rms_run_opts* o) {
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     LaunchPlan p;
     int rc = plan_launch(jobs, o, p);
     if (rc) return rc;
     if (p.prec == RMS_PREC_SPLIT)
         std::memcpy(p.d->h_axons.p, p.axons.data(), sizeof(AxonDesc) * p.naxons);
+    const auto t1 = clk::now();
     rc = enqueue_launch(p, jobs[0].s, true);
     if (rc) return rc;
-    return finish_launch(jobs, p, true);
+    const auto t2 = clk::now();
+    rc = finish_launch(jobs, p, true);
+    if (rc == RMS_OK && trace_enabled()) {
+        const auto t3 = clk::now();
+        auto ms = [](clk::time_point a, clk::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        std::fprintf(stderr,
+                     "rms trace: %s %d sim(s) %lld walker-steps: plan %.3f ms, enqueue %.3f ms, finish %.3f ms; "
+                     "kernels: walk %.3f ms, walk+reduce %.3f ms; grid %d x %d\n",
+                     p.prec == RMS_PREC_SPLIT ? "split" : "compat", p.naxons,
+                     (long long)[&] {
+                         long long n = 0;
+                         for (const LaunchJob& j : jobs) n += (long long)(j.w1 - j.w0) * j.s->tn;
+                         return n;
+                     }(),
+                     ms(t0, t1), ms(t1, t2), ms(t2, t3), jobs[0].s->walk_ms, jobs[0].s->run_ms, p.grid, p.block);
+    }
+    return rc;
 }
 
 }  // namespace
