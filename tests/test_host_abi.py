@@ -74,6 +74,12 @@ def test_pij_table_is_used_as_given():
     (dict(diffusivity=[0, 2.0, 300.0]), -4),         # step >= one voxel
     (dict(dt=-1.0), -4),
     (dict(diffusivity=[0] + [1.0] * 9, t2=[80] * 10), -4),   # Nc above the kernels' limit
+    # NaN parameters (the reference would walk with them)
+    (dict(dt=float("nan")), -4),
+    (dict(res=float("nan")), -4),
+    (dict(t2=[80, float("nan"), 40]), -4),
+    (dict(diffusivity=[0, float("nan"), 1.0]), -4),
+    (dict(permeation="kappa", kappa=float("nan")), -4),
 ])
 def test_invalid_configurations_are_rejected(over, code):
     with pytest.raises(engine.RmsError) as e:
@@ -166,6 +172,25 @@ def test_load_dir_errors(tmp_path):
     with pytest.raises(engine.RmsError) as e:
         engine.Sim.from_dir(d, mode="pgse")
     assert e.value.code == -3
+
+
+@pytest.mark.parametrize("fn,content,code", [
+    ("diffusivity.txt", "0 abc 1.0", -3),        # a token that is not a number
+    ("T2.txt", "80 nan 40", -3),
+    ("bval.txt", "1 2 x 4 5 6", -3),
+    ("fiber.txt", "junk", -3),
+    ("simParamInput.txt", None, -4),             # NPar = -5
+])
+def test_corrupt_input_files_are_rejected(tmp_path, fn, content, code):
+    d = unpack_golden("narrow_3comp", str(tmp_path), inputs_only=True)
+    if content is None:
+        vals = open(os.path.join(d, fn)).read().split()
+        vals[2] = "-5"
+        content = " ".join(vals)
+    open(os.path.join(d, fn), "w").write(content)
+    with pytest.raises(engine.RmsError) as e:
+        engine.Sim.from_dir(d)
+    assert e.value.code == code, str(e.value)
 
 
 def test_run_without_gpu_fails_loudly():
