@@ -34,12 +34,28 @@ def write_lattice(path: str, labels: np.ndarray) -> None:
     newline (setupRMS.m:17-23); the reader takes NPix1*NPix2*NPix3 integers
     in that order (main.cu:461-466)."""
     lab = np.ascontiguousarray(labels, dtype=np.uint8).reshape(-1)
-    digits = np.char.mod("%u ", lab)
-    with open(path, "w") as f:
-        # chunked join keeps memory bounded for 1e8-voxel lattices
-        step = 1 << 22
+    with open(path, "wb") as f:
+        # the bytes are assembled from digit arrays, 16 M voxels at a time
+        step = 1 << 24
         for s in range(0, lab.size, step):
-            f.write("".join(digits[s:s + step].tolist()))
+            f.write(_label_text(lab[s:s + step]))
+
+
+def _label_text(v: np.ndarray) -> bytes:
+    """ASCII of "%u " for each uint8 in v, concatenated."""
+    v = v.astype(np.int32)
+    nd = 1 + (v >= 10) + (v >= 100)          # digits per label
+    end = np.cumsum(nd + 1)                  # one past each label's space
+    out = np.empty(int(end[-1]) if v.size else 0, dtype=np.uint8)
+    if not v.size:
+        return b""
+    out[end - 1] = ord(" ")
+    out[end - 2] = ord("0") + v % 10
+    m = nd >= 2
+    out[end[m] - 3] = ord("0") + (v[m] // 10) % 10
+    m = nd == 3
+    out[end[m] - 4] = ord("0") + v[m] // 100
+    return out.tobytes()
 
 
 def write_lattice_binary(path: str, labels: np.ndarray) -> None:

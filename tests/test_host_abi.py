@@ -279,3 +279,19 @@ def test_reference_mat_files_are_read(tmp_path):
     s = engine.Sim(got[0][0], dt=2e-4, tn=1000, npar=4, res=got[0][1], diffusivity=[0, 2.0, 1.0],
                    t2=[80, 80, 40], bval=bval, bvec=bv)
     np.testing.assert_array_equal(s.get("bval"), bval)
+
+
+def test_lattice_text_writer_matches_the_reference_format(tmp_path):
+    # setupRMS.m:17-23 writes sprintf('%u ', ...) per label, i outer, k fastest
+    import gzip
+    from rms_b200 import runio
+    v = np.arange(256, dtype=np.uint8)
+    lab = np.concatenate([v, np.random.default_rng(5).integers(0, 256, size=4096 - 256)]).astype(np.uint8)
+    runio.write_lattice(str(tmp_path / "f.txt"), lab.reshape(16, 16, 16))
+    assert open(tmp_path / "f.txt", "rb").read() == "".join("%u " % x for x in lab).encode()
+    # the golden run directories' fiber.txt, which the reference program read
+    want = gzip.open(os.path.join(os.path.dirname(__file__), "golden", "narrow_3comp", "fiber.txt.gz")).read()
+    runio.write_lattice(str(tmp_path / "g.txt"), np.array(want.split(), dtype=np.uint8).reshape(-1, 1, 1))
+    assert open(tmp_path / "g.txt", "rb").read() == want
+    runio.write_lattice(str(tmp_path / "e.txt"), np.zeros((0, 1, 1), dtype=np.uint8))
+    assert open(tmp_path / "e.txt", "rb").read() == b""
