@@ -468,6 +468,12 @@ class Graph:
         _check(lib().rms_batch_graph_create(arr, len(sims), C.byref(opts), C.byref(self._h)))
 
     def run(self, seed: int):
+        # the captured launch refers to its simulations: a closed one (or a
+        # closed graph) would leave it pointing at freed memory
+        if not (self._h and self._h.value):
+            raise RmsError(-7, "the graph is closed")
+        if any(not (s._h and s._h.value) for s in self.sims):
+            raise RmsError(-7, "a simulation of the graph was closed: create the graph again")
         _check(lib().rms_graph_run(self._h, int(seed) & ((1 << 64) - 1)))
 
     def close(self):

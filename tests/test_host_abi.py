@@ -295,3 +295,21 @@ def test_lattice_text_writer_matches_the_reference_format(tmp_path):
     assert open(tmp_path / "g.txt", "rb").read() == want
     runio.write_lattice(str(tmp_path / "e.txt"), np.zeros((0, 1, 1), dtype=np.uint8))
     assert open(tmp_path / "e.txt", "rb").read() == b""
+
+
+def test_graph_refuses_closed_simulations():
+    # Graph.run checks its simulations before the library sees the graph
+    # (a stand-in graph object: capturing one needs a GPU)
+    s = small_sim()
+    g = engine.Graph.__new__(engine.Graph)
+    g._h = engine.C.c_void_p(1)          # never reaches the library
+    g.sims = [s]
+    s.close()
+    try:
+        with pytest.raises(engine.RmsError) as e:
+            g.run(1)
+        assert e.value.code == -7
+    finally:
+        g._h = engine.C.c_void_p()
+    with pytest.raises(engine.RmsError):
+        g.run(1)
