@@ -69,7 +69,7 @@ struct WalkArgs {
     const float* t2invf;        // [nc] 1 / (T2 in steps)
     const float* pijf;          // [nc*nc]
     int* err;                   // device error word (kErr* bits), zeroed per run
-    unsigned long long* tile_ctr;   // multi-axon launches: next tile to hand out, zeroed per run
+    unsigned long long* tile_ctr;   // table-form launches: next tile to hand out, zeroed per run
     int table_form;             // walk even one axon from the axon table (what a graph replay rewrites)
     // split launches: the axons and their tiles; with several axons each warp
     // adds its rows into out_rows[axon][timepoints][nvals] / out_sig[axon][ngrad_pad]

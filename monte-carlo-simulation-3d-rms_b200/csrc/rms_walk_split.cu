@@ -30,8 +30,8 @@
 //  - per-walker sums that grow over the walk (T2 exponent, PGSE displacement
 //    sums) are carried in FP32 for at most 32 steps and folded into FP64;
 //  - cross-walker sums: FP32 products per walker, warp reduce-scatter in
-//    FP64, per-warp FP64 rows, then an ordered FP64 reduction (rms_reduce.cu)
-//    for one axon, or FP64 atomic adds into each axon's totals for several.
+//    FP64, per-warp FP64 rows, added into each axon's totals with FP64 atomics
+//    (the no-allocation walk: an ordered FP64 reduction, rms_reduce.cu).
 //
 // Mirror walls: the reference mirrors the origin image at the end of a step
 // for each wall the step touched (main.cu:302-310).  A step shorter than a
@@ -133,8 +133,8 @@ __device__ __noinline__ void wave_final(const double* ph, int nthr, int nwave, d
     }
 }
 
-// ONE: the launch has one axon, whose scalars are read from the kernel
-// parameters (a.axon0) instead of being held in registers.
+// ONE: the no-allocation walk's form -- one axon, whose scalars are read from
+// the kernel parameters (a.axon0); every other launch reads the axon table.
 template <int NCMAX, int BITS, int BLOCK, int MINB, bool ONE, int RULE = 0, int MODE = 0>
 __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs a) {
     // per warp, the current axon's tables: step (voxels), T2 exponent per voxel
@@ -155,26 +155,25 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     const bool mirror = (a.boundary == 0);
     constexpr int kWall = wall_code<BITS>();
 
-    // Tiles are walked in strided order (warp w: tiles w, w + nwarps, ...), so at
-    // any moment the grid works on one narrow window of the tile list -- one or
-    // two axons, whose lattices then share the L2.  A one-axon launch keeps
-    // one accumulator row set per warp, summed in order afterwards.  A
-    // multi-axon launch keeps the warp's rows for its current axon and adds
-    // them into that axon's totals (FP64 atomics) when the warp moves on.
+    // A warp keeps its rows for its current axon and, in the table form, adds
+    // them into that axon's totals (FP64 atomics) when it moves on to another
+    // axon or finishes.  ONE (the no-allocation walk) keeps one row set per
+    // warp, summed in order afterwards.
     int ax = 0;          // current axon
     int held = -1;       // axon whose records the warp's rows hold
     int64_t next_tb = ONE ? INT64_MAX : ((a.naxons > 1) ? a.axons[1].tile_begin : INT64_MAX);
-    // a field of the current axon: kernel parameters for a one-axon launch,
-    // else the axon table (read where used, so it holds no registers)
+    // a field of the current axon: kernel parameters for ONE, else the axon
+    // table (read where used, so it holds no registers)
 #define AXF(f) (ONE ? a.axon0.f : a.axons[ax].f)
     double* slot = a.slots + (size_t)warp_global * a.timepoints * a.nvals;
     double* sig_slot = sums ? a.sig_slots + (size_t)warp_global * a.ngrad_pad : nullptr;
 
-    // One axon: tiles in strided order (warp w: w, w + nwarps, ...), so each
-    // warp's rows, reduced in a fixed order, are the same every run.  Several
-    // axons: a queue (one counter per launch) hands out tiles in order, so the
-    // tiles in flight stay one narrow window of the list -- one or two axons,
-    // whose lattices then share the L2 -- however far warps drift apart.
+    // The table form (every SPLIT launch but the no-allocation walk, one axon
+    // or many): a queue (one counter per launch) hands out tiles in order, so
+    // the tiles in flight stay one narrow window of the list -- one or two
+    // axons, whose lattices then share the L2 -- however far warps drift
+    // apart.  ONE: tiles in strided order (warp w: w, w + nwarps, ...), so each
+    // warp's rows, reduced in a fixed order, are the same every run.
     auto claim = [&]() -> int64_t {
         unsigned long long t = 0;
         if (lane == 0) t = atomicAdd(a.tile_ctr, 1ull);
