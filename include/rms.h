@@ -163,6 +163,8 @@ typedef struct rms_sim rms_sim;
 #define RMS_FIELD_BVEC 12       /* [nbvec*3]      bvec.txt rows (narrow pulses; main.cu:477-482) */
 #define RMS_FIELD_GRAD 13       /* [ngrad*6]      gradient_time.txt rows: Delta delta |g| gx gy gz
                                                    (PGSE; main_PGSE.cu:501-506) */
+#define RMS_FIELD_SIM_PARA 14   /* [4]            sim_para.txt: dt (ms), TN, NPar, voxel size (um)
+                                                   (main.cu:606-609), available without a run */
 
 /* Build a simulation from a configuration (what main.cu:414-487 derives from
  * the text inputs).  Replaces: the input parsing + table set-up of

@@ -1066,6 +1066,7 @@ bool field_size(const rms_sim* s, int field, size_t& n) {
         case RMS_FIELD_BVAL: n = s->mode == RMS_MODE_NARROW ? (size_t)s->nbvec() : 0; return true;
         case RMS_FIELD_BVEC: n = s->mode == RMS_MODE_NARROW ? (size_t)3 * s->nbvec() : 0; return true;
         case RMS_FIELD_GRAD: n = s->mode == RMS_MODE_PGSE ? (size_t)6 * s->ngrad() : 0; return true;
+        case RMS_FIELD_SIM_PARA: n = 4; return true;
         default: return false;
     }
 }
@@ -1375,6 +1376,13 @@ int rms_sim_get(const rms_sim* s, int field, double* out, size_t n) {
     if (field == RMS_FIELD_BVAL) table = &s->bval;
     if (field == RMS_FIELD_BVEC) table = &s->bvec;
     if (field == RMS_FIELD_GRAD) table = &s->grad;
+    if (field == RMS_FIELD_SIM_PARA) {
+        out[0] = s->dt;
+        out[1] = (double)s->tn;
+        out[2] = (double)s->npar;
+        out[3] = s->res;
+        return RMS_OK;
+    }
     if (table) {
         std::copy(table->begin(), table->begin() + want, out);
         return RMS_OK;

@@ -7,7 +7,10 @@
 // reference's spelling, which analysis/read_slurm_cuda.m:9-11 parses).
 //
 //   rms_main [--dir D] [--pgse|--narrow] [--seed S] [--precision compat|split]
-//            [--device N]
+//            [--device N] [--metrics]
+// --metrics adds one JSON line on stderr after the run: walker-steps, the
+// walk and run kernel times (CUDA events), the wall time of the run call and
+// the walker-steps/s of each (stdout stays the reference's lines).
 // The mode defaults to PGSE when gradient_time.txt exists.  The seed defaults
 // to 8 bytes of /dev/urandom, like the reference's /dev/random read
 // (main.cu:492-496).
@@ -30,6 +33,7 @@ int main(int argc, char** argv) {
     std::string dir = ".";
     int mode = RMS_MODE_AUTO;
     bool have_seed = false;
+    bool metrics = false;
     unsigned long long seed = 0;
     rms_run_opts opts{};
     opts.precision = RMS_PREC_COMPAT;
@@ -44,6 +48,7 @@ int main(int argc, char** argv) {
         else if (a == "--narrow") mode = RMS_MODE_NARROW;
         else if (a == "--seed") { seed = std::strtoull(next("--seed"), nullptr, 0); have_seed = true; }
         else if (a == "--device") opts.device = std::atoi(next("--device"));
+        else if (a == "--metrics") metrics = true;
         else if (a == "--precision") {
             std::string p = next("--precision");
             if (p == "compat") opts.precision = RMS_PREC_COMPAT;
@@ -51,7 +56,7 @@ int main(int argc, char** argv) {
             else { std::fprintf(stderr, "rms_main: unknown precision %s\n", p.c_str()); return 2; }
         } else {
             std::fprintf(stderr, "usage: rms_main [--dir D] [--pgse|--narrow] [--seed S] "
-                                 "[--precision compat|split] [--device N]\n");
+                                 "[--precision compat|split] [--device N] [--metrics]\n");
             return 2;
         }
     }
@@ -79,6 +84,18 @@ int main(int argc, char** argv) {
     rms_sim_last_timing(sim, &walk_ms, &run_ms);
     const long secs = (long)std::chrono::duration<double>(t1 - t0).count();
     std::cout << "Done! Elpased time " << double(secs) << " s" << std::endl;   // main.cu:540
+    if (metrics) {
+        double para[4] = {0, 0, 0, 0};      // dt, TN, NPar, res
+        rms_sim_get(sim, RMS_FIELD_SIM_PARA, para, 4);
+        const double steps = para[1] * para[2];
+        const double wall_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        std::fprintf(stderr,
+                     "{\"walker_steps\": %.0f, \"precision\": \"%s\", \"seed\": %llu, \"walk_ms\": %.3f, "
+                     "\"run_ms\": %.3f, \"wall_ms\": %.3f, \"walker_steps_per_s_walk\": %.6g, "
+                     "\"walker_steps_per_s_wall\": %.6g}\n",
+                     steps, opts.precision == RMS_PREC_SPLIT ? "split" : "compat", seed, walk_ms, run_ms, wall_ms,
+                     walk_ms > 0 ? steps / (walk_ms * 1e-3) : 0.0, wall_ms > 0 ? steps / (wall_ms * 1e-3) : 0.0);
+    }
     if (rms_sim_write_dir(sim, dir.c_str()) != RMS_OK) { rms_sim_destroy(sim); return fail("writing outputs"); }
     rms_sim_destroy(sim);
     return 0;

@@ -21,7 +21,8 @@ BOUNDARY = {"mirror": 0, "periodic": 1}
 PERMEATION = {"reference": 0, "kappa": 1, "table": 2}
 PRECISION = {"compat": 0, "split": 1}
 FIELD = {"sig0": 0, "dx2": 1, "dx4": 2, "sigre": 3, "sig": 4, "npar_count": 5, "td": 6,
-         "diffusivity": 7, "step": 8, "pij": 9, "sigw": 10, "bval": 11, "bvec": 12, "grad": 13}
+         "diffusivity": 7, "step": 8, "pij": 9, "sigw": 10, "bval": 11, "bvec": 12, "grad": 13,
+         "sim_para": 14}
 ERRORS = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "RANGE", -5: "CUDA", -6: "NOMEM",
           -7: "STATE", -8: "TIMEOUT"}
 

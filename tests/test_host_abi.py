@@ -313,3 +313,13 @@ def test_graph_refuses_closed_simulations():
         g._h = engine.C.c_void_p()
     with pytest.raises(engine.RmsError):
         g.run(1)
+
+
+def test_sim_para_field_and_cli_flags():
+    # sim_para.txt's values without a run (main.cu:606-609)
+    s = small_sim()
+    np.testing.assert_array_equal(s.get("sim_para"), [2e-4, 1000, 32, 0.1])
+    # the CLI knows --metrics; without a GPU it still fails loudly, after parsing
+    import subprocess
+    r = subprocess.run([engine.CLI_PATH, "--metrics", "--bogus"], capture_output=True, text=True)
+    assert r.returncode == 2 and "--metrics" in r.stderr
