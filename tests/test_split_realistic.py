@@ -74,3 +74,28 @@ def test_compartments_and_relaxation_agree(walks):
     assert np.all(np.abs(fr - vol) < 5 * sd) and np.all(np.abs(fs - vol) < 5 * sd)
     # T2-weighted signal (T2 = 20 ms in the mitochondria)
     np.testing.assert_allclose(spl["sig0"] / N, ref["sig0"] / N, rtol=5e-3)
+
+
+def test_pgse_signal_on_the_undulating_axon():
+    """The PGSE signal of the split walk's replay against the reference walk on
+    the reference's first undulating axon (tests/golden/realistic_undulation_pgse),
+    b = 1 ms/um^2 (Delta 0.3 ms, delta 0.1 ms) along, across and oblique to the
+    axon: S ~ 0.21 along it, 0.93-0.96 across.  Per walker Var(cos phi) <= 1/2,
+    so a difference of two 32768-walker walks has sigma <= 0.0055; the bar is
+    0.025 (two seed pairs differed by 0.009 and 0.003)."""
+    import tempfile
+    d = unpack_golden("realistic_undulation_pgse", tempfile.mkdtemp(), inputs_only=True)
+    lab = np.array(open(os.path.join(d, "fiber.txt")).read().split(), dtype=np.uint8).reshape(100, 100, 180)
+    D, T2, tn = [0.0, 2.0, 2.0], [80.0, 80.0, 80.0], 2000
+    step, t2s, pij, td = pyoracle.reference_tables(2e-4, 0.1, D, T2, 100, tn)
+    dirs = np.array([[0, 0, 1], [1, 0, 0], [0, 1, 0], [0.48, 0.6, 0.64], [0.6, 0, 0.8], [0, 0.6, 0.8]])
+    g = float(analysis.pgse_gradient_for_b(1.0, 0.3, 0.1))
+    grad = np.column_stack([np.full(6, 0.3), np.full(6, 0.1), np.full(6, g), dirs])
+    threads = max(1, min(16, os.cpu_count() or 1))
+    sig = {}
+    for name, split, seed in (("reference", False, 1), ("split", True, 2)):
+        job = pyoracle.Job(lab, dt=2e-4, tn=tn, npar=N, res=0.1, step=step, t2_steps=t2s, pij=pij, seed=seed,
+                           timepoints=100, td=td, grad=grad)
+        sig[name] = pyoracle.run_oracle(job, nthreads=threads, split=split)["sig"] / N
+    np.testing.assert_allclose(sig["split"], sig["reference"], atol=0.025)
+    assert sig["reference"][0] < 0.3 and sig["reference"][1] > 0.9      # along vs across the axon
