@@ -477,8 +477,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
     if isinstance(lab, list):
-        if world > 1:
-            sim_kw = [dict(kw, npar=kw["npar"] // world) for kw in sim_kw]
+        # weak scaling: every rank walks the whole batch, on its own seeds
         job = BatchJob(lab, sim_kw, rank, local, sh)
     else:
         job = SingleJob(lab, sim_kw, per_gpu, rank, local, sh)
