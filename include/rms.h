@@ -140,6 +140,15 @@ typedef struct rms_run_opts {
                                   walker_begin), then n*nbins*3 lo parts -- the
                                   same bytes as the FP32 form; the input of
                                   RMS_CONTRACT_BF16X3_PRESPLIT */
+    int shard_index;           /* shard_count > 1: every simulation of the call */
+    int shard_count;           /* walks only its walkers [npar*shard_index/shard_count,
+                                  npar*(shard_index+1)/shard_count): one rank's part
+                                  of a job or of a batch.  Walker ids, and so the
+                                  random streams, are the whole job's, so the
+                                  shards' sums add up to the unsharded result.  A
+                                  shard may be empty (npar < shard_count): its
+                                  results are zero.  0 or 1 = all walkers; not
+                                  combined with walker_begin/walker_end. */
 } rms_run_opts;
 
 typedef struct rms_sim rms_sim;
@@ -336,7 +345,10 @@ int rms_split_variant(int k, int* block, int* min_blocks_per_sm);
  * must not hit cudaMalloc/cudaFree because they synchronise the whole device.
  * Runs the SPLIT walk of `sim` (its configuration and tables; the sim itself is
  * not changed) on device buffers the caller owns:
- *   d_labels  [n1*n2*n3] uint8 lattice, n3 fastest, labels < nc (nc <= 7)
+ *   d_labels  [n1*n2*n3] uint8 lattice, n3 fastest, labels < nc (nc <= 7);
+ *             checked on the device before the walk, as rms_sim_set_lattice
+ *             checks a host lattice (RMS_ERR_RANGE: a label >= nc, or fewer
+ *             than 1e-7 of the voxels labelled)
  *   d_rows    [timepoints * W] doubles, W = 32 (PGSE) or 32 + 32*ceil(nbvec/32)
  *             (narrow); row t holds sig0 at column 0, dx2 at 1-6, dx4 at 7-21,
  *             compartment counts at 22.., sigRe at 32..

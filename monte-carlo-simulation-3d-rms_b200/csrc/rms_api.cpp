@@ -176,6 +176,52 @@ void build_pgse_schedule(rms_sim* s) {
 
 }  // namespace
 
+// Walkers [w0, w1) of simulation s that a call asks for: an explicit range
+// (walker_begin/walker_end), shard shard_index of shard_count, or all of them.
+// Only a shard may be empty (a job with fewer walkers than shards).
+int walker_range(const rms_sim* s, const rms_run_opts* o, int64_t& w0, int64_t& w1) {
+    w0 = o ? o->walker_begin : 0;
+    w1 = o ? o->walker_end : 0;
+    const int nsh = o ? o->shard_count : 0;
+    if (nsh > 1) {
+        if (w0 != 0 || w1 != 0) return set_error(RMS_ERR_ARG, "give a walker range or a shard, not both");
+        const int r = o->shard_index;
+        if (r < 0 || r >= nsh) return set_error(RMS_ERR_ARG, "shard_index outside [0, shard_count)");
+        w0 = (int64_t)((__int128)s->npar * r / nsh);
+        w1 = (int64_t)((__int128)s->npar * (r + 1) / nsh);
+        return RMS_OK;
+    }
+    if (nsh < 0 || (o && (o->shard_index < 0 || (nsh <= 1 && o->shard_index > 0))))
+        return set_error(RMS_ERR_ARG, "shard_index outside [0, shard_count)");
+    if (w0 == 0 && w1 == 0) w1 = s->npar;
+    if (w0 < 0 || w1 > s->npar || w0 >= w1) return set_error(RMS_ERR_ARG, "walker range outside [0, NPar)");
+    return RMS_OK;
+}
+
+// Results of a simulation that walked no walkers (an empty shard): zeros in
+// the shapes a run leaves.
+void zero_results(rms_sim* s) {
+    const int T = s->timepoints, nb = s->nbvec();
+    s->sig0.assign(T, 0.0);
+    s->dx2.assign((size_t)T * 6, 0.0);
+    s->dx4.assign((size_t)T * 15, 0.0);
+    s->npar_count.assign((size_t)T * s->nc, 0.0);
+    s->sigre.assign((size_t)T * nb, 0.0);
+    s->sig.assign(s->mode == RMS_MODE_PGSE ? s->ngrad() : 0, 0.0);
+    s->sigw.assign(s->mode == RMS_MODE_WAVEFORM ? 2 * s->nwave : 0, 0.0);
+    s->trace_n = 0;
+    s->walk_ms = s->run_ms = 0.0;
+    s->have_results = true;
+}
+
+// The walkers a batch call walks in simulation s: all of them, or the call's
+// shard (a batch ignores walker_begin/walker_end).
+int batch_range(const rms_sim* s, const rms_run_opts* o, int64_t& w0, int64_t& w1) {
+    rms_run_opts x = o ? *o : rms_run_opts{};
+    x.walker_begin = x.walker_end = 0;
+    return walker_range(s, &x, w0, w1);
+}
+
 void fill_axon_desc(AxonDesc& x, const rms_sim* s, int64_t w0, int64_t w1, int64_t tile_begin, uint64_t seed,
                     const uint8_t* lat) {
     std::memset(&x, 0, sizeof x);
@@ -806,7 +852,12 @@ int graph_create(rms_sim* const* sims, int n, const rms_run_opts* o, rms_graph**
     if (o->trace_walkers > 0 || o->traj_out) return set_error(RMS_ERR_ARG, "a graph records no traces or trajectories");
     std::unique_ptr<rms_graph> g(new rms_graph());
     g->device = o->device;
-    for (int i = 0; i < n; ++i) g->jobs.push_back(LaunchJob{sims[i], 0, sims[i]->npar, o->seed + (uint64_t)i * kBatchSeedStep});
+    for (int i = 0; i < n; ++i) {
+        int64_t w0 = 0, w1 = 0;
+        int rc = batch_range(sims[i], o, w0, w1);
+        if (rc) return rc;
+        g->jobs.push_back(LaunchJob{sims[i], w0, w1, o->seed + (uint64_t)i * kBatchSeedStep});
+    }
     rms_run_opts oo = *o;
     int rc = plan_launch(g->jobs, &oo, g->plan);
     if (rc) return rc;
@@ -865,10 +916,13 @@ int autotune(rms_sim* const* sims, int n, const rms_run_opts* opts, int* variant
     int nc_max = 0;
     double vox = 0.0;
     int64_t total = 0;
+    std::vector<int64_t> r0(n), r1(n);
     for (int i = 0; i < n; ++i) {
+        int rc = batch_range(sims[i], opts, r0[i], r1[i]);
+        if (rc) return rc;
         nc_max = std::max(nc_max, sims[i]->nc);
         vox += (double)sims[i]->n1 * sims[i]->n2 * sims[i]->n3;
-        total += sims[i]->npar;
+        total += r1[i] - r0[i];
     }
     const TuneKey key{device, split_lattice_bits(nc_max), nc_max, n, (int)std::log2(std::max(vox, 1.0)),
                       (int)std::log2((double)std::max(sims[0]->tn, 1)), sims[0]->mode};
@@ -891,8 +945,9 @@ int autotune(rms_sim* const* sims, int n, const rms_run_opts* opts, int* variant
     std::vector<LaunchJob> jobs;
     const uint64_t seed = opts ? opts->seed : 0;
     for (int i = 0; i < n; ++i) {
-        const int64_t m = std::max<int64_t>(std::min<int64_t>(32, sims[i]->npar), (int64_t)std::ceil(f * sims[i]->npar));
-        jobs.push_back(LaunchJob{sims[i], 0, std::min<int64_t>(m, sims[i]->npar), seed + (uint64_t)i * kBatchSeedStep});
+        const int64_t ni = r1[i] - r0[i];
+        const int64_t m = std::max<int64_t>(std::min<int64_t>(32, ni), (int64_t)std::ceil(f * ni));
+        jobs.push_back(LaunchJob{sims[i], r0[i], r0[i] + std::min<int64_t>(m, ni), seed + (uint64_t)i * kBatchSeedStep});
     }
     rms_run_opts o = opts ? *opts : rms_run_opts{};
     o.precision = RMS_PREC_SPLIT;
@@ -923,9 +978,14 @@ int autotune(rms_sim* const* sims, int n, const rms_run_opts* opts, int* variant
 }
 
 int run_one(rms_sim* s, const rms_run_opts* o) {
-    int64_t w0 = o ? o->walker_begin : 0, w1 = o ? o->walker_end : 0;
-    if (w0 == 0 && w1 == 0) w1 = s->npar;
-    if (w0 < 0 || w1 > s->npar || w0 >= w1) return set_error(RMS_ERR_ARG, "walker range outside [0, NPar)");
+    int64_t w0 = 0, w1 = 0;
+    int rc = walker_range(s, o, w0, w1);
+    if (rc) return rc;
+    if (w0 == w1) {
+        // an empty shard: nothing to walk, zero results
+        zero_results(s);
+        return RMS_OK;
+    }
     std::vector<LaunchJob> jobs{LaunchJob{s, w0, w1, o ? o->seed : 0}};
     return run_launch(jobs, o);
 }
@@ -945,9 +1005,10 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
             return set_error(RMS_ERR_ARG, "the adjoint needs one diffusivity for all labelled compartments");
     }
     if (!(D > 0.0)) return set_error(RMS_ERR_ARG, "the adjoint needs a positive diffusivity");
-    int64_t w0 = o ? o->walker_begin : 0, w1 = o ? o->walker_end : 0;
-    if (w0 == 0 && w1 == 0) w1 = s->npar;
-    if (w0 < 0 || w1 > s->npar || w0 >= w1) return set_error(RMS_ERR_ARG, "walker range outside [0, NPar)");
+    int64_t w0 = 0, w1 = 0;
+    int rc0 = walker_range(s, o, w0, w1);
+    if (rc0) return rc0;
+    if (w0 == w1) return set_error(RMS_ERR_ARG, "the adjoint's shard holds no walkers");
     const int device = o ? o->device : 0;
     int rc = ensure_device(s, device);
     if (rc) return rc;
@@ -1332,8 +1393,12 @@ int rms_batch_run(rms_sim* const* sims, int n, const rms_run_opts* opts) {
         if (prec == RMS_PREC_SPLIT) {
             // one persistent launch over all simulations
             std::vector<LaunchJob> jobs;
-            for (int i = 0; i < n; ++i)
-                jobs.push_back(LaunchJob{sims[i], 0, sims[i]->npar, seed + (uint64_t)i * kBatchSeedStep});
+            for (int i = 0; i < n; ++i) {
+                int64_t w0 = 0, w1 = 0;
+                int rc = batch_range(sims[i], opts, w0, w1);
+                if (rc) return rc;
+                jobs.push_back(LaunchJob{sims[i], w0, w1, seed + (uint64_t)i * kBatchSeedStep});
+            }
             return run_launch(jobs, opts);
         }
         for (int i = 0; i < n; ++i) {

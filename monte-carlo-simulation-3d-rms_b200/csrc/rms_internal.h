@@ -107,8 +107,8 @@ bool split_variant_walks(int variant, int mode, int rule);   // variants past th
 int split_variant_block(int variant);   // threads per block of a launch variant
 int split_variant_minb(int variant);    // its minimum resident blocks per SM
 // The split walk's lattice: (n1+2) x (n2+2) x (n3+2) with a wall-code border;
-// 4 bits per voxel (3-bit label + free-flight flag) when Nc <= 7, else one
-// byte; 2 bits (labels only, Nc <= 3) for the no-allocation walk.
+// 4 bits per voxel (3-bit label + free-flight flag) when Nc <= 7 (every split
+// walk, the no-allocation one included), else one byte.
 int split_lattice_bits(int nc);
 size_t padded_lattice_bytes(int n1, int n2, int n3, int bits);
 int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits, uint8_t* out, void* stream);

@@ -20,7 +20,9 @@
 // reads the same padded, packed lattice as rms_sim_run (4 bits per voxel with
 // the free-flight flags, Nc <= 7), built in the scratch too: 68 MB for
 // 256x256x2048.  Same lattice, same kernel, same walkers: the results equal
-// rms_sim_run's up to the order of the final sums.
+// rms_sim_run's up to the order of the final sums.  The caller's lattice is
+// checked on the device first (labels below Nc, enough labelled voxels), as
+// rms_sim_set_lattice checks a host lattice.
 //
 // Host code cannot use the array's name as a device address (in host code it
 // names a host-side stand-in).  The first call on each device, with that
@@ -32,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
 #include <sstream>
 
@@ -45,6 +48,8 @@ namespace {
 constexpr size_t kScratchBytes = RMS_NOALLOC_SCRATCH_BYTES;
 constexpr int kMaxDevices = 64;
 constexpr int kVariant = 0;   // 256 threads, >= 4 resident blocks per SM
+constexpr int kNoallocNc = 7;  // compartments of the 4-bit packed lattice (label 7 is the wall code)
+constexpr int kTabMax = 2 * kNoallocNc + kNoallocNc * kNoallocNc;   // step, T2, Pij
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -80,6 +85,41 @@ struct Carve {
     }
 };
 
+// The caller's device lattice, checked as rms_sim_set_lattice checks a host
+// one: counts[0] = voxels with a label >= nc, counts[1] = labelled voxels.
+// 16-byte loads over the aligned middle, byte loads at the two ends.
+__global__ void check_labels_kernel(const uint8_t* __restrict__ lab, size_t n, unsigned nc,
+                                    unsigned long long* counts) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t nthr = (size_t)gridDim.x * blockDim.x;
+    const size_t mis = (size_t)((16u - ((uintptr_t)lab & 15u)) & 15u);
+    const size_t head = mis < n ? mis : n;
+    const size_t nvec = (n - head) / 16;
+    const unsigned ncr = nc * 0x01010101u;
+    unsigned bad = 0, labelled = 0;
+    auto one = [&](unsigned v) { bad += v >= nc; labelled += v != 0; };
+    if (tid < head) one(lab[tid]);
+    const uint4* vec = reinterpret_cast<const uint4*>(lab + head);
+    for (size_t i = tid; i < nvec; i += nthr) {
+        const uint4 q = __ldg(vec + i);
+        const unsigned w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            bad += __popc(__vcmpgeu4(w[k], ncr)) >> 3;     // 0xff per byte >= nc
+            labelled += 4 - (__popc(__vcmpeq4(w[k], 0u)) >> 3);
+        }
+    }
+    for (size_t i = head + nvec * 16 + tid; i < n; i += nthr) one(lab[i]);
+    for (int o = 16; o > 0; o >>= 1) {
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
+        labelled += __shfl_xor_sync(0xffffffffu, labelled, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (bad) atomicAdd(counts, (unsigned long long)bad);
+        if (labelled) atomicAdd(counts + 1, (unsigned long long)labelled);
+    }
+}
+
 template <class T>
 cudaError_t put(T* dst, const T* src, size_t count, cudaStream_t st) {
     if (!count) return cudaSuccess;
@@ -98,7 +138,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     if (s->rule != RMS_RULE_REFLECT) return set_error(RMS_ERR_ARG, "the no-allocation walk reflects at membranes");
     if (o->traj_out) return set_error(RMS_ERR_ARG, "the no-allocation walk writes no trajectory");
     if (s->mode == RMS_MODE_PGSE && !d_sig) return set_error(RMS_ERR_ARG, "PGSE needs the sig buffer");
-    if (s->nc > 7) return set_error(RMS_ERR_RANGE, "the no-allocation walk supports Nc <= 7");
+    if (s->nc > kNoallocNc) return set_error(RMS_ERR_RANGE, "the no-allocation walk supports Nc <= 7");
     cudaError_t e = cudaSetDevice(o->device);
     if (e != cudaSuccess) return set_error(RMS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     unsigned char* base = nullptr;
@@ -106,9 +146,10 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)o->stream;
 
-    int64_t w0 = o->walker_begin, w1 = o->walker_end;
-    if (w0 == 0 && w1 == 0) w1 = s->npar;
-    if (w0 < 0 || w1 > s->npar || w0 >= w1) return set_error(RMS_ERR_ARG, "walker range outside [0, NPar)");
+    int64_t w0 = 0, w1 = 0;
+    rc = walker_range(s, o, w0, w1);
+    if (rc) return rc;
+    if (w0 == w1) return set_error(RMS_ERR_ARG, "the call's shard holds no walkers");
 
     const int T = s->timepoints, nc = s->nc, nb = s->nbvec(), ngrad = s->ngrad();
     const int nvals = (s->mode == RMS_MODE_NARROW) ? kRowHead + ((nb + 31) / 32) * 32 : kRowHead;
@@ -124,7 +165,8 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
                          align256(sizeof(float) * (2 * nc + nc * nc)) + align256(sizeof(double) * s->qtab.size()) +
                          align256(sizeof(double) * s->bvec.size()) + align256(sizeof(double) * s->grad.size()) +
                          align256(sizeof(int) * s->gpair.size()) + align256(sizeof(int) * s->ev_step.size()) +
-                         align256(sizeof(int) * s->ev_pair.size()) + align256(sizeof(double) * s->ev_coef.size()) + 256;
+                         align256(sizeof(int) * s->ev_pair.size()) + align256(sizeof(double) * s->ev_coef.size()) +
+                         align256(2 * sizeof(unsigned long long)) + 256;
     // per block: its warps' rows, PGSE signal rows and per-thread window sums
     const size_t per_block = (size_t)warps_per_block * row * sizeof(double) +
                              (s->mode == RMS_MODE_PGSE ? (size_t)warps_per_block * ngrad_pad * sizeof(double) +
@@ -151,6 +193,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     uint8_t* d_lat = c.take<uint8_t>(lat_bytes);
     AxonDesc* d_axon = c.take<AxonDesc>(1);
     int* d_err = c.take<int>(1);
+    unsigned long long* d_counts = c.take<unsigned long long>(2);
     double* d_tab = c.take<double>(2 * nc + nc * nc);
     float* d_tabf = c.take<float>(2 * nc + nc * nc);
     double* d_qtab = c.take<double>(s->qtab.size());
@@ -165,9 +208,9 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     double* d_vscr = c.take<double>(s->mode == RMS_MODE_PGSE ? (size_t)s->npairs * 3 * nthr : 1);
     if (c.used > kScratchBytes) return set_error(RMS_ERR_RANGE, "no-allocation scratch overflow");
 
-    // tables (FP32 copies built on the stack: Nc <= 4)
-    double tab[2 * 4 + 16];
-    float tabf[2 * 4 + 16];
+    // tables (FP64 and FP32 copies built on the stack: Nc <= kNoallocNc)
+    double tab[kTabMax];
+    float tabf[kTabMax];
     for (int i = 0; i < nc; ++i) {
         tab[i] = s->step[i];
         tab[nc + i] = s->t2_steps[i];
@@ -198,6 +241,28 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
         (s->mode == RMS_MODE_PGSE &&
          (e = cudaMemsetAsync(d_sigslots, 0, (size_t)nslots * ngrad_pad * sizeof(double), st)) != cudaSuccess))
         return set_error(RMS_ERR_CUDA, std::string("scratch clear: ") + cudaGetErrorString(e));
+
+    // the lattice is the caller's device memory: check it before walking it (a
+    // label >= Nc would index the compartment tables past their Nc entries)
+    const size_t nvox = (size_t)s->n1 * s->n2 * s->n3;
+    unsigned long long hcount[2] = {0, 0};
+    if ((e = cudaMemsetAsync(d_counts, 0, sizeof(hcount), st)) != cudaSuccess)
+        return set_error(RMS_ERR_CUDA, std::string("scratch clear: ") + cudaGetErrorString(e));
+    check_labels_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(4 * dev_sms, (int64_t)(nvox / 4096) + 1)), 256, 0,
+                          st>>>(d_labels, nvox, (unsigned)nc, d_counts);
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hcount, d_counts, sizeof(hcount), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return set_error(RMS_ERR_CUDA, std::string("lattice check: ") + cudaGetErrorString(e));
+    if (hcount[0]) {
+        std::ostringstream m;
+        m << hcount[0] << " voxel(s) of the device lattice carry a label that is not below Nc = " << nc;
+        return set_error(RMS_ERR_RANGE, m.str());
+    }
+    if (hcount[1] == 0) return set_error(RMS_ERR_RANGE, "lattice has no voxel with a non-zero label");
+    if ((double)hcount[1] / (double)nvox < 1e-7)
+        return set_error(RMS_ERR_RANGE, "labelled voxels are below 1e-7 of the lattice; "
+                                        "rejection-sampled initial positions would not finish");
 
     int pe = pack_lattice_padded(d_labels, s->n1, s->n2, s->n3, bits, d_lat, st);
     if (pe) return set_error(RMS_ERR_CUDA, std::string("lattice packing: ") + cudaGetErrorString((cudaError_t)pe));

@@ -66,6 +66,12 @@ struct AxonDesc;
 // describe one simulation as an axon of a split launch (rms_internal.h)
 void fill_axon_desc(AxonDesc& x, const rms_sim* s, int64_t w0, int64_t w1, int64_t tile_begin, uint64_t seed,
                     const uint8_t* lat);
+// walkers [w0, w1) a call asks of s: its walker range, its shard, or all
+// (only a shard can be empty); batch_range ignores the walker range
+int walker_range(const rms_sim* s, const rms_run_opts* o, int64_t& w0, int64_t& w1);
+int batch_range(const rms_sim* s, const rms_run_opts* o, int64_t& w0, int64_t& w1);
+// zero results of a simulation that walked no walkers (an empty shard)
+void zero_results(rms_sim* s);
 // error reporting (thread-local message behind rms_last_error)
 int set_error(int code, const std::string& msg);
 // derive tables and validate a filled-in configuration

@@ -70,7 +70,20 @@ class RunOpts(C.Structure):
         ("stream", C.c_void_p), ("trace_walkers", C.c_int), ("variant", C.c_int),
         ("walker_begin", C.c_int64), ("walker_end", C.c_int64),
         ("traj_out", C.c_void_p), ("traj_split", C.c_int),
+        ("shard_index", C.c_int), ("shard_count", C.c_int),
     ]
+
+
+def _opts(seed=0, precision="split", device=0, stream=None, trace_walkers=0, variant=0, walker_range=None,
+          traj_out=0, traj_split=False, shard=None) -> RunOpts:
+    """rms_run_opts of a call; ``shard`` = (index, count) walks only that
+    shard of every simulation's walkers (one rank's part of a job or batch)."""
+    w0, w1 = walker_range if walker_range is not None else (0, 0)
+    si, sc = shard if shard is not None else (0, 0)
+    st = None if stream is None else C.c_void_p(int(stream))
+    return RunOpts(int(seed) & ((1 << 64) - 1), PRECISION[precision], int(device), st, int(trace_walkers),
+                   int(variant), int(w0), int(w1), C.c_void_p(int(traj_out)) if traj_out else None,
+                   1 if traj_split else 0, int(si), int(sc))
 
 
 class AdjointGrads(C.Structure):
@@ -222,16 +235,14 @@ class Sim:
 
     def run(self, seed: int = 0, precision: str = "compat", device: int = 0, stream=None,
             trace_walkers: int = 0, variant: int = 0, walker_range=None, traj_out: int = 0,
-            traj_split: bool = False):
+            traj_split: bool = False, shard=None):
         """``traj_out``: device address of a float32 [walkers, nbins, 3] buffer
         for the bins' mean displacements (waveform mode, SPLIT); with
         ``traj_split`` the same bytes hold BF16 hi parts then lo parts (the
-        input of contract_phases(method="bf16x3_presplit"))."""
-        w0, w1 = walker_range if walker_range is not None else (0, 0)
-        st = None if stream is None else C.c_void_p(int(stream))
-        opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION[precision], int(device), st,
-                       int(trace_walkers), int(variant), int(w0), int(w1),
-                       C.c_void_p(int(traj_out)) if traj_out else None, 1 if traj_split else 0)
+        input of contract_phases(method="bf16x3_presplit")).  ``shard`` =
+        (index, count): walk only that shard of the walkers."""
+        opts = _opts(seed, precision, device, stream, trace_walkers, variant, walker_range, traj_out, traj_split,
+                     shard)
         _check(lib().rms_sim_run(self._h, C.byref(opts)))
         return self
 
@@ -239,9 +250,7 @@ class Sim:
                     stream=None, walker_range=None):
         """The split walk on caller-owned device buffers (raw device addresses),
         allocating nothing; see rms_sim_run_noalloc in include/rms.h."""
-        w0, w1 = walker_range if walker_range is not None else (0, 0)
-        st = None if stream is None else C.c_void_p(int(stream))
-        opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION["split"], int(device), st, 0, 0, int(w0), int(w1))
+        opts = _opts(seed, "split", device, stream, walker_range=walker_range)
         _check(lib().rms_sim_run_noalloc(self._h, C.byref(opts), C.c_void_p(int(d_labels)),
                                          C.c_void_p(int(d_rows)), C.c_void_p(int(d_sig)) if d_sig else None))
         return self
@@ -256,9 +265,7 @@ class Sim:
         g = _arr(g_sigw)
         if g.size != 2 * nw:
             raise ValueError("g_sigw must hold (cos, sin) weights per waveform")
-        w0, w1 = walker_range if walker_range is not None else (0, 0)
-        st = None if stream is None else C.c_void_p(int(stream))
-        opts = RunOpts(int(seed) & ((1 << 64) - 1), PRECISION["split"], int(device), st, 0, 0, int(w0), int(w1), None)
+        opts = _opts(seed, "split", device, stream, walker_range=walker_range)
         dwave = np.zeros(nw * nb * 3)
         sigw = np.zeros(2 * nw)
         out = AdjointGrads(_ptr(dwave), 0.0, 0.0, (C.c_double * 8)(), 0.0, _ptr(sigw))
@@ -374,10 +381,13 @@ class Sim:
         self.close()
 
 
-def batch_run(sims, seed: int = 0, precision: str = "compat", device: int = 0, stream=None, variant: int = 0):
+def batch_run(sims, seed: int = 0, precision: str = "compat", device: int = 0, stream=None, variant: int = 0,
+              shard=None):
+    """Walk a batch of simulations (SPLIT: one persistent launch; COMPAT: one
+    launch per simulation).  ``shard`` = (index, count): every simulation
+    walks only that shard of its walkers (a rank's part of the batch)."""
     arr = (C.c_void_p * len(sims))(*[s._h.value for s in sims])
-    st = None if stream is None else C.c_void_p(int(stream))
-    opts = RunOpts(int(seed), PRECISION[precision], int(device), st, 0, int(variant), 0, 0, None)
+    opts = _opts(seed, precision, device, stream, variant=variant, shard=shard)
     _check(lib().rms_batch_run(arr, len(sims), C.byref(opts)))
 
 
@@ -460,12 +470,11 @@ class Graph:
     """A batch launch captured as a CUDA graph (rms_batch_graph_create) and
     replayed per seed (rms_graph_run); results land in the simulations."""
 
-    def __init__(self, sims, seed: int = 0, device: int = 0, stream=None, variant: int = 0):
+    def __init__(self, sims, seed: int = 0, device: int = 0, stream=None, variant: int = 0, shard=None):
         self._h = C.c_void_p()
         self.sims = list(sims)
         arr = (C.c_void_p * len(sims))(*[s._h.value for s in sims])
-        st = None if stream is None else C.c_void_p(int(stream))
-        opts = RunOpts(int(seed), PRECISION["split"], int(device), st, 0, int(variant), 0, 0, None)
+        opts = _opts(seed, "split", device, stream, variant=variant, shard=shard)
         _check(lib().rms_batch_graph_create(arr, len(sims), C.byref(opts), C.byref(self._h)))
 
     def run(self, seed: int):
@@ -489,12 +498,11 @@ class Graph:
             pass
 
 
-def autotune(sims, seed: int = 0, device: int = 0, stream=None):
+def autotune(sims, seed: int = 0, device: int = 0, stream=None, shard=None):
     """(variant, [walk ms per variant]) of the SPLIT walk for this batch; pass
     the variant to run()/batch_run().  Cached per job class."""
     arr = (C.c_void_p * len(sims))(*[s._h.value for s in sims])
-    st = None if stream is None else C.c_void_p(int(stream))
-    opts = RunOpts(int(seed), PRECISION["split"], int(device), st, 0, 0, 0, 0, None)
+    opts = _opts(seed, "split", device, stream, shard=shard)
     v = C.c_int()
     ms = np.zeros(len(split_variants()))
     _check(lib().rms_autotune(arr, len(sims), C.byref(opts), C.byref(v), _ptr(ms)))

@@ -36,6 +36,58 @@ def _rank(rank, world, port, q):
     dist.destroy_process_group()
 
 
+def _batch():
+    """Three axons of uneven lattices and walker counts (one with fewer
+    walkers than ranks), as a batch would hold them."""
+    jobs = []
+    for k, (shape, npar) in enumerate((((12, 12, 16), 37), ((10, 14, 20), 64), ((8, 8, 12), 1))):
+        lab = geometry.axon_lattice(*shape, 0.1, seed=10 + k, exterior=2, r0=0.35)
+        step, t2s, pij, td = pyoracle.reference_tables(2e-4, 0.1, [0, 2.0, 1.5], [80, 80, 40], 1000, 1000,
+                                                       kappa=0.02 * k)
+        jobs.append(pyoracle.Job(lab, dt=2e-4, tn=1000, npar=npar, res=0.1, step=step, t2_steps=t2s, pij=pij,
+                                 seed=100 + k, td=td, bval=[1.0], bvec=[[0, 0, 1]]))
+    return jobs
+
+
+def _batch_rank(rank, world, port, q):
+    """One rank of a batch split into shards: walkers [npar r / N, npar (r+1) / N)
+    of every axon (what rms_run_opts.shard_index/shard_count selects in the
+    library), then the per-axon sums added across ranks in rank order."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    fields = {}
+    for k, job in enumerate(_batch()):
+        w0, w1 = shards.split_range(job.npar, rank, world)
+        o = pyoracle.run_oracle(job, w0, w1) if w1 > w0 else job.empty_outputs()
+        for f in ("sig0", "dx2", "dx4", "sigre", "npar_count"):
+            fields[f"{k}/{f}"] = o[f]
+    tot = shards.gather_sum(fields)
+    if rank == 0:
+        q.put({k: v.copy() for k, v in tot.items()})
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_batch_shards_sum_to_the_whole_batch():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for k, job in enumerate(_batch()):
+        whole = pyoracle.run_oracle(job)
+        assert np.array_equal(got[f"{k}/npar_count"], whole["npar_count"]), k
+        for f in ("sig0", "dx2", "dx4", "sigre"):
+            np.testing.assert_allclose(got[f"{k}/{f}"], whole[f], rtol=1e-12,
+                                       atol=1e-12 * np.abs(whole[f]).max())
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))

@@ -116,3 +116,44 @@ def test_one_simulation_graph_equals_a_plain_run():
     np.testing.assert_array_equal(p["npar_count"], o["npar_count"])
     assert_fp64_close(p["dx2"], o["dx2"], 1e-9, "dx2")
     g.close()
+
+
+@pytest.mark.parametrize("precision", ["split", "compat"])
+def test_batch_shards_sum_to_the_whole_batch(precision):
+    """A batch split into ranks' shards (shard r of N of every axon's walkers,
+    rms_run_opts.shard_index/shard_count): the shards' sums add up to the
+    unsharded batch -- counts exactly, FP64 sums up to their order.  Three
+    shards, one of them empty for the smallest axon (npar < shards)."""
+    sims = axon_sims()[:3]
+    tiny = engine.Sim(geometry.axon_lattice(12, 12, 16, 0.1, seed=4, exterior=2, r0=0.4), dt=2e-4, tn=1000, npar=2,
+                      res=0.1, diffusivity=[0, 2.0, 2.0], t2=[80, 80, 60], bval=[1.0, 2.0],
+                      bvec=[[1, 0, 0], [0, 0, 1]])
+    sims.append(tiny)
+    engine.batch_run(sims, seed=9, precision=precision)
+    whole = [s.outputs() for s in sims]
+    parts = []
+    for r in range(3):
+        engine.batch_run(sims, seed=9, precision=precision, shard=(r, 3))
+        parts.append([s.outputs() for s in sims])
+    for k in range(len(sims)):
+        cnt = sum(p[k]["npar_count"] for p in parts)
+        assert np.array_equal(cnt, whole[k]["npar_count"]), k
+        for f in ("sig0", "dx2", "dx4", "sigre"):
+            assert_fp64_close(sum(p[k][f] for p in parts), whole[k][f], 1e-9, f"axon {k} {f}")
+    # the graph walks the same shard
+    g = engine.Graph(sims, seed=0, shard=(1, 3)) if precision == "split" else None
+    if g is not None:
+        g.run(9)
+        for k, s in enumerate(sims):
+            np.testing.assert_array_equal(s.outputs()["npar_count"], parts[1][k]["npar_count"])
+        g.close()
+
+
+def test_shard_arguments_are_checked():
+    sims = axon_sims()[:1]
+    for bad in ((3, 3), (-1, 2)):
+        with pytest.raises(engine.RmsError) as e:
+            engine.batch_run(sims, seed=1, precision="split", shard=bad)
+        assert e.value.code == -1
+    with pytest.raises(engine.RmsError):
+        sims[0].run(seed=1, precision="split", walker_range=(0, 10), shard=(0, 2))

@@ -65,6 +65,73 @@ def test_noalloc_walk_matches_rms_sim_run(mode):
             assert_fp64_close(sig.cpu().numpy()[:3], want["sig"], 1e-9, f"call {call}: sig")
 
 
+def _many_compartments(nc: int) -> np.ndarray:
+    """Axon (label 1) in label-2 exterior, the exterior cut into z slabs that
+    carry labels 3 .. nc-1."""
+    lab = geometry.axon_lattice(16, 16, 40, 0.1, seed=5, exterior=2, r0=0.5)
+    slab = 40 // nc
+    for c in range(3, nc):
+        part = lab[:, :, (c - 2) * slab:(c - 1) * slab]
+        part[part == 2] = c
+    lab[:1] = 0
+    return lab
+
+
+@pytest.mark.parametrize("nc", [5, 7])
+def test_noalloc_many_compartments_match_rms_sim_run(nc):
+    """Nc up to the no-allocation walk's limit of 7: the compartment tables
+    it builds on the host stack hold 2 Nc + Nc^2 entries."""
+    import torch
+    lab = _many_compartments(nc)
+    D = [0.0] + [1.0 + 0.15 * c for c in range(1, nc)]
+    T2 = [80.0] + [30.0 + 10.0 * c for c in range(1, nc)]
+    kw = dict(dt=2e-4, tn=1000, npar=8192, res=0.1, diffusivity=D, t2=T2, bval=[1.0, 2.0],
+              bvec=[[1.0, 0, 0], [0, 0.6, 0.8]])
+    sim = engine.Sim(lab, **kw)
+    want = sim.run(seed=3, precision="split").outputs()
+    assert (want["npar_count"][0, 3:] > 0).all(), "every extra compartment holds walkers"
+    T, W = 1000, 64
+    d_lab = torch.from_numpy(np.ascontiguousarray(lab)).cuda()
+    rows = torch.empty(T * W, dtype=torch.float64, device="cuda")
+    for call in range(2):
+        rows.fill_(float("nan"))
+        torch.cuda.synchronize()
+        sim.run_noalloc(d_lab.data_ptr(), rows.data_ptr(), 0, seed=3)
+        got = unpack(rows.cpu().numpy(), T, 2, nc, "narrow")
+        assert np.array_equal(got["npar_count"], want["npar_count"]), f"call {call}: counts differ"
+        for k in ("sig0", "dx2", "dx4", "sigre"):
+            assert_fp64_close(got[k], want[k], 1e-9, f"call {call}: {k}")
+
+
+def test_noalloc_checks_the_device_lattice():
+    """The caller's device lattice is checked before the walk: a label >= Nc
+    and a lattice without labelled voxels are refused (RMS_ERR_RANGE), and a
+    good lattice still runs afterwards."""
+    import torch
+    lab = geometry.axon_lattice(12, 12, 16, 0.1, seed=2, exterior=2, r0=0.4)
+    sim = engine.Sim(lab, dt=2e-4, tn=1000, npar=256, res=0.1, diffusivity=[0, 2.0, 1.0], t2=[80, 80, 40],
+                     bval=[1.0], bvec=[[1.0, 0, 0]])
+    rows = torch.empty(1000 * 64, dtype=torch.float64, device="cuda")
+    for bad_label in (3, 7, 9):
+        bad = lab.copy()
+        bad[5, 6, 7] = bad_label
+        d_bad = torch.from_numpy(bad).cuda()
+        with pytest.raises(engine.RmsError) as e:
+            sim.run_noalloc(d_bad.data_ptr(), rows.data_ptr(), 0, seed=1)
+        assert e.value.code == -4 and "not below Nc" in str(e.value)
+    d_zero = torch.zeros(lab.shape, dtype=torch.uint8, device="cuda")
+    with pytest.raises(engine.RmsError) as e:
+        sim.run_noalloc(d_zero.data_ptr(), rows.data_ptr(), 0, seed=1)
+    assert e.value.code == -4
+    # an odd start address exercises the check's unaligned head and tail
+    buf = torch.zeros(lab.size + 1, dtype=torch.uint8, device="cuda")
+    buf[1:] = torch.from_numpy(lab.reshape(-1))
+    sim.run_noalloc(buf.data_ptr() + 1, rows.data_ptr(), 0, seed=1)
+    want = sim.run(seed=1, precision="split").outputs()
+    got = unpack(rows.cpu().numpy(), 1000, 1, 3, "narrow")
+    assert np.array_equal(got["npar_count"], want["npar_count"])
+
+
 def test_noalloc_refuses_oversized_job():
     import torch
     lab = np.ones((8, 8, 8), dtype=np.uint8)
