@@ -16,17 +16,29 @@ Workload ``single``: the 64 x 64 x 512 single-axon lattice (labels 0/1),
 1e5 walkers, 5,000 steps, impermeable, no T2, periodic walls, moments every
 10 steps.  Inputs are synthetic and seeded.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-cuda]
                   [--precision split|compat] [--workload batch|production|single|contraction|adjoint]
-                  [--plain-ratio]
+                  [--scaling strong|weak] [--plain-steps P]
+
+Several ranks (torchrun, one per GPU) split the batch: every rank walks its
+shard of every axon's walkers (walker ids, and so random streams, are the whole
+job's), and the per-axon sums are added in rank order (--scaling strong, the
+default); --scaling weak gives every rank the whole batch on its own seeds.
 
 ``value``: walker-steps/s of the whole job, lattice already resident on the
 GPU, timed with CUDA events on the launching stream (max over ranks).
 ``e2e``: the same through the public API with the lattice handed over from
-pinned host memory and the results read back every step (host clock around
-synchronised steps).  ``--impl reference`` times the reference simulator's
-own step loop (hpc_code/lib/main_PGSE.cu compiled for the host, all cores)
-on a bounded sample of the same workload.
+pinned host memory and the results read back (and, with several ranks, summed
+across them) every step (host clock around synchronised steps).
+``plain``: the plain form on the same job -- the FP64 walk in the reference's
+arithmetic (COMPAT), one launch per axon -- timed the same way; the metric is
+value / plain.  ``error``: D(t) and K(t) of the timed split walk against the
+FP64 replay of the same walkers (oracle), on a walker subset of four axons.
+``reference_cuda``: the reference's own CUDA programs (main.cu, main_PGSE.cu
+built unchanged for sm_100a) beside rms_main on one run directory each.
+``--impl reference`` times the reference simulator's own step loop
+(hpc_code/lib/main.cu or main_PGSE.cu compiled for the host, all cores) on a
+bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -50,6 +62,7 @@ UNIT = "walker-steps/s"
 # step/voxel = 0.49, each a 32-byte sector -> 23.4 B; 105 thread-ops.
 BYTES_PER_WALKER_STEP = 23.4
 OPS_PER_WALKER_STEP = 105.0
+BATCH_SEED_STEP = 0x9E3779B97F4A7C15   # batch member k walks with seed + k * this (include/rms.h)
 
 
 def fib_directions(n: int) -> np.ndarray:
@@ -62,8 +75,10 @@ def fib_directions(n: int) -> np.ndarray:
 
 
 def workload(name: str, world: int, walkers: int | None = None, tn: int | None = None,
-             timepoints: int | None = None):
-    lab, sim_kw, per_gpu, cfg = _workload(name, world)
+             timepoints: int | None = None, scaling: str = "strong"):
+    """(lattice(s), Sim keywords, walkers per GPU, config) of a workload; the
+    config is the same dict in both arms (this engine and the reference)."""
+    lab, sim_kw, per_gpu, cfg = _workload(name, world, scaling)
     if timepoints:
         if isinstance(sim_kw, list):
             sim_kw = [dict(kw, timepoints=int(timepoints)) for kw in sim_kw]
@@ -75,8 +90,8 @@ def workload(name: str, world: int, walkers: int | None = None, tn: int | None =
             scale = walkers / per_gpu
             sim_kw = [dict(kw, npar=max(32, int(kw["npar"] * scale))) for kw in sim_kw]
             per_gpu = sum(kw["npar"] for kw in sim_kw)
-            cfg["walkers_per_gpu"] = per_gpu
-            cfg["workload"] += f" [walkers/GPU overridden: {per_gpu}]"
+            cfg["walkers"] = per_gpu
+            cfg["workload"] += f" [walkers overridden: {per_gpu}]"
         if tn:
             sim_kw = [dict(kw, tn=int(tn)) for kw in sim_kw]
             cfg["steps_per_walk"] = int(tn)
@@ -94,7 +109,7 @@ def workload(name: str, world: int, walkers: int | None = None, tn: int | None =
     return lab, sim_kw, per_gpu, cfg
 
 
-def _workload(name: str, world: int):
+def _workload(name: str, world: int, scaling: str = "strong"):
     from rms_b200 import analysis, geometry
     if name == "production":
         lab = geometry.axon_lattice(256, 256, 2048, 0.1, seed=0, exterior=2)
@@ -112,7 +127,9 @@ def _workload(name: str, world: int):
         cfg = dict(workload="production: 256x256x2048 lattice, 1e7 walkers/GPU, 50000 steps, "
                             "kappa=0.01 um/ms, T2 80/60 ms, PGSE 540 gradients",
                    lattice=[256, 256, 2048], walkers_per_gpu=per_gpu, steps_per_walk=50_000,
-                   ngrad=len(rows), mode="pgse")
+                   ngrad=len(rows), mode="pgse",
+                   l2="flushed between timed steps (256 MiB write); the packed lattice is 68 MB",
+                   parallelism=f"walker shards x{world} (weak: 1e7 walkers per rank)")
     elif name == "batch":
         # 64 axons, lattices of log-uniform voxel counts between 64x64x256 and
         # 256x256x2048, walkers proportional to the intra-axonal volume (5e7 in
@@ -129,11 +146,17 @@ def _workload(name: str, world: int):
                         diffusivity=[0.0, float(D0[k]), float(D0[k])], t2=[1e12, 1e12, 1e12],
                         bval=[], bvec=np.zeros((0, 3)), permeation="kappa", kappa=float(kap[k]))
                    for k in range(64)]
+        weak = scaling == "weak"
         cfg = dict(workload="batch: 64 axons, lattices 64x64x256..256x256x2048 (log-uniform voxels), "
-                            "5e7 walkers/GPU in proportion to intra-axonal volume, D0~U(1.5,2.5), "
+                            "5e7 walkers in proportion to intra-axonal volume, D0~U(1.5,2.5), "
                             "kappa~U(0,0.05), 20000 steps, moments only",
                    axons=64, lattice_voxels=int(sum(l.size for l in lattices)),
-                   walkers_per_gpu=int(npar.sum()), steps_per_walk=20_000, mode="narrow (no b-table)")
+                   walkers=int(npar.sum()) * (world if weak else 1), steps_per_walk=20_000,
+                   mode="narrow (no b-table)",
+                   l2="flushed between timed steps (256 MiB write); the 64 lattices (1.71 GB) are larger than L2",
+                   parallelism=(f"{world} rank(s), each walking the whole batch on its own seeds (weak)" if weak else
+                                f"{world} rank(s), each walking its 1/{world} shard of every axon's walkers "
+                                "(strong; per-axon sums added in rank order)"))
         return lattices, sims_kw, int(npar.sum()), cfg
     elif name == "single":
         lab = geometry.axon_lattice(64, 64, 512, 0.1, seed=0, exterior=0)
@@ -143,7 +166,8 @@ def _workload(name: str, world: int):
                       boundary="periodic")
         cfg = dict(workload="single: 64x64x512 axon, 1e5 walkers/GPU, 5000 steps, moments every 10 steps",
                    lattice=[64, 64, 512], walkers_per_gpu=per_gpu, steps_per_walk=5_000,
-                   mode="narrow")
+                   mode="narrow", l2="flushed between timed steps (256 MiB write)",
+                   parallelism=f"walker shards x{world} (weak: 1e5 walkers per rank)")
     else:
         raise SystemExit(f"unknown workload {name}")
     return lab, sim_kw, per_gpu, cfg
@@ -211,12 +235,12 @@ def cpu_reference_rate(lab, sim_kw, target_s: float, nthreads: int | None = None
     cores; n is chosen so one sample takes about target_s seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    from rms_b200 import engine
-    probe = engine.Sim(None, shape=lab.shape, **{k: v for k, v in sim_kw.items()})
-    step, pij = probe.get("step"), probe.get("pij")
-    probe.close()
     dt, tn = sim_kw["dt"], sim_kw["tn"]
-    t2s = np.array(sim_kw["t2"], dtype=np.float64) / dt
+    # the derived tables (main.cu:433-458; the kappa rule of interaction.m:437-439)
+    # from the oracle: this arm loads nothing of the engine
+    kap = sim_kw.get("kappa") if sim_kw.get("permeation") == "kappa" else None
+    step, t2s, pij, _ = pyoracle.reference_tables(dt, sim_kw["res"], sim_kw["diffusivity"], sim_kw["t2"],
+                                                  kappa=kap)
     timepoints = sim_kw.get("timepoints", 0) or 1000
     kw = dict(dt=dt, tn=tn, npar=sim_kw["npar"], res=sim_kw["res"], step=step, t2_steps=t2s,
               pij=pij, seed=1, timepoints=1000)
@@ -245,66 +269,28 @@ def cpu_reference_rate(lab, sim_kw, target_s: float, nthreads: int | None = None
 
 
 def run_reference_cuda(args):
-    """The reference's own CUDA program beside this engine's drop-in, process
-    against process on the same run directory: main.cu built unchanged for
-    sm_100a (oracle/_ref/main_cuda) and rms_main (split and compat precision).
-    Workload: the 64x64x512 single-axon lattice in the reference's file
-    contract (mirror walls, 1000 records, b = 1 and 2 ms/um^2 along x and z),
-    1e5 walkers x 5000 steps.  Each process is timed by the wall clock: both
-    read fiber.txt, create a CUDA context, walk, and write the output files.
-    D(t) and K(t) along x and z at the last record come from each one's
-    output files (readRMS.m formulas); the reference seeds cuRAND from
-    /dev/random, so they agree within Monte-Carlo error, not bit for bit."""
-    import shutil
-    import subprocess
-    import tempfile
-    from rms_b200 import analysis, geometry, runio
+    """The reference's own CUDA programs beside this engine's drop-in, process
+    against process on one run directory each: main.cu and main_PGSE.cu built
+    unchanged for sm_100a (oracle/_ref/main_cuda, main_pgse_cuda) and rms_main
+    (split and compat precision).  Workload: the 64x64x512 single-axon lattice
+    in the reference's file contract (mirror walls, 1000 records), 1e6 walkers
+    x 5000 steps; narrow pulses b = 1, 2 ms/um^2 along x and z, and PGSE with
+    6 directions x b = 1, 2 ms/um^2 at Delta = 0.6 ms, delta = 0.2 ms.  Each
+    process is timed by the wall clock: all read fiber.txt, create a CUDA
+    context, walk, and write the output files.  D(t) and K(t) along x and z at
+    the last record come from each one's output files (readRMS.m formulas); the
+    reference seeds cuRAND from /dev/random, so they agree within Monte-Carlo
+    error, not bit for bit."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    exe = os.path.join(ROOT, "oracle", "_ref", "main_cuda")
-    ours = os.path.join(ROOT, "monte-carlo-simulation-3d-rms_b200", "_build", "rms_main")
-    if not (os.path.exists(exe) and os.path.exists(ours)):
-        print(json.dumps({"impl": "reference-cuda", "unavailable": "oracle/_ref/main_cuda or rms_main not built"}))
-        return
-    npar, tn = args.walkers or 100_000, args.tn or 5_000
-    lab = geometry.axon_lattice(64, 64, 512, 0.1, seed=0, exterior=0)
-    kw = dict(dt=2e-4, tn=tn, npar=npar, res=0.1, diffusivity=[0.0, 2.0], t2=[1e12, 1e12],
-              bval=[1.0, 2.0], bvec=[[1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
-    top = tempfile.mkdtemp(prefix="rms_refcuda_")
-    runs = {}
-    try:
-        for name, cmd in (("reference main.cu", [exe]),
-                          ("rms_main split", [ours, "--precision", "split", "--seed", "7"]),
-                          ("rms_main compat", [ours, "--precision", "compat", "--seed", "7"])):
-            d = os.path.join(top, name.replace(" ", "_").replace(".", "_"))
-            runio.write_inputs(d, lab, **kw)
-            t0 = time.perf_counter()
-            try:
-                r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=600)
-            except subprocess.TimeoutExpired:
-                runs[name] = {"error": "timed out after 600 s"}
-                continue
-            wall = time.perf_counter() - t0
-            if r.returncode != 0:
-                runs[name] = {"error": f"exit {r.returncode}: {(r.stderr or r.stdout)[-300:]}"}
-                continue
-            sig0 = np.loadtxt(os.path.join(d, "sig0.txt"))
-            dx2 = np.loadtxt(os.path.join(d, "dx2.txt"))
-            dx4 = np.loadtxt(os.path.join(d, "dx4.txt"))
-            td = np.loadtxt(os.path.join(d, "diff_time.txt"))
-            D, K = analysis.axis_dk(sig0, dx2, dx4, td)
-            runs[name] = {"wall_s": wall, "walker_steps_per_s": npar * tn / wall,
-                          "D_x": float(D[-1, 0]), "D_z": float(D[-1, 2]),
-                          "K_x": float(K[-1, 0]), "K_z": float(K[-1, 2]),
-                          "stdout_tail": r.stdout.strip().splitlines()[-1:]}
-    finally:
-        shutil.rmtree(top, ignore_errors=True)
-    ref = runs.get("reference main.cu", {})
+    npar, tn = args.walkers or args.refcuda_walkers, args.tn or 5_000
+    runs = reference_cuda_runs(npar, tn)
+    ref = runs.get("reference main.cu", {}) if isinstance(runs, dict) else {}
     line = {"metric": METRIC, "value": ref.get("walker_steps_per_s"), "unit": UNIT, "n_gpus": 1,
             "higher_is_better": True, "impl": "reference-cuda", "data": "synthetic (seeded)",
-            "config": {"workload": f"64x64x512 axon (mirror walls, 1000 records, 2 b-values), {npar} walkers, "
-                                   f"{tn} steps: the reference's CUDA program and rms_main on the same run "
-                                   "directory, wall time per process (text I/O and context creation included)"},
+            "config": {"workload": f"64x64x512 axon (mirror walls, 1000 records), {npar} walkers, {tn} steps: "
+                                   "the reference's CUDA programs (narrow pulse, PGSE) and rms_main on the same "
+                                   "run directories, wall time per process (text I/O and context creation included)"},
             "runs": runs}
     print(json.dumps(line), flush=True)
 
@@ -315,7 +301,9 @@ def run_reference_arm(args):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    lab, sim_kw, per_gpu, cfg = workload(args.workload, 1, args.walkers, args.tn, args.timepoints)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn, args.timepoints,
+                                         args.scaling)
     if isinstance(lab, list):
         # a batch: time the reference loop on the axon with the most walkers
         k = int(np.argmax([kw["npar"] for kw in sim_kw]))
@@ -338,7 +326,8 @@ def run_reference_arm(args):
     line = {
         "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "scaling": args.scaling if args.workload == "batch" else "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
         "config": cfg, "impl": "reference",
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -392,16 +381,25 @@ class SingleJob:
 
 
 class BatchJob:
-    """Many axons walked by one launch (rms_batch_run); every rank walks its own
-    copy of the batch with its own seed (weak scaling)."""
+    """Many axons walked by one launch (rms_batch_run, or its captured CUDA
+    graph).  Strong scaling: rank r walks shard r of every axon's walkers, so
+    the ranks together walk the one job once.  Weak scaling: every rank walks
+    the whole batch on its own seeds."""
 
-    def __init__(self, labs, kws, rank, device, stream):
+    def __init__(self, labs, kws, rank, world, device, stream, scaling="strong"):
         from rms_b200 import engine
         self.engine = engine
         self.labs, self.kws = labs, kws
         self.sims = [engine.Sim(l, **kw) for l, kw in zip(labs, kws)]
-        self.rank, self.device, self.stream = rank, device, stream
-        self.walker_steps = sum(kw["npar"] * kw["tn"] for kw in kws)
+        self.rank, self.world, self.device, self.stream = rank, world, device, stream
+        self.weak = scaling == "weak"
+        self.shard = None if (self.weak or world == 1) else (rank, world)
+        self.seed_offset = (rank << 40) if self.weak else 0
+        if self.shard is None:
+            self.walker_steps = sum(kw["npar"] * kw["tn"] for kw in kws)
+        else:
+            self.walker_steps = sum((kw["npar"] * (rank + 1) // world - kw["npar"] * rank // world) * kw["tn"]
+                                    for kw in kws)
         # split: one persistent walk (multi-axon launches sum into the axon
         # totals, no separate reduction); compat: one walk + one reduction per axon
         self.launches_per_step = 1
@@ -414,19 +412,19 @@ class BatchJob:
         and capture the batch launch as a CUDA graph (rms_batch_graph_create)."""
         if precision == "split":
             self.variant, self.variant_ms = self.engine.autotune(self.sims, seed=1, device=self.device,
-                                                                  stream=self.stream)
+                                                                  stream=self.stream, shard=self.shard)
             self.graph = self.engine.Graph(self.sims, seed=0, device=self.device, stream=self.stream,
-                                           variant=self.variant)
+                                           variant=self.variant, shard=self.shard)
         else:
             self.launches_per_step = 2 * len(self.sims)
 
     def run(self, seed, precision):
         if self.graph is not None and precision == "split":
-            self.graph.run(seed + (self.rank << 40))
+            self.graph.run(seed + self.seed_offset)
             return
-        self.engine.batch_run(self.sims, seed=seed + (self.rank << 40), precision=precision,
+        self.engine.batch_run(self.sims, seed=seed + self.seed_offset, precision=precision,
                               device=self.device, stream=self.stream,
-                              variant=self.variant if precision == "split" else 0)
+                              variant=self.variant if precision == "split" else 0, shard=self.shard)
 
     def walk_ms(self):
         return self.sims[0].timing()[0]
@@ -455,11 +453,139 @@ class BatchJob:
         k = int(np.argmax([kw["npar"] for kw in self.kws]))
         return self.labs[k], self.kws[k]
 
+    def error_vs_fp64(self, seed, nsub=16384, axons=None, nthreads=None):
+        """D(t), K(t) of the split walk against the oracle's FP64 replay of
+        the same walkers: walkers [0, nsub) of four axons (the smallest, two
+        in between, the largest lattice), walked with the seed the timed step
+        gave each axon.  Bar: D within 0.5 %, K within 2 % (absolute 0.02
+        where |K| < 1), records 50 on."""
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+        from rms_b200 import analysis
+        sizes = np.array([l.size for l in self.labs])
+        order = np.argsort(sizes, kind="stable")
+        if axons is None:
+            axons = sorted({int(order[0]), int(order[len(order) // 3]), int(order[2 * len(order) // 3]),
+                            int(order[-1])})
+        nthreads = nthreads or os.cpu_count() or 1
+        per_axon, dD_max, dK_max = [], 0.0, 0.0
+        sl = slice(50, None)
+        for k in axons:
+            kw, sim = self.kws[k], self.sims[k]
+            n = int(min(nsub, kw["npar"]))
+            sk = (seed + self.seed_offset + k * BATCH_SEED_STEP) & ((1 << 64) - 1)
+            got = sim.run(seed=sk, precision="split", device=self.device, stream=self.stream,
+                          walker_range=(0, n)).outputs()
+            kap = kw["kappa"] if kw.get("permeation") == "kappa" else None
+            step, t2s, pij, td = pyoracle.reference_tables(kw["dt"], kw["res"], kw["diffusivity"], kw["t2"],
+                                                           1000, kw["tn"], kappa=kap)
+            job = pyoracle.Job(self.labs[k], dt=kw["dt"], tn=kw["tn"], npar=kw["npar"], res=kw["res"], step=step,
+                               t2_steps=t2s, pij=pij, seed=sk, td=td, bval=[], bvec=np.zeros((0, 3)))
+            t0 = time.perf_counter()
+            want = pyoracle.run_oracle(job, 0, n, nthreads=nthreads, split=True)
+            cpu_s = time.perf_counter() - t0
+            Dg, Kg = analysis.axis_dk(got["sig0"], got["dx2"], got["dx4"], got["td"])
+            Dw, Kw = analysis.axis_dk(want["sig0"], want["dx2"], want["dx4"], got["td"])
+            dD = float(np.abs(Dg[sl] / Dw[sl] - 1).max())
+            dK = float((np.abs(Kg[sl] - Kw[sl]) / np.maximum(np.abs(Kw[sl]), 1.0)).max())
+            counts_equal = bool(np.array_equal(got["npar_count"].sum(axis=1), want["npar_count"].sum(axis=1)))
+            per_axon.append({"axon": int(k), "lattice": list(self.labs[k].shape), "walkers": n,
+                             "dD_rel": dD, "dK": dK, "D_late": [round(float(x), 5) for x in Dw[-1]],
+                             "K_late": [round(float(x), 4) for x in Kw[-1]], "walker_count_conserved": counts_equal,
+                             "replay_s": round(cpu_s, 2)})
+            dD_max, dK_max = max(dD_max, dD), max(dK_max, dK)
+        return {"dD_max": dD_max, "dK_max": dK_max, "bar": {"dD": 0.005, "dK": 0.02},
+                "within_bar": bool(dD_max <= 0.005 and dK_max <= 0.02),
+                "against": "FP64 replay of the same walkers and random streams (oracle or_run_split)",
+                "definition": "max over records 50..999 and axes x, y, z of |D/D64 - 1| and "
+                              "|K - K64| / max(|K64|, 1)",
+                "steps_per_walk": int(self.kws[0]["tn"]), "per_axon": per_axon}
+
     def close(self):
         if self.graph is not None:
             self.graph.close()
         for sim in self.sims:
             sim.close()
+
+
+def issue_peak(sm_mhz):
+    """Thread-instruction issue peak of a B200: 148 SMs x 4 schedulers x 32
+    lanes per clock, at the SM clock sampled during the timed region."""
+    return 148 * 4 * 32 * (sm_mhz or 1965.0) * 1e6
+
+
+def profile_figures(precision, workload):
+    """Per-walker-step figures of the ncu capture summarised in profiles/
+    (measured on a smaller case of the same kernel and workload shape)."""
+    out = {}
+    prof = os.path.join(ROOT, "profiles", f"walk_{precision}_kernel__{workload}.md")
+    if os.path.exists(prof):
+        for ln in open(prof):
+            for key in ("traffic_bytes_per_walker_step", "warp_inst_per_warp_step", "issue_active"):
+                if ln.startswith(key + ":"):
+                    out[key] = float(ln.split(":")[1].split()[0])
+    return out
+
+
+def reference_cuda_runs(npar, tn, nthreads=None):
+    """The reference's own CUDA programs beside rms_main, process against
+    process: see run_reference_cuda.  Returns the runs dict."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "main_cuda")
+    exe_pgse = os.path.join(ROOT, "oracle", "_ref", "main_pgse_cuda")
+    ours = os.path.join(ROOT, "monte-carlo-simulation-3d-rms_b200", "_build", "rms_main")
+    import shutil
+    import tempfile
+    from rms_b200 import analysis, geometry, runio
+    if not (os.path.exists(exe) and os.path.exists(exe_pgse) and os.path.exists(ours)):
+        return {"unavailable": "oracle/_ref/main_cuda, main_pgse_cuda or rms_main not built"}
+    lab = geometry.axon_lattice(64, 64, 512, 0.1, seed=0, exterior=0)
+    base = dict(dt=2e-4, tn=tn, npar=npar, res=0.1, diffusivity=[0.0, 2.0], t2=[1e12, 1e12])
+    narrow = dict(base, bval=[1.0, 2.0], bvec=[[1.0, 0.0, 0.0], [0.0, 0.0, 1.0]])
+    # PGSE: 6 directions x b in {1, 2} ms/um^2 at Delta = 0.6 ms, delta = 0.2 ms (fits the 1 ms walk)
+    dirs = fib_directions(6)
+    from rms_b200 import analysis as an
+    grad = np.array([[0.6, 0.2, float(an.pgse_gradient_for_b(b, 0.6, 0.2)), *d] for b in (1.0, 2.0) for d in dirs])
+    pgse = dict(base, grad=grad)
+    top = tempfile.mkdtemp(prefix="rms_refcuda_")
+    runs = {}
+    try:
+        for name, cmd, kw in (("reference main.cu", [exe], narrow),
+                              ("rms_main split (narrow)", [ours, "--precision", "split", "--seed", "7"], narrow),
+                              ("rms_main compat (narrow)", [ours, "--precision", "compat", "--seed", "7"], narrow),
+                              ("reference main_PGSE.cu", [exe_pgse], pgse),
+                              ("rms_main split (pgse)", [ours, "--precision", "split", "--seed", "7"], pgse),
+                              ("rms_main compat (pgse)", [ours, "--precision", "compat", "--seed", "7"], pgse)):
+            d = os.path.join(top, "".join(c if c.isalnum() else "_" for c in name))
+            runio.write_inputs(d, lab, lattice="txt", **kw)
+            t0 = time.perf_counter()
+            try:
+                r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=900)
+            except subprocess.TimeoutExpired:
+                runs[name] = {"error": "timed out after 900 s"}
+                continue
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                runs[name] = {"error": f"exit {r.returncode}: {(r.stderr or r.stdout)[-300:]}"}
+                continue
+            sig0 = np.loadtxt(os.path.join(d, "sig0.txt"))
+            dx2 = np.loadtxt(os.path.join(d, "dx2.txt"))
+            dx4 = np.loadtxt(os.path.join(d, "dx4.txt"))
+            td = np.loadtxt(os.path.join(d, "diff_time.txt"))
+            D, K = analysis.axis_dk(sig0, dx2, dx4, td)
+            runs[name] = {"wall_s": round(wall, 3), "walker_steps_per_s": npar * tn / wall,
+                          "D_x": float(D[-1, 0]), "D_z": float(D[-1, 2]),
+                          "K_x": float(K[-1, 0]), "K_z": float(K[-1, 2])}
+            if "grad" in kw:
+                sig = np.atleast_1d(np.loadtxt(os.path.join(d, "sig.txt")))
+                runs[name]["S_over_S0"] = [round(float(x), 5) for x in sig / sig0[-1]]
+    finally:
+        shutil.rmtree(top, ignore_errors=True)
+    for prog in ("narrow", "pgse"):
+        ref = runs.get("reference main.cu" if prog == "narrow" else "reference main_PGSE.cu", {})
+        ours_s = runs.get(f"rms_main split ({prog})", {})
+        if ref.get("wall_s") and ours_s.get("wall_s"):
+            runs[f"process_ratio_split_{prog}"] = ref["wall_s"] / ours_s["wall_s"]
+    return runs
 
 
 def run_ours(args):
@@ -473,12 +599,13 @@ def run_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn, args.timepoints)
+    lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn, args.timepoints,
+                                         args.scaling)
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
-    if isinstance(lab, list):
-        # weak scaling: every rank walks the whole batch, on its own seeds
-        job = BatchJob(lab, sim_kw, rank, local, sh)
+    batch = isinstance(lab, list)
+    if batch:
+        job = BatchJob(lab, sim_kw, rank, world, local, sh, scaling=args.scaling)
     else:
         job = SingleJob(lab, sim_kw, per_gpu, rank, local, sh)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -495,6 +622,16 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return tuple(float(x) for x in t)
 
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        return float(t[0])
+
+    # every rank's walker-steps, summed: the units all ranks walked per step
+    total_walker_steps = sum_over_ranks(job.walker_steps)
+
     if hasattr(job, "tune"):
         job.tune(precision)   # outside the timed region
     for i in range(args.warmup):
@@ -503,34 +640,49 @@ def run_ours(args):
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    timed_seed = 2000
     with ClockSampler(local) as clk:
         e0.record(stream)
         for i in range(args.steps):
             flush.zero_()
-            job.run(2000 + i, precision)
+            job.run(timed_seed + i, precision)
             walk_ms.append(job.walk_ms())
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
     ms, walk = max_over_ranks(e0.elapsed_time(e1) / args.steps, float(np.mean(walk_ms)))
-    value = world * job.walker_steps / (ms * 1e-3)
+    value = total_walker_steps / (ms * 1e-3)
+    clocks = clk.summary()
 
-    # the plain FP64 walk on the same workload (one launch per axon), for the
-    # split / plain ratio
+    # the plain form on the same job: the FP64 walk in the reference's
+    # arithmetic (COMPAT), one launch per axon, each rank its own shard
     plain = None
-    if args.plain_ratio and precision == "split":
-        job.run(999, "compat")
-        torch.cuda.synchronize()
-        e0.record(stream)
-        job.run(998, "compat")
-        e1.record(stream)
-        torch.cuda.synchronize()
-        (pms,) = max_over_ranks(e0.elapsed_time(e1))
-        plain = {"value": world * job.walker_steps / (pms * 1e-3), "ms_per_step": pms,
-                 "precision": "compat (FP64), one launch per axon", "steps": 1}
+    if args.plain_steps > 0 and precision == "split":
+        if batch:
+            small = int(np.argmin([l.size for l in job.labs]))
+            job.sims[small].run(seed=999, precision="compat", device=local, stream=sh,
+                                walker_range=(0, min(4096, job.kws[small]["npar"])))   # module load, untimed
+        else:
+            job.run(999, "compat")
+        pms = []
+        for i in range(args.plain_steps):
+            barrier()
+            torch.cuda.synchronize()
+            flush.zero_()
+            e0.record(stream)
+            job.run(timed_seed + i, "compat")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            pms.append(e0.elapsed_time(e1))
+        (pms_max,) = max_over_ranks(float(np.mean(pms)))
+        pval = total_walker_steps / (pms_max * 1e-3)
+        plain = {"value": pval, "unit": UNIT, "ms_per_step": pms_max, "steps": args.plain_steps,
+                 "form": "COMPAT: FP64 positions and sums in the reference's operation order, one launch "
+                         "(walk + ordered reduction) per axon, the same walkers and seeds",
+                 "batched_split_over_plain": value / pval, "target": 3.0}
 
     # end to end through the public API: lattices from pinned host memory,
-    # results read back, every step
+    # results read back (and summed across ranks), every step
     e2e_steps = max(1, min(args.steps, 3))
     barrier()
     torch.cuda.synchronize()
@@ -548,23 +700,45 @@ def run_ours(args):
     d2h = int(sum(v.nbytes for v in out.values()))
     h2d = job.input_bytes()
 
-    # roofline of the walk kernel (the dominant launch)
+    # the split walk's D(t), K(t) error against the FP64 replay (rank 0, one GPU)
+    error = None
+    if batch and precision == "split" and rank == 0 and world == 1 and not args.no_error:
+        error = job.error_vs_fp64(timed_seed)
+
+    # roofline of the walk kernel (the dominant launch): issue-bound (the
+    # algorithmic thread-op model against the issue peak), with the byte model
+    # and the measured DRAM traffic beside it
     walker_steps = job.walker_steps
-    achieved_gbs = walker_steps * BYTES_PER_WALKER_STEP / (walk * 1e-3) / 1e9
+    prof = profile_figures(precision, args.workload)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    # DRAM bytes per launch from the ncu capture summarised in profiles/
-    # (measured per walker-step on a case of the same shape, scaled to this launch)
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", f"walk_{precision}_kernel__{args.workload}.md")
-    if os.path.exists(prof):
-        for ln in open(prof):
-            if ln.startswith("traffic_bytes_per_walker_step:"):
-                traffic = float(ln.split(":")[1]) * walker_steps
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    ops_rate = walker_steps * OPS_PER_WALKER_STEP / (walk * 1e-3)
+    ipeak = issue_peak(clocks.get("sm_mhz"))
+    traffic = prof["traffic_bytes_per_walker_step"] * walker_steps if "traffic_bytes_per_walker_step" in prof else None
+    roofline = {
+        "bound": "issue", "achieved": ops_rate / 1e12, "peak": ipeak / 1e12, "unit": "T thread-op/s",
+        "frac": ops_rate / ipeak, "traffic": traffic,
+        "model": f"{OPS_PER_WALKER_STEP:.0f} algorithmic thread-ops/walker-step x {walker_steps:.3g} walker-steps / "
+                 f"walk kernel {walk:.1f} ms; peak 148 SM x 128 lanes x {clocks.get('sm_mhz') or 1965:.0f} MHz",
+        "executed": ({"warp_inst_per_warp_step": prof["warp_inst_per_warp_step"],
+                      "issue_slot_frac": walker_steps / 32 * prof["warp_inst_per_warp_step"] / (walk * 1e-3)
+                                         / (ipeak / 32),
+                      "source": f"ncu smsp__inst_executed, profiles/walk_{precision}_kernel__{args.workload}.md"}
+                     if "warp_inst_per_warp_step" in prof else None),
+        "bytes": {"model_gbs": walker_steps * BYTES_PER_WALKER_STEP / (walk * 1e-3) / 1e9,
+                  "model": f"{BYTES_PER_WALKER_STEP} B/walker-step (0.73 label gathers x 32 B sector)",
+                  "measured_dram_gbs": (traffic / (walk * 1e-3) / 1e9) if traffic else None,
+                  "hbm_peak_gbs": hbm_peak,
+                  "peak_source": "measured hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
+    }
+
+    refcuda = None
+    if rank == 0 and world == 1 and not args.no_reference_cuda and args.workload == "batch":
+        refcuda = reference_cuda_runs(args.refcuda_walkers, 5000)
 
     if rank == 0:
         cpu = None
@@ -578,35 +752,33 @@ def run_ours(args):
                 pyoracle.run_reference_walkers(cjob, n, cores)
                 el = time.perf_counter() - t0
                 cpu = {"value": n * cjob.tn / el, "unit": UNIT, "cores": cores, "kind": kind,
-                       "sample": f"walkers [0,{n}) x {cjob.tn} steps, reference propagate() "
-                                 f"(oracle/_ref) on {cores} host threads, {el:.1f} s"}
+                       "sample": f"walkers [0,{n}) x {cjob.tn} steps of the axon with the most walkers, reference "
+                                 f"propagate() (oracle/_ref) on {cores} host threads, {el:.1f} s"}
             except Exception as e:
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                        "sample": f"unavailable: {e}"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": args.scaling if batch else "weak",
             "vs_baseline": None, "dtype": "f64" if precision == "compat" else "f32+i32 (f64 sums)",
             "data": "synthetic (seeded axon lattices)",
-            "config": dict(cfg, precision=precision, parallelism=f"walker shards x{world}",
-                           l2="flushed between steps (256 MiB write); lattices larger than L2",
-                           **({"launch": "CUDA graph replay (rms_graph_run) of one persistent split launch",
-                               "launch_variant": int(job.variant),
-                               "autotune_walk_ms": [round(float(x), 2) for x in job.variant_ms]}
-                              if getattr(job, "variant_ms", None) is not None else {})),
-            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
-                         "frac": achieved_gbs / peak, "traffic": traffic,
-                         "model": f"{BYTES_PER_WALKER_STEP} B/walker-step x {walker_steps:.3g} walker-steps "
-                                  f"/ walk kernel {walk:.1f} ms (peak: measured hbm_gbs)"},
-            "issue": {"achieved_thread_ops_per_s": walker_steps * OPS_PER_WALKER_STEP / (walk * 1e-3),
-                      "ops_per_walker_step": OPS_PER_WALKER_STEP},
+            "config": cfg,
+            "setup": dict(precision=precision,
+                          **({"launch": "CUDA graph replay (rms_graph_run) of one persistent split launch",
+                              "launch_variant": int(job.variant),
+                              "autotune_walk_ms": [round(float(x), 2) for x in job.variant_ms]}
+                             if getattr(job, "variant_ms", None) is not None else {})),
+            "roofline": roofline,
             "walk_ms": walk,
             "plain": plain,
-            "e2e": {"value": world * walker_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "error": error,
+            "e2e": {"value": total_walker_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": job.launches_per_step * args.steps,
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "cpu_baseline": cpu,
+            "reference_cuda": refcuda,
         }
         print(json.dumps(line), flush=True)
     job.close()
@@ -864,8 +1036,15 @@ def main():
     ap.add_argument("--workload", default="batch", choices=["production", "batch", "single", "contraction", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--walkers", type=int, default=None, help="walkers per GPU (smaller case, e.g. for ncu)")
-    ap.add_argument("--plain-ratio", action="store_true",
-                    help="also time one run of the plain FP64 walk on the same workload")
+    ap.add_argument("--plain-steps", type=int, default=1,
+                    help="timed runs of the plain FP64 walk on the same job (0: none)")
+    ap.add_argument("--scaling", default="strong", choices=["strong", "weak"],
+                    help="batch under several ranks: split the one job (strong) or walk it per rank (weak)")
+    ap.add_argument("--no-error", action="store_true", help="skip the D/K error against the FP64 replay")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip the reference's own CUDA programs beside rms_main")
+    ap.add_argument("--refcuda-walkers", type=int, default=1_000_000,
+                    help="walkers of the reference-CUDA comparison (64x64x512 axon, 5000 steps)")
     ap.add_argument("--tn", type=int, default=None, help="steps per walk (smaller case, e.g. for ncu)")
     ap.add_argument("--timepoints", type=int, default=None,
                     help="records per walk (keep steps/record when shortening the walk)")

@@ -86,9 +86,13 @@ def _dp(a: np.ndarray):
 
 
 def reference_tables(dt: float, res: float, diffusivity, t2, timepoints: int = 1000,
-                     tn: Optional[int] = None):
+                     tn: Optional[int] = None, kappa: Optional[float] = None):
     """Derived tables exactly as hpc_code/lib/main.cu:421-458, 484-487 computes
-    them: step (voxels), T2/dt, Pij, TD."""
+    them: step (voxels), T2/dt, Pij, TD.  With ``kappa`` (um/ms) the
+    permeation probability between two labelled compartments follows the
+    membrane permeability instead: the 3-D rule of analysis/interaction.m:
+    437-439, P = (2/3) kappa ds / D_i with ds = sqrt(6 D_i dt), used as
+    P / (1 + P) (the library's RMS_PERM_KAPPA)."""
     d = [float(x) for x in diffusivity]
     nc = len(d)
     step = np.array([math.sqrt(6.0 * dt * x) / res for x in d])
@@ -100,6 +104,10 @@ def reference_tables(dt: float, res: float, diffusivity, t2, timepoints: int = 1
                 pij[i * nc + j] = 0.0
             elif i == j:
                 pij[i * nc + j] = 1.0
+            elif kappa is not None:
+                ds = math.sqrt(6.0 * d[i] * dt)
+                P = 2.0 / 3.0 * float(kappa) * ds / d[i] if d[i] > 0.0 else 0.0
+                pij[i * nc + j] = P / (1.0 + P)
             else:
                 pij[i * nc + j] = min(1.0, math.sqrt(d[j] / d[i]))
     td = None

@@ -61,3 +61,28 @@ def test_contraction_of_one_walker_and_one_waveform():
         torch.cuda.synchronize()
         engine.contract_phases(d_pos.data_ptr(), 1, 8, d_wave.data_ptr(), 1, out.data_ptr(), method=method)
         assert np.abs(out.cpu().numpy() - want).max() < tol, method
+
+
+def test_trace_and_metrics_lines(tmp_path):
+    """RMS_TRACE prints one phase line per launch on stderr, and
+    rms_main --metrics one JSON line of throughput; stdout keeps the
+    reference's lines and the outputs are the reference program's."""
+    import json
+    import os
+    import subprocess
+    from conftest import golden_seed, unpack_golden
+    from rms_b200 import runio
+    d = unpack_golden("narrow_3comp", str(tmp_path / "run"), inputs_only=True)
+    want = runio.read_outputs(unpack_golden("narrow_3comp", str(tmp_path / "want")))
+    env = dict(os.environ, RMS_TRACE="1")
+    r = subprocess.run([engine.CLI_PATH, "--seed", str(golden_seed("narrow_3comp")), "--metrics"], cwd=d, env=env,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "Done! Elpased time" in r.stdout and "rms trace" not in r.stdout
+    trace = [ln for ln in r.stderr.splitlines() if ln.startswith("rms trace: compat 1 sim(s)")]
+    assert len(trace) == 1 and "kernels: walk" in trace[0], r.stderr
+    m = json.loads([ln for ln in r.stderr.splitlines() if ln.startswith("{")][-1])
+    assert m["walker_steps"] == 64 * 1000 and m["precision"] == "compat"
+    assert m["walk_ms"] > 0 and m["walker_steps_per_s_walk"] > 0 and m["wall_ms"] >= m["run_ms"] > 0
+    got = runio.read_outputs(d)
+    assert np.array_equal(got.npar_count, want.npar_count)

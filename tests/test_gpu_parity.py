@@ -160,10 +160,15 @@ def test_rerun_is_bitwise_repeatable():
         assert np.array_equal(a[k], b[k]), k
 
 
-@pytest.mark.parametrize("case", ["narrow_3comp", "pgse_3comp"])
+@pytest.mark.parametrize("case", ["narrow_3comp", "pgse_3comp", "realistic_mito_1", "realistic_undulation_pgse"])
 def test_matches_reference_program_outputs(case, tmp_path):
     """The golden run directories hold the reference program's own output
-    files (hpc_code/lib/main*.cu run on the host with the same seed)."""
+    files (hpc_code/lib/main*.cu run on the host with the same seed).  The
+    realistic cases walk the reference's own axons: realistic_mito_1 (its
+    first mitochondria axon, 0.2 % of the voxels labelled -- rejection-sampled
+    starts take ~480 tries, main.cu:117-125 -- and partial permeation into the
+    mitochondria, P = 0.258, main.cu:274-289) and realistic_undulation_pgse
+    (its first undulating axon under five PGSE gradients, main_PGSE.cu)."""
     d = unpack_golden(case, str(tmp_path / "run"), inputs_only=True)
     want_dir = unpack_golden(case, str(tmp_path / "want"))
     sim = engine.Sim.from_dir(d).run(seed=golden_seed(case))
