@@ -378,15 +378,23 @@ int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint
  *   d_t2[c]                dL/dT2_c (ms), analytic through s0
  *   d_kappa                dL/dkappa, score function of the permeation
  *                          draws (RMS_PERM_KAPPA with kappa > 0, else 0)
- *   d_diffusivity          dL/dD, pathwise through the step length with the
- *                          event sequence fixed, plus the score through the
- *                          kappa-mode permeation probability; the T2 weight's
- *                          dependence on D (through residence times) is not
- *                          included: it vanishes when T2 is equal across
- *                          compartments.  With mirror walls the walk's
- *                          displacement jumps when a walker meets a wall (the
- *                          origin image is mirrored, main.cu:302-310), which
- *                          this term does not see: use periodic walls
+ *   d_diffusivity          dL/dD by time rescaling: a walk with D(1 + eps)
+ *                          and kappa(1 + eps) over [0, T] is, in law, the
+ *                          D-walk over [0, T(1 + eps)], so D dL/dD is the
+ *                          derivative of the walk stretched in time (phases
+ *                          through the waveform's bin edges, the T2 weight
+ *                          through the final compartment) minus kappa dL/dkappa.
+ *                          It includes the jumps of the walk's output at
+ *                          voxel corners, mirror walls and changed permeation
+ *                          draws; it is exact for the continuum process and
+ *                          carries the walk's time-discretisation error
+ *   d_diffusivity_pathwise dL/dD through the step length with the event
+ *                          sequence fixed (plus the score through the
+ *                          kappa-mode permeation probability): low variance,
+ *                          exact where the walk is continuous in the step
+ *                          length (flat membranes, periodic walls), blind to
+ *                          the jumps above; the T2 weight's dependence on D
+ *                          through residence times is not included
  * Each walker is walked twice from its random streams (nothing stored).
  * d_wave (caller-allocated host array) and sigw (optional, [nwave*2], the
  * run's own signal sums) may be NULL. */
@@ -397,6 +405,7 @@ typedef struct rms_adjoint_grads {
     double d_t2[8];
     double loss;
     double* sigw;
+    double d_diffusivity_pathwise;
 } rms_adjoint_grads;
 int rms_adjoint_run(rms_sim* sim, const rms_run_opts* opts, const double* g_sigw, rms_adjoint_grads* out);
 

@@ -7,9 +7,9 @@ labelled compartment), the membrane permeability kappa and the per-compartment
 T2.  The forward pass is the split walk (rms_sim_run); the backward pass walks
 the same walkers again from their counter-based random streams
 (rms_adjoint_run) instead of storing trajectories.  Gradients: exact pathwise
-for the waveforms, analytic for T2, pathwise with the event sequence fixed
-plus the permeation score for D, score function for kappa.  torch is the
-plumbing here; all arithmetic runs in librms.
+for the waveforms, analytic for T2, time rescaling (minus the kappa term) for
+D, score function for kappa.  torch is the plumbing here; all arithmetic runs
+in librms.
 """
 from __future__ import annotations
 

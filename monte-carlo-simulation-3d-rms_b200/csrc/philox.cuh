@@ -59,7 +59,14 @@ RMS_HD double u53_to_double(uint32_t lo, uint32_t hi) {
 }
 
 RMS_HD float u32_to_float(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    // the same value from the bits: 1 + k 2^-23 (k = x >> 9) minus
+    // (1 - 2^-24) is (2k + 1) 2^-24, and the subtraction is exact (Sterbenz:
+    // both operands lie within a factor of two of each other)
+    return __uint_as_float(0x3f800000u | (x >> 9)) - (1.0f - 0x1p-24f);
+#else
     return (float)(2u * (x >> 9) + 1u) * 0x1p-24f;
+#endif
 }
 
 // Walker stream drawing doubles: holds the unread half of the last block in

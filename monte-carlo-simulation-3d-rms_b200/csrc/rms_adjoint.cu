@@ -24,16 +24,26 @@
 // The host turns the sums into dL/dwave, dL/dT2_c (analytic), dL/dkappa
 // (score function: dP/dkappa = P/kappa, with the walkers' mean loss as the
 // baseline -- sum_w (L_w - mean L) E_w, unbiased since E[E_w] = 0, and far
-// less noisy than sum_w L_w E_w) and dL/dD (pathwise via dl/dD = l/(2D), plus
-// the score through dP/dD = -P/(2D)).  The walk itself is
-// the split walk's step for step (same streams, same arithmetic), so the
-// gradients belong to the function the forward run evaluates.
+// less noisy than sum_w L_w E_w) and dL/dD.  dL/dD comes from time rescaling:
+// a walk with diffusivity D(1 + eps) (and permeability kappa(1 + eps)) over
+// [0, T] is, in law, the D-walk over [0, T(1 + eps)], so with x(t) the
+// displacement, g_j the piecewise-constant waveform and W the T2 exponent
+//   dphi_j/deps = -phi_j + sum_b t_b+1 (g_j,b - g_j,b+1) . x(t_b+1)  (g_j,nbins = 0)
+//   dW/deps     = -W + T / T2(c_T)
+// and D dL/dD = sum_w dL_w/deps - kappa dL/dkappa.  It sees the jumps of the
+// walk at voxel corners, mirror walls and changed permeation draws, which the
+// pathwise derivative through the step length (events frozen, also summed)
+// does not; it is exact for the continuum process and carries the walk's
+// time-discretisation error.  Both passes walk the split walk's step
+// (split_step.cuh: same streams, same arithmetic), so the gradients belong to
+// the function the forward run evaluates.
 #include <cuda_runtime.h>
 #include <math.h>
 
 #include "philox.cuh"
 #include "rms_internal.h"
 #include "split_lattice.cuh"
+#include "split_step.cuh"
 #include "warp_reduce.cuh"
 
 namespace rms {
@@ -57,6 +67,31 @@ __device__ __forceinline__ float warp_reduce_scatter16f(float (&v)[16], int lane
     return v[0];
 }
 
+// What pass 1 records during a step (split_step's hooks): the path per
+// compartment, the displacement's tangent with respect to the step length
+// (flipped at every reflection) and the permeation score.
+template <int NC>
+struct AdjHooks {
+    bool rec;             // pass 1 records; pass 2 only walks
+    float tc[NC];         // path per compartment (voxels)
+    float T0, T1, T2;     // d(displacement)/dl, voxels per voxel of step
+    float E;              // sum over Bernoulli draws of 1[crossed] - Pij
+    __device__ __forceinline__ void path(int c, float len) {
+        if (rec) {
+#pragma unroll
+            for (int k = 0; k < NC; ++k) tc[k] += (c == k) ? len : 0.0f;
+        }
+    }
+    __device__ __forceinline__ void reflect(int axis) {
+        if (rec) {
+            if (axis == 0) T0 = -T0; else if (axis == 1) T1 = -T1; else T2 = -T2;
+        }
+    }
+    __device__ __forceinline__ void bernoulli(bool cross, float P) {
+        if (rec) E += (cross ? 1.0f : 0.0f) - P;   // d log p / d log P
+    }
+};
+
 __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constant__ AdjArgs a) {
     constexpr int NC = kAdjNc, BITS = 4, NW = kAdjWaves;
     constexpr int kTab = 2 * NC + 2 * NC * NC;
@@ -75,7 +110,6 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
     const int warp_global = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
     const bool mirror = (a.boundary == 0);
-    constexpr int kWall = wall_code<BITS>();
     const uint32_t key0 = (uint32_t)a.seed, key1 = (uint32_t)(a.seed >> 32);
     const uint8_t* lat = a.lat;
     const int s0 = a.s0, s1 = a.s1;
@@ -84,13 +118,15 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
         const int64_t w = a.walker_begin + tile * 32 + lane;
         const bool live = w < a.walker_end;
         const uint32_t wlo = (uint32_t)w, whi = (uint32_t)((uint64_t)w >> 32);
-        float phi[NW], dphi[NW], aj[NW], tc[NC];
+        float phi[NW], dphi[NW], aj[NW];
 #pragma unroll
         for (int j = 0; j < NW; ++j) phi[j] = dphi[j] = aj[j] = 0.0f;
+        AdjHooks<NC> h;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) tc[c] = 0.0f;
-        float E = 0.0f;
+        for (int c = 0; c < NC; ++c) h.tc[c] = 0.0f;
+        h.E = 0.0f;
         double w64 = 0.0;
+        float tr = 0.0f;   // this walker's time-rescaling derivative dL_w/d(eps)
 
         for (int pass = 0; pass < 2; ++pass) {
             // start position: uniform in the labelled voxels (the split walk's draws)
@@ -112,19 +148,17 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                     if (++tries >= kInitTryCap) { atomicOr(a.err, kErrInitCap); active = false; break; }
                 }
             }
-            int ai = active ? label_at<BITS>(lat, lin) : 0;
-            float cur_step = t_step[ai], cur_k = t_k[ai];
-            int D0 = 0, D1 = 0, D2 = 0;
-            float Fm0 = f0, Fm1 = f1, Fm2 = f2;
-            float d0 = f0, d1 = f1, d2 = f2;
-            unsigned up = 0u;
+            const int ai0 = active ? label_at<BITS>(lat, lin) : 0;
+            SplitWalker wk{lin, 0u, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0, t_step[ai0], t_k[ai0], 0.0f};
+            const SplitGeom geo{lat, s0, s1, a.nite, (bool)a.flight, (bool)a.same_cross, mirror};
+            auto nsize = [&](int axis) { return axis == 0 ? a.n1 : (axis == 1 ? a.n2 : a.n3); };
             DomainStream perm;
             perm.init(a.seed, (uint64_t)w, kDomPerm);
             w64 = 0.0;
-            float w32 = 0.0f;
             double P0 = 0.0, P1 = 0.0, P2 = 0.0;     // bin displacement sums (voxels), folded
             float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f;
-            float T0 = 0.0f, T1 = 0.0f, T2 = 0.0f;  // d(displacement)/dl (voxels per voxel of step)
+            h.T0 = h.T1 = h.T2 = 0.0f;
+            h.rec = (pass == 0);
             float B0 = 0.0f, B1 = 0.0f, B2 = 0.0f;  // bin sums of the tangent
             int bin = 0, next_bin = a.bin_steps;
             uint32_t spare_u1 = 0u, spare_u2 = 0u;
@@ -139,139 +173,24 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                     r1 = spare_u1; r2 = spare_u2;
                 }
                 if (active) {
-                    const float u1 = u32_to_float(r1), u2 = u32_to_float(r2);
-                    const float cz = 1.0f - 2.0f * u1;
-                    const float s2 = u1 * (1.0f - u1);
-                    const float sz = 2.0f * s2 * rsqrtf(s2);
-                    float sp, cp;
-                    __sincosf(6.283185307179586f * (u2 - 0.5f), &sp, &cp);
-                    const float v0 = sz * cp, v1 = sz * sp, v2 = cz;
-                    if (p1st) { T0 += v0; T1 += v1; T2 += v2; }
-                    const unsigned nu = (v0 > 0.0f ? 1u : 0u) | (v1 > 0.0f ? 2u : 0u) | (v2 > 0.0f ? 4u : 0u);
-                    if (a.flight && (cell_at<BITS>(lat, lin) & flight_bit<BITS>())) {
-                        const float x0 = fmaf(cur_step, v0, (up & 1u) ? 1.0f - d0 : d0);
-                        const float x1 = fmaf(cur_step, v1, (up & 2u) ? 1.0f - d1 : d1);
-                        const float x2 = fmaf(cur_step, v2, (up & 4u) ? 1.0f - d2 : d2);
-                        const float k0 = floorf(x0), k1 = floorf(x1), k2 = floorf(x2);
-                        const int ik0 = (int)k0, ik1 = (int)k1, ik2 = (int)k2;
-                        const float o0n = x0 - k0, o1n = x1 - k1, o2n = x2 - k2;
-                        lin += (unsigned)(ik0 * s0 + ik1 * s1 + ik2);
-                        D0 += ik0; D1 += ik1; D2 += ik2;
-                        w32 = fmaf(cur_step, cur_k, w32);
-                        if (p1st) {
-#pragma unroll
-                            for (int c = 0; c < NC; ++c) tc[c] += (ai == c) ? cur_step : 0.0f;
-                        }
-                        d0 = (nu & 1u) ? 1.0f - o0n : o0n;
-                        d1 = (nu & 2u) ? 1.0f - o1n : o1n;
-                        d2 = (nu & 4u) ? 1.0f - o2n : o2n;
-                        up = nu;
-                    } else {
-                        const unsigned turn = nu ^ up;
-                        if (turn & 1u) d0 = 1.0f - d0;
-                        if (turn & 2u) d1 = 1.0f - d1;
-                        if (turn & 4u) d2 = 1.0f - d2;
-                        up = nu;
-                        const float av0 = fabsf(v0), av1 = fabsf(v1), av2 = fabsf(v2);
-                        const float iv0 = __fdividef(1.0f, av0), iv1 = __fdividef(1.0f, av1), iv2 = __fdividef(1.0f, av2);
-                        int dl0 = (up & 1u) ? s0 : -s0;
-                        int dl1 = (up & 2u) ? s1 : -s1;
-                        int dl2 = (up & 4u) ? 1 : -1;
-                        float rem = cur_step;
-                        for (int j = 0; j < a.nite; ++j) {
-                            const float t0 = d0 * iv0, t1 = d1 * iv1, t2 = d2 * iv2;
-                            const float tm = fminf(t0, fminf(t1, t2));
-                            if (rem < tm) {
-                                d0 = fmaf(-rem, av0, d0); d1 = fmaf(-rem, av1, d1); d2 = fmaf(-rem, av2, d2);
-                                w32 = fmaf(rem, cur_k, w32);
-                                if (p1st) {
-#pragma unroll
-                                    for (int c = 0; c < NC; ++c) tc[c] += (ai == c) ? rem : 0.0f;
-                                }
-                                rem = 0.0f;
-                                break;
-                            }
-                            const int hit = (t0 == tm) ? 0 : ((t1 == tm) ? 1 : 2);
-                            const float tcs = fmaxf(tm, 0.0f);
-                            d0 = fmaf(-tcs, av0, d0); d1 = fmaf(-tcs, av1, d1); d2 = fmaf(-tcs, av2, d2);
-                            w32 = fmaf(tcs, cur_k, w32);
-                            if (p1st) {
-#pragma unroll
-                                for (int c = 0; c < NC; ++c) tc[c] += (ai == c) ? tcs : 0.0f;
-                            }
-                            rem -= tcs;
-                            const int dl = hit == 0 ? dl0 : (hit == 1 ? dl1 : dl2);
-                            unsigned lj = lin + (unsigned)dl;
-                            int aj2 = label_at<BITS>(lat, lj);
-                            bool cross;
-                            if (aj2 == ai && a.same_cross) {
-                                cross = true;
-                            } else {
-                                if (aj2 == kWall) {
-                                    const bool hi = (up >> hit) & 1u;
-                                    const int nh = hit == 0 ? a.n1 : (hit == 1 ? a.n2 : a.n3);
-                                    if (mirror) {
-                                        const int g = hi ? nh - 1 : 0;
-                                        if (hit == 0) { int I = g - D0; mirror_origin(I, Fm0, hi, nh); D0 = g - I; }
-                                        else if (hit == 1) { int I = g - D1; mirror_origin(I, Fm1, hi, nh); D1 = g - I; }
-                                        else { int I = g - D2; mirror_origin(I, Fm2, hi, nh); D2 = g - I; }
-                                        aj2 = -1;
-                                    } else {
-                                        const int sh = hit == 0 ? s0 : (hit == 1 ? s1 : 1);
-                                        lj = hi ? lin - (unsigned)(nh - 1) * (unsigned)sh
-                                                : lin + (unsigned)(nh - 1) * (unsigned)sh;
-                                        aj2 = label_at<BITS>(lat, lj);
-                                    }
-                                }
-                                if (aj2 < 0) {
-                                    cross = false;
-                                } else {
-                                    const float P = t_pij[ai * NC + aj2];
-                                    if (P > 0.999999f) {
-                                        cross = true;
-                                    } else if (P >= 0.000001f) {
-                                        cross = perm.next() < P;
-                                        if (p1st) E += (cross ? 1.0f : 0.0f) - P;   // d log p / d log P
-                                    } else {
-                                        cross = false;
-                                    }
-                                }
-                            }
-                            if (cross) {
-                                if (aj2 != ai) {
-                                    rem *= t_ratio[ai * NC + aj2];
-                                    cur_step = t_step[aj2];
-                                    cur_k = t_k[aj2];
-                                    ai = aj2;
-                                }
-                                lin = lj;
-                                const int du = ((up >> hit) & 1u) ? 1 : -1;
-                                if (hit == 0) D0 += du; else if (hit == 1) D1 += du; else D2 += du;
-                            } else {
-                                up ^= 1u << hit;
-                                if (hit == 0) dl0 = -dl0; else if (hit == 1) dl1 = -dl1; else dl2 = -dl2;
-                                if (p1st) {   // a reflection flips the tangent's component
-                                    if (hit == 0) T0 = -T0; else if (hit == 1) T1 = -T1; else T2 = -T2;
-                                }
-                            }
-                            if (hit == 0) d0 = 1.0f; else if (hit == 1) d1 = 1.0f; else d2 = 1.0f;
-                            if (!(rem > 0.0f)) break;
-                        }
-                    }
+                    float v0, v1, v2;
+                    split_direction(u32_to_float(r1), u32_to_float(r2), v0, v1, v2);
+                    if (p1st) { h.T0 += v0; h.T1 += v1; h.T2 += v2; }
+                    split_step<NC, BITS, 0>(wk, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio, perm, nsize, h);
                 }
-                const float o0 = (up & 1u) ? 1.0f - d0 : d0;
-                const float o1 = (up & 2u) ? 1.0f - d1 : d1;
-                const float o2 = (up & 4u) ? 1.0f - d2 : d2;
+                const float o0 = wk.o0(), o1 = wk.o1(), o2 = wk.o2();
+                const int D0 = wk.D0, D1 = wk.D1, D2 = wk.D2;
+                const float Fm0 = wk.Fm0, Fm1 = wk.Fm1, Fm2 = wk.Fm2;
                 p0 += (float)D0 + (o0 - Fm0);
                 p1 += (float)D1 + (o1 - Fm1);
                 p2 += (float)D2 + (o2 - Fm2);
-                if (p1st) { B0 += T0; B1 += T1; B2 += T2; }
+                if (p1st) { B0 += h.T0; B1 += h.T1; B2 += h.T2; }
                 const bool event = (i + 1 == next_bin);
                 if (event || (i & 31) == 31) {
                     P0 += (double)p0; P1 += (double)p1; P2 += (double)p2;
                     p0 = p1 = p2 = 0.0f;
-                    w64 += (double)w32;
-                    w32 = 0.0f;
+                    w64 += (double)wk.w32;
+                    wk.w32 = 0.0f;
                 }
                 if (event) {
                     const double x0 = P0 * (double)a.res, x1 = P1 * (double)a.res, x2 = P2 * (double)a.res;
@@ -287,6 +206,22 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                         }
                         B0 = B1 = B2 = 0.0f;
                     } else {
+                        // time rescaling: at the end of bin b (time t = (b + 1) bin_steps dt)
+                        // sum_j a_jw t (g_j,b - g_j,b+1) . x(t), g_j,nbins = 0
+                        const float xe0 = ((float)D0 + (o0 - Fm0)) * a.res, xe1 = ((float)D1 + (o1 - Fm1)) * a.res,
+                                    xe2 = ((float)D2 + (o2 - Fm2)) * a.res;
+                        const float tb = (float)(i + 1);   // steps (the waveform table carries dt)
+                        const double* wn = wv + a.nwave * 3;
+                        const bool last = bin + 1 >= a.nbins;
+#pragma unroll
+                        for (int j = 0; j < NW; ++j) {
+                            if (j < a.nwave) {
+                                const float q0 = (float)(__ldg(wv + 3 * j) - (last ? 0.0 : __ldg(wn + 3 * j)));
+                                const float q1 = (float)(__ldg(wv + 3 * j + 1) - (last ? 0.0 : __ldg(wn + 3 * j + 1)));
+                                const float q2 = (float)(__ldg(wv + 3 * j + 2) - (last ? 0.0 : __ldg(wn + 3 * j + 2)));
+                                tr = fmaf(aj[j] * tb, q0 * xe0 + q1 * xe1 + q2 * xe2, tr);
+                            }
+                        }
                         // dL/dwave[bin][j] += a_jw X_wb, summed over the warp's walkers
                         const float xs[3] = {(float)x0, (float)x1, (float)x2};
 #pragma unroll
@@ -303,7 +238,8 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                     next_bin += a.bin_steps;
                 }
             }
-            w64 += (double)w32;
+            w64 += (double)wk.w32;
+            wk.w32 = 0.0f;
 
             if (p1st) {
                 // this walker's loss, its derivatives, and the forward signal
@@ -320,14 +256,17 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                     Lw += s0w * (gc * cs + gs * sn);
                     aj[j] = s0w * (gs * cs - gc * sn);
                     G += aj[j] * dphi[j];
+                    tr -= aj[j] * phi[j];
                     const double C = warp_sum((double)(s0w * cs)), S = warp_sum((double)(s0w * sn));
                     if (lane == 0 && j < a.nwave) {
                         atomicAdd(a.sums + kAdjSumSig + 2 * j, C);
                         atomicAdd(a.sums + kAdjSumSig + 2 * j + 1, S);
                     }
                 }
-                const double L = warp_sum((double)Lw), LE = warp_sum((double)Lw * (double)E),
-                             GP = warp_sum((double)G), ES = warp_sum(active ? (double)E : 0.0);
+                // the T2 weight under time rescaling: dW/d(eps) = -W + T / T2(c_T)
+                tr += Lw * (float)(w64 - (double)a.tn * (double)(t_step[wk.ai] * t_k[wk.ai]));
+                const double L = warp_sum((double)Lw), LE = warp_sum((double)Lw * (double)h.E),
+                             GP = warp_sum((double)G), ES = warp_sum(active ? (double)h.E : 0.0);
                 if (lane == 0) {
                     atomicAdd(a.sums + kAdjSumL, L);
                     atomicAdd(a.sums + kAdjSumLE, LE);
@@ -338,9 +277,12 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                 for (int c = 0; c < NC; ++c) {
                     // residence time in steps: path in compartment c / its step length
                     const float st = t_step[c];
-                    const double LT = warp_sum(st > 0.0f ? (double)Lw * (double)(tc[c] / st) : 0.0);
+                    const double LT = warp_sum(st > 0.0f ? (double)Lw * (double)(h.tc[c] / st) : 0.0);
                     if (lane == 0) atomicAdd(a.sums + kAdjSumLT + c, LT);
                 }
+            } else {
+                const double TR = warp_sum((double)tr);
+                if (lane == 0) atomicAdd(a.sums + kAdjSumTR, TR);
             }
         }
     }

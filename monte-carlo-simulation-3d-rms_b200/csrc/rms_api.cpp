@@ -1095,10 +1095,16 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
     // score of the permeation draws with the mean loss as baseline:
     // sum_w (L_w - L/N) E_w (E[E_w] = 0 keeps it unbiased)
     const double score = sums[kAdjSumLE] - sums[kAdjSumL] / (double)(w1 - w0) * sums[kAdjSumE];
-    // l = sqrt(6 D dt) / res: dl/dD = l / (2 D); in kappa mode P ~ kappa D^(-1/2)
+    // time rescaling: D dL/dD = sum_w dL_w/deps - kappa dL/dkappa.  In kappa mode
+    // kappa dL/dkappa is the score; with a fixed permeation probability the
+    // continuum permeability of the rescaled walk scales as (1 + eps)^(-1/2)
+    // relative to kappa (1 + eps), so half the score comes off.
     const bool kap = s->permeation == RMS_PERM_KAPPA;
+    out->d_diffusivity = (sums[kAdjSumTR] - (kap ? score : 0.5 * score)) / D;
+    // pathwise, events frozen: l = sqrt(6 D dt) / res, dl/dD = l / (2 D); in
+    // kappa mode P ~ kappa D^(-1/2)
     const double step = s->step[s->nc > 1 ? 1 : 0];
-    out->d_diffusivity = (sums[kAdjSumPath] * step / 2.0 - (kap ? score / 2.0 : 0.0)) / D;
+    out->d_diffusivity_pathwise = (sums[kAdjSumPath] * step / 2.0 - (kap ? score / 2.0 : 0.0)) / D;
     out->d_kappa = (kap && s->kappa > 0.0) ? score / s->kappa : 0.0;
     for (int c = 0; c < 8; ++c) out->d_t2[c] = 0.0;
     for (int c = 0; c < s->nc; ++c) {

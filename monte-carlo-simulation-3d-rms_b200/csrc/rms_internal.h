@@ -127,11 +127,11 @@ int build_tube_lattice(uint8_t* d_out, int n1, int n2, int n3, double res, const
 constexpr int kAdjWaves = 16;
 constexpr int kAdjNc = 4;
 // sums[]: sum_w L_w, sum_w L_w E_w, sum_w sum_j a_jw dphi_jw, sum_w L_w t_wc
-// (steps, per compartment), sum_w E_w, then the signal sums (cos, sin) per
-// waveform
+// (steps, per compartment), sum_w E_w, the signal sums (cos, sin) per
+// waveform, then sum_w dL_w/deps of the time rescaling (rms_adjoint.cu)
 constexpr int kAdjSumL = 0, kAdjSumLE = 1, kAdjSumPath = 2, kAdjSumLT = 3, kAdjSumE = 3 + kAdjNc,
-              kAdjSumSig = 4 + kAdjNc;
-constexpr int kAdjSums = kAdjSumSig + 2 * kAdjWaves;
+              kAdjSumSig = 4 + kAdjNc, kAdjSumTR = kAdjSumSig + 2 * kAdjWaves;
+constexpr int kAdjSums = kAdjSumTR + 1;
 struct AdjArgs {
     const uint8_t* lat;          // padded 4-bit lattice with free-flight flags
     int n1, n2, n3, s0, s1;

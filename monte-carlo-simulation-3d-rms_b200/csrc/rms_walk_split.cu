@@ -22,9 +22,8 @@
 //    the face loop's own outcome (every face on the way is a same-label face,
 //    always crossed) with at most three crossings, within the nite = 4 cap;
 //  - labels packed 4 bits per voxel (3-bit label, wall = 7, plus the flag;
-//    a padded 256x256x2048 lattice is 68 MB and stays in the 126 MB L2), one
-//    byte for Nc = 8, or 2 bits without flags (wall = 3) for the
-//    no-allocation walk;
+//    a padded 256x256x2048 lattice is 68 MB and stays in the 126 MB L2), or
+//    one byte for Nc = 8;
 //  - FP32 uniforms, one Philox4x32-10 block per two steps; hardware
 //    sine/cosine and reciprocal for the direction and face times;
 //  - per-walker sums that grow over the walk (T2 exponent, PGSE displacement
@@ -49,6 +48,7 @@
 #include "philox.cuh"
 #include "rms_internal.h"
 #include "split_lattice.cuh"
+#include "split_step.cuh"
 #include "warp_reduce.cuh"
 
 namespace rms {
@@ -153,7 +153,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     constexpr bool wave = (MODE == 2);
     constexpr bool sums = pgse || wave;   // displacement sums over the walk
     const bool mirror = (a.boundary == 0);
-    constexpr int kWall = wall_code<BITS>();
 
     // A warp keeps its rows for its current axon and, in the table form, adds
     // them into that axon's totals (FP64 atomics) when it moves on to another
@@ -212,7 +211,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         const uint8_t* lat = AXF(lat);
         const int s0 = AXF(s0), s1 = AXF(s1);
         const uint64_t seed = AXF(seed);   // a graph captures the table form, whose seed a replay rewrites
-        const bool flight = (BITS != 2) && AXF(flight);
+        const bool flight = AXF(flight);
         const bool same_certain = AXF(same_cross);
         const float* t_step = tab;
         const float* t_k = tab + NCMAX;
@@ -243,20 +242,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 if (++tries >= kInitTryCap) { atomicOr(a.err, kErrInitCap); active = false; break; }
             }
         }
-        int ai = active ? label_at<BITS>(lat, lin) : 0;
-        float cur_step = t_step[ai], cur_k = t_k[ai];
-        // displacement = D + (offset - Fm) per axis; offset = up ? 1 - d : d
-        int D0 = 0, D1 = 0, D2 = 0;
-        float Fm0 = f0, Fm1 = f1, Fm2 = f2;    // origin fractions (mirrored at walls)
-        float d0 = f0, d1 = f1, d2 = f2;       // as if travelling down
-        unsigned up = 0u;                      // bit a: travelling up along axis a
+        const int ai0 = active ? label_at<BITS>(lat, lin) : 0;
+        // displacement = D + (offset - Fm) per axis; the walker starts
+        // travelling down along every axis (d = offset)
+        SplitWalker wk{lin, 0u, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0, t_step[ai0], t_k[ai0], 0.0f};
+        const SplitGeom geo{lat, s0, s1, a.nite, flight, same_certain, mirror};
+        auto nsize = [&](int axis) { return axis == 0 ? AXF(n1) : (axis == 1 ? AXF(n2) : AXF(n3)); };
+        NoHooks hooks;
         DomainStream perm;
         perm.init(seed, (uint64_t)w, kDomPerm);
 
         double w64 = 0.0;          // T2 exponent, folded
-        float w32 = 0.0f;          // T2 exponent since the last fold
         double P0 = 0.0, P1 = 0.0, P2 = 0.0;   // displacement sums (voxels), folded
         float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f;
+        int next_rec = 0, rec = 0;   // the next recorded step (0, tstep, 2 tstep, ...) and its record
         int evi = 0;   // next PGSE event, or current waveform bin
         int next_ev = pgse ? (a.nevents > 0 ? a.ev_step[0] : -1) : (wave ? a.bin_steps : -1);
         if (sums)
@@ -275,141 +274,30 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
             if (active) {
                 float u1 = u32_to_float(r1), u2 = u32_to_float(r2);
                 // RULE != 0: the step's start, restored when a membrane turns the step back
-                unsigned sv_lin = lin, sv_up = up;
-                float sv_d0 = d0, sv_d1 = d1, sv_d2 = d2, sv_w32 = w32, sv_F0 = Fm0, sv_F1 = Fm1, sv_F2 = Fm2;
-                float sv_step = cur_step, sv_k = cur_k;
-                int sv_D0 = D0, sv_D1 = D1, sv_D2 = D2, sv_ai = ai;
+                const SplitWalker start = wk;
                 for (int attempt = 0;; ++attempt) {
-                bool turned_back = false;
-                const float cz = 1.0f - 2.0f * u1;
-                const float s2 = u1 * (1.0f - u1);
-                const float sz = 2.0f * s2 * rsqrtf(s2);
-                float sp, cp;
-                // azimuth 2 pi (u2 - 1/2): uniform on [-pi, pi), within the
-                // hardware sine/cosine's accurate range
-                __sincosf(6.283185307179586f * (u2 - 0.5f), &sp, &cp);
-                const float v0 = sz * cp, v1 = sz * sp, v2 = cz;
-                const unsigned nu = (v0 > 0.0f ? 1u : 0u) | (v1 > 0.0f ? 2u : 0u) | (v2 > 0.0f ? 4u : 0u);
-                if (flight && (cell_at<BITS>(lat, lin) & flight_bit<BITS>())) {
-                    // free flight: straight line, at most one voxel per axis
-                    const float x0 = fmaf(cur_step, v0, (up & 1u) ? 1.0f - d0 : d0);
-                    const float x1 = fmaf(cur_step, v1, (up & 2u) ? 1.0f - d1 : d1);
-                    const float x2 = fmaf(cur_step, v2, (up & 4u) ? 1.0f - d2 : d2);
-                    const float k0 = floorf(x0), k1 = floorf(x1), k2 = floorf(x2);
-                    const int ik0 = (int)k0, ik1 = (int)k1, ik2 = (int)k2;
-                    const float o0n = x0 - k0, o1n = x1 - k1, o2n = x2 - k2;
-                    lin += (unsigned)(ik0 * s0 + ik1 * s1 + ik2);
-                    D0 += ik0; D1 += ik1; D2 += ik2;
-                    w32 = fmaf(cur_step, cur_k, w32);
-                    d0 = (nu & 1u) ? 1.0f - o0n : o0n;
-                    d1 = (nu & 2u) ? 1.0f - o1n : o1n;
-                    d2 = (nu & 4u) ? 1.0f - o2n : o2n;
-                    up = nu;
-                } else {
-                const unsigned turn = nu ^ up;
-                if (turn & 1u) d0 = 1.0f - d0;
-                if (turn & 2u) d1 = 1.0f - d1;
-                if (turn & 4u) d2 = 1.0f - d2;
-                up = nu;
-                const float av0 = fabsf(v0), av1 = fabsf(v1), av2 = fabsf(v2);
-                const float iv0 = __fdividef(1.0f, av0), iv1 = __fdividef(1.0f, av1), iv2 = __fdividef(1.0f, av2);
-                // signed lattice step along each axis in the direction of travel
-                int dl0 = (up & 1u) ? s0 : -s0;
-                int dl1 = (up & 2u) ? s1 : -s1;
-                int dl2 = (up & 4u) ? 1 : -1;
-                float rem = cur_step;        // path left in this step, voxels
-                for (int j = 0; j < a.nite; ++j) {
-                    const float t0 = d0 * iv0, t1 = d1 * iv1, t2 = d2 * iv2;
-                    const float tm = fminf(t0, fminf(t1, t2));
-                    if (rem < tm) {
-                        // the step ends inside the voxel
-                        d0 = fmaf(-rem, av0, d0); d1 = fmaf(-rem, av1, d1); d2 = fmaf(-rem, av2, d2);
-                        w32 = fmaf(rem, cur_k, w32);
-                        rem = 0.0f;
+                    float v0, v1, v2;
+                    split_direction(u1, u2, v0, v1, v2);
+                    const bool back = split_step<NCMAX, BITS, RULE>(wk, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio,
+                                                                    perm, nsize, hooks);
+                    if (RULE == 0 || !back) break;
+                    // the step is taken back (interaction.m:256-345): rejection
+                    // sampling stays put for the step; the equal-step-length leap
+                    // redraws the direction (partial-permeation stream) and walks
+                    // the step again, up to kLeapCap tries, then stays
+                    wk = start;
+                    if (RULE == 1 || attempt + 1 >= kLeapCap) {
+                        wk.w32 = fmaf(wk.cur_step, wk.cur_k, wk.w32);   // the step's time passes in place
                         break;
                     }
-                    // onto the nearest face (lowest axis on ties, like the reference's scan)
-                    const int hit = (t0 == tm) ? 0 : ((t1 == tm) ? 1 : 2);
-                    const float tc = fmaxf(tm, 0.0f);
-                    d0 = fmaf(-tc, av0, d0); d1 = fmaf(-tc, av1, d1); d2 = fmaf(-tc, av2, d2);
-                    w32 = fmaf(tc, cur_k, w32);
-                    rem -= tc;
-                    const int dl = hit == 0 ? dl0 : (hit == 1 ? dl1 : dl2);
-                    unsigned lj = lin + (unsigned)dl;
-                    int aj = label_at<BITS>(lat, lj);
-                    bool cross;
-                    if (aj == ai && same_certain) {
-                        cross = true;
-                    } else {
-                        if (aj == kWall) {
-                            const bool hi = (up >> hit) & 1u;
-                            const int nh = hit == 0 ? AXF(n1) : (hit == 1 ? AXF(n2) : AXF(n3));
-                            if (mirror) {
-                                // mirror wall: reflect, and mirror the origin image
-                                const int g = hi ? nh - 1 : 0;
-                                if (hit == 0) { int I = g - D0; mirror_origin(I, Fm0, hi, nh); D0 = g - I; }
-                                else if (hit == 1) { int I = g - D1; mirror_origin(I, Fm1, hi, nh); D1 = g - I; }
-                                else { int I = g - D2; mirror_origin(I, Fm2, hi, nh); D2 = g - I; }
-                                aj = -1;   // reflect below
-                            } else {
-                                // periodic: the neighbour is on the far side; the
-                                // unfolded displacement just continues
-                                const int sh = hit == 0 ? s0 : (hit == 1 ? s1 : 1);
-                                lj = hi ? lin - (unsigned)(nh - 1) * (unsigned)sh
-                                        : lin + (unsigned)(nh - 1) * (unsigned)sh;
-                                aj = label_at<BITS>(lat, lj);
-                            }
-                        }
-                        if (aj < 0) {
-                            cross = false;
-                        } else {
-                            const float P = t_pij[ai * NCMAX + aj];
-                            cross = (P > 0.999999f) || (P >= 0.000001f && perm.next() < P);
-                            if (RULE != 0 && !cross) {
-                                turned_back = true;   // a membrane sends the walker back: the rule decides
-                                break;
-                            }
-                        }
-                    }
-                    if (cross) {
-                        if (aj != ai) {
-                            rem *= t_ratio[ai * NCMAX + aj];
-                            cur_step = t_step[aj];
-                            cur_k = t_k[aj];
-                            ai = aj;
-                        }
-                        lin = lj;
-                        const int du = ((up >> hit) & 1u) ? 1 : -1;
-                        if (hit == 0) D0 += du; else if (hit == 1) D1 += du; else D2 += du;
-                    } else {
-                        up ^= 1u << hit;
-                        if (hit == 0) dl0 = -dl0; else if (hit == 1) dl1 = -dl1; else dl2 = -dl2;
-                    }
-                    // on the face, a whole voxel ahead
-                    if (hit == 0) d0 = 1.0f; else if (hit == 1) d1 = 1.0f; else d2 = 1.0f;
-                    if (!(rem > 0.0f)) break;
-                }
-                }
-                if (RULE == 0 || !turned_back) break;
-                // the step is taken back (interaction.m:256-345): rejection
-                // sampling stays put for the step; the equal-step-length leap
-                // redraws the direction (partial-permeation stream) and walks
-                // the step again, up to kLeapCap tries, then stays
-                lin = sv_lin; up = sv_up; d0 = sv_d0; d1 = sv_d1; d2 = sv_d2; w32 = sv_w32;
-                Fm0 = sv_F0; Fm1 = sv_F1; Fm2 = sv_F2; D0 = sv_D0; D1 = sv_D1; D2 = sv_D2;
-                ai = sv_ai; cur_step = sv_step; cur_k = sv_k;
-                if (RULE == 1 || attempt + 1 >= kLeapCap) {
-                    w32 = fmaf(cur_step, cur_k, w32);   // the step's time passes in place
-                    break;
-                }
-                u1 = perm.next();
-                u2 = perm.next();
+                    u1 = perm.next();
+                    u2 = perm.next();
                 }
             }
             // in-voxel offsets of the current position
-            const float o0 = (up & 1u) ? 1.0f - d0 : d0;
-            const float o1 = (up & 2u) ? 1.0f - d1 : d1;
-            const float o2 = (up & 4u) ? 1.0f - d2 : d2;
+            const float o0 = wk.o0(), o1 = wk.o1(), o2 = wk.o2();
+            const int D0 = wk.D0, D1 = wk.D1, D2 = wk.D2;
+            const float Fm0 = wk.Fm0, Fm1 = wk.Fm1, Fm2 = wk.Fm2;
 
             if (sums) {
                 // displacement sums (voxels): PGSE, prefix sums read at the
@@ -440,10 +328,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     next_ev = (evi < a.nevents) ? a.ev_step[evi] : -1;
                 }
                 if (i == a.tn - 1 && wave) {
-                    wave_final(a.vscr + gtid, nthr, a.nwave, active ? exp(-(w64 + (double)w32)) : 0.0, sig_slot, lane);
+                    wave_final(a.vscr + gtid, nthr, a.nwave, active ? exp(-(w64 + (double)wk.w32)) : 0.0, sig_slot, lane);
                 } else if (i == a.tn - 1) {
                     // final T2-weighted signal: phase_j = |g| (g_hat . V) res dt
-                    const double s0 = active ? exp(-(w64 + (double)w32)) : 0.0;
+                    const double s0 = active ? exp(-(w64 + (double)wk.w32)) : 0.0;
                     const double scale = a.res * a.dt;
                     for (int base = 0; base < a.ngrad; base += 32) {
                         double mine = 0.0;
@@ -462,12 +350,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 }
             }
 
-            if ((i % a.tstep) == 0) {
-                const int tidx = i / a.tstep;
+            if (i == next_rec) {
+                const int tidx = rec++;
+                next_rec += a.tstep;
                 if (tidx < a.timepoints) {
-                    w64 += (double)w32;
-                    w32 = 0.0f;
-                    const float s0 = active ? (float)exp(-w64) : 0.0f;
+                    w64 += (double)wk.w32;
+                    wk.w32 = 0.0f;
+                    const float s0 = active ? expf(-(float)w64) : 0.0f;
                     const float res = AXF(res);
                     const float dx = ((float)D0 + (o0 - Fm0)) * res;
                     const float dy = ((float)D1 + (o1 - Fm1)) * res;
@@ -492,7 +381,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                         v[0] = szz * dx * dz;  v[1] = syy * yy;       v[2] = syy * dy * dz;
                         v[3] = syy * zz;       v[4] = szz * dy * dz;  v[5] = szz * zz;
 #pragma unroll
-                        for (int c = 0; c < 10; ++c) v[6 + c] = (active && ai == c) ? 1.0 : 0.0;
+                        for (int c = 0; c < 10; ++c) v[6 + c] = (active && wk.ai == c) ? 1.0 : 0.0;
                         const double rb = warp_reduce_scatter16(v, lane);
                         if (lane >= 16) r = rb;
                     }
@@ -546,7 +435,7 @@ __global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int 
                 const long i = (long)pi - 1, j = (long)pj - 1, kk = (long)pk - 1;
                 const unsigned lab = labels[((size_t)i * n2 + j) * (size_t)n3 + kk];
                 cell = lab & label_mask<BITS>();
-                if (BITS != 2 && i >= 1 && i + 1 < n1 && j >= 1 && j + 1 < n2 && kk >= 1 && kk + 1 < n3) {
+                if (i >= 1 && i + 1 < n1 && j >= 1 && j + 1 < n2 && kk >= 1 && kk + 1 < n3) {
                     bool same = true;
                     for (int di = -1; di <= 1 && same; ++di)
                         for (int dj = -1; dj <= 1 && same; ++dj)
@@ -639,8 +528,7 @@ int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits,
     const size_t nbytes = padded_lattice_bytes(n1, n2, n3, bits);
     size_t grid = (nbytes + 255) / 256;
     if (grid > 16384) grid = 16384;
-    if (bits == 2) pad_pack_kernel<2><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
-    else if (bits == 4) pad_pack_kernel<4><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
+    if (bits == 4) pad_pack_kernel<4><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
     else pad_pack_kernel<8><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
     return (int)cudaGetLastError();
 }

@@ -8,16 +8,15 @@ namespace rms {
 
 // Lattice cell: label in the low bits, free-flight flag in the top bit
 // (BITS = 4: 3 + 1 bits, two voxels per byte, voxel v in bits 4(v % 2);
-// BITS = 8: 7 + 1; BITS = 2: label only, voxel v in bits 2(v % 4)).
+// BITS = 8: 7 + 1).
 template <int BITS>
 __device__ __forceinline__ unsigned cell_at(const uint8_t* __restrict__ lat, unsigned lin) {
-    if (BITS == 2) return (__ldg(lat + (lin >> 2)) >> ((lin & 3u) * 2u)) & 3u;
     if (BITS == 4) return (__ldg(lat + (lin >> 1)) >> ((lin & 1u) * 4u)) & 15u;
     return __ldg(lat + lin);
 }
 
-template <int BITS> __host__ __device__ constexpr unsigned label_mask() { return BITS == 2 ? 3u : (BITS == 4 ? 7u : 127u); }
-template <int BITS> __host__ __device__ constexpr unsigned flight_bit() { return BITS == 2 ? 0u : (BITS == 4 ? 8u : 128u); }
+template <int BITS> __host__ __device__ constexpr unsigned label_mask() { return BITS == 4 ? 7u : 127u; }
+template <int BITS> __host__ __device__ constexpr unsigned flight_bit() { return BITS == 4 ? 8u : 128u; }
 
 template <int BITS>
 __device__ __forceinline__ int label_at(const uint8_t* __restrict__ lat, unsigned lin) {

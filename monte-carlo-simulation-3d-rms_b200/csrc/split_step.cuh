@@ -1,0 +1,223 @@
+// split_step.cuh -- one step of the split-precision walk.  The walk
+// (rms_walk_split.cu) and its adjoint (rms_adjoint.cu) both call split_step,
+// so the adjoint's trajectories are the forward walk's by construction; the
+// adjoint adds its bookkeeping through the Hooks argument.
+//
+// The step is the reference's (hpc_code/lib/main.cu:140-300): a fixed-length
+// step in an isotropic direction, split at voxel faces into at most nite
+// segments, each face crossed or reflected -- always crossed between voxels of
+// one label, reflected at compartment 0 and at mirror walls, Bernoulli(Pij)
+// otherwise -- in the split representation (voxel index + FP32 distances to
+// the next faces, see rms_walk_split.cu).
+#pragma once
+#include <cstdint>
+
+#include "philox.cuh"
+#include "split_lattice.cuh"
+
+namespace rms {
+
+// A walker between steps.
+struct SplitWalker {
+    unsigned lin;            // voxel: linear index into the padded lattice
+    unsigned up;             // bit a: travelling up along axis a
+    float d0, d1, d2;        // distance to the next face in the direction of travel (0..1)
+    int D0, D1, D2;          // integer part of the displacement: voxel - origin image
+    float Fm0, Fm1, Fm2;     // fractional part of the origin image (mirrored at walls)
+    int ai;                  // compartment (label)
+    float cur_step, cur_k;   // step length (voxels), T2 exponent per voxel of path
+    float w32;               // T2 exponent since the last fold
+
+    // in-voxel offset of the position along each axis
+    __device__ __forceinline__ float o0() const { return (up & 1u) ? 1.0f - d0 : d0; }
+    __device__ __forceinline__ float o1() const { return (up & 2u) ? 1.0f - d1 : d1; }
+    __device__ __forceinline__ float o2() const { return (up & 4u) ? 1.0f - d2 : d2; }
+};
+
+// What one step reads besides the walker: the padded lattice and its strides,
+// the sub-segment cap and the per-axon switches.
+struct SplitGeom {
+    const uint8_t* lat;
+    int s0, s1;              // padded strides of axes 0 and 1 (axis 2: 1)
+    int nite;
+    bool flight;             // straight moves allowed (same-label faces always crossed, nite >= 4)
+    bool same_certain;       // same-label faces are crossed without a draw
+    bool mirror;             // mirror walls (else periodic)
+};
+
+// The forward walk's hooks: nothing.  The adjoint's record the path per
+// compartment, flip the displacement tangent at reflections and score the
+// Bernoulli draws.
+struct NoHooks {
+    __device__ __forceinline__ void path(int, float) {}
+    __device__ __forceinline__ void reflect(int) {}
+    __device__ __forceinline__ void bernoulli(bool, float) {}
+};
+
+// One step of walker s in direction v (unit vector).  Tables: t_step[c],
+// t_k[c], t_pij[a * NCMAX + b], t_ratio[a * NCMAX + b] (step[b] / step[a]).
+// nsize(axis) gives the lattice size along an axis (read where needed so it
+// holds no registers).  Returns true when RULE != 0 and a membrane turned the
+// step back (the caller's rule decides); the walker is then mid-step.
+template <int NCMAX, int BITS, int RULE, class NSize, class Hooks>
+__device__ __forceinline__ bool split_step(SplitWalker& s, float v0, float v1, float v2, const SplitGeom& g,
+                                           const float* t_step, const float* t_k, const float* t_pij,
+                                           const float* t_ratio, DomainStream& perm, NSize nsize, Hooks& h) {
+    constexpr int kWall = wall_code<BITS>();
+    const uint8_t* __restrict__ lat = g.lat;
+    const int s0 = g.s0, s1 = g.s1;
+    const unsigned nu = (v0 > 0.0f ? 1u : 0u) | (v1 > 0.0f ? 2u : 0u) | (v2 > 0.0f ? 4u : 0u);
+    // The step as one straight line (at most one voxel per axis, step < 1
+    // voxel).  It is the face loop's own outcome whenever every voxel of the
+    // box the line spans -- the start voxel's neighbours across the faces it
+    // crosses, and their common edge/corner neighbours -- carries the walker's
+    // label: every face on the way is then a same-label face, always crossed,
+    // with at most three crossings (within nite = 4).  Voxels flagged for free
+    // flight (all 26 neighbours share the label) need no look; otherwise the
+    // box is checked, which settles most steps next to a membrane or a wall
+    // without the face loop.
+    bool straight = false;
+    int ik0 = 0, ik1 = 0, ik2 = 0;
+    float o0n = 0.0f, o1n = 0.0f, o2n = 0.0f;
+    if (g.flight) {
+        const float x0 = fmaf(s.cur_step, v0, s.o0());
+        const float x1 = fmaf(s.cur_step, v1, s.o1());
+        const float x2 = fmaf(s.cur_step, v2, s.o2());
+        const float k0 = floorf(x0), k1 = floorf(x1), k2 = floorf(x2);
+        ik0 = (int)k0; ik1 = (int)k1; ik2 = (int)k2;
+        o0n = x0 - k0; o1n = x1 - k1; o2n = x2 - k2;
+        straight = (cell_at<BITS>(lat, s.lin) & flight_bit<BITS>()) != 0u;
+        if (!straight) {
+            const int e0 = ik0 * s0, e1 = ik1 * s1, e2 = ik2;
+            const unsigned want = (unsigned)s.ai;
+            unsigned diff = 0u;   // nonzero: a box voxel with another label (or a wall)
+            if (e0) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)e0) ^ want;
+            if (e1) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)e1) ^ want;
+            if (e2) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)e2) ^ want;
+            if (!diff && (e0 != 0) + (e1 != 0) + (e2 != 0) >= 2) {
+                if (e0 && e1) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)(e0 + e1)) ^ want;
+                if (e0 && e2) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)(e0 + e2)) ^ want;
+                if (e1 && e2) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)(e1 + e2)) ^ want;
+                if (e0 && e1 && e2) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)(e0 + e1 + e2)) ^ want;
+            }
+            straight = diff == 0u;
+        }
+    }
+    if (straight) {
+        s.lin += (unsigned)(ik0 * s0 + ik1 * s1 + ik2);
+        s.D0 += ik0; s.D1 += ik1; s.D2 += ik2;
+        s.w32 = fmaf(s.cur_step, s.cur_k, s.w32);
+        h.path(s.ai, s.cur_step);
+        s.d0 = (nu & 1u) ? 1.0f - o0n : o0n;
+        s.d1 = (nu & 2u) ? 1.0f - o1n : o1n;
+        s.d2 = (nu & 4u) ? 1.0f - o2n : o2n;
+        s.up = nu;
+        return false;
+    }
+    // the face loop: up to nite segments, one face event each
+    const unsigned turn = nu ^ s.up;
+    if (turn & 1u) s.d0 = 1.0f - s.d0;
+    if (turn & 2u) s.d1 = 1.0f - s.d1;
+    if (turn & 4u) s.d2 = 1.0f - s.d2;
+    s.up = nu;
+    const float av0 = fabsf(v0), av1 = fabsf(v1), av2 = fabsf(v2);
+    const float iv0 = __fdividef(1.0f, av0), iv1 = __fdividef(1.0f, av1), iv2 = __fdividef(1.0f, av2);
+    // signed lattice step along each axis in the direction of travel
+    int dl0 = (s.up & 1u) ? s0 : -s0;
+    int dl1 = (s.up & 2u) ? s1 : -s1;
+    int dl2 = (s.up & 4u) ? 1 : -1;
+    float rem = s.cur_step;        // path left in this step, voxels
+    for (int j = 0; j < g.nite; ++j) {
+        const float t0 = s.d0 * iv0, t1 = s.d1 * iv1, t2 = s.d2 * iv2;
+        const float tm = fminf(t0, fminf(t1, t2));
+        if (rem < tm) {
+            // the step ends inside the voxel
+            s.d0 = fmaf(-rem, av0, s.d0); s.d1 = fmaf(-rem, av1, s.d1); s.d2 = fmaf(-rem, av2, s.d2);
+            s.w32 = fmaf(rem, s.cur_k, s.w32);
+            h.path(s.ai, rem);
+            rem = 0.0f;
+            break;
+        }
+        // onto the nearest face (lowest axis on ties, like the reference's scan)
+        const int hit = (t0 == tm) ? 0 : ((t1 == tm) ? 1 : 2);
+        const float tc = fmaxf(tm, 0.0f);
+        s.d0 = fmaf(-tc, av0, s.d0); s.d1 = fmaf(-tc, av1, s.d1); s.d2 = fmaf(-tc, av2, s.d2);
+        s.w32 = fmaf(tc, s.cur_k, s.w32);
+        h.path(s.ai, tc);
+        rem -= tc;
+        const int dl = hit == 0 ? dl0 : (hit == 1 ? dl1 : dl2);
+        unsigned lj = s.lin + (unsigned)dl;
+        int aj = label_at<BITS>(lat, lj);
+        bool cross;
+        if (aj == s.ai && g.same_certain) {
+            cross = true;
+        } else {
+            if (aj == kWall) {
+                const bool hi = (s.up >> hit) & 1u;
+                const int nh = nsize(hit);
+                if (g.mirror) {
+                    // mirror wall: reflect, and mirror the origin image
+                    const int gw = hi ? nh - 1 : 0;
+                    if (hit == 0) { int I = gw - s.D0; mirror_origin(I, s.Fm0, hi, nh); s.D0 = gw - I; }
+                    else if (hit == 1) { int I = gw - s.D1; mirror_origin(I, s.Fm1, hi, nh); s.D1 = gw - I; }
+                    else { int I = gw - s.D2; mirror_origin(I, s.Fm2, hi, nh); s.D2 = gw - I; }
+                    aj = -1;   // reflect below
+                } else {
+                    // periodic: the neighbour is on the far side; the
+                    // unfolded displacement just continues
+                    const int sh = hit == 0 ? s0 : (hit == 1 ? s1 : 1);
+                    lj = hi ? s.lin - (unsigned)(nh - 1) * (unsigned)sh : s.lin + (unsigned)(nh - 1) * (unsigned)sh;
+                    aj = label_at<BITS>(lat, lj);
+                }
+            }
+            if (aj < 0) {
+                cross = false;
+            } else {
+                const float P = t_pij[s.ai * NCMAX + aj];
+                if (P > 0.999999f) {
+                    cross = true;
+                } else if (P >= 0.000001f) {
+                    cross = perm.next() < P;
+                    h.bernoulli(cross, P);
+                } else {
+                    cross = false;
+                }
+                if (RULE != 0 && !cross) return true;   // a membrane sends the walker back: the rule decides
+            }
+        }
+        if (cross) {
+            if (aj != s.ai) {
+                rem *= t_ratio[s.ai * NCMAX + aj];
+                s.cur_step = t_step[aj];
+                s.cur_k = t_k[aj];
+                s.ai = aj;
+            }
+            s.lin = lj;
+            const int du = ((s.up >> hit) & 1u) ? 1 : -1;
+            if (hit == 0) s.D0 += du; else if (hit == 1) s.D1 += du; else s.D2 += du;
+        } else {
+            s.up ^= 1u << hit;
+            if (hit == 0) dl0 = -dl0; else if (hit == 1) dl1 = -dl1; else dl2 = -dl2;
+            h.reflect(hit);
+        }
+        // on the face, a whole voxel ahead
+        if (hit == 0) s.d0 = 1.0f; else if (hit == 1) s.d1 = 1.0f; else s.d2 = 1.0f;
+        if (!(rem > 0.0f)) break;
+    }
+    return false;
+}
+
+// The isotropic direction of a step from two uniforms (u1: cos of the polar
+// angle, u2: azimuth), in the split walk's FP32 arithmetic.
+__device__ __forceinline__ void split_direction(float u1, float u2, float& v0, float& v1, float& v2) {
+    const float cz = 1.0f - 2.0f * u1;
+    const float s2 = u1 * (1.0f - u1);
+    const float sz = 2.0f * s2 * rsqrtf(s2);
+    float sp, cp;
+    // azimuth 2 pi (u2 - 1/2): uniform on [-pi, pi), within the hardware
+    // sine/cosine's accurate range
+    __sincosf(6.283185307179586f * (u2 - 0.5f), &sp, &cp);
+    v0 = sz * cp; v1 = sz * sp; v2 = cz;
+}
+
+}  // namespace rms

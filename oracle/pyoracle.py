@@ -307,30 +307,35 @@ def adjoint_split(job: "Job", gup, w_begin: int = 0, w_end: Optional[int] = None
     if w_end is None:
         w_end = job.npar
     g = np.ascontiguousarray(np.asarray(gup, dtype=np.float64).reshape(-1))
-    sums = np.zeros(4 + job.nc + 2 * job.nwave)
+    sums = np.zeros(4 + job.nc + 2 * job.nwave + 1)
     dw = np.zeros(job.nbins * job.nwave * 3)
     p = job.params()
     rc = lib.or_adjoint_split(C.byref(p), _dp(g), C.c_int64(w_begin), C.c_int64(w_end), _dp(sums), _dp(dw))
     if rc != 0:
         raise RuntimeError(f"or_adjoint_split failed: {rc}")
-    nc = job.nc
+    nc, nw = job.nc, job.nwave
     return dict(L=sums[0], LE=sums[1], path=sums[2], E=sums[3], LT=sums[4:4 + nc].copy(),
-                sigw=sums[4 + nc:].reshape(-1, 2).copy(), dwave=dw.reshape(job.nbins, job.nwave, 3))
+                sigw=sums[4 + nc:4 + nc + 2 * nw].reshape(-1, 2).copy(), TR=sums[4 + nc + 2 * nw],
+                dwave=dw.reshape(job.nbins, job.nwave, 3))
 
 
 def adjoint_gradients(job: "Job", sums: dict, D: float, t2, kappa: Optional[float] = None, nwalk: Optional[int] = None):
     """The gradients the library's host code forms from the adjoint walker sums
     (monte-carlo-simulation-3d-rms_b200/csrc/rms_api.cpp, run_adjoint):
     dL/dwave = dt sum a X; the permeation score with the mean loss as baseline;
-    dL/dD = (path l / 2 - score / 2 [kappa mode]) / D (l = sqrt(6 D dt)/res);
-    dL/dkappa = score / kappa; dL/dT2_c = sum L t_c dt / T2_c^2."""
+    dL/dD by time rescaling, (TR - score [kappa mode] or TR - score / 2) / D;
+    the pathwise dL/dD = (path l / 2 - score / 2 [kappa mode]) / D
+    (l = sqrt(6 D dt)/res); dL/dkappa = score / kappa;
+    dL/dT2_c = sum L t_c dt / T2_c^2."""
     n = job.npar if nwalk is None else nwalk
     score = sums["LE"] - sums["L"] / n * sums["E"]
     step = float(job.step[1 if job.nc > 1 else 0])
     kap = kappa is not None
     d_wave = job.dt * np.transpose(sums["dwave"], (1, 0, 2))
-    d_D = (sums["path"] * step / 2.0 - (score / 2.0 if kap else 0.0)) / D
+    d_D = (sums["TR"] - (score if kap else 0.5 * score)) / D
+    d_D_path = (sums["path"] * step / 2.0 - (score / 2.0 if kap else 0.0)) / D
     d_kappa = score / kappa if kap and kappa > 0 else 0.0
     t2 = np.asarray(t2, dtype=np.float64)
     d_t2 = sums["LT"] * job.dt / t2 ** 2
-    return dict(d_wave=d_wave, d_diffusivity=d_D, d_kappa=d_kappa, d_t2=d_t2, loss=sums["L"])
+    return dict(d_wave=d_wave, d_diffusivity=d_D, d_diffusivity_pathwise=d_D_path, d_kappa=d_kappa, d_t2=d_t2,
+                loss=sums["L"])

@@ -278,6 +278,28 @@ static int homogeneous(const or_params* p, const int g[3]) {
     return 1;
 }
 
+/* The split walk's box check: a step whose straight line (at most one voxel
+ * per axis) stays in voxels of the walker's label -- every voxel of the box
+ * spanned by the start and end voxels inside the lattice and labelled ai --
+ * is walked as that straight line, the face loop's outcome when every face on
+ * the way is a same-label face (monte-carlo-simulation-3d-rms_b200/csrc/
+ * rms_walk_split.cu, the straight move). */
+static int box_same(const or_params* p, const int g[3], const double f[3], const double v[3], double rem, int ai) {
+    const int NPix[3] = {p->n1, p->n2, p->n3};
+    int k[3];
+    for (int a = 0; a < 3; a++) k[a] = (int)floor(f[a] + rem * v[a]);
+    for (int a = 0; a <= (k[0] != 0); a++)
+        for (int b = 0; b <= (k[1] != 0); b++)
+            for (int c = 0; c <= (k[2] != 0); c++) {
+                if (!a && !b && !c) continue;
+                const int q[3] = {g[0] + a * k[0], g[1] + b * k[1], g[2] + c * k[2]};
+                for (int e = 0; e < 3; e++)
+                    if (q[e] < 0 || q[e] >= NPix[e]) return 0;
+                if (p->labels[lin(p, q[0], q[1], q[2])] != ai) return 0;
+            }
+    return 1;
+}
+
 /* Adjoint bookkeeping of one walker (or_adjoint_split; the GPU kernel's
  * pass-1 quantities, restated in FP64): the tangent of the displacement with
  * respect to the step length l with the event sequence frozen (gains the step
@@ -289,6 +311,8 @@ typedef struct {
     double T[3], B[3], E, tc[8], wexp;
     double* dphi;   /* [nwave] */
     double* xbin;   /* [nbins*3], um */
+    double* rs;     /* [nwave]: sum over bin ends t (g_j,b - g_j,b+1) . x(t) (time rescaling) */
+    int ai_end;     /* compartment after the last step */
 } or_adj;
 
 static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, double* phase,
@@ -345,8 +369,8 @@ static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, doub
         rem = p->step[ai];
         flo = 0; fhi = 0; nev = 0;
         ev = 0;
-        if (flight && homogeneous(p, g)) {
-            /* a straight line within the homogeneous neighbourhood */
+        if (flight && (homogeneous(p, g) || box_same(p, g, f, v, rem, ai))) {
+            /* a straight line within voxels of the walker's label */
             for (int a = 0; a < 3; a++) {
                 const double x = f[a] + rem * v[a];
                 const double k = floor(x);
@@ -478,6 +502,14 @@ static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, doub
                 if (adj) {
                     for (int a = 0; a < 3; a++) adj->xbin[3 * b + a] = X[a];
                     adj->B[0] = adj->B[1] = adj->B[2] = 0.0;
+                    /* time rescaling: the waveform's step at this bin end, t = (b + 1) bin_steps dt */
+                    const double tb = (double)(i + 1) * p->dt;
+                    for (int j = 0; j < p->nwave; j++) {
+                        const double* wv = p->wave + ((size_t)j * p->nbins + b) * 3;
+                        const double* wn = b + 1 < p->nbins ? wv + 3 : NULL;
+                        adj->rs[j] += tb * ((wv[0] - (wn ? wn[0] : 0.0)) * dx + (wv[1] - (wn ? wn[1] : 0.0)) * dy +
+                                            (wv[2] - (wn ? wn[2] : 0.0)) * dz);
+                    }
                 }
                 if (tr_bin)
                     for (int a = 0; a < 3; a++) tr_bin[3 * b + a] = X[a] / (double)bin_steps;
@@ -516,7 +548,10 @@ static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, doub
             }
         }
     }
-    if (adj) adj->wexp = wexp;
+    if (adj) {
+        adj->wexp = wexp;
+        adj->ai_end = ai;
+    }
 }
 
 static void walk_one_split(const or_params* p, int64_t w, or_outputs* out, double* phase,
@@ -547,10 +582,11 @@ int or_adjoint_split(const or_params* p, const double* gup, int64_t w_begin, int
     double* phase = (double*)calloc((size_t)nw, sizeof(double));
     double* dphi = (double*)calloc((size_t)nw, sizeof(double));
     double* xbin = (double*)calloc((size_t)nb * 3, sizeof(double));
+    double* rs = (double*)calloc((size_t)nw + 1, sizeof(double));
     or_outputs scratch;
     double* sbuf = (double*)calloc((size_t)p->timepoints * (1 + 6 + 15 + nc) + 2 * (size_t)nw + 1, sizeof(double));
-    if (!phase || !dphi || !xbin || !sbuf) {
-        free(phase); free(dphi); free(xbin); free(sbuf);
+    if (!phase || !dphi || !xbin || !sbuf || !rs) {
+        free(phase); free(dphi); free(xbin); free(sbuf); free(rs);
         return -10;
     }
     scratch.sig0 = sbuf;
@@ -565,23 +601,29 @@ int or_adjoint_split(const or_params* p, const double* gup, int64_t w_begin, int
         memset(&adj, 0, sizeof adj);
         memset(phase, 0, sizeof(double) * (size_t)nw);
         memset(dphi, 0, sizeof(double) * (size_t)nw);
+        memset(rs, 0, sizeof(double) * (size_t)nw);
         adj.dphi = dphi;
         adj.xbin = xbin;
+        adj.rs = rs;
         walk_split_core(p, w, &scratch, phase, NULL, NULL, NULL, NULL, NULL, &adj);
         /* this walker's loss L_w = s0 sum_j (gC_j cos phi_j + gS_j sin phi_j)
          * and a_j = dL_w / dphi_j */
         const double s0 = exp(-adj.wexp);
-        double Lw = 0.0, G = 0.0;
+        double Lw = 0.0, G = 0.0, TR = 0.0;
         for (int j = 0; j < nw; j++) {
             const double c = cos(phase[j]), sn = sin(phase[j]);
             const double a = s0 * (gup[2 * j + 1] * c - gup[2 * j] * sn);
             Lw += s0 * (gup[2 * j] * c + gup[2 * j + 1] * sn);
             G += a * dphi[j];
+            TR += a * (rs[j] - phase[j]);   /* dphi_j / deps of the time rescaling */
             sums[4 + nc + 2 * j] += s0 * c;
             sums[4 + nc + 2 * j + 1] += s0 * sn;
             for (int b = 0; b < nb; b++)
                 for (int k = 0; k < 3; k++) dwave[((size_t)b * nw + j) * 3 + k] += a * xbin[3 * b + k];
         }
+        /* the T2 exponent under time rescaling: dW/deps = -W + T / T2(c_T) */
+        TR += Lw * (adj.wexp - (double)p->tn / p->t2[adj.ai_end]);
+        sums[4 + nc + 2 * nw] += TR;
         sums[0] += Lw;
         sums[1] += Lw * adj.E;
         sums[2] += G;
@@ -589,7 +631,7 @@ int or_adjoint_split(const or_params* p, const double* gup, int64_t w_begin, int
         for (int c = 0; c < nc; c++)
             if (p->step[c] > 0.0) sums[4 + c] += Lw * adj.tc[c] / p->step[c];
     }
-    free(phase); free(dphi); free(xbin); free(sbuf);
+    free(phase); free(dphi); free(xbin); free(sbuf); free(rs);
     return 0;
 }
 

@@ -55,3 +55,15 @@ def test_double_map_is_exact():
     lo, hi = 0x6627E8D5, 0xE169C58D
     m = ((hi << 32) | lo) >> 12
     assert engine.rng_doubles(0, 0, 1)[0] == (2 * m + 1) * 2.0 ** -53
+
+
+def test_float_map_from_bits_is_exact():
+    """The kernels form a uniform float from the word's top 23 bits as
+    (1 + k 2^-23) - (1 - 2^-24) (bits of 1.0 or'ed with k); that equals the
+    stream's defined value (2k + 1) 2^-24 for every k: the FP32 subtraction
+    is exact."""
+    k = np.arange(1 << 23, dtype=np.uint32)
+    from_bits = (np.uint32(0x3F800000) | k).view(np.float32) - np.float32(1.0 - 2.0 ** -24)
+    defined = ((2 * k.astype(np.float64) + 1) * 2.0 ** -24).astype(np.float32)
+    assert np.array_equal(from_bits, defined)
+    assert np.array_equal(defined.astype(np.float64), (2 * k.astype(np.float64) + 1) * 2.0 ** -24)
