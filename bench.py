@@ -859,6 +859,21 @@ def run_adjoint_bench(args):
         sl = float(np.polyfit(xs, [f(x) for x in xs], 1)[0])
         out[k]["slope_5pct"] = sl
         out[k]["rel_err_vs_slope"] = abs(out[k]["adjoint"] / sl - 1) if sl else None
+    # spread of the Monte Carlo estimators: the same walkers as 8 shards, each
+    # shard's gradient scaled to the whole job; standard error of their mean
+    shard_g = {"D": [], "D_pathwise": [], "kappa": []}
+    for k in range(8):
+        rk = s0.adjoint(W.reshape(-1) / npar, seed=9, walker_range=(npar * k // 8, npar * (k + 1) // 8))
+        shard_g["D"].append(8 * rk["d_diffusivity"])
+        shard_g["D_pathwise"].append(8 * rk["d_diffusivity_pathwise"])
+        shard_g["kappa"].append(8 * rk["d_kappa"])
+    for key, name in (("D", "D"), ("kappa", "kappa")):
+        se = float(np.std(shard_g[key], ddof=1) / np.sqrt(8))
+        out[name]["std_err"] = se
+        ref = out[name]["slope_5pct"]
+        out[name]["z_vs_slope"] = (out[name]["adjoint"] - ref) / se if se > 0 else None
+    out["D"]["pathwise"] = r["d_diffusivity_pathwise"]
+    out["D"]["pathwise_rel_err_vs_slope"] = abs(r["d_diffusivity_pathwise"] / out["D"]["slope_5pct"] - 1)
     ws = npar * tn * 2
     line = {
         "metric": ADJOINT_METRIC, "value": ws / (adj_ms * 1e-3), "unit": "walker-steps/s", "n_gpus": 1, "steps": 1,

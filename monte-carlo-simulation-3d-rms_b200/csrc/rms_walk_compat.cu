@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(kBlock) walk_compat_kernel(const WalkArgs a) {
         if (pgse)
             for (int k = 0; k < a.npairs * 3; ++k) a.vscr[(size_t)k * nthr + gtid] = 0.0;
 
+        int next_rec = 0, rec = 0;   // the next recorded step and its record
         for (int i = 0; i < a.tn; ++i) {                            // main.cu:134
             if (active) {
                 double fstep = 1.0;
@@ -268,9 +269,10 @@ __global__ void __launch_bounds__(kBlock) walk_compat_kernel(const WalkArgs a) {
                 }
             }
 
-            // record every tstep steps (main.cu:333-379)
-            if ((i % a.tstep) == 0) {
-                const int tidx = i / a.tstep;
+            // record every tstep steps (main.cu:333-379; i % tstep == 0 as a countdown)
+            if (i == next_rec) {
+                const int tidx = rec++;
+                next_rec += a.tstep;
                 if (tidx < a.timepoints) {
                     double s0 = 0.0;
 #pragma unroll

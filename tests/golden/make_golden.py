@@ -36,7 +36,9 @@ import pyoracle  # noqa: E402
 from rms_b200 import geometry, runio  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("RMS_REFERENCE", "/root/reference")
+# the reference checkout: $RMS_REFERENCE, else "reference" beside the repository
+REF = os.environ.get("RMS_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(
+    os.path.dirname(os.path.abspath(__file__))))), "reference"))
 
 
 def lattice(seed: int) -> np.ndarray:
