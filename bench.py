@@ -12,6 +12,8 @@ Workload ``production``: a 256 x 256 x 2048 label lattice at 0.1 um
 compartments, membrane permeability kappa = 0.01 um/ms, T2 = 80 / 60 ms, and
 the PGSE signal of 30 directions x b in {0..5} ms/um^2 x Delta in {4, 5, 6} ms
 at delta = 4 ms (540 gradients; Delta + delta fits the 10 ms walk).
+``production-full``: the same with Delta in {4, ..., 10} ms (1260 gradients),
+which needs 70,000 steps (Delta + delta = 14 ms).
 Workload ``single``: the 64 x 64 x 512 single-axon lattice (labels 0/1),
 1e5 walkers, 5,000 steps, impermeable, no T2, periodic walls, moments every
 10 steps.  Inputs are synthetic and seeded.
@@ -111,22 +113,28 @@ def workload(name: str, world: int, walkers: int | None = None, tn: int | None =
 
 def _workload(name: str, world: int, scaling: str = "strong"):
     from rms_b200 import analysis, geometry
-    if name == "production":
+    if name in ("production", "production-full"):
+        # 50,000 steps of 2e-4 ms walk 10 ms: Delta + delta fits for Delta <= 6 ms.
+        # production-full walks the whole Delta range 4..10 ms: 70,000 steps.
+        full = name == "production-full"
+        tn = 70_000 if full else 50_000
+        deltas = (4.0, 5.0, 6.0, 7.0, 8.0, 9.0, 10.0) if full else (4.0, 5.0, 6.0)
         lab = geometry.axon_lattice(256, 256, 2048, 0.1, seed=0, exterior=2)
         dirs = fib_directions(30)
         rows = []
-        for Delta in (4.0, 5.0, 6.0):
+        for Delta in deltas:
             for b in (0.0, 1.0, 2.0, 3.0, 4.0, 5.0):
                 g = float(analysis.pgse_gradient_for_b(b, Delta, 4.0))
                 for d in dirs:
                     rows.append([Delta, 4.0, g, *d])
         per_gpu = 10_000_000
-        sim_kw = dict(dt=2e-4, tn=50_000, npar=per_gpu * world, res=0.1,
+        sim_kw = dict(dt=2e-4, tn=tn, npar=per_gpu * world, res=0.1,
                       diffusivity=[0.0, 2.0, 2.0], t2=[80.0, 80.0, 60.0],
                       grad=np.array(rows), permeation="kappa", kappa=0.01)
-        cfg = dict(workload="production: 256x256x2048 lattice, 1e7 walkers/GPU, 50000 steps, "
-                            "kappa=0.01 um/ms, T2 80/60 ms, PGSE 540 gradients",
-                   lattice=[256, 256, 2048], walkers_per_gpu=per_gpu, steps_per_walk=50_000,
+        cfg = dict(workload=f"{name}: 256x256x2048 lattice, 1e7 walkers/GPU, {tn} steps, "
+                            f"kappa=0.01 um/ms, T2 80/60 ms, PGSE {len(rows)} gradients "
+                            f"(Delta {deltas[0]:g}..{deltas[-1]:g} ms, delta 4 ms)",
+                   lattice=[256, 256, 2048], walkers_per_gpu=per_gpu, steps_per_walk=tn,
                    ngrad=len(rows), mode="pgse",
                    l2="flushed between timed steps (256 MiB write); the packed lattice is 68 MB",
                    parallelism=f"walker shards x{world} (weak: 1e7 walkers per rank)")
@@ -1048,7 +1056,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-cuda"])
     ap.add_argument("--precision", default="split", choices=["split", "compat"])
-    ap.add_argument("--workload", default="batch", choices=["production", "batch", "single", "contraction", "adjoint"])
+    ap.add_argument("--workload", default="batch",
+                    choices=["production", "production-full", "batch", "single", "contraction", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--walkers", type=int, default=None, help="walkers per GPU (smaller case, e.g. for ncu)")
     ap.add_argument("--plain-steps", type=int, default=1,

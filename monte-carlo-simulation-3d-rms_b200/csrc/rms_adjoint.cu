@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
             const bool p1st = (pass == 0);
 
             for (int i = 0; i < a.tn; ++i) {
+                const unsigned cell = (active && a.flight) ? cell_at<BITS>(lat, wk.lin) : 0u;
                 uint32_t r1, r2;
                 if ((i & 1) == 0) {
                     const U4 b = dir_block((uint32_t)(i >> 1), key0, key1, wlo, whi);
@@ -176,7 +177,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                     float v0, v1, v2;
                     split_direction(u32_to_float(r1), u32_to_float(r2), v0, v1, v2);
                     if (p1st) { h.T0 += v0; h.T1 += v1; h.T2 += v2; }
-                    split_step<NC, BITS, 0>(wk, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio, perm, nsize, h);
+                    split_step<NC, BITS, 0>(wk, cell, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio, perm, nsize, h);
                 }
                 const float o0 = wk.o0(), o1 = wk.o1(), o2 = wk.o2();
                 const int D0 = wk.D0, D1 = wk.D1, D2 = wk.D2;

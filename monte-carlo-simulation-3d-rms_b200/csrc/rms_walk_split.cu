@@ -263,6 +263,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         uint32_t spare_u1 = 0u, spare_u2 = 0u;
 
         for (int i = 0; i < a.tn; ++i) {
+            // the walker's cell (free-flight flag), loaded before the random
+            // numbers so their arithmetic covers the load
+            const unsigned cell = (active && flight) ? cell_at<BITS>(lat, wk.lin) : 0u;
             // direction uniforms: one Philox block per two steps, in lock step
             uint32_t r1, r2;
             if ((i & 1) == 0) {
@@ -278,8 +281,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 for (int attempt = 0;; ++attempt) {
                     float v0, v1, v2;
                     split_direction(u1, u2, v0, v1, v2);
-                    const bool back = split_step<NCMAX, BITS, RULE>(wk, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio,
-                                                                    perm, nsize, hooks);
+                    const bool back = split_step<NCMAX, BITS, RULE>(wk, cell, v0, v1, v2, geo, t_step, t_k, t_pij,
+                                                                    t_ratio, perm, nsize, hooks);
                     if (RULE == 0 || !back) break;
                     // the step is taken back (interaction.m:256-345): rejection
                     // sampling stays put for the step; the equal-step-length leap

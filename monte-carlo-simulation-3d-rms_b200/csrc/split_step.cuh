@@ -54,13 +54,15 @@ struct NoHooks {
     __device__ __forceinline__ void bernoulli(bool, float) {}
 };
 
-// One step of walker s in direction v (unit vector).  Tables: t_step[c],
-// t_k[c], t_pij[a * NCMAX + b], t_ratio[a * NCMAX + b] (step[b] / step[a]).
+// One step of walker s in direction v (unit vector).  cell: the lattice cell
+// of the walker's voxel (cell_at(lat, s.lin)), loaded by the caller ahead of
+// the step's other work.  Tables: t_step[c], t_k[c], t_pij[a * NCMAX + b],
+// t_ratio[a * NCMAX + b] (step[b] / step[a]).
 // nsize(axis) gives the lattice size along an axis (read where needed so it
 // holds no registers).  Returns true when RULE != 0 and a membrane turned the
 // step back (the caller's rule decides); the walker is then mid-step.
 template <int NCMAX, int BITS, int RULE, class NSize, class Hooks>
-__device__ __forceinline__ bool split_step(SplitWalker& s, float v0, float v1, float v2, const SplitGeom& g,
+__device__ __forceinline__ bool split_step(SplitWalker& s, unsigned cell, float v0, float v1, float v2, const SplitGeom& g,
                                            const float* t_step, const float* t_k, const float* t_pij,
                                            const float* t_ratio, DomainStream& perm, NSize nsize, Hooks& h) {
     constexpr int kWall = wall_code<BITS>();
@@ -86,7 +88,7 @@ __device__ __forceinline__ bool split_step(SplitWalker& s, float v0, float v1, f
         const float k0 = floorf(x0), k1 = floorf(x1), k2 = floorf(x2);
         ik0 = (int)k0; ik1 = (int)k1; ik2 = (int)k2;
         o0n = x0 - k0; o1n = x1 - k1; o2n = x2 - k2;
-        straight = (cell_at<BITS>(lat, s.lin) & flight_bit<BITS>()) != 0u;
+        straight = (cell & flight_bit<BITS>()) != 0u;
         if (!straight) {
             const int e0 = ik0 * s0, e1 = ik1 * s1, e2 = ik2;
             const unsigned want = (unsigned)s.ai;
