@@ -864,8 +864,10 @@ def run_adjoint_bench(args):
     # reported beside it
     for k, x0, f in (("D", 2.0, lambda x: loss(D=x)), ("kappa", 0.02, lambda x: loss(kappa=x))):
         xs = x0 * (1 + 0.05 * np.linspace(-1, 1, 7))
-        sl = float(np.polyfit(xs, [f(x) for x in xs], 1)[0])
+        coef, cov = np.polyfit(xs, [f(x) for x in xs], 1, cov=True)
+        sl = float(coef[0])
         out[k]["slope_5pct"] = sl
+        out[k]["slope_std_err"] = float(np.sqrt(cov[0, 0]))   # from the fit's residuals (jumps)
         out[k]["rel_err_vs_slope"] = abs(out[k]["adjoint"] / sl - 1) if sl else None
     # spread of the Monte Carlo estimators: the same walkers as 8 shards, each
     # shard's gradient scaled to the whole job; standard error of their mean
@@ -880,8 +882,10 @@ def run_adjoint_bench(args):
         out[name]["std_err"] = se
         ref = out[name]["slope_5pct"]
         out[name]["z_vs_slope"] = (out[name]["adjoint"] - ref) / se if se > 0 else None
-    out["D"]["pathwise"] = r["d_diffusivity_pathwise"]
-    out["D"]["pathwise_rel_err_vs_slope"] = abs(r["d_diffusivity_pathwise"] / out["D"]["slope_5pct"] - 1)
+    # the frozen-event (pathwise) D estimate beside the time-rescaling one
+    se_p = float(np.std(shard_g["D_pathwise"], ddof=1) / np.sqrt(8))
+    out["D"]["pathwise"] = {"value": r["d_diffusivity_pathwise"], "std_err": se_p,
+                            "rel_err_vs_slope": abs(r["d_diffusivity_pathwise"] / out["D"]["slope_5pct"] - 1)}
     ws = npar * tn * 2
     line = {
         "metric": ADJOINT_METRIC, "value": ws / (adj_ms * 1e-3), "unit": "walker-steps/s", "n_gpus": 1, "steps": 1,
