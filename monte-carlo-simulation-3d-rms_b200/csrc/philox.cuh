@@ -119,13 +119,17 @@ struct FloatStream {
 };
 
 // Streams of the split-precision walk.  Three counter domains per walker
-// (counter word 1 = domain), all read as floats:
-//   kDomDir  block k = the direction uniforms of steps 2k and 2k+1
-//            (x, y -> step 2k; z, w -> step 2k+1): a pure function of the step
-//            index, so the lanes of a warp generate blocks in lock step however
-//            many other draws each lane made;
+// (counter word 1 = domain):
+//   kDomDir  block k = the direction uniforms of steps 3k, 3k+1 and 3k+2: the
+//            block's 128 bits (x the most significant word) cut into six 21-bit
+//            fields from the top, fields 2j and 2j+1 for step 3k+j, each field f
+//            read as u = (2f + 1) 2^-22 (dir_fields, u21_to_float; the two low
+//            bits are unused): a pure function of the step index, so the lanes
+//            of a warp generate blocks in lock step however many other draws
+//            each lane made;
 //   kDomInit sequential words for the rejection-sampled start position;
-//   kDomPerm sequential words for partial-permeation draws.
+//   kDomPerm sequential words for partial-permeation draws
+// (the last two read as floats, u32_to_float).
 // counter = (k, domain, walker_lo, walker_hi), key = (seed_lo, seed_hi).
 constexpr uint32_t kDomDir = 0u;
 constexpr uint32_t kDomInit = 1u;
@@ -133,6 +137,26 @@ constexpr uint32_t kDomPerm = 2u;
 
 RMS_HD U4 dir_block(uint32_t k, uint32_t k0, uint32_t k1, uint32_t w0, uint32_t w1) {
     return philox4x32_10(U4{k, kDomDir, w0, w1}, k0, k1);
+}
+
+// A 21-bit field f as the uniform (2f + 1) 2^-22, in (0, 1).
+RMS_HD float u21_to_float(uint32_t f) {
+#if defined(__CUDA_ARCH__)
+    // 1 + f 2^-21 from the bits, minus (1 - 2^-22): exact (Sterbenz)
+    return __uint_as_float(0x3f800000u | ((f & 0x1fffffu) << 2)) - (1.0f - 0x1p-22f);
+#else
+    return (float)(2u * (f & 0x1fffffu) + 1u) * 0x1p-22f;
+#endif
+}
+
+// The six direction uniforms of a kDomDir block: u[2j], u[2j+1] for step 3k+j.
+RMS_HD void dir_fields(const U4& b, float u[6]) {
+    u[0] = u21_to_float(b.x >> 11);
+    u[1] = u21_to_float((b.x << 10) | (b.y >> 22));
+    u[2] = u21_to_float(b.y >> 1);
+    u[3] = u21_to_float((b.y << 20) | (b.z >> 12));
+    u[4] = u21_to_float((b.z << 9) | (b.w >> 23));
+    u[5] = u21_to_float(b.w >> 2);
 }
 
 // Sequential floats of one counter domain.

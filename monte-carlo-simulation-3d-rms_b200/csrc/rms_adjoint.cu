@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                 }
             }
             const int ai0 = active ? label_at<BITS>(lat, lin) : 0;
-            SplitWalker wk{lin, 0u, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0, t_step[ai0], t_k[ai0], 0.0f};
+            SplitWalker wk{lin, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0, t_step[ai0], t_k[ai0], 0.0f};
             const SplitGeom geo{lat, s0, s1, a.nite, (bool)a.flight, (bool)a.same_cross, mirror};
             auto nsize = [&](int axis) { return axis == 0 ? a.n1 : (axis == 1 ? a.n2 : a.n3); };
             DomainStream perm;
@@ -161,25 +161,31 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
             h.rec = (pass == 0);
             float B0 = 0.0f, B1 = 0.0f, B2 = 0.0f;  // bin sums of the tangent
             int bin = 0, next_bin = a.bin_steps;
-            uint32_t spare_u1 = 0u, spare_u2 = 0u;
+            float q0 = 0.0f, q1 = 0.0f, q2 = 0.0f, q3 = 0.0f;   // the split walk's direction stream
+            int phase = 0;
+            uint32_t dblk = 0u;
             const bool p1st = (pass == 0);
 
             for (int i = 0; i < a.tn; ++i) {
                 const unsigned cell = (active && a.flight) ? cell_at<BITS>(lat, wk.lin) : 0u;
-                uint32_t r1, r2;
-                if ((i & 1) == 0) {
-                    const U4 b = dir_block((uint32_t)(i >> 1), key0, key1, wlo, whi);
-                    r1 = b.x; r2 = b.y; spare_u1 = b.z; spare_u2 = b.w;
+                float u1, u2;
+                if (phase == 0) {
+                    float u[6];
+                    dir_fields(dir_block(dblk++, key0, key1, wlo, whi), u);
+                    u1 = u[0]; u2 = u[1]; q0 = u[2]; q1 = u[3]; q2 = u[4]; q3 = u[5];
+                    phase = 1;
+                } else if (phase == 1) {
+                    u1 = q0; u2 = q1; phase = 2;
                 } else {
-                    r1 = spare_u1; r2 = spare_u2;
+                    u1 = q2; u2 = q3; phase = 0;
                 }
                 if (active) {
                     float v0, v1, v2;
-                    split_direction(u32_to_float(r1), u32_to_float(r2), v0, v1, v2);
+                    split_direction(u1, u2, v0, v1, v2);
                     if (p1st) { h.T0 += v0; h.T1 += v1; h.T2 += v2; }
                     split_step<NC, BITS, 0>(wk, cell, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio, perm, nsize, h);
                 }
-                const float o0 = wk.o0(), o1 = wk.o1(), o2 = wk.o2();
+                const float o0 = wk.o0, o1 = wk.o1, o2 = wk.o2;
                 const int D0 = wk.D0, D1 = wk.D1, D2 = wk.D2;
                 const float Fm0 = wk.Fm0, Fm1 = wk.Fm1, Fm2 = wk.Fm2;
                 p0 += (float)D0 + (o0 - Fm0);

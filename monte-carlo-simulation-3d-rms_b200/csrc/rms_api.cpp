@@ -1533,12 +1533,13 @@ int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out)
     if (n < 0 || (n && !out)) return set_error(RMS_ERR_ARG, "bad buffer");
     if (domain < 0 || domain > 2) return set_error(RMS_ERR_ARG, "domain must be 0, 1 or 2");
     if (domain == (int)kDomDir) {
+        // step i's pair: fields 2(i % 3), 2(i % 3) + 1 of block i / 3
         for (int i = 0; 2 * i < n; ++i) {
-            const U4 b = dir_block((uint32_t)(i >> 1), (uint32_t)seed, (uint32_t)(seed >> 32),
-                                   (uint32_t)walker, (uint32_t)(walker >> 32));
-            const uint32_t x = (i & 1) ? b.z : b.x, y = (i & 1) ? b.w : b.y;
-            out[2 * i] = u32_to_float(x);
-            if (2 * i + 1 < n) out[2 * i + 1] = u32_to_float(y);
+            float u[6];
+            dir_fields(dir_block((uint32_t)(i / 3), (uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)walker,
+                                 (uint32_t)(walker >> 32)), u);
+            out[2 * i] = u[2 * (i % 3)];
+            if (2 * i + 1 < n) out[2 * i + 1] = u[2 * (i % 3) + 1];
         }
         return RMS_OK;
     }

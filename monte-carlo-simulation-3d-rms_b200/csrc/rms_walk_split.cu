@@ -6,11 +6,12 @@
 // walls, T2 weighting, moments and signal at the same records -- in the
 // arithmetic a B200 issues fastest:
 //
-//  - position = voxel + FP32 offset inside it, carried per axis as d_a, the
-//    distance to the next face in the current direction of travel (0..1).
-//    The time to a face is one multiply, and after any face event -- a cross
-//    into the neighbour or a reflection -- the walker sits on that face with a
-//    whole voxel ahead: d = 1 exactly, so no drift accumulates;
+//  - position = voxel + FP32 offset inside it per axis (0..1, split_step.cuh).
+//    A straight move is one FMA and a floor per axis.  The face loop works on
+//    d_a, the distance to the next face in the direction of travel: the time
+//    to a face is one multiply, and after any face event -- a cross into the
+//    neighbour or a reflection -- the walker sits on that face with a whole
+//    voxel ahead, d = 1 exactly, so no drift accumulates;
 //  - the voxel is one linear index into a lattice padded with a one-voxel
 //    border that holds a wall code: a face step is `lin += stride`, and
 //    reaching a wall is a label like any other (rare branch); the integer
@@ -24,23 +25,24 @@
 //  - labels packed 4 bits per voxel (3-bit label, wall = 7, plus the flag;
 //    a padded 256x256x2048 lattice is 68 MB and stays in the 126 MB L2), or
 //    one byte for Nc = 8;
-//  - FP32 uniforms, one Philox4x32-10 block per two steps; hardware
-//    sine/cosine and reciprocal for the direction and face times;
+//  - FP32 uniforms (21-bit), one Philox4x32-10 block per three steps;
+//    hardware sine/cosine and reciprocal for the direction and face times;
 //  - per-walker sums that grow over the walk (T2 exponent, PGSE displacement
 //    sums) are carried in FP32 for at most 32 steps and folded into FP64;
-//  - cross-walker sums: FP32 products per walker, warp reduce-scatter in
-//    FP64, per-warp FP64 rows, added into each axon's totals with FP64 atomics
-//    (the no-allocation walk: an ordered FP64 reduction, rms_reduce.cu).
+//  - cross-walker sums: FP32 products per walker, staged in shared memory and
+//    summed per column over the warp in FP64, per-warp FP64 rows, added into
+//    each axon's totals with FP64 atomics (the no-allocation walk: an ordered
+//    FP64 reduction, rms_reduce.cu).
 //
 // Mirror walls: the reference mirrors the origin image at the end of a step
 // for each wall the step touched (main.cu:302-310).  A step shorter than a
 // voxel touches a wall at most once per axis and nothing else moves the
 // origin during the step, so the mirror is applied at the wall event itself.
 //
-// Random streams (philox.cuh): per walker, direction uniforms of steps 2k and
-// 2k+1 come from one Philox4x32-10 block indexed by k, so all lanes of a warp
-// generate in lock step; start positions and partial-permeation draws read
-// their own sequential counter domains.
+// Random streams (philox.cuh): per walker, direction uniforms of steps 3k,
+// 3k+1 and 3k+2 come from one Philox4x32-10 block indexed by k, so all lanes of
+// a warp generate in lock step; start positions and partial-permeation draws
+// read their own sequential counter domains.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -133,6 +135,53 @@ __device__ __noinline__ void wave_final(const double* ph, int nthr, int nwave, d
     }
 }
 
+// A record of the warp's 32 walkers added into the warp's row (row layout of
+// rms_internal.h): each lane stages its 22 moments [sig0, dx2 x6, dx4 x15]
+// (FP32 products) in shared memory, and lane c < 22 adds column c over the 32
+// walkers in FP64, in lane order (four interleaved partials, combined in a
+// fixed order); lanes 22.. take the compartment counts (integer warp sums).
+// KC columns per pass.  Not inlined: the step loop keeps its registers (the
+// inlined form cost the batch walk ~3 % more time).
+template <int KC>
+__device__ __noinline__ void record_row(double* row, float s0, float dx, float dy, float dz, int ai, bool active,
+                                        int lane, float (*stage)[KC + 1]) {
+    const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
+    const float sxx = s0 * xx, syy = s0 * yy, szz = s0 * zz;
+    const float mv[22] = {s0,      sxx,          s0 * dx * dy, s0 * dx * dz, syy,
+                          s0 * dy * dz, szz,     sxx * xx,     sxx * dx * dy, sxx * dx * dz,
+                          sxx * yy, sxx * dy * dz, sxx * zz,   syy * dx * dy, syy * dx * dz,
+                          szz * dx * dy, szz * dx * dz, syy * yy, syy * dy * dz, syy * zz,
+                          szz * dy * dz, szz * zz};
+    double r = 0.0;
+#pragma unroll
+    for (int pass = 0; pass < 22 / KC; ++pass) {
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < KC; ++c) stage[lane][c] = mv[pass * KC + c];
+        __syncwarp();
+        const int col = lane - pass * KC;
+        if (col >= 0 && col < KC) {
+            double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;
+#pragma unroll
+            for (int l = 0; l < 32; l += 4) {
+                q0 += (double)stage[l][col];
+                q1 += (double)stage[l + 1][col];
+                q2 += (double)stage[l + 2][col];
+                q3 += (double)stage[l + 3][col];
+            }
+            r = (q0 + q1) + (q2 + q3);
+        }
+    }
+    unsigned cnt = 0u;
+#pragma unroll
+    for (int c = 0; c < 10; ++c) {
+        const unsigned n = __reduce_add_sync(0xffffffffu, (active && ai == c) ? 1u : 0u);
+        if (lane == kColCount + c) cnt = n;
+    }
+    if (lane >= kColCount) r = (double)cnt;
+    row[lane] += r;
+}
+
 // ONE: the no-allocation walk's form -- one axon, whose scalars are read from
 // the kernel parameters (a.axon0); every other launch reads the axon table.
 template <int NCMAX, int BITS, int BLOCK, int MINB, bool ONE, int RULE = 0, int MODE = 0>
@@ -141,6 +190,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
     // of path, Pij and the step-length ratio that rescales the rest of a step
     constexpr int kTab = 2 * NCMAX + 2 * NCMAX * NCMAX;
     __shared__ float s_tab[BLOCK / 32][kTab];
+    // per warp, a record's 22 moments of its 32 walkers, staged for the column
+    // sums (all 22 at once up to 256 threads a block, else in two halves: the
+    // static shared memory stays under 48 KB a block)
+    constexpr int kCols = BLOCK <= 256 ? 22 : 11;
+    __shared__ float s_stage[BLOCK / 32][32][kCols + 1];
 
     const int lane = threadIdx.x & 31;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -243,9 +297,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
             }
         }
         const int ai0 = active ? label_at<BITS>(lat, lin) : 0;
-        // displacement = D + (offset - Fm) per axis; the walker starts
-        // travelling down along every axis (d = offset)
-        SplitWalker wk{lin, 0u, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0, t_step[ai0], t_k[ai0], 0.0f};
+        // displacement = D + (offset - Fm) per axis
+        SplitWalker wk{lin, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0, t_step[ai0], t_k[ai0], 0.0f};
         const SplitGeom geo{lat, s0, s1, a.nite, flight, same_certain, mirror};
         auto nsize = [&](int axis) { return axis == 0 ? AXF(n1) : (axis == 1 ? AXF(n2) : AXF(n3)); };
         NoHooks hooks;
@@ -260,22 +313,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         int next_ev = pgse ? (a.nevents > 0 ? a.ev_step[0] : -1) : (wave ? a.bin_steps : -1);
         if (sums)
             for (int k = 0; k < (pgse ? a.npairs * 3 : a.nwave); ++k) a.vscr[(size_t)k * nthr + gtid] = 0.0;
-        uint32_t spare_u1 = 0u, spare_u2 = 0u;
+        // direction uniforms: one Philox block per three steps, in lock step;
+        // the next two steps' pairs wait in q0..q3
+        float q0 = 0.0f, q1 = 0.0f, q2 = 0.0f, q3 = 0.0f;
+        int phase = 0;
+        uint32_t dblk = 0u;
 
         for (int i = 0; i < a.tn; ++i) {
             // the walker's cell (free-flight flag), loaded before the random
             // numbers so their arithmetic covers the load
             const unsigned cell = (active && flight) ? cell_at<BITS>(lat, wk.lin) : 0u;
-            // direction uniforms: one Philox block per two steps, in lock step
-            uint32_t r1, r2;
-            if ((i & 1) == 0) {
-                const U4 b = dir_block((uint32_t)(i >> 1), key0, key1, wlo, whi);
-                r1 = b.x; r2 = b.y; spare_u1 = b.z; spare_u2 = b.w;
+            float u1, u2;
+            if (phase == 0) {
+                float u[6];
+                dir_fields(dir_block(dblk++, key0, key1, wlo, whi), u);
+                u1 = u[0]; u2 = u[1]; q0 = u[2]; q1 = u[3]; q2 = u[4]; q3 = u[5];
+                phase = 1;
+            } else if (phase == 1) {
+                u1 = q0; u2 = q1; phase = 2;
             } else {
-                r1 = spare_u1; r2 = spare_u2;
+                u1 = q2; u2 = q3; phase = 0;
             }
             if (active) {
-                float u1 = u32_to_float(r1), u2 = u32_to_float(r2);
                 // RULE != 0: the step's start, restored when a membrane turns the step back
                 const SplitWalker start = wk;
                 for (int attempt = 0;; ++attempt) {
@@ -298,7 +357,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 }
             }
             // in-voxel offsets of the current position
-            const float o0 = wk.o0(), o1 = wk.o1(), o2 = wk.o2();
+            const float o0 = wk.o0, o1 = wk.o1, o2 = wk.o2;
             const int D0 = wk.D0, D1 = wk.D1, D2 = wk.D2;
             const float Fm0 = wk.Fm0, Fm1 = wk.Fm1, Fm2 = wk.Fm2;
 
@@ -364,31 +423,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                     const float dx = ((float)D0 + (o0 - Fm0)) * res;
                     const float dy = ((float)D1 + (o1 - Fm1)) * res;
                     const float dz = ((float)D2 + (o2 - Fm2)) * res;
-                    const float xx = dx * dx, yy = dy * dy, zz = dz * dz;
-                    const float sxx = s0 * xx, syy = s0 * yy, szz = s0 * zz;
                     double* row = slot + (size_t)tidx * a.nvals;
-                    // two rounds of 16 values: [sig0, dx2 x6, dx4 0..8], [dx4 9..14, counts]
-                    double r;
-                    {
-                        double v[16];
-                        v[0] = s0;
-                        v[1] = sxx;  v[2] = s0 * dx * dy;  v[3] = s0 * dx * dz;
-                        v[4] = syy;  v[5] = s0 * dy * dz;  v[6] = szz;
-                        v[7] = sxx * xx;        v[8] = sxx * dx * dy;   v[9] = sxx * dx * dz;
-                        v[10] = sxx * yy;       v[11] = sxx * dy * dz;  v[12] = sxx * zz;
-                        v[13] = syy * dx * dy;  v[14] = syy * dx * dz;  v[15] = szz * dx * dy;
-                        r = warp_reduce_scatter16(v, lane);
-                    }
-                    {
-                        double v[16];
-                        v[0] = szz * dx * dz;  v[1] = syy * yy;       v[2] = syy * dy * dz;
-                        v[3] = syy * zz;       v[4] = szz * dy * dz;  v[5] = szz * zz;
-#pragma unroll
-                        for (int c = 0; c < 10; ++c) v[6 + c] = (active && wk.ai == c) ? 1.0 : 0.0;
-                        const double rb = warp_reduce_scatter16(v, lane);
-                        if (lane >= 16) r = rb;
-                    }
-                    row[lane] += r;
+                    record_row<kCols>(row, s0, dx, dy, dz, wk.ai, active, lane, s_stage[threadIdx.x >> 5]);
                     if (!sums) {
                         for (int base = 0; base < a.nbvec; base += 32) {
                             double mine = 0.0;

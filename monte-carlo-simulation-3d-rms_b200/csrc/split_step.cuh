@@ -7,8 +7,10 @@
 // step in an isotropic direction, split at voxel faces into at most nite
 // segments, each face crossed or reflected -- always crossed between voxels of
 // one label, reflected at compartment 0 and at mirror walls, Bernoulli(Pij)
-// otherwise -- in the split representation (voxel index + FP32 distances to
-// the next faces, see rms_walk_split.cu).
+// otherwise -- in the split representation (see rms_walk_split.cu): between
+// steps a walker is its voxel and its FP32 in-voxel offsets; the face loop
+// works on the distances to the next faces along the direction of travel and
+// converts back when it ends.
 #pragma once
 #include <cstdint>
 
@@ -20,18 +22,12 @@ namespace rms {
 // A walker between steps.
 struct SplitWalker {
     unsigned lin;            // voxel: linear index into the padded lattice
-    unsigned up;             // bit a: travelling up along axis a
-    float d0, d1, d2;        // distance to the next face in the direction of travel (0..1)
+    float o0, o1, o2;        // in-voxel offset along each axis, 0..1 (1: on the upper face)
     int D0, D1, D2;          // integer part of the displacement: voxel - origin image
     float Fm0, Fm1, Fm2;     // fractional part of the origin image (mirrored at walls)
     int ai;                  // compartment (label)
     float cur_step, cur_k;   // step length (voxels), T2 exponent per voxel of path
     float w32;               // T2 exponent since the last fold
-
-    // in-voxel offset of the position along each axis
-    __device__ __forceinline__ float o0() const { return (up & 1u) ? 1.0f - d0 : d0; }
-    __device__ __forceinline__ float o1() const { return (up & 2u) ? 1.0f - d1 : d1; }
-    __device__ __forceinline__ float o2() const { return (up & 4u) ? 1.0f - d2 : d2; }
 };
 
 // What one step reads besides the walker: the padded lattice and its strides,
@@ -69,72 +65,54 @@ __device__ __forceinline__ bool split_step(SplitWalker& s, unsigned cell, float 
     const uint8_t* __restrict__ lat = g.lat;
     const int s0 = g.s0, s1 = g.s1;
     const unsigned nu = (v0 > 0.0f ? 1u : 0u) | (v1 > 0.0f ? 2u : 0u) | (v2 > 0.0f ? 4u : 0u);
-    // The step as one straight line (at most one voxel per axis, step < 1
-    // voxel).  It is the face loop's own outcome whenever every voxel of the
-    // box the line spans -- the start voxel's neighbours across the faces it
-    // crosses, and their common edge/corner neighbours -- carries the walker's
-    // label: every face on the way is then a same-label face, always crossed,
-    // with at most three crossings (within nite = 4).  Voxels flagged for free
-    // flight (all 26 neighbours share the label) need no look; otherwise the
-    // box is checked, which settles most steps next to a membrane or a wall
-    // without the face loop.
+    // Free flight: a voxel whose 26 neighbours all carry its label (none a
+    // wall) has a flag bit; a step from there (shorter than a voxel) moves as
+    // one straight line -- the face loop's own outcome, since every face on the
+    // way is a same-label face, always crossed, with at most three crossings
+    // (within nite = 4).  Other voxels take the face loop.  (Checking the
+    // neighbours a step from an unflagged voxel actually passes settles more
+    // steps without the face loop, but measured on the 64-axon batch it costs
+    // every warp with such a lane more than the face loops it saves.)
     bool straight = false;
     int ik0 = 0, ik1 = 0, ik2 = 0;
     float o0n = 0.0f, o1n = 0.0f, o2n = 0.0f;
     if (g.flight) {
-        const float x0 = fmaf(s.cur_step, v0, s.o0());
-        const float x1 = fmaf(s.cur_step, v1, s.o1());
-        const float x2 = fmaf(s.cur_step, v2, s.o2());
+        const float x0 = fmaf(s.cur_step, v0, s.o0);
+        const float x1 = fmaf(s.cur_step, v1, s.o1);
+        const float x2 = fmaf(s.cur_step, v2, s.o2);
         const float k0 = floorf(x0), k1 = floorf(x1), k2 = floorf(x2);
         ik0 = (int)k0; ik1 = (int)k1; ik2 = (int)k2;
         o0n = x0 - k0; o1n = x1 - k1; o2n = x2 - k2;
         straight = (cell & flight_bit<BITS>()) != 0u;
-        if (!straight) {
-            const int e0 = ik0 * s0, e1 = ik1 * s1, e2 = ik2;
-            const unsigned want = (unsigned)s.ai;
-            unsigned diff = 0u;   // nonzero: a box voxel with another label (or a wall)
-            if (e0) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)e0) ^ want;
-            if (e1) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)e1) ^ want;
-            if (e2) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)e2) ^ want;
-            if (!diff && (e0 != 0) + (e1 != 0) + (e2 != 0) >= 2) {
-                if (e0 && e1) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)(e0 + e1)) ^ want;
-                if (e0 && e2) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)(e0 + e2)) ^ want;
-                if (e1 && e2) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)(e1 + e2)) ^ want;
-                if (e0 && e1 && e2) diff |= (unsigned)label_at<BITS>(lat, s.lin + (unsigned)(e0 + e1 + e2)) ^ want;
-            }
-            straight = diff == 0u;
-        }
     }
     if (straight) {
         s.lin += (unsigned)(ik0 * s0 + ik1 * s1 + ik2);
         s.D0 += ik0; s.D1 += ik1; s.D2 += ik2;
         s.w32 = fmaf(s.cur_step, s.cur_k, s.w32);
         h.path(s.ai, s.cur_step);
-        s.d0 = (nu & 1u) ? 1.0f - o0n : o0n;
-        s.d1 = (nu & 2u) ? 1.0f - o1n : o1n;
-        s.d2 = (nu & 4u) ? 1.0f - o2n : o2n;
-        s.up = nu;
+        s.o0 = o0n; s.o1 = o1n; s.o2 = o2n;
         return false;
     }
-    // the face loop: up to nite segments, one face event each
-    const unsigned turn = nu ^ s.up;
-    if (turn & 1u) s.d0 = 1.0f - s.d0;
-    if (turn & 2u) s.d1 = 1.0f - s.d1;
-    if (turn & 4u) s.d2 = 1.0f - s.d2;
-    s.up = nu;
+    // the face loop: up to nite segments, one face event each, on the distances
+    // to the next faces along the direction of travel (a face event leaves the
+    // walker on the face with a whole voxel ahead: d = 1 exactly)
+    unsigned up = nu;
+    float d0 = (nu & 1u) ? 1.0f - s.o0 : s.o0;
+    float d1 = (nu & 2u) ? 1.0f - s.o1 : s.o1;
+    float d2 = (nu & 4u) ? 1.0f - s.o2 : s.o2;
     const float av0 = fabsf(v0), av1 = fabsf(v1), av2 = fabsf(v2);
     const float iv0 = __fdividef(1.0f, av0), iv1 = __fdividef(1.0f, av1), iv2 = __fdividef(1.0f, av2);
     // signed lattice step along each axis in the direction of travel
-    int dl0 = (s.up & 1u) ? s0 : -s0;
-    int dl1 = (s.up & 2u) ? s1 : -s1;
-    int dl2 = (s.up & 4u) ? 1 : -1;
+    int dl0 = (up & 1u) ? s0 : -s0;
+    int dl1 = (up & 2u) ? s1 : -s1;
+    int dl2 = (up & 4u) ? 1 : -1;
     float rem = s.cur_step;        // path left in this step, voxels
     for (int j = 0; j < g.nite; ++j) {
-        const float t0 = s.d0 * iv0, t1 = s.d1 * iv1, t2 = s.d2 * iv2;
+        const float t0 = d0 * iv0, t1 = d1 * iv1, t2 = d2 * iv2;
         const float tm = fminf(t0, fminf(t1, t2));
         if (rem < tm) {
             // the step ends inside the voxel
-            s.d0 = fmaf(-rem, av0, s.d0); s.d1 = fmaf(-rem, av1, s.d1); s.d2 = fmaf(-rem, av2, s.d2);
+            d0 = fmaf(-rem, av0, d0); d1 = fmaf(-rem, av1, d1); d2 = fmaf(-rem, av2, d2);
             s.w32 = fmaf(rem, s.cur_k, s.w32);
             h.path(s.ai, rem);
             rem = 0.0f;
@@ -143,7 +121,7 @@ __device__ __forceinline__ bool split_step(SplitWalker& s, unsigned cell, float 
         // onto the nearest face (lowest axis on ties, like the reference's scan)
         const int hit = (t0 == tm) ? 0 : ((t1 == tm) ? 1 : 2);
         const float tc = fmaxf(tm, 0.0f);
-        s.d0 = fmaf(-tc, av0, s.d0); s.d1 = fmaf(-tc, av1, s.d1); s.d2 = fmaf(-tc, av2, s.d2);
+        d0 = fmaf(-tc, av0, d0); d1 = fmaf(-tc, av1, d1); d2 = fmaf(-tc, av2, d2);
         s.w32 = fmaf(tc, s.cur_k, s.w32);
         h.path(s.ai, tc);
         rem -= tc;
@@ -155,7 +133,7 @@ __device__ __forceinline__ bool split_step(SplitWalker& s, unsigned cell, float 
             cross = true;
         } else {
             if (aj == kWall) {
-                const bool hi = (s.up >> hit) & 1u;
+                const bool hi = (up >> hit) & 1u;
                 const int nh = nsize(hit);
                 if (g.mirror) {
                     // mirror wall: reflect, and mirror the origin image
@@ -195,17 +173,20 @@ __device__ __forceinline__ bool split_step(SplitWalker& s, unsigned cell, float 
                 s.ai = aj;
             }
             s.lin = lj;
-            const int du = ((s.up >> hit) & 1u) ? 1 : -1;
+            const int du = ((up >> hit) & 1u) ? 1 : -1;
             if (hit == 0) s.D0 += du; else if (hit == 1) s.D1 += du; else s.D2 += du;
         } else {
-            s.up ^= 1u << hit;
+            up ^= 1u << hit;
             if (hit == 0) dl0 = -dl0; else if (hit == 1) dl1 = -dl1; else dl2 = -dl2;
             h.reflect(hit);
         }
         // on the face, a whole voxel ahead
-        if (hit == 0) s.d0 = 1.0f; else if (hit == 1) s.d1 = 1.0f; else s.d2 = 1.0f;
+        if (hit == 0) d0 = 1.0f; else if (hit == 1) d1 = 1.0f; else d2 = 1.0f;
         if (!(rem > 0.0f)) break;
     }
+    s.o0 = (up & 1u) ? 1.0f - d0 : d0;
+    s.o1 = (up & 2u) ? 1.0f - d1 : d1;
+    s.o2 = (up & 4u) ? 1.0f - d2 : d2;
     return false;
 }
 

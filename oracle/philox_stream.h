@@ -119,19 +119,29 @@ static inline float or_stream_float(or_stream* s) {
 
 /* Streams of the engine's split-precision walk: Philox counter
  * (k, domain, walker_lo, walker_hi).  Domain 0: block k holds the direction
- * uniforms of steps 2k (words 0, 1) and 2k+1 (words 2, 3).  Domain 1: start
- * positions, sequential.  Domain 2: partial-permeation draws, sequential. */
+ * uniforms of steps 3k, 3k+1, 3k+2: its 128 bits (word 0 the most
+ * significant) cut into six 21-bit fields from the top, fields 2j and 2j+1
+ * for step 3k+j, a field f read as (2f + 1) 2^-22.  Domain 1: start
+ * positions, sequential.  Domain 2: partial-permeation draws, sequential
+ * (words read as floats, or_u32_to_float). */
 #define OR_DOM_DIR 0u
 #define OR_DOM_INIT 1u
 #define OR_DOM_PERM 2u
 
+static inline float or_u21_to_float(uint32_t f) {
+    return (float)(2u * (f & 0x1fffffu) + 1u) * 0x1p-22f;
+}
+
 static inline void or_dir_uniforms(uint64_t seed, uint64_t walker, uint32_t step, float* u1, float* u2) {
-    uint32_t ctr[4] = {step >> 1, OR_DOM_DIR, (uint32_t)walker, (uint32_t)(walker >> 32)};
+    uint32_t ctr[4] = {step / 3u, OR_DOM_DIR, (uint32_t)walker, (uint32_t)(walker >> 32)};
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-    uint32_t out[4];
-    or_philox4x32(ctr, key, 10, out);
-    *u1 = or_u32_to_float(out[(step & 1) ? 2 : 0]);
-    *u2 = or_u32_to_float(out[(step & 1) ? 3 : 1]);
+    uint32_t b[4];
+    or_philox4x32(ctr, key, 10, b);
+    const uint32_t f[6] = {b[0] >> 11, (b[0] << 10) | (b[1] >> 22), b[1] >> 1, (b[1] << 20) | (b[2] >> 12),
+                           (b[2] << 9) | (b[3] >> 23), b[3] >> 2};
+    const unsigned j = step % 3u;
+    *u1 = or_u21_to_float(f[2 * j]);
+    *u2 = or_u21_to_float(f[2 * j + 1]);
 }
 
 typedef struct or_dstream {

@@ -278,28 +278,6 @@ static int homogeneous(const or_params* p, const int g[3]) {
     return 1;
 }
 
-/* The split walk's box check: a step whose straight line (at most one voxel
- * per axis) stays in voxels of the walker's label -- every voxel of the box
- * spanned by the start and end voxels inside the lattice and labelled ai --
- * is walked as that straight line, the face loop's outcome when every face on
- * the way is a same-label face (monte-carlo-simulation-3d-rms_b200/csrc/
- * rms_walk_split.cu, the straight move). */
-static int box_same(const or_params* p, const int g[3], const double f[3], const double v[3], double rem, int ai) {
-    const int NPix[3] = {p->n1, p->n2, p->n3};
-    int k[3];
-    for (int a = 0; a < 3; a++) k[a] = (int)floor(f[a] + rem * v[a]);
-    for (int a = 0; a <= (k[0] != 0); a++)
-        for (int b = 0; b <= (k[1] != 0); b++)
-            for (int c = 0; c <= (k[2] != 0); c++) {
-                if (!a && !b && !c) continue;
-                const int q[3] = {g[0] + a * k[0], g[1] + b * k[1], g[2] + c * k[2]};
-                for (int e = 0; e < 3; e++)
-                    if (q[e] < 0 || q[e] >= NPix[e]) return 0;
-                if (p->labels[lin(p, q[0], q[1], q[2])] != ai) return 0;
-            }
-    return 1;
-}
-
 /* Adjoint bookkeeping of one walker (or_adjoint_split; the GPU kernel's
  * pass-1 quantities, restated in FP64): the tangent of the displacement with
  * respect to the step length l with the event sequence frozen (gains the step
@@ -369,8 +347,8 @@ static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, doub
         rem = p->step[ai];
         flo = 0; fhi = 0; nev = 0;
         ev = 0;
-        if (flight && (homogeneous(p, g) || box_same(p, g, f, v, rem, ai))) {
-            /* a straight line within voxels of the walker's label */
+        if (flight && homogeneous(p, g)) {
+            /* a straight line within the homogeneous neighbourhood */
             for (int a = 0; a < 3; a++) {
                 const double x = f[a] + rem * v[a];
                 const double k = floor(x);

@@ -67,3 +67,26 @@ def test_float_map_from_bits_is_exact():
     defined = ((2 * k.astype(np.float64) + 1) * 2.0 ** -24).astype(np.float32)
     assert np.array_equal(from_bits, defined)
     assert np.array_equal(defined.astype(np.float64), (2 * k.astype(np.float64) + 1) * 2.0 ** -24)
+    # the direction stream's 21-bit fields: (1 + f 2^-21) - (1 - 2^-22) = (2f + 1) 2^-22
+    f = np.arange(1 << 21, dtype=np.uint32)
+    from_bits = (np.uint32(0x3F800000) | (f << np.uint32(2))).view(np.float32) - np.float32(1.0 - 2.0 ** -22)
+    assert np.array_equal(from_bits.astype(np.float64), (2 * f.astype(np.float64) + 1) * 2.0 ** -22)
+
+
+def test_direction_stream_layout():
+    """The split walk's direction uniforms: Philox4x32-10 block k of domain 0
+    (counter (k, 0, walker_lo, walker_hi), key = seed) serves steps 3k, 3k+1,
+    3k+2 -- its 128 bits cut into six 21-bit fields from the top word down,
+    fields 2j and 2j+1 for step 3k+j, field f read as (2f + 1) 2^-22."""
+    seed, walker, nsteps = 0x1234ABCD5678EF01, 77, 31
+    got = engine.rng_split(seed, walker, 0, 2 * nsteps)
+    want = []
+    for i in range(nsteps):
+        b = [int(x) for x in pyoracle.philox4x32_10([i // 3, 0, walker & 0xFFFFFFFF, walker >> 32],
+                                                   [seed & 0xFFFFFFFF, seed >> 32])]
+        bits = (b[0] << 96) | (b[1] << 64) | (b[2] << 32) | b[3]
+        f = [(bits >> (107 - 21 * m)) & 0x1FFFFF for m in range(6)]
+        j = i % 3
+        want += [(2 * f[2 * j] + 1) * 2.0 ** -22, (2 * f[2 * j + 1] + 1) * 2.0 ** -22]
+    assert np.array_equal(got.astype(np.float64), np.array(want))
+    assert np.array_equal(got, pyoracle.split_dir_uniforms(seed, walker, nsteps))
