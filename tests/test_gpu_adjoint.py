@@ -18,7 +18,8 @@ weights.  Bars:
     FP64 walks cannot part (reflections and crossings are continuous there);
   - kappa: a score-function (Monte Carlo) estimate, and the finite difference
     jumps wherever a crossing decision flips, so the reference is the
-    least-squares slope of L over +-15 %, seven points, and the bar 20 %.
+    least-squares slope of L over +-15 %, seven points; both are averaged over
+    8 seeds and compared within their statistical error.
 Walls are periodic.  Two places where the walk's output is not continuous in
 the step length, so the frozen-event D term misses jumps: a mirror wall (the
 reference mirrors the origin image, hpc_code/lib/main.cu:302-310, so a
@@ -164,13 +165,32 @@ def test_adjoint_sums_equal_the_oracle_walker_set():
 
 
 def test_kappa_gradient_permeable_axon():
-    # score-function spread over seeds at 65536 walkers was ~6 % here; 4x the
-    # walkers halves it
+    """The score-function kappa gradient against the +-15 % slope of the loss,
+    both averaged over 8 seeds (262144 walkers each): on this axon the slope
+    is the noisier of the two (crossing decisions flip in jumps; measured on
+    the oracle at 65536 walkers: adjoint spread ~17 %, slope spread ~45 % per
+    seed).  The means must agree within 3 standard errors of their difference
+    (from the seed spreads) and within 40 %."""
     wave = base_waves()
     kw = dict(kappa=0.05, t2=(1e6, 70.0, 70.0), npar=4 * NPAR)
-    r = adj(wave, **kw)
-    want = slope(lambda k: loss(wave, **dict(kw, kappa=k)), 0.05, 0.15)
-    assert abs(r["d_kappa"] / want - 1) < 0.2, (r["d_kappa"], want)
+    adjs, slopes = [], []
+    for seed in range(5, 13):
+        sim = make(wave, **kw)
+        adjs.append(sim.adjoint(WEIGHTS.reshape(-1) / kw["npar"], seed=seed)["d_kappa"])
+        sim.close()
+
+        def f(k):
+            sk = make(wave, **dict(kw, kappa=k))
+            sk.run(seed=seed, precision="split")
+            v = float((sk.get("sigw").reshape(-1, 2) * WEIGHTS).sum() / kw["npar"])
+            sk.close()
+            return v
+
+        slopes.append(slope(f, 0.05, 0.15))
+    a, b = np.mean(adjs), np.mean(slopes)
+    se = np.sqrt(np.var(adjs, ddof=1) / len(adjs) + np.var(slopes, ddof=1) / len(slopes))
+    assert abs(a - b) < 3 * se, (adjs, slopes)
+    assert abs(a / b - 1) < 0.4, (a, b)
 
 
 def test_torch_autograd_through_rotations():
