@@ -82,6 +82,7 @@ struct rms_device_state {
     HostPinned h_out, h_axons;
     size_t labels_bytes = 0;
     bool packed_valid = false;
+    int packed_bits = 0;       // cell width of the packed lattice (4 or 8)
 
     ~rms_device_state() {
         if (device >= 0) cudaSetDevice(device);
@@ -456,11 +457,14 @@ int prepare_lattice(rms_sim* s, cudaStream_t st, bool split, int bits) {
         d->packed_valid = false;
         s->lattice_dirty = false;
     }
-    if (split && !d->packed_valid) {
+    // packed again when the launch needs another cell width (a batch's widest
+    // Nc decides it for all its members)
+    if (split && (!d->packed_valid || d->packed_bits != bits)) {
         RMS_CUDA(d->packed.ensure(padded_lattice_bytes(s->n1, s->n2, s->n3, bits)));
         int pe = pack_lattice_padded(d->labels.as<uint8_t>(), s->n1, s->n2, s->n3, bits, d->packed.as<uint8_t>(), st);
         if (pe) return cuda_fail((cudaError_t)pe, "label packing");
         d->packed_valid = true;
+        d->packed_bits = bits;
     }
     return RMS_OK;
 }
@@ -882,7 +886,7 @@ int graph_create(rms_sim* const* sims, int n, const rms_run_opts* o, rms_graph**
 
 int graph_run(rms_graph* g, uint64_t seed) {
     for (const LaunchJob& j : g->jobs)
-        if (j.s->lattice_dirty || !j.s->dev || !j.s->dev->packed_valid)
+        if (j.s->lattice_dirty || !j.s->dev || !j.s->dev->packed_valid || j.s->dev->packed_bits != g->plan.bits)
             return set_error(RMS_ERR_STATE, "a simulation of the graph has a new lattice: create the graph again");
     if (graph_buffers(g) != g->buffers)
         return set_error(RMS_ERR_STATE, "the graph's device buffers were reallocated by another run: create the graph again");

@@ -157,3 +157,21 @@ def test_shard_arguments_are_checked():
         assert e.value.code == -1
     with pytest.raises(engine.RmsError):
         sims[0].run(seed=1, precision="split", walker_range=(0, 10), shard=(0, 2))
+
+
+def test_batch_with_a_wider_lattice_encoding_repacks_its_members():
+    """A simulation walked alone packs its lattice 4 bits a voxel (Nc <= 7);
+    walked in a batch with an Nc = 8 member every lattice is packed 8 bits a
+    voxel.  The member must be packed again, not walked on its 4-bit cells:
+    its batch result equals its own run with the batch seed."""
+    sims = axon_sims()[:2]
+    lab8 = geometry.axon_lattice(16, 16, 24, 0.1, seed=3, exterior=2, r0=0.5)
+    lab8[:, :, :4][lab8[:, :, :4] == 2] = 7
+    wide = engine.Sim(lab8, dt=2e-4, tn=1000, npar=500, res=0.1, diffusivity=[0, 2.0, 2.0, 1, 1, 1, 1, 1.5],
+                      t2=[80.0] * 8, permeation="kappa", kappa=0.02, bval=[1.0, 2.0], bvec=[[1, 0, 0], [0, 0, 1]])
+    alone = [s.run(seed=(3 + k * PHI64) % (1 << 64), precision="split").outputs() for k, s in enumerate(sims)]
+    engine.batch_run(sims + [wide], seed=3, precision="split")
+    for k, s in enumerate(sims):
+        o = s.outputs()
+        assert np.array_equal(o["npar_count"], alone[k]["npar_count"]), k
+        assert_fp64_close(o["dx2"], alone[k]["dx2"], 1e-9, f"axon {k} dx2")
