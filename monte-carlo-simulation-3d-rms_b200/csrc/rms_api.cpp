@@ -1243,9 +1243,32 @@ int rms_sim_set_lattice(rms_sim* s, const uint8_t* labels, int n1, int n2, int n
     if (rc) return rc;
     s->labels.resize(n);
     uint8_t* dst = s->labels.data();
+    // A simulation that has run has its device: the lattice goes up straight
+    // from the caller's buffer on the simulation's own stream (a DMA from a
+    // pinned buffer, overlapping the host copy below) instead of from the host
+    // copy at the next run.  The call returns once neither reads the caller's
+    // buffer any more; if the upload cannot start, the next run uploads.
+    rms_device_state* d = s->dev;
+    int prev = -1;
+    bool uploading = false;
+    if (d && cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(d->device) == cudaSuccess &&
+        d->labels.ensure(n) == cudaSuccess)
+        uploading = cudaMemcpyAsync(d->labels.p, labels, n, cudaMemcpyHostToDevice, d->own) == cudaSuccess;
     host_parallel(n, [&](size_t lo, size_t hi, int) { std::memcpy(dst + lo, labels + lo, hi - lo); });
     s->have_lattice = true;
     s->lattice_dirty = true;
+    if (uploading) {
+        const cudaError_t e = cudaStreamSynchronize(d->own);
+        if (e == cudaSuccess) {
+            d->labels_bytes = n;
+            d->packed_valid = false;
+            s->lattice_dirty = false;
+        }
+        if (prev >= 0) cudaSetDevice(prev);
+        if (e != cudaSuccess) return cuda_fail(e, "lattice upload");
+    } else if (prev >= 0) {
+        cudaSetDevice(prev);
+    }
     return RMS_OK;
 }
 

@@ -86,3 +86,26 @@ def test_trace_and_metrics_lines(tmp_path):
     assert m["walk_ms"] > 0 and m["walker_steps_per_s_walk"] > 0 and m["wall_ms"] >= m["run_ms"] > 0
     got = runio.read_outputs(d)
     assert np.array_equal(got.npar_count, want.npar_count)
+
+
+@pytest.mark.parametrize("precision", ["split", "compat"])
+def test_new_lattice_after_a_run_walks_the_new_lattice(precision):
+    """rms_sim_set_lattice on a simulation that has run uploads the lattice
+    straight from the caller's buffer; the next run equals a fresh
+    simulation's run on that lattice (and the caller may reuse its buffer as
+    soon as the call returns)."""
+    import torch
+    kw = dict(dt=2e-4, tn=500, npar=2000, res=0.1, diffusivity=[0.0, 2.0, 1.0], t2=[80.0, 80.0, 40.0],
+              bval=[1.0], bvec=[[1, 0, 0]], timepoints=500)
+    a = geometry.axon_lattice(16, 16, 24, 0.1, seed=1, exterior=2, r0=0.5)
+    b = geometry.axon_lattice(16, 16, 24, 0.1, seed=2, exterior=2, r0=0.7)
+    sim = engine.Sim(a, **kw)
+    sim.run(seed=4, precision=precision)
+    buf = torch.from_numpy(np.ascontiguousarray(b)).pin_memory()
+    sim.set_lattice(buf.numpy())
+    buf.zero_()                                # the caller's buffer is free again
+    got = sim.run(seed=4, precision=precision).outputs()
+    want = engine.Sim(b, **kw).run(seed=4, precision=precision).outputs()
+    assert np.array_equal(got["npar_count"], want["npar_count"])
+    assert_fp64_close(got["dx2"], want["dx2"], 1e-9, "dx2")
+    assert_fp64_close(got["sigre"], want["sigre"], 1e-9, "sigre")
