@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                 }
             }
             const int ai0 = active ? label_at<BITS>(lat, lin) : 0;
-            SplitWalker wk{lin, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0, t_step[ai0], t_k[ai0], 0.0f};
+            SplitWalker wk{lin, active ? cell_at<BITS>(lat, lin) : 0u, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0,
+                        t_step[ai0], t_k[ai0], 0.0f};
             const SplitGeom geo{lat, s0, s1, a.nite, (bool)a.flight, (bool)a.same_cross, mirror};
             auto nsize = [&](int axis) { return axis == 0 ? a.n1 : (axis == 1 ? a.n2 : a.n3); };
             DomainStream perm;
@@ -167,7 +168,6 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
             const bool p1st = (pass == 0);
 
             for (int i = 0; i < a.tn; ++i) {
-                const unsigned cell = (active && a.flight) ? cell_at<BITS>(lat, wk.lin) : 0u;
                 float u1, u2;
                 if (phase == 0) {
                     float u[6];
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                     float v0, v1, v2;
                     split_direction(u1, u2, v0, v1, v2);
                     if (p1st) { h.T0 += v0; h.T1 += v1; h.T2 += v2; }
-                    split_step<NC, BITS, 0>(wk, cell, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio, perm, nsize, h);
+                    split_step<NC, BITS, 0>(wk, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio, perm, nsize, h);
                 }
                 const float o0 = wk.o0, o1 = wk.o1, o2 = wk.o2;
                 const int D0 = wk.D0, D1 = wk.D1, D2 = wk.D2;

@@ -461,7 +461,8 @@ int prepare_lattice(rms_sim* s, cudaStream_t st, bool split, int bits) {
     // Nc decides it for all its members)
     if (split && (!d->packed_valid || d->packed_bits != bits)) {
         RMS_CUDA(d->packed.ensure(padded_lattice_bytes(s->n1, s->n2, s->n3, bits)));
-        int pe = pack_lattice_padded(d->labels.as<uint8_t>(), s->n1, s->n2, s->n3, bits, d->packed.as<uint8_t>(), st);
+        int pe = pack_lattice_padded(d->labels.as<uint8_t>(), s->n1, s->n2, s->n3, bits,
+                                     s->boundary == RMS_BOUNDARY_MIRROR ? 1 : 0, d->packed.as<uint8_t>(), st);
         if (pe) return cuda_fail((cudaError_t)pe, "label packing");
         d->packed_valid = true;
         d->packed_bits = bits;

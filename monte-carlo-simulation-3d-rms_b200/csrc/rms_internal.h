@@ -111,7 +111,9 @@ int split_variant_minb(int variant);    // its minimum resident blocks per SM
 // walk, the no-allocation one included), else one byte.
 int split_lattice_bits(int nc);
 size_t padded_lattice_bytes(int n1, int n2, int n3, int bits);
-int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits, uint8_t* out, void* stream);
+// mirror: flag voxels at the lattice's faces too (mirror walls; see pad_pack_kernel)
+int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits, int mirror, uint8_t* out,
+                        void* stream);
 int launch_reduce_slots(const double* slots, int nslots, size_t row, double* out, void* stream);
 // Resident blocks per SM of the walk kernels (occupancy API); -1 on error.
 int walk_compat_blocks_per_sm(int nc, bool trace);

@@ -264,7 +264,8 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
         return set_error(RMS_ERR_RANGE, "labelled voxels are below 1e-7 of the lattice; "
                                         "rejection-sampled initial positions would not finish");
 
-    int pe = pack_lattice_padded(d_labels, s->n1, s->n2, s->n3, bits, d_lat, st);
+    int pe = pack_lattice_padded(d_labels, s->n1, s->n2, s->n3, bits, s->boundary == RMS_BOUNDARY_MIRROR ? 1 : 0,
+                                 d_lat, st);
     if (pe) return set_error(RMS_ERR_CUDA, std::string("lattice packing: ") + cudaGetErrorString((cudaError_t)pe));
 
     WalkArgs a{};

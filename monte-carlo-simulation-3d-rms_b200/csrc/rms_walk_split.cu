@@ -298,7 +298,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         }
         const int ai0 = active ? label_at<BITS>(lat, lin) : 0;
         // displacement = D + (offset - Fm) per axis
-        SplitWalker wk{lin, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0, t_step[ai0], t_k[ai0], 0.0f};
+        SplitWalker wk{lin, active ? cell_at<BITS>(lat, lin) : 0u, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0,
+                        t_step[ai0], t_k[ai0], 0.0f};
         const SplitGeom geo{lat, s0, s1, a.nite, flight, same_certain, mirror};
         auto nsize = [&](int axis) { return axis == 0 ? AXF(n1) : (axis == 1 ? AXF(n2) : AXF(n3)); };
         NoHooks hooks;
@@ -320,9 +321,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
         uint32_t dblk = 0u;
 
         for (int i = 0; i < a.tn; ++i) {
-            // the walker's cell (free-flight flag), loaded before the random
-            // numbers so their arithmetic covers the load
-            const unsigned cell = (active && flight) ? cell_at<BITS>(lat, wk.lin) : 0u;
             float u1, u2;
             if (phase == 0) {
                 float u[6];
@@ -340,8 +338,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
                 for (int attempt = 0;; ++attempt) {
                     float v0, v1, v2;
                     split_direction(u1, u2, v0, v1, v2);
-                    const bool back = split_step<NCMAX, BITS, RULE>(wk, cell, v0, v1, v2, geo, t_step, t_k, t_pij,
-                                                                    t_ratio, perm, nsize, hooks);
+                    const bool back = split_step<NCMAX, BITS, RULE>(wk, v0, v1, v2, geo, t_step, t_k, t_pij, t_ratio,
+                                                                    perm, nsize, hooks);
                     if (RULE == 0 || !back) break;
                     // the step is taken back (interaction.m:256-345): rejection
                     // sampling stays put for the step; the equal-step-length leap
@@ -453,10 +451,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) walk_split_kernel(const WalkArgs 
 #undef AXF
 
 // Padded lattice: (n1+2) x (n2+2) x (n3+2), interior = the labels, border =
-// the wall code.  With BITS = 4 or 8 an interior voxel also gets the
-// free-flight flag when its 26 neighbours are interior and share its label.
+// the wall code.  An interior voxel also gets the free-flight flag when its 26
+// neighbours carry its label -- with mirror walls counting only the neighbours
+// inside the lattice (a straight line out through a wall is reflected in the
+// walk), with periodic walls only for voxels off the lattice's faces.
 template <int BITS>
-__global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int n2, int n3,
+__global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int n2, int n3, int mirror,
                                 uint8_t* __restrict__ out, size_t nbytes) {
     const size_t P3 = (size_t)n3 + 2, P2 = (size_t)n2 + 2;
     const size_t nvox = ((size_t)n1 + 2) * P2 * P3;
@@ -474,15 +474,19 @@ __global__ void pad_pack_kernel(const uint8_t* __restrict__ labels, int n1, int 
                 const long i = (long)pi - 1, j = (long)pj - 1, kk = (long)pk - 1;
                 const unsigned lab = labels[((size_t)i * n2 + j) * (size_t)n3 + kk];
                 cell = lab & label_mask<BITS>();
-                if (i >= 1 && i + 1 < n1 && j >= 1 && j + 1 < n2 && kk >= 1 && kk + 1 < n3) {
+                const bool inner = i >= 1 && i + 1 < n1 && j >= 1 && j + 1 < n2 && kk >= 1 && kk + 1 < n3;
+                if (mirror || inner) {
                     bool same = true;
                     for (int di = -1; di <= 1 && same; ++di)
                         for (int dj = -1; dj <= 1 && same; ++dj)
-                            for (int dk = -1; dk <= 1; ++dk)
-                                if (labels[((size_t)(i + di) * n2 + (j + dj)) * (size_t)n3 + (kk + dk)] != lab) {
+                            for (int dk = -1; dk <= 1; ++dk) {
+                                const long qi = i + di, qj = j + dj, qk = kk + dk;
+                                if (qi < 0 || qi >= n1 || qj < 0 || qj >= n2 || qk < 0 || qk >= n3) continue;
+                                if (labels[((size_t)qi * n2 + qj) * (size_t)n3 + qk] != lab) {
                                     same = false;
                                     break;
                                 }
+                            }
                     if (same) cell |= flight_bit<BITS>();
                 }
             }
@@ -563,12 +567,15 @@ size_t padded_lattice_bytes(int n1, int n2, int n3, int bits) {
     return (nv * (size_t)bits + 7) / 8;
 }
 
-int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits, uint8_t* out, void* stream) {
+int pack_lattice_padded(const uint8_t* labels, int n1, int n2, int n3, int bits, int mirror, uint8_t* out,
+                        void* stream) {
     const size_t nbytes = padded_lattice_bytes(n1, n2, n3, bits);
     size_t grid = (nbytes + 255) / 256;
     if (grid > 16384) grid = 16384;
-    if (bits == 4) pad_pack_kernel<4><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
-    else pad_pack_kernel<8><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, out, nbytes);
+    if (bits == 4)
+        pad_pack_kernel<4><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, mirror, out, nbytes);
+    else
+        pad_pack_kernel<8><<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(labels, n1, n2, n3, mirror, out, nbytes);
     return (int)cudaGetLastError();
 }
 

@@ -22,6 +22,7 @@ namespace rms {
 // A walker between steps.
 struct SplitWalker {
     unsigned lin;            // voxel: linear index into the padded lattice
+    unsigned cell;           // its lattice cell (label + free-flight flag)
     float o0, o1, o2;        // in-voxel offset along each axis, 0..1 (1: on the upper face)
     int D0, D1, D2;          // integer part of the displacement: voxel - origin image
     float Fm0, Fm1, Fm2;     // fractional part of the origin image (mirrored at walls)
@@ -50,47 +51,75 @@ struct NoHooks {
     __device__ __forceinline__ void bernoulli(bool, float) {}
 };
 
-// One step of walker s in direction v (unit vector).  cell: the lattice cell
-// of the walker's voxel (cell_at(lat, s.lin)), loaded by the caller ahead of
-// the step's other work.  Tables: t_step[c], t_k[c], t_pij[a * NCMAX + b],
-// t_ratio[a * NCMAX + b] (step[b] / step[a]).
+// One step of walker s in direction v (unit vector); s.cell is the cell of
+// the walker's voxel, and the step leaves the new voxel's cell there.
+// Tables: t_step[c], t_k[c], t_pij[a * NCMAX + b], t_ratio[a * NCMAX + b]
+// (step[b] / step[a]).
 // nsize(axis) gives the lattice size along an axis (read where needed so it
 // holds no registers).  Returns true when RULE != 0 and a membrane turned the
 // step back (the caller's rule decides); the walker is then mid-step.
 template <int NCMAX, int BITS, int RULE, class NSize, class Hooks>
-__device__ __forceinline__ bool split_step(SplitWalker& s, unsigned cell, float v0, float v1, float v2, const SplitGeom& g,
+__device__ __forceinline__ bool split_step(SplitWalker& s, float v0, float v1, float v2, const SplitGeom& g,
                                            const float* t_step, const float* t_k, const float* t_pij,
                                            const float* t_ratio, DomainStream& perm, NSize nsize, Hooks& h) {
     constexpr int kWall = wall_code<BITS>();
     const uint8_t* __restrict__ lat = g.lat;
     const int s0 = g.s0, s1 = g.s1;
     const unsigned nu = (v0 > 0.0f ? 1u : 0u) | (v1 > 0.0f ? 2u : 0u) | (v2 > 0.0f ? 4u : 0u);
-    // Free flight: a voxel whose 26 neighbours all carry its label (none a
-    // wall) has a flag bit; a step from there (shorter than a voxel) moves as
-    // one straight line -- the face loop's own outcome, since every face on the
-    // way is a same-label face, always crossed, with at most three crossings
-    // (within nite = 4).  Other voxels take the face loop.  (Checking the
-    // neighbours a step from an unflagged voxel actually passes settles more
-    // steps without the face loop, but measured on the 64-axon batch it costs
-    // every warp with such a lane more than the face loops it saves.)
-    bool straight = false;
-    int ik0 = 0, ik1 = 0, ik2 = 0;
-    float o0n = 0.0f, o1n = 0.0f, o2n = 0.0f;
-    if (g.flight) {
-        const float x0 = fmaf(s.cur_step, v0, s.o0);
-        const float x1 = fmaf(s.cur_step, v1, s.o1);
-        const float x2 = fmaf(s.cur_step, v2, s.o2);
-        const float k0 = floorf(x0), k1 = floorf(x1), k2 = floorf(x2);
-        ik0 = (int)k0; ik1 = (int)k1; ik2 = (int)k2;
-        o0n = x0 - k0; o1n = x1 - k1; o2n = x2 - k2;
-        straight = (cell & flight_bit<BITS>()) != 0u;
-    }
-    if (straight) {
-        s.lin += (unsigned)(ik0 * s0 + ik1 * s1 + ik2);
+    // Free flight: a voxel whose 26 neighbours all carry its label has a flag
+    // bit; a step from there (shorter than a voxel) moves as one straight line
+    // -- the face loop's own outcome, since every face on the way is a
+    // same-label face, always crossed, with at most three crossings (within
+    // nite = 4).  With mirror walls, voxels at the lattice's faces are flagged
+    // when their neighbours inside the lattice carry their label: a line that
+    // leaves through a wall is reflected there (the origin image mirrored), as
+    // the face loop reflects it.  The new voxel's cell, which the next step
+    // needs anyway, tells: it is a wall only if the line left the lattice.
+    // Other voxels take the face loop.  (Checking the neighbours a step from an
+    // unflagged voxel actually passes settles more steps without the face loop,
+    // but measured on the 64-axon batch it costs every warp with such a lane
+    // more than the face loops it saves.)
+    if (g.flight && (s.cell & flight_bit<BITS>())) {
+        float x0 = fmaf(s.cur_step, v0, s.o0);
+        float x1 = fmaf(s.cur_step, v1, s.o1);
+        float x2 = fmaf(s.cur_step, v2, s.o2);
+        float k0 = floorf(x0), k1 = floorf(x1), k2 = floorf(x2);
+        int ik0 = (int)k0, ik1 = (int)k1, ik2 = (int)k2;
+        unsigned lj = s.lin + (unsigned)(ik0 * s0 + ik1 * s1 + ik2);
+        unsigned cj = cell_at<BITS>(lat, lj);
+        if ((cj & label_mask<BITS>()) == (unsigned)kWall) {
+            // out through one or more mirror walls: reflect on each axis whose
+            // face neighbour is a wall (x -> -x below the voxel, 2 - x above)
+            if (ik0 != 0 && label_at<BITS>(lat, s.lin + (unsigned)(ik0 * s0)) == kWall) {
+                const bool hi = ik0 > 0;
+                const int nh = nsize(0), gw = hi ? nh - 1 : 0;
+                int I = gw - s.D0; mirror_origin(I, s.Fm0, hi, nh); s.D0 = gw - I;
+                x0 = hi ? 2.0f - x0 : -x0; k0 = 0.0f; ik0 = 0;
+                h.reflect(0);
+            }
+            if (ik1 != 0 && label_at<BITS>(lat, s.lin + (unsigned)(ik1 * s1)) == kWall) {
+                const bool hi = ik1 > 0;
+                const int nh = nsize(1), gw = hi ? nh - 1 : 0;
+                int I = gw - s.D1; mirror_origin(I, s.Fm1, hi, nh); s.D1 = gw - I;
+                x1 = hi ? 2.0f - x1 : -x1; k1 = 0.0f; ik1 = 0;
+                h.reflect(1);
+            }
+            if (ik2 != 0 && label_at<BITS>(lat, s.lin + (unsigned)ik2) == kWall) {
+                const bool hi = ik2 > 0;
+                const int nh = nsize(2), gw = hi ? nh - 1 : 0;
+                int I = gw - s.D2; mirror_origin(I, s.Fm2, hi, nh); s.D2 = gw - I;
+                x2 = hi ? 2.0f - x2 : -x2; k2 = 0.0f; ik2 = 0;
+                h.reflect(2);
+            }
+            lj = s.lin + (unsigned)(ik0 * s0 + ik1 * s1 + ik2);
+            cj = cell_at<BITS>(lat, lj);
+        }
+        s.lin = lj;
+        s.cell = cj;
         s.D0 += ik0; s.D1 += ik1; s.D2 += ik2;
         s.w32 = fmaf(s.cur_step, s.cur_k, s.w32);
         h.path(s.ai, s.cur_step);
-        s.o0 = o0n; s.o1 = o1n; s.o2 = o2n;
+        s.o0 = x0 - k0; s.o1 = x1 - k1; s.o2 = x2 - k2;
         return false;
     }
     // the face loop: up to nite segments, one face event each, on the distances
@@ -187,6 +216,7 @@ __device__ __forceinline__ bool split_step(SplitWalker& s, unsigned cell, float 
     s.o0 = (up & 1u) ? 1.0f - d0 : d0;
     s.o1 = (up & 2u) ? 1.0f - d1 : d1;
     s.o2 = (up & 4u) ? 1.0f - d2 : d2;
+    s.cell = cell_at<BITS>(lat, s.lin);
     return false;
 }
 

@@ -278,6 +278,22 @@ static int homogeneous(const or_params* p, const int g[3]) {
     return 1;
 }
 
+/* Free flight with mirror walls: the voxel's neighbours inside the lattice
+ * all carry its label (monte-carlo-simulation-3d-rms_b200/csrc/split_step.cuh:
+ * a straight line out through a mirror wall is reflected there, the face
+ * loop's own outcome). */
+static int homogeneous_walls(const or_params* p, const int g[3]) {
+    const uint8_t lab = p->labels[lin(p, g[0], g[1], g[2])];
+    for (int a = -1; a <= 1; a++)
+        for (int b = -1; b <= 1; b++)
+            for (int c = -1; c <= 1; c++) {
+                const int q0 = g[0] + a, q1 = g[1] + b, q2 = g[2] + c;
+                if (q0 < 0 || q0 >= p->n1 || q1 < 0 || q1 >= p->n2 || q2 < 0 || q2 >= p->n3) continue;
+                if (p->labels[lin(p, q0, q1, q2)] != lab) return 0;
+            }
+    return 1;
+}
+
 /* Adjoint bookkeeping of one walker (or_adjoint_split; the GPU kernel's
  * pass-1 quantities, restated in FP64): the tangent of the displacement with
  * respect to the step length l with the event sequence frozen (gains the step
@@ -347,11 +363,19 @@ static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, doub
         rem = p->step[ai];
         flo = 0; fhi = 0; nev = 0;
         ev = 0;
-        if (flight && homogeneous(p, g)) {
-            /* a straight line within the homogeneous neighbourhood */
+        if (flight && (p->boundary == OR_BOUNDARY_MIRROR ? homogeneous_walls(p, g) : homogeneous(p, g))) {
+            /* a straight line within the homogeneous neighbourhood, reflected at
+             * mirror walls (the origin image mirrored at the end of the step) */
             for (int a = 0; a < 3; a++) {
-                const double x = f[a] + rem * v[a];
-                const double k = floor(x);
+                double x = f[a] + rem * v[a];
+                double k = floor(x);
+                if (g[a] + (int)k < 0) {
+                    x = -x; k = 0.0; flo |= 1 << a;
+                    if (adj) adj->T[a] = -adj->T[a];
+                } else if (g[a] + (int)k >= NPix[a]) {
+                    x = 2.0 - x; k = 0.0; fhi |= 1 << a;
+                    if (adj) adj->T[a] = -adj->T[a];
+                }
                 g[a] += (int)k;
                 f[a] = x - k;
             }
