@@ -35,7 +35,7 @@ class OrParams(C.Structure):
         ("nbvec", C.c_int), ("bval", C.POINTER(C.c_double)), ("bvec", C.POINTER(C.c_double)),
         ("td", C.POINTER(C.c_double)), ("ngrad", C.c_int), ("grad", C.POINTER(C.c_double)),
         ("nwave", C.c_int), ("nbins", C.c_int), ("wave", C.POINTER(C.c_double)),
-        ("rule", C.c_int),
+        ("rule", C.c_int), ("no_flight", C.c_int),
     ]
 
 
@@ -122,7 +122,7 @@ class Job:
 
     def __init__(self, labels, *, dt, tn, npar, res, step, t2_steps, pij, seed,
                  timepoints=1000, nite=4, boundary=BOUNDARY_MIRROR,
-                 bval=None, bvec=None, td=None, grad=None, wave=None, rule=0):
+                 bval=None, bvec=None, td=None, grad=None, wave=None, rule=0, no_flight=False):
         self.labels = np.ascontiguousarray(labels, dtype=np.uint8)
         self.n1, self.n2, self.n3 = self.labels.shape
         self.dt, self.tn, self.npar, self.res = float(dt), int(tn), int(npar), float(res)
@@ -137,6 +137,7 @@ class Job:
         self.wave = np.ascontiguousarray(wave if wave is not None else np.zeros((0, 0, 3)), dtype=np.float64)
         self.nwave, self.nbins = (self.wave.shape[0], self.wave.shape[1]) if wave is not None else (0, 0)
         self.rule = int(rule)
+        self.no_flight = int(bool(no_flight))   # split replay: every step through the face loop
         self.bval = np.ascontiguousarray(bval if bval is not None else np.zeros(0), dtype=np.float64)
         self.bvec = np.ascontiguousarray(bvec if bvec is not None else np.zeros(0), dtype=np.float64).reshape(-1)
         self.nbvec = self.bval.size if self.mode == MODE_NARROW else 0
@@ -154,7 +155,7 @@ class Job:
             _dp(self.step), _dp(self.t2), _dp(self.pij),
             self.labels.ctypes.data_as(C.POINTER(C.c_uint8)),
             self.nbvec, _dp(self.bval), _dp(self.bvec), _dp(self.td),
-            self.ngrad, _dp(self.grad), self.nwave, self.nbins, _dp(self.wave), self.rule)
+            self.ngrad, _dp(self.grad), self.nwave, self.nbins, _dp(self.wave), self.rule, self.no_flight)
 
     def empty_outputs(self):
         T = self.timepoints

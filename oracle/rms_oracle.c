@@ -315,7 +315,7 @@ static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, doub
     const int Nc = p->nc;
     /* free flight applies when same-label faces are always crossed, no walker
      * can enter compartment 0, and three crossings fit the sub-segment cap */
-    int flight = p->nite >= 4;
+    int flight = p->nite >= 4 && !p->no_flight;
     for (int c = 1; c < Nc; c++)
         if (!(p->pij[c * Nc + c] > 0.999999) || !(p->pij[c * Nc] < 0.000001)) flight = 0;
     const int Tstep = p->tn / p->timepoints;

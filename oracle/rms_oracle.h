@@ -63,6 +63,8 @@ typedef struct or_params {
     /* membrane rule of the split replay: reflect (the reference), reject
      * (stay for the step) or leap (redraw the direction), interaction.m */
     int rule;
+    int no_flight;       /* 1: every split-replay step through the face loop (a
+                            check that the straight moves are its outcome) */
 } or_params;
 
 #define OR_RULE_REFLECT 0
