@@ -835,12 +835,16 @@ def run_adjoint_bench(args):
                           wave=np.einsum("jab,nb->jna", R, gg), timepoints=1000, boundary="periodic",
                           permeation="kappa", kappa=kappa)
 
-    def loss(gg=g, D=par["D"], kappa=par["kappa"], t2=par["t2"]):
+    def signal(gg=g, D=par["D"], kappa=par["kappa"], t2=par["t2"]):
+        """Normalised signal per direction, [nw, 2] (cos, sin sums / walkers)."""
         s_ = sim(gg, D, kappa, t2)
         s_.run(seed=9, precision="split")
-        v = float((s_.get("sigw").reshape(-1, 2) * W).sum() / npar)
+        v = s_.get("sigw").reshape(-1, 2) / npar
         s_.close()
         return v
+
+    def loss(**kw):
+        return float((signal(**kw) * W).sum())
 
     s0 = sim(g, **par)
     for _ in range(args.warmup):
@@ -897,6 +901,7 @@ def run_adjoint_bench(args):
     se_p = float(np.std(shard_g["D_pathwise"], ddof=1) / np.sqrt(8))
     out["D"]["pathwise"] = {"value": r["d_diffusivity_pathwise"], "std_err": se_p,
                             "rel_err_vs_slope": abs(r["d_diffusivity_pathwise"] / out["D"]["slope_5pct"] - 1)}
+    per_dir = per_direction_checks(s0, signal, npar, nw, par, h)
     ws = npar * tn * 2
     line = {
         "metric": ADJOINT_METRIC, "value": ws / (adj_ms * 1e-3), "unit": "walker-steps/s", "n_gpus": 1, "steps": 1,
@@ -908,9 +913,65 @@ def run_adjoint_bench(args):
         "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
         "e2e": {"value": ws / adj_s, "unit": "walker-steps/s", "h2d_bytes_per_step": int(lab.nbytes),
                 "d2h_bytes_per_step": int(r["d_wave"].nbytes)},
-        "gradient_checks": out, "loss": r["loss"], "gpu_launches": 1,
+        "gradient_checks": out, "signal_gradients": per_dir, "loss": r["loss"], "gpu_launches": 1,
     }
     print(json.dumps(line), flush=True)
+
+
+def per_direction_checks(s0, signal, npar, nw, par, h):
+    """dS_j/dtheta for each direction's signal S_j = mean s0 cos(phi_j) (the
+    reference's PGSE signal, main_PGSE.cu:348-357) and theta = D, kappa, T2:
+    one reverse pass per direction (the adjoint with unit weight on C_j),
+    each as 8 walker shards for its standard error, against central finite
+    differences with common random numbers (h relative) and a least-squares
+    slope over +-5 % (7 points; its standard error from the fit)."""
+    adj = {"D": np.zeros((8, nw)), "kappa": np.zeros((8, nw)), "T2[1]": np.zeros((8, nw)), "T2[2]": np.zeros((8, nw))}
+    for j in range(nw):
+        gup = np.zeros((nw, 2))
+        gup[j, 0] = 1.0 / npar
+        for k in range(8):
+            rk = s0.adjoint(gup.reshape(-1), seed=9, walker_range=(npar * k // 8, npar * (k + 1) // 8))
+            adj["D"][k, j] = rk["d_diffusivity"]
+            adj["kappa"][k, j] = rk["d_kappa"]
+            adj["T2[1]"][k, j] = rk["d_t2"][1]
+            adj["T2[2]"][k, j] = rk["d_t2"][2]
+    t2 = par["t2"]
+
+    def vary(name, x):
+        if name == "D":
+            return signal(D=x)[:, 0]
+        if name == "kappa":
+            return signal(kappa=x)[:, 0]
+        c = int(name[3])
+        tt = t2.copy()
+        tt[c] = x
+        return signal(t2=tt)[:, 0]
+
+    x0s = {"D": par["D"], "kappa": par["kappa"], "T2[1]": t2[1], "T2[2]": t2[2]}
+    res = {}
+    for name, x0 in x0s.items():
+        a = adj[name].sum(axis=0)
+        se = adj[name].std(axis=0, ddof=1) * np.sqrt(8)
+        fd = (vary(name, x0 * (1 + h)) - vary(name, x0 * (1 - h))) / (2 * h * x0)
+        ent = {"adjoint": a.tolist(), "adjoint_std_err": se.tolist(), "finite_difference": fd.tolist(),
+               "rel_err_vs_fd": np.abs(a / fd - 1).tolist()}
+        if name in ("D", "kappa"):
+            xs = x0 * (1 + 0.05 * np.linspace(-1, 1, 7))
+            ys = np.stack([vary(name, x) for x in xs])          # [7, nw]
+            sl, sl_se = np.zeros(nw), np.zeros(nw)
+            for j in range(nw):
+                coef, cov = np.polyfit(xs, ys[:, j], 1, cov=True)
+                sl[j], sl_se[j] = coef[0], np.sqrt(cov[0, 0])
+            ent.update(slope_5pct=sl.tolist(), slope_std_err=sl_se.tolist(),
+                       rel_err_vs_slope=np.abs(a / sl - 1).tolist(),
+                       z_vs_slope=((a - sl) / np.sqrt(se ** 2 + sl_se ** 2)).tolist())
+        rel = np.array(ent.get("rel_err_vs_slope", ent["rel_err_vs_fd"]))
+        ent["summary"] = {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+                          "max_rel_err_vs_fd": float(np.max(ent["rel_err_vs_fd"])),
+                          "median_rel_std_err": float(np.median(np.abs(se / a)))}
+        res[name] = ent
+    return {"of": "S_j = mean over walkers of s0 cos(phi_j), each of the 16 directions", "walkers": npar,
+            "shards": 8, "h": h, **res}
 
 
 CONTRACT_METRIC = "walker-waveform phases/s of the multi-waveform phase contraction (signal mean(cos, sin))"
