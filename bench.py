@@ -835,10 +835,10 @@ def run_adjoint_bench(args):
                           wave=np.einsum("jab,nb->jna", R, gg), timepoints=1000, boundary="periodic",
                           permeation="kappa", kappa=kappa)
 
-    def signal(gg=g, D=par["D"], kappa=par["kappa"], t2=par["t2"]):
+    def signal(gg=g, D=par["D"], kappa=par["kappa"], t2=par["t2"], seed=9):
         """Normalised signal per direction, [nw, 2] (cos, sin sums / walkers)."""
         s_ = sim(gg, D, kappa, t2)
-        s_.run(seed=9, precision="split")
+        s_.run(seed=seed, precision="split")
         v = s_.get("sigw").reshape(-1, 2) / npar
         s_.close()
         return v
@@ -918,60 +918,77 @@ def run_adjoint_bench(args):
     print(json.dumps(line), flush=True)
 
 
-def per_direction_checks(s0, signal, npar, nw, par, h):
+def per_direction_checks(s0, signal, npar, nw, par, h, seeds=range(21, 29)):
     """dS_j/dtheta for each direction's signal S_j = mean s0 cos(phi_j) (the
     reference's PGSE signal, main_PGSE.cu:348-357) and theta = D, kappa, T2:
     one reverse pass per direction (the adjoint with unit weight on C_j),
-    each as 8 walker shards for its standard error, against central finite
-    differences with common random numbers (h relative) and a least-squares
-    slope over +-5 % (7 points; its standard error from the fit)."""
-    adj = {"D": np.zeros((8, nw)), "kappa": np.zeros((8, nw)), "T2[1]": np.zeros((8, nw)), "T2[2]": np.zeros((8, nw))}
-    for j in range(nw):
-        gup = np.zeros((nw, 2))
-        gup[j, 0] = 1.0 / npar
-        for k in range(8):
-            rk = s0.adjoint(gup.reshape(-1), seed=9, walker_range=(npar * k // 8, npar * (k + 1) // 8))
-            adj["D"][k, j] = rk["d_diffusivity"]
-            adj["kappa"][k, j] = rk["d_kappa"]
-            adj["T2[1]"][k, j] = rk["d_t2"][1]
-            adj["T2[2]"][k, j] = rk["d_t2"][2]
+    against central finite differences with common random numbers (h
+    relative) and the least-squares slope over +-5 % (7 points).  Every
+    estimate is repeated over independent seeds and compared as seed means
+    with standard errors from the seed spread: with common random numbers the
+    7 points of one slope share their walkers, so a fit's residuals
+    understate its error."""
     t2 = par["t2"]
-
-    def vary(name, x):
-        if name == "D":
-            return signal(D=x)[:, 0]
-        if name == "kappa":
-            return signal(kappa=x)[:, 0]
-        c = int(name[3])
-        tt = t2.copy()
-        tt[c] = x
-        return signal(t2=tt)[:, 0]
-
+    names = ("D", "kappa", "T2[1]", "T2[2]")
     x0s = {"D": par["D"], "kappa": par["kappa"], "T2[1]": t2[1], "T2[2]": t2[2]}
+    ns = len(seeds)
+    adj = {k: np.zeros((ns, nw)) for k in names + ("kappa_score",)}
+    fd = {k: np.zeros((ns, nw)) for k in names}
+    sl = {k: np.zeros((ns, nw)) for k in ("D", "kappa")}
+
+    def vary(name, x, seed):
+        if name == "D":
+            return signal(D=x, seed=seed)[:, 0]
+        if name == "kappa":
+            return signal(kappa=x, seed=seed)[:, 0]
+        tt = t2.copy()
+        tt[int(name[3])] = x
+        return signal(t2=tt, seed=seed)[:, 0]
+
+    for si, seed in enumerate(seeds):
+        for j in range(nw):
+            gup = np.zeros((nw, 2))
+            gup[j, 0] = 1.0 / npar
+            r = s0.adjoint(gup.reshape(-1), seed=seed)
+            adj["D"][si, j] = r["d_diffusivity"]
+            adj["kappa"][si, j] = r["d_kappa"]
+            adj["kappa_score"][si, j] = r["d_kappa_score"]
+            adj["T2[1]"][si, j] = r["d_t2"][1]
+            adj["T2[2]"][si, j] = r["d_t2"][2]
+        for name, x0 in x0s.items():
+            fd[name][si] = (vary(name, x0 * (1 + h), seed) - vary(name, x0 * (1 - h), seed)) / (2 * h * x0)
+        for name in ("D", "kappa"):
+            xs = x0s[name] * (1 + 0.05 * np.linspace(-1, 1, 7))
+            ys = np.stack([vary(name, x, seed) for x in xs])          # [7, nw]
+            sl[name][si] = np.polyfit(xs, ys, 1)[0]
+
+    def mse(a):
+        return a.mean(axis=0), a.std(axis=0, ddof=1) / np.sqrt(ns)
+
     res = {}
-    for name, x0 in x0s.items():
-        a = adj[name].sum(axis=0)
-        se = adj[name].std(axis=0, ddof=1) * np.sqrt(8)
-        fd = (vary(name, x0 * (1 + h)) - vary(name, x0 * (1 - h))) / (2 * h * x0)
-        ent = {"adjoint": a.tolist(), "adjoint_std_err": se.tolist(), "finite_difference": fd.tolist(),
-               "rel_err_vs_fd": np.abs(a / fd - 1).tolist()}
-        if name in ("D", "kappa"):
-            xs = x0 * (1 + 0.05 * np.linspace(-1, 1, 7))
-            ys = np.stack([vary(name, x) for x in xs])          # [7, nw]
-            sl, sl_se = np.zeros(nw), np.zeros(nw)
-            for j in range(nw):
-                coef, cov = np.polyfit(xs, ys[:, j], 1, cov=True)
-                sl[j], sl_se[j] = coef[0], np.sqrt(cov[0, 0])
-            ent.update(slope_5pct=sl.tolist(), slope_std_err=sl_se.tolist(),
-                       rel_err_vs_slope=np.abs(a / sl - 1).tolist(),
-                       z_vs_slope=((a - sl) / np.sqrt(se ** 2 + sl_se ** 2)).tolist())
-        rel = np.array(ent.get("rel_err_vs_slope", ent["rel_err_vs_fd"]))
+    for name in names:
+        a, ase = mse(adj[name])
+        f, fse = mse(fd[name])
+        ent = {"adjoint": a.tolist(), "adjoint_std_err": ase.tolist(), "finite_difference": f.tolist(),
+               "finite_difference_std_err": fse.tolist(), "rel_err_vs_fd": np.abs(a / f - 1).tolist(),
+               "z_vs_fd": ((a - f) / np.hypot(ase, fse)).tolist()}
+        ref = f
+        if name in sl:
+            b, bse = mse(sl[name])
+            ent.update(slope_5pct=b.tolist(), slope_std_err=bse.tolist(), rel_err_vs_slope=np.abs(a / b - 1).tolist(),
+                       z_vs_slope=((a - b) / np.hypot(ase, bse)).tolist())
+            ref = b
+        if name == "kappa":
+            c, cse = mse(adj["kappa_score"])
+            ent["score_function"] = {"value": c.tolist(), "std_err": cse.tolist()}
+        rel = np.abs(a / ref - 1)
         ent["summary"] = {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
                           "max_rel_err_vs_fd": float(np.max(ent["rel_err_vs_fd"])),
-                          "median_rel_std_err": float(np.median(np.abs(se / a)))}
+                          "median_rel_std_err": float(np.median(np.abs(ase / a))),
+                          "median_abs_z": float(np.median(np.abs(ent.get("z_vs_slope", ent["z_vs_fd"]))))}
         res[name] = ent
-    return {"of": "S_j = mean over walkers of s0 cos(phi_j), each of the 16 directions", "walkers": npar,
-            "shards": 8, "h": h, **res}
+    return {"of": "S_j = mean over walkers of s0 cos(phi_j), each of the 16 directions", "walkers_per_seed": npar,
+            "seeds": list(seeds), "h": h, **res}
 
 
 CONTRACT_METRIC = "walker-waveform phases/s of the multi-waveform phase contraction (signal mean(cos, sin))"

@@ -376,8 +376,16 @@ int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint
  *   d_wave[nwave*nbins*3]  dL/dwave, the layout of rms_config.wave; exact
  *                          pathwise (the phase is linear in the waveform)
  *   d_t2[c]                dL/dT2_c (ms), analytic through s0
- *   d_kappa                dL/dkappa, score function of the permeation
- *                          draws (RMS_PERM_KAPPA with kappa > 0, else 0)
+ *   d_kappa                dL/dkappa (RMS_PERM_KAPPA with kappa > 0, else
+ *                          0) by forced draws: per walker with nb > 0
+ *                          permeation draws, one of them (chosen uniformly)
+ *                          is walked the other way with the rest of the walk
+ *                          on the same streams, and nb Pij (1 - Pij)
+ *                          (L[crossed] - L[reflected]) / kappa is summed (the
+ *                          weak derivative of the Bernoulli draws; unbiased)
+ *   d_kappa_score          the same derivative by the score function of the
+ *                          draws, sum_w (L_w - mean L) sum (1[crossed] - Pij)
+ *                          / kappa (unbiased, noisier where crossings are rare)
  *   d_diffusivity          dL/dD by time rescaling: a walk with D(1 + eps)
  *                          and kappa(1 + eps) over [0, T] is, in law, the
  *                          D-walk over [0, T(1 + eps)], so D dL/dD is the
@@ -389,15 +397,16 @@ int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint
  *                          draws; it is exact for the continuum process and
  *                          carries the walk's time-discretisation error
  *   d_diffusivity_pathwise dL/dD through the step length with the event
- *                          sequence fixed (plus the score through the
- *                          kappa-mode permeation probability): low variance,
+ *                          sequence fixed (plus the forced-draw term through
+ *                          the kappa-mode permeation probability): low variance,
  *                          exact where the walk is continuous in the step
  *                          length (flat membranes, periodic walls), blind to
  *                          the jumps above; the T2 weight's dependence on D
  *                          through residence times is not included
- * Each walker is walked twice from its random streams (nothing stored).
- * d_wave (caller-allocated host array) and sigw (optional, [nwave*2], the
- * run's own signal sums) may be NULL. */
+ * Each walker is walked two or three times from its random streams (nothing
+ * stored; the third walk only with permeation draws).  d_wave
+ * (caller-allocated host array) and sigw (optional, [nwave*2], the run's own
+ * signal sums) may be NULL. */
 typedef struct rms_adjoint_grads {
     double* d_wave;
     double d_diffusivity;
@@ -406,6 +415,7 @@ typedef struct rms_adjoint_grads {
     double loss;
     double* sigw;
     double d_diffusivity_pathwise;
+    double d_kappa_score;
 } rms_adjoint_grads;
 int rms_adjoint_run(rms_sim* sim, const rms_run_opts* opts, const double* g_sigw, rms_adjoint_grads* out);
 

@@ -8,8 +8,8 @@ T2.  The forward pass is the split walk (rms_sim_run); the backward pass walks
 the same walkers again from their counter-based random streams
 (rms_adjoint_run) instead of storing trajectories.  Gradients: exact pathwise
 for the waveforms, analytic for T2, time rescaling (minus the kappa term) for
-D, score function for kappa.  torch is the plumbing here; all arithmetic runs
-in librms.
+D, forced permeation draws (the weak derivative of the Bernoulli draws) for
+kappa.  torch is the plumbing here; all arithmetic runs in librms.
 """
 from __future__ import annotations
 

@@ -128,12 +128,14 @@ struct FloatStream {
 //            of a warp generate blocks in lock step however many other draws
 //            each lane made;
 //   kDomInit sequential words for the rejection-sampled start position;
-//   kDomPerm sequential words for partial-permeation draws
-// (the last two read as floats, u32_to_float).
+//   kDomPerm sequential words for partial-permeation draws;
+//   kDomForce sequential words of the adjoint's forced-decision choice
+// (the last three read as floats, u32_to_float).
 // counter = (k, domain, walker_lo, walker_hi), key = (seed_lo, seed_hi).
 constexpr uint32_t kDomDir = 0u;
 constexpr uint32_t kDomInit = 1u;
 constexpr uint32_t kDomPerm = 2u;
+constexpr uint32_t kDomForce = 3u;
 
 RMS_HD U4 dir_block(uint32_t k, uint32_t k0, uint32_t k1, uint32_t w0, uint32_t w1) {
     return philox4x32_10(U4{k, kDomDir, w0, w1}, k0, k1);

@@ -19,12 +19,19 @@
 //    sum_j a_jw dphi_jw and L_w t_wc are summed over walkers;
 //  pass 2 walks the walker again and adds a_jw X_wb (X_wb: the bin's
 //    displacement sum, um) into dL/dwave[b][j] -- the phase is linear in the
-//    waveform, so this gradient is exact pathwise.
+//    waveform, so this gradient is exact pathwise;
+//  pass 3 (with permeable membranes) walks every walker that made nb_w > 0
+//    permeation draws once more, with one of those draws, chosen uniformly
+//    (its own counter domain), forced the other way and the rest of the walk
+//    on the same streams, and sums nb_w Pij (1 - Pij) (L_w[crossed] -
+//    L_w[reflected]): the weak derivative of the Bernoulli draws, an unbiased
+//    estimate of dL/dlog P that measures what a crossing changes instead of
+//    correlating the loss with rare crossings as the score function does.
 //
 // The host turns the sums into dL/dwave, dL/dT2_c (analytic), dL/dkappa
-// (score function: dP/dkappa = P/kappa, with the walkers' mean loss as the
-// baseline -- sum_w (L_w - mean L) E_w, unbiased since E[E_w] = 0, and far
-// less noisy than sum_w L_w E_w) and dL/dD.  dL/dD comes from time rescaling:
+// (dP/dkappa = P/kappa: the forced-draw sum / kappa; the score function
+// sum_w (L_w - mean L) E_w / kappa -- unbiased since E[E_w] = 0 -- is kept for
+// comparison) and dL/dD.  dL/dD comes from time rescaling:
 // a walk with diffusivity D(1 + eps) (and permeability kappa(1 + eps)) over
 // [0, T] is, in law, the D-walk over [0, T(1 + eps)], so with x(t) the
 // displacement, g_j the piecewise-constant waveform and W the T2 exponent
@@ -72,10 +79,15 @@ __device__ __forceinline__ float warp_reduce_scatter16f(float (&v)[16], int lane
 // (flipped at every reflection) and the permeation score.
 template <int NC>
 struct AdjHooks {
-    bool rec;             // pass 1 records; pass 2 only walks
+    bool rec;             // pass 1 records; the others only walk
+    bool force;           // pass 3: draw number force_at goes the other way
     float tc[NC];         // path per compartment (voxels)
     float T0, T1, T2;     // d(displacement)/dl, voxels per voxel of step
     float E;              // sum over Bernoulli draws of 1[crossed] - Pij
+    int nb;               // Bernoulli draws so far
+    int force_at;         // pass 3: the draw to flip
+    float Pf;             // pass 3: its Pij
+    bool xf;              // pass 3: its outcome before the flip
     __device__ __forceinline__ void path(int c, float len) {
         if (rec) {
 #pragma unroll
@@ -87,8 +99,15 @@ struct AdjHooks {
             if (axis == 0) T0 = -T0; else if (axis == 1) T1 = -T1; else T2 = -T2;
         }
     }
-    __device__ __forceinline__ void bernoulli(bool cross, float P) {
+    __device__ __forceinline__ bool bernoulli(bool cross, float P) {
         if (rec) E += (cross ? 1.0f : 0.0f) - P;   // d log p / d log P
+        if (force && nb == force_at) {
+            Pf = P;
+            xf = cross;
+            cross = !cross;
+        }
+        ++nb;
+        return cross;
     }
 };
 
@@ -125,12 +144,20 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
 #pragma unroll
         for (int c = 0; c < NC; ++c) h.tc[c] = 0.0f;
         h.E = 0.0f;
+        h.force_at = -1;
+        h.Pf = 0.0f;
+        h.xf = false;
         double w64 = 0.0;
         float tr = 0.0f;   // this walker's time-rescaling derivative dL_w/d(eps)
+        float Lkeep = 0.0f;   // this walker's loss (pass 1)
+        int nb_w = 0;         // its Bernoulli draws (pass 1)
 
-        for (int pass = 0; pass < 2; ++pass) {
+        for (int pass = 0; pass < (a.force ? 3 : 2); ++pass) {
+            // pass 3 walks only the walkers that made a draw, and a warp with
+            // none of them skips it
+            if (pass == 2 && !__any_sync(kFullMask, live && nb_w > 0)) break;
             // start position: uniform in the labelled voxels (the split walk's draws)
-            bool active = live;
+            bool active = live && (pass < 2 || nb_w > 0);
             float f0 = 0.5f, f1 = 0.5f, f2 = 0.5f;
             unsigned lin = 0;
             if (active) {
@@ -160,6 +187,16 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
             float p0 = 0.0f, p1 = 0.0f, p2 = 0.0f;
             h.T0 = h.T1 = h.T2 = 0.0f;
             h.rec = (pass == 0);
+            h.force = (pass == 2);
+            h.nb = 0;
+            if (pass == 2) {
+                // the draw to flip, uniform over this walker's nb_w draws
+                DomainStream fs;
+                fs.init(a.seed, (uint64_t)w, kDomForce);
+                h.force_at = min((int)(fs.next() * (float)nb_w), nb_w - 1);
+#pragma unroll
+                for (int j = 0; j < NW; ++j) phi[j] = 0.0f;
+            }
             float B0 = 0.0f, B1 = 0.0f, B2 = 0.0f;  // bin sums of the tangent
             int bin = 0, next_bin = a.bin_steps;
             float q0 = 0.0f, q1 = 0.0f, q2 = 0.0f, q3 = 0.0f;   // the split walk's direction stream
@@ -202,13 +239,14 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                 if (event) {
                     const double x0 = P0 * (double)a.res, x1 = P1 * (double)a.res, x2 = P2 * (double)a.res;
                     const double* wv = a.wave + (size_t)bin * a.nwave * 3;
-                    if (p1st) {
+                    if (pass != 1) {
+                        // the phases (pass 1: and their tangents; pass 3: of the forced walk)
 #pragma unroll
                         for (int j = 0; j < NW; ++j) {
                             if (j < a.nwave) {
                                 const double g0 = __ldg(wv + 3 * j), g1 = __ldg(wv + 3 * j + 1), g2 = __ldg(wv + 3 * j + 2);
                                 phi[j] += (float)(g0 * x0 + g1 * x1 + g2 * x2);
-                                dphi[j] += (float)((g0 * B0 + g1 * B1 + g2 * B2) * (double)a.res);
+                                if (p1st) dphi[j] += (float)((g0 * B0 + g1 * B1 + g2 * B2) * (double)a.res);
                             }
                         }
                         B0 = B1 = B2 = 0.0f;
@@ -272,6 +310,8 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                 }
                 // the T2 weight under time rescaling: dW/d(eps) = -W + T / T2(c_T)
                 tr += Lw * (float)(w64 - (double)a.tn * (double)(t_step[wk.ai] * t_k[wk.ai]));
+                Lkeep = Lw;
+                nb_w = active ? h.nb : 0;
                 const double L = warp_sum((double)Lw), LE = warp_sum((double)Lw * (double)h.E),
                              GP = warp_sum((double)G), ES = warp_sum(active ? (double)h.E : 0.0);
                 if (lane == 0) {
@@ -287,9 +327,25 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                     const double LT = warp_sum(st > 0.0f ? (double)Lw * (double)(h.tc[c] / st) : 0.0);
                     if (lane == 0) atomicAdd(a.sums + kAdjSumLT + c, LT);
                 }
-            } else {
+            } else if (pass == 1) {
                 const double TR = warp_sum((double)tr);
                 if (lane == 0) atomicAdd(a.sums + kAdjSumTR, TR);
+            } else {
+                // nb_w Pij (1 - Pij) (L[crossed] - L[reflected]) of the forced walk
+                const float s0f = active ? (float)exp(-w64) : 0.0f;
+                float Lf = 0.0f;
+#pragma unroll
+                for (int j = 0; j < NW; ++j) {
+                    if (j < a.nwave) {
+                        float sn, cs;
+                        sincosf(phi[j], &sn, &cs);
+                        Lf += s0f * (__ldg(a.gup + 2 * j) * cs + __ldg(a.gup + 2 * j + 1) * sn);
+                    }
+                }
+                const float dL = h.xf ? Lkeep - Lf : Lf - Lkeep;
+                const double Fw = active ? (double)nb_w * (double)h.Pf * (1.0 - (double)h.Pf) * (double)dL : 0.0;
+                const double F = warp_sum(Fw);
+                if (lane == 0) atomicAdd(a.sums + kAdjSumForce, F);
             }
         }
     }

@@ -1035,6 +1035,13 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
     a.nite = s->nite; a.boundary = s->boundary;
     a.res = x.res;
     a.flight = x.flight; a.same_cross = x.same_cross;
+    // the forced-draw pass runs when some face is crossed by a draw
+    a.force = 0;
+    for (int c = 0; c < s->nc; ++c)
+        for (int e = 0; e < s->nc; ++e) {
+            const float P = x.pij[c * kNcMax + e];
+            if (P >= 0.000001f && !(P > 0.999999f)) a.force = 1;
+        }
     for (int c = 0; c < kAdjNc; ++c) {
         a.step[c] = c < s->nc ? x.step[c] : 0.0f;
         a.kexp[c] = c < s->nc ? x.k[c] : 0.0f;
@@ -1097,20 +1104,24 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
                     out->d_wave[((size_t)j * s->nbins + b) * 3 + k] =
                         s->dt * (double)dw[((size_t)b * s->nwave + j) * 3 + k];
     out->loss = sums[kAdjSumL];
-    // score of the permeation draws with the mean loss as baseline:
+    // dL/dlog P of the permeation draws (Pij = P / (1 + P)), two unbiased
+    // estimates: the forced draws, sum_w nb_w Pij (1 - Pij) (L[crossed] -
+    // L[reflected]); and the score with the mean loss as baseline,
     // sum_w (L_w - L/N) E_w (E[E_w] = 0 keeps it unbiased)
+    const double forced = sums[kAdjSumForce];
     const double score = sums[kAdjSumLE] - sums[kAdjSumL] / (double)(w1 - w0) * sums[kAdjSumE];
     // time rescaling: D dL/dD = sum_w dL_w/deps - kappa dL/dkappa.  In kappa mode
-    // kappa dL/dkappa is the score; with a fixed permeation probability the
+    // kappa dL/dkappa = dL/dlog P; with a fixed permeation probability the
     // continuum permeability of the rescaled walk scales as (1 + eps)^(-1/2)
-    // relative to kappa (1 + eps), so half the score comes off.
+    // relative to kappa (1 + eps), so half of it comes off.
     const bool kap = s->permeation == RMS_PERM_KAPPA;
-    out->d_diffusivity = (sums[kAdjSumTR] - (kap ? score : 0.5 * score)) / D;
+    out->d_diffusivity = (sums[kAdjSumTR] - (kap ? forced : 0.5 * forced)) / D;
     // pathwise, events frozen: l = sqrt(6 D dt) / res, dl/dD = l / (2 D); in
     // kappa mode P ~ kappa D^(-1/2)
     const double step = s->step[s->nc > 1 ? 1 : 0];
-    out->d_diffusivity_pathwise = (sums[kAdjSumPath] * step / 2.0 - (kap ? score / 2.0 : 0.0)) / D;
-    out->d_kappa = (kap && s->kappa > 0.0) ? score / s->kappa : 0.0;
+    out->d_diffusivity_pathwise = (sums[kAdjSumPath] * step / 2.0 - (kap ? forced / 2.0 : 0.0)) / D;
+    out->d_kappa = (kap && s->kappa > 0.0) ? forced / s->kappa : 0.0;
+    out->d_kappa_score = (kap && s->kappa > 0.0) ? score / s->kappa : 0.0;
     for (int c = 0; c < 8; ++c) out->d_t2[c] = 0.0;
     for (int c = 0; c < s->nc; ++c) {
         const double T2 = s->t2[c];

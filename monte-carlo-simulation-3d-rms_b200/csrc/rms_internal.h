@@ -132,8 +132,8 @@ constexpr int kAdjNc = 4;
 // (steps, per compartment), sum_w E_w, the signal sums (cos, sin) per
 // waveform, then sum_w dL_w/deps of the time rescaling (rms_adjoint.cu)
 constexpr int kAdjSumL = 0, kAdjSumLE = 1, kAdjSumPath = 2, kAdjSumLT = 3, kAdjSumE = 3 + kAdjNc,
-              kAdjSumSig = 4 + kAdjNc, kAdjSumTR = kAdjSumSig + 2 * kAdjWaves;
-constexpr int kAdjSums = kAdjSumTR + 1;
+              kAdjSumSig = 4 + kAdjNc, kAdjSumTR = kAdjSumSig + 2 * kAdjWaves, kAdjSumForce = kAdjSumTR + 1;
+constexpr int kAdjSums = kAdjSumForce + 1;
 struct AdjArgs {
     const uint8_t* lat;          // padded 4-bit lattice with free-flight flags
     int n1, n2, n3, s0, s1;
@@ -142,6 +142,7 @@ struct AdjArgs {
     int tn, nbins, bin_steps, nwave, nite, boundary;
     float res;
     int flight, same_cross;
+    int force;                   // a third pass: one permeation decision per walker forced the other way
     float step[kAdjNc], kexp[kAdjNc], pij[kAdjNc * kAdjNc], ratio[kAdjNc * kAdjNc];
     const double* wave;          // [bin][waveform][axis], x dt
     const float* gup;            // [waveform][2]: dL/d(sum cos), dL/d(sum sin)

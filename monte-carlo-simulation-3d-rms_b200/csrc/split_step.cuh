@@ -43,12 +43,13 @@ struct SplitGeom {
 };
 
 // The forward walk's hooks: nothing.  The adjoint's record the path per
-// compartment, flip the displacement tangent at reflections and score the
-// Bernoulli draws.
+// compartment, flip the displacement tangent at reflections, score the
+// Bernoulli draws and, in its forced pass, flip one draw's outcome (bernoulli
+// returns the outcome the step takes).
 struct NoHooks {
     __device__ __forceinline__ void path(int, float) {}
     __device__ __forceinline__ void reflect(int) {}
-    __device__ __forceinline__ void bernoulli(bool, float) {}
+    __device__ __forceinline__ bool bernoulli(bool cross, float) { return cross; }
 };
 
 // One step of walker s in direction v (unit vector); s.cell is the cell of
@@ -186,8 +187,7 @@ __device__ __forceinline__ bool split_step(SplitWalker& s, float v0, float v1, f
                 if (P > 0.999999f) {
                     cross = true;
                 } else if (P >= 0.000001f) {
-                    cross = perm.next() < P;
-                    h.bernoulli(cross, P);
+                    cross = h.bernoulli(perm.next() < P, P);
                 } else {
                     cross = false;
                 }

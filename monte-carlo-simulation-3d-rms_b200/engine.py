@@ -89,7 +89,7 @@ def _opts(seed=0, precision="split", device=0, stream=None, trace_walkers=0, var
 class AdjointGrads(C.Structure):
     _fields_ = [("d_wave", _DP), ("d_diffusivity", C.c_double), ("d_kappa", C.c_double),
                 ("d_t2", C.c_double * 8), ("loss", C.c_double), ("sigw", _DP),
-                ("d_diffusivity_pathwise", C.c_double)]
+                ("d_diffusivity_pathwise", C.c_double), ("d_kappa_score", C.c_double)]
 
 
 _lib = None
@@ -269,11 +269,11 @@ class Sim:
         opts = _opts(seed, "split", device, stream, walker_range=walker_range)
         dwave = np.zeros(nw * nb * 3)
         sigw = np.zeros(2 * nw)
-        out = AdjointGrads(_ptr(dwave), 0.0, 0.0, (C.c_double * 8)(), 0.0, _ptr(sigw), 0.0)
+        out = AdjointGrads(_ptr(dwave), 0.0, 0.0, (C.c_double * 8)(), 0.0, _ptr(sigw), 0.0, 0.0)
         _check(lib().rms_adjoint_run(self._h, C.byref(opts), _ptr(g), C.byref(out)))
         return dict(d_wave=dwave.reshape(nw, nb, 3), d_diffusivity=out.d_diffusivity, d_kappa=out.d_kappa,
                     d_t2=np.array(out.d_t2[:]), loss=out.loss, sigw=sigw.reshape(nw, 2),
-                    d_diffusivity_pathwise=out.d_diffusivity_pathwise)
+                    d_diffusivity_pathwise=out.d_diffusivity_pathwise, d_kappa_score=out.d_kappa_score)
 
     def cumulants(self, dirs=None):
         """(D, K), [timepoints, ndir], along unit directions dirs [ndir, 3]

@@ -122,11 +122,13 @@ static inline float or_stream_float(or_stream* s) {
  * uniforms of steps 3k, 3k+1, 3k+2: its 128 bits (word 0 the most
  * significant) cut into six 21-bit fields from the top, fields 2j and 2j+1
  * for step 3k+j, a field f read as (2f + 1) 2^-22.  Domain 1: start
- * positions, sequential.  Domain 2: partial-permeation draws, sequential
- * (words read as floats, or_u32_to_float). */
+ * positions, sequential.  Domain 2: partial-permeation draws, sequential.
+ * Domain 3: the adjoint's choice of the permeation decision it forces,
+ * sequential (words read as floats, or_u32_to_float). */
 #define OR_DOM_DIR 0u
 #define OR_DOM_INIT 1u
 #define OR_DOM_PERM 2u
+#define OR_DOM_FORCE 3u
 
 static inline float or_u21_to_float(uint32_t f) {
     return (float)(2u * (f & 0x1fffffu) + 1u) * 0x1p-22f;

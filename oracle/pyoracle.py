@@ -303,12 +303,14 @@ def contract_phases_fp64(pos, wave, chunk: int = 65536):
 def adjoint_split(job: "Job", gup, w_begin: int = 0, w_end: Optional[int] = None):
     """Walker sums of the split walk's adjoint in waveform mode (or_adjoint_split,
     the FP64 restatement of csrc/rms_adjoint.cu): dict with L, LE, path, E,
-    LT [nc], sigw [nwave, 2] and dwave [nbins, nwave, 3] (sum of a_jw X_wb, um)."""
+    LT [nc], sigw [nwave, 2], TR (time rescaling), F (forced permeation
+    decisions: the sum of nb Pij (1 - Pij) (L[crossed] - L[reflected])) and
+    dwave [nbins, nwave, 3] (sum of a_jw X_wb, um)."""
     lib = oracle_lib()
     if w_end is None:
         w_end = job.npar
     g = np.ascontiguousarray(np.asarray(gup, dtype=np.float64).reshape(-1))
-    sums = np.zeros(4 + job.nc + 2 * job.nwave + 1)
+    sums = np.zeros(4 + job.nc + 2 * job.nwave + 2)
     dw = np.zeros(job.nbins * job.nwave * 3)
     p = job.params()
     rc = lib.or_adjoint_split(C.byref(p), _dp(g), C.c_int64(w_begin), C.c_int64(w_end), _dp(sums), _dp(dw))
@@ -317,26 +319,30 @@ def adjoint_split(job: "Job", gup, w_begin: int = 0, w_end: Optional[int] = None
     nc, nw = job.nc, job.nwave
     return dict(L=sums[0], LE=sums[1], path=sums[2], E=sums[3], LT=sums[4:4 + nc].copy(),
                 sigw=sums[4 + nc:4 + nc + 2 * nw].reshape(-1, 2).copy(), TR=sums[4 + nc + 2 * nw],
+                F=sums[5 + nc + 2 * nw],
                 dwave=dw.reshape(job.nbins, job.nwave, 3))
 
 
 def adjoint_gradients(job: "Job", sums: dict, D: float, t2, kappa: Optional[float] = None, nwalk: Optional[int] = None):
     """The gradients the library's host code forms from the adjoint walker sums
     (monte-carlo-simulation-3d-rms_b200/csrc/rms_api.cpp, run_adjoint):
-    dL/dwave = dt sum a X; the permeation score with the mean loss as baseline;
-    dL/dD by time rescaling, (TR - score [kappa mode] or TR - score / 2) / D;
-    the pathwise dL/dD = (path l / 2 - score / 2 [kappa mode]) / D
-    (l = sqrt(6 D dt)/res); dL/dkappa = score / kappa;
+    dL/dwave = dt sum a X; dL/dlog P from the forced decisions (F), beside the
+    score function with the mean loss as baseline; dL/dD by time rescaling,
+    (TR - F [kappa mode] or TR - F / 2) / D; the pathwise
+    dL/dD = (path l / 2 - F / 2 [kappa mode]) / D (l = sqrt(6 D dt)/res);
+    dL/dkappa = F / kappa (score / kappa as d_kappa_score);
     dL/dT2_c = sum L t_c dt / T2_c^2."""
     n = job.npar if nwalk is None else nwalk
     score = sums["LE"] - sums["L"] / n * sums["E"]
+    F = sums["F"]
     step = float(job.step[1 if job.nc > 1 else 0])
     kap = kappa is not None
     d_wave = job.dt * np.transpose(sums["dwave"], (1, 0, 2))
-    d_D = (sums["TR"] - (score if kap else 0.5 * score)) / D
-    d_D_path = (sums["path"] * step / 2.0 - (score / 2.0 if kap else 0.0)) / D
-    d_kappa = score / kappa if kap and kappa > 0 else 0.0
+    d_D = (sums["TR"] - (F if kap else 0.5 * F)) / D
+    d_D_path = (sums["path"] * step / 2.0 - (F / 2.0 if kap else 0.0)) / D
+    d_kappa = F / kappa if kap and kappa > 0 else 0.0
+    d_kappa_score = score / kappa if kap and kappa > 0 else 0.0
     t2 = np.asarray(t2, dtype=np.float64)
     d_t2 = sums["LT"] * job.dt / t2 ** 2
-    return dict(d_wave=d_wave, d_diffusivity=d_D, d_diffusivity_pathwise=d_D_path, d_kappa=d_kappa, d_t2=d_t2,
-                loss=sums["L"])
+    return dict(d_wave=d_wave, d_diffusivity=d_D, d_diffusivity_pathwise=d_D_path, d_kappa=d_kappa,
+                d_kappa_score=d_kappa_score, d_t2=d_t2, loss=sums["L"])

@@ -307,6 +307,10 @@ typedef struct {
     double* xbin;   /* [nbins*3], um */
     double* rs;     /* [nwave]: sum over bin ends t (g_j,b - g_j,b+1) . x(t) (time rescaling) */
     int ai_end;     /* compartment after the last step */
+    int nb;         /* permeation decisions drawn (0 < Pij < 1), counted */
+    int force_at;   /* the decision whose outcome is flipped (-1: none) */
+    double Pf;      /* its Pij */
+    int xf;         /* its outcome before the flip */
 } or_adj;
 
 static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, double* phase,
@@ -420,8 +424,16 @@ static void walk_split_core(const or_params* p, int64_t w, or_outputs* out, doub
             gn[hit] = gj;
             const int aj = APix[lin(p, gn[0], gn[1], gn[2])];
             const double P = p->pij[ai * Nc + aj];
-            const int cross = (P > 0.999999) || (P >= 0.000001 && (double)or_dstream_float(&perm) < P);
-            if (adj && !(P > 0.999999) && P >= 0.000001) adj->E += (cross ? 1.0 : 0.0) - P;
+            int cross = (P > 0.999999) || (P >= 0.000001 && (double)or_dstream_float(&perm) < P);
+            if (adj && !(P > 0.999999) && P >= 0.000001) {
+                adj->E += (cross ? 1.0 : 0.0) - P;
+                if (adj->nb == adj->force_at) {
+                    adj->Pf = P;
+                    adj->xf = cross;
+                    cross = !cross;
+                }
+                adj->nb++;
+            }
             if (p->rule != OR_RULE_REFLECT && !cross) {
                 turned = 1;   /* the rule decides, after the loop */
                 break;
@@ -607,6 +619,7 @@ int or_adjoint_split(const or_params* p, const double* gup, int64_t w_begin, int
         adj.dphi = dphi;
         adj.xbin = xbin;
         adj.rs = rs;
+        adj.force_at = -1;
         walk_split_core(p, w, &scratch, phase, NULL, NULL, NULL, NULL, NULL, &adj);
         /* this walker's loss L_w = s0 sum_j (gC_j cos phi_j + gS_j sin phi_j)
          * and a_j = dL_w / dphi_j */
@@ -632,6 +645,31 @@ int or_adjoint_split(const or_params* p, const double* gup, int64_t w_begin, int
         sums[3] += adj.E;
         for (int c = 0; c < nc; c++)
             if (p->step[c] > 0.0) sums[4 + c] += Lw * adj.tc[c] / p->step[c];
+        /* forced decision: one of the walker's nb permeation decisions, chosen
+         * uniformly (domain 3), is flipped and the walk repeated with the same
+         * streams; nb Pij (1 - Pij) (L[crossed] - L[reflected]) estimates
+         * d L_w / d log P (the weak derivative of the Bernoulli draws) */
+        if (adj.nb > 0) {
+            or_dstream fs;
+            or_dstream_init(&fs, p->seed, (uint64_t)w, OR_DOM_FORCE);
+            const float u = or_dstream_float(&fs);
+            int K = (int)(u * (float)adj.nb);
+            if (K > adj.nb - 1) K = adj.nb - 1;
+            or_adj fa;
+            memset(&fa, 0, sizeof fa);
+            memset(phase, 0, sizeof(double) * (size_t)nw);
+            fa.dphi = dphi;
+            fa.xbin = xbin;
+            fa.rs = rs;
+            fa.force_at = K;
+            walk_split_core(p, w, &scratch, phase, NULL, NULL, NULL, NULL, NULL, &fa);
+            const double s0f = exp(-fa.wexp);
+            double Lf = 0.0;
+            for (int j = 0; j < nw; j++)
+                Lf += s0f * (gup[2 * j] * cos(phase[j]) + gup[2 * j + 1] * sin(phase[j]));
+            const double dL = fa.xf ? Lw - Lf : Lf - Lw;
+            sums[5 + nc + 2 * nw] += (double)adj.nb * fa.Pf * (1.0 - fa.Pf) * dL;
+        }
     }
     free(phase); free(dphi); free(xbin); free(sbuf); free(rs);
     return 0;

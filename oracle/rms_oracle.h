@@ -121,6 +121,10 @@ int or_run_split_parallel(const or_params* p, int64_t w_begin, int64_t w_end, in
  *   sums[0] = sum L_w, sums[1] = sum L_w E_w, sums[2] = sum_w sum_j a_jw dphi_jw,
  *   sums[3] = sum E_w, sums[4+c] = sum L_w t_wc / step_c (c < nc),
  *   sums[4+nc+2j], [4+nc+2j+1] = sum s0 cos phi_j, sum s0 sin phi_j;
+ *   sums[4+nc+2nwave] = sum of the time-rescaling derivatives dL_w/deps;
+ *   sums[5+nc+2nwave] = sum nb_w Pij (1 - Pij) (L_w[crossed] - L_w[reflected])
+ *     over walkers with nb_w > 0 permeation draws, one of them (chosen from
+ *     domain 3) flipped and the walk repeated on the same streams;
  *   dwave[(b*nwave + j)*3 + k] += sum a_jw X_wbk (um).
  * The same sums as the GPU adjoint kernel (csrc/rms_adjoint.cu); the caller
  * zeroes them.  Returns -6 for other modes or rules. */

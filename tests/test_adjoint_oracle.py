@@ -130,3 +130,36 @@ def test_time_rescaling_sees_the_corner_jumps_of_a_voxelised_axon():
     want = float(np.mean(ref))
     assert float(np.mean(tr)) == pytest.approx(want, rel=0.15), (tr, ref)
     assert float(np.mean(path)) / want < 0.6, (path, ref)
+
+
+def test_forced_draws_and_score_function_agree_on_kappa():
+    """Two unbiased estimates of dL/dkappa on a permeable voxelised axon
+    (kappa = 0.05, T2 80 / 20 ms so that a crossing changes the loss): the
+    forced draws (one permeation draw per walker walked the other way, the
+    rest of the walk on the same streams) and the score function.  Over 8
+    walker shards of 2048 their means agree within 3 standard errors of the
+    difference, and the forced draws' spread is under half the score's
+    (measured: 0.012 vs 0.053 for this seed)."""
+    from rms_b200 import geometry
+    wave = base_waves()
+    lab = geometry.axon_lattice(24, 24, 48, RES, seed=4, exterior=2, r0=0.6)
+    t2, n, kap = (1e6, 80.0, 20.0), 16384, 0.05
+    j = job(lab, wave, kappa=kap, t2=t2, npar=n, seed=7)
+    forced, score = [], []
+    for k in range(8):
+        sk = pyoracle.adjoint_split(j, W.reshape(-1) / n, n * k // 8, n * (k + 1) // 8)
+        assert sk["F"] != 0.0
+        gk = pyoracle.adjoint_gradients(j, sk, 2.0, t2, kap, nwalk=n // 8)
+        forced.append(8 * gk["d_kappa"])
+        score.append(8 * gk["d_kappa_score"])
+    se_f = np.std(forced, ddof=1) / np.sqrt(8)
+    se_s = np.std(score, ddof=1) / np.sqrt(8)
+    assert abs(np.mean(forced) - np.mean(score)) < 3 * np.hypot(se_f, se_s), (forced, score)
+    assert se_f < 0.5 * se_s, (se_f, se_s)
+
+
+def test_forced_draws_vanish_without_permeation():
+    """kappa = 0: no permeation draw is made, so the forced-draw sum is 0."""
+    wave = base_waves()
+    sums, g = grads(job(planes(), wave))
+    assert sums["F"] == 0.0 and sums["E"] == 0.0

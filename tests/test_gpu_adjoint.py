@@ -16,10 +16,11 @@ weights.  Bars:
   - the kernel's walker sums against the oracle's FP64 restatement
     (or_adjoint_split) of the same walkers, on flat planes where the FP32 and
     FP64 walks cannot part (reflections and crossings are continuous there);
-  - kappa: a score-function (Monte Carlo) estimate, and the finite difference
-    jumps wherever a crossing decision flips, so the reference is the
-    least-squares slope of L over +-15 %, seven points; both are averaged over
-    8 seeds and compared within their statistical error.
+  - kappa: a Monte Carlo estimate (forced permeation draws; the score
+    function beside it), and the finite difference jumps wherever a crossing
+    decision flips, so the reference is the least-squares slope of L over
+    +-15 %, seven points; both are averaged over 8 seeds and compared within
+    their statistical error.
 Walls are periodic.  Two places where the walk's output is not continuous in
 the step length, so the frozen-event D term misses jumps: a mirror wall (the
 reference mirrors the origin image, hpc_code/lib/main.cu:302-310, so a
@@ -158,25 +159,30 @@ def test_adjoint_sums_equal_the_oracle_walker_set():
     scale = np.abs(want["d_wave"]).max()
     np.testing.assert_allclose(r["d_wave"], want["d_wave"], rtol=0, atol=1e-3 * scale)
     assert r["d_diffusivity_pathwise"] == pytest.approx(want["d_diffusivity_pathwise"], rel=2e-3), "pathwise D"
-    # the score and time-rescaling sums are differences of larger sums: FP32 per walker shows at 1e-3
-    for k in ("d_diffusivity", "d_kappa"):
+    # the score, forced-draw and time-rescaling sums are differences of larger
+    # sums: FP32 per walker shows at 1e-3
+    for k in ("d_diffusivity", "d_kappa", "d_kappa_score"):
         assert r[k] == pytest.approx(want[k], rel=1e-2), k
     np.testing.assert_allclose(r["d_t2"][:3], want["d_t2"], rtol=2e-3, atol=1e-12)
 
 
 def test_kappa_gradient_permeable_axon():
-    """The score-function kappa gradient against the +-15 % slope of the loss,
+    """The kappa gradient (forced draws) against the +-15 % slope of the loss,
     both averaged over 8 seeds (262144 walkers each): on this axon the slope
     is the noisier of the two (crossing decisions flip in jumps; measured on
-    the oracle at 65536 walkers: adjoint spread ~17 %, slope spread ~45 % per
-    seed).  The means must agree within 3 standard errors of their difference
-    (from the seed spreads) and within 40 %."""
+    the oracle at 65536 walkers: score-function spread ~17 %, slope spread
+    ~45 % per seed; the forced draws spread less than the score function).
+    The means must agree within 3 standard errors of their difference (from
+    the seed spreads) and within 40 %; the forced draws' seed spread must be
+    below the score function's."""
     wave = base_waves()
     kw = dict(kappa=0.05, t2=(1e6, 70.0, 70.0), npar=4 * NPAR)
-    adjs, slopes = [], []
+    adjs, scores, slopes = [], [], []
     for seed in range(5, 13):
         sim = make(wave, **kw)
-        adjs.append(sim.adjoint(WEIGHTS.reshape(-1) / kw["npar"], seed=seed)["d_kappa"])
+        r = sim.adjoint(WEIGHTS.reshape(-1) / kw["npar"], seed=seed)
+        adjs.append(r["d_kappa"])
+        scores.append(r["d_kappa_score"])
         sim.close()
 
         def f(k):
@@ -191,6 +197,7 @@ def test_kappa_gradient_permeable_axon():
     se = np.sqrt(np.var(adjs, ddof=1) / len(adjs) + np.var(slopes, ddof=1) / len(slopes))
     assert abs(a - b) < 3 * se, (adjs, slopes)
     assert abs(a / b - 1) < 0.4, (a, b)
+    assert np.std(adjs) < np.std(scores), (adjs, scores)
 
 
 def test_torch_autograd_through_rotations():
