@@ -186,7 +186,12 @@ int rms_sim_create(const rms_config* cfg, rms_sim** out);
  * Replaces: the ifstream readers of main.cu:414-482, main_PGSE.cu:440-506. */
 int rms_sim_load_dir(const char* dir, int mode, rms_sim** out);
 
-/* Set (copy in) the label lattice, n3 fastest.  Labels must be < nc.
+/* Set (copy in) the label lattice, n3 fastest.  Labels must be < nc, and at
+ * least 1e-7 of the voxels labelled (RMS_ERR_RANGE otherwise; a refused
+ * lattice leaves the simulation's own in place).  Once the simulation has run
+ * (it holds its device), the lattice is uploaded straight from `labels` (a
+ * DMA when the buffer is pinned) and checked on the GPU; otherwise it is
+ * checked and copied on the host.  Returns when `labels` is no longer read.
  * Replaces: fiber.txt -> APix (main.cu:461-466, :532). */
 int rms_sim_set_lattice(rms_sim* sim, const uint8_t* labels, int n1, int n2, int n3);
 
@@ -256,7 +261,7 @@ int rms_rng_split(uint64_t seed, uint64_t walker, int domain, int n, float* out)
  * caliber variation and undulation of an axon, analysis/visualizeaxon.m:28-67).
  * Every operation is rounded on its own, so the lattice equals one built on
  * the host in FP64 from the same tables.  Replaces the sim's lattice (a host
- * copy is kept, as with rms_sim_set_lattice). */
+ * copy is kept). */
 int rms_sim_set_tube_lattice(rms_sim* sim, const double* r2, const double* cx, const double* cy, int inside,
                              int outside, int device);
 

@@ -78,7 +78,7 @@ struct rms_device_state {
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     DevBuf labels, packed, axons, wavef, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
-        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave;
+        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave, stage, counts;
     HostPinned h_out, h_axons;
     size_t labels_bytes = 0;
     bool packed_valid = false;
@@ -88,7 +88,7 @@ struct rms_device_state {
         if (device >= 0) cudaSetDevice(device);
         for (DevBuf* b : {&labels, &packed, &axons, &wavef, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
-                          &tr_vox, &tr_ev, &tr_pos, &adj_g, &adj_sums, &adj_dwave})
+                          &tr_vox, &tr_ev, &tr_pos, &adj_g, &adj_sums, &adj_dwave, &stage, &counts})
             b->release();
         h_out.release();
         h_axons.release();
@@ -410,8 +410,25 @@ int validate_lattice(const uint8_t* labels, size_t n, int nc) {
     return RMS_OK;
 }
 
+// The device holds the simulation's current lattice and the host copy is
+// older (rms_sim_set_lattice checked and kept a lattice on the device only):
+// copy it back, for a path that walks from the host copy.
+int sync_host_labels(rms_sim* s) {
+    if (!s->host_stale) return RMS_OK;
+    rms_device_state* d = s->dev;
+    const size_t n = (size_t)s->n1 * s->n2 * s->n3;
+    s->labels.resize(n);
+    RMS_CUDA(cudaSetDevice(d->device));
+    RMS_CUDA(cudaMemcpyAsync(s->labels.data(), d->labels.p, n, cudaMemcpyDeviceToHost, d->own));
+    RMS_CUDA(cudaStreamSynchronize(d->own));
+    s->host_stale = false;
+    return RMS_OK;
+}
+
 int ensure_device(rms_sim* s, int device) {
     if (s->dev && s->dev->device == device) return RMS_OK;
+    int rc = sync_host_labels(s);
+    if (rc) return rc;
     delete s->dev;
     s->dev = nullptr;
     int count = 0;
@@ -451,6 +468,7 @@ struct LaunchJob {
 int prepare_lattice(rms_sim* s, cudaStream_t st, bool split, int bits) {
     rms_device_state* d = s->dev;
     if (s->lattice_dirty || d->labels_bytes != s->labels.size()) {
+        if (s->host_stale) return set_error(RMS_ERR_STATE, "the simulation's lattice is on a device it no longer holds");
         RMS_CUDA(d->labels.ensure(s->labels.size()));
         RMS_CUDA(cudaMemcpyAsync(d->labels.p, s->labels.data(), s->labels.size(), cudaMemcpyHostToDevice, st));
         d->labels_bytes = s->labels.size();
@@ -1154,6 +1172,44 @@ bool field_size(const rms_sim* s, int field, size_t& n) {
     }
 }
 
+constexpr int kNoDevicePath = 1;   // set_lattice_on_device: take the host path instead
+
+int set_lattice_on_device(rms_sim* s, const uint8_t* labels, size_t n) {
+    rms_device_state* d = s->dev;
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(d->device) != cudaSuccess) return kNoDevicePath;
+    struct Restore {
+        int dev;
+        ~Restore() { if (dev >= 0) cudaSetDevice(dev); }
+    } restore{prev};
+    if (d->stage.ensure(n) != cudaSuccess || d->counts.ensure(2 * sizeof(unsigned long long)) != cudaSuccess) {
+        d->stage.release();
+        return kNoDevicePath;
+    }
+    int sms = 0;
+    RMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device));
+    unsigned long long hcount[2] = {0, 0};
+    RMS_CUDA(cudaMemsetAsync(d->counts.p, 0, sizeof(hcount), d->own));
+    RMS_CUDA(cudaMemcpyAsync(d->stage.p, labels, n, cudaMemcpyHostToDevice, d->own));
+    const int e = check_labels(d->stage.as<uint8_t>(), n, (unsigned)s->nc, d->counts.as<unsigned long long>(), sms,
+                               d->own);
+    if (e) return cuda_fail((cudaError_t)e, "lattice check launch");
+    RMS_CUDA(cudaMemcpyAsync(hcount, d->counts.p, sizeof(hcount), cudaMemcpyDeviceToHost, d->own));
+    RMS_CUDA(cudaStreamSynchronize(d->own));
+    if (hcount[0] || hcount[1] == 0 || (double)hcount[1] / (double)n < 1e-7) {
+        // refused: the host scan names the first offending voxel
+        const int rc = validate_lattice(labels, n, s->nc);
+        return rc ? rc : set_error(RMS_ERR_RANGE, "lattice refused by the device check");
+    }
+    std::swap(d->labels, d->stage);
+    d->labels_bytes = n;
+    d->packed_valid = false;
+    s->have_lattice = true;
+    s->lattice_dirty = false;
+    s->host_stale = true;
+    return RMS_OK;
+}
+
 }  // namespace
 }  // namespace rms
 
@@ -1241,6 +1297,7 @@ int rms_sim_load_dir(const char* dir, int mode, rms_sim** out) {
     return RMS_OK;
 }
 
+
 int rms_sim_set_lattice(rms_sim* s, const uint8_t* labels, int n1, int n2, int n3) {
     if (!s || !labels) return set_error(RMS_ERR_ARG, "null argument");
     if (n1 != s->n1 || n2 != s->n2 || n3 != s->n3) {
@@ -1250,37 +1307,26 @@ int rms_sim_set_lattice(rms_sim* s, const uint8_t* labels, int n1, int n2, int n
         return set_error(RMS_ERR_ARG, m.str());
     }
     const size_t n = (size_t)n1 * n2 * n3;
-    // checked before it is copied: a rejected lattice leaves the sim's own as it was
+    // A simulation that has run has its device: the lattice goes up straight
+    // from the caller's buffer (a DMA when it is pinned) into a staging buffer
+    // and is checked there by one GPU pass; only a lattice that passes becomes
+    // the simulation's device lattice, and the host copy is brought up to date
+    // only if a later call needs it.  Without a device, the lattice is checked
+    // and copied on the host.  Either way a rejected lattice leaves the
+    // simulation's own as it was, and the call returns once the caller's
+    // buffer is no longer read.
+    if (s->dev) {
+        int rc = set_lattice_on_device(s, labels, n);
+        if (rc != kNoDevicePath) return rc;
+    }
     int rc = validate_lattice(labels, n, s->nc);
     if (rc) return rc;
     s->labels.resize(n);
     uint8_t* dst = s->labels.data();
-    // A simulation that has run has its device: the lattice goes up straight
-    // from the caller's buffer on the simulation's own stream (a DMA from a
-    // pinned buffer, overlapping the host copy below) instead of from the host
-    // copy at the next run.  The call returns once neither reads the caller's
-    // buffer any more; if the upload cannot start, the next run uploads.
-    rms_device_state* d = s->dev;
-    int prev = -1;
-    bool uploading = false;
-    if (d && cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(d->device) == cudaSuccess &&
-        d->labels.ensure(n) == cudaSuccess)
-        uploading = cudaMemcpyAsync(d->labels.p, labels, n, cudaMemcpyHostToDevice, d->own) == cudaSuccess;
     host_parallel(n, [&](size_t lo, size_t hi, int) { std::memcpy(dst + lo, labels + lo, hi - lo); });
     s->have_lattice = true;
     s->lattice_dirty = true;
-    if (uploading) {
-        const cudaError_t e = cudaStreamSynchronize(d->own);
-        if (e == cudaSuccess) {
-            d->labels_bytes = n;
-            d->packed_valid = false;
-            s->lattice_dirty = false;
-        }
-        if (prev >= 0) cudaSetDevice(prev);
-        if (e != cudaSuccess) return cuda_fail(e, "lattice upload");
-    } else if (prev >= 0) {
-        cudaSetDevice(prev);
-    }
+    s->host_stale = false;
     return RMS_OK;
 }
 

@@ -123,6 +123,10 @@ const char* cuda_error_string(int code);
 // A tube lattice on the device (rms_geometry.cu).
 int build_tube_lattice(uint8_t* d_out, int n1, int n2, int n3, double res, const double* d_r2, const double* d_cx,
                        const double* d_cy, uint8_t inside, uint8_t outside, void* stream);
+// A lattice in device memory checked on the GPU: d_counts[0] += voxels with a
+// label >= nc, d_counts[1] += labelled voxels (the caller zeroes d_counts).
+int check_labels(const uint8_t* d_labels, size_t n, unsigned nc, unsigned long long* d_counts, int sms,
+                 void* stream);
 
 // Adjoint of the waveform-mode split walk (rms_adjoint.cu): one axon, labels
 // below kAdjNc, at most kAdjWaves waveforms.

@@ -85,41 +85,6 @@ struct Carve {
     }
 };
 
-// The caller's device lattice, checked as rms_sim_set_lattice checks a host
-// one: counts[0] = voxels with a label >= nc, counts[1] = labelled voxels.
-// 16-byte loads over the aligned middle, byte loads at the two ends.
-__global__ void check_labels_kernel(const uint8_t* __restrict__ lab, size_t n, unsigned nc,
-                                    unsigned long long* counts) {
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t nthr = (size_t)gridDim.x * blockDim.x;
-    const size_t mis = (size_t)((16u - ((uintptr_t)lab & 15u)) & 15u);
-    const size_t head = mis < n ? mis : n;
-    const size_t nvec = (n - head) / 16;
-    const unsigned ncr = nc * 0x01010101u;
-    unsigned bad = 0, labelled = 0;
-    auto one = [&](unsigned v) { bad += v >= nc; labelled += v != 0; };
-    if (tid < head) one(lab[tid]);
-    const uint4* vec = reinterpret_cast<const uint4*>(lab + head);
-    for (size_t i = tid; i < nvec; i += nthr) {
-        const uint4 q = __ldg(vec + i);
-        const unsigned w[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            bad += __popc(__vcmpgeu4(w[k], ncr)) >> 3;     // 0xff per byte >= nc
-            labelled += 4 - (__popc(__vcmpeq4(w[k], 0u)) >> 3);
-        }
-    }
-    for (size_t i = head + nvec * 16 + tid; i < n; i += nthr) one(lab[i]);
-    for (int o = 16; o > 0; o >>= 1) {
-        bad += __shfl_xor_sync(0xffffffffu, bad, o);
-        labelled += __shfl_xor_sync(0xffffffffu, labelled, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        if (bad) atomicAdd(counts, (unsigned long long)bad);
-        if (labelled) atomicAdd(counts + 1, (unsigned long long)labelled);
-    }
-}
-
 template <class T>
 cudaError_t put(T* dst, const T* src, size_t count, cudaStream_t st) {
     if (!count) return cudaSuccess;
@@ -248,9 +213,7 @@ extern "C" int rms_sim_run_noalloc(const rms_sim* s, const rms_run_opts* o, cons
     unsigned long long hcount[2] = {0, 0};
     if ((e = cudaMemsetAsync(d_counts, 0, sizeof(hcount), st)) != cudaSuccess)
         return set_error(RMS_ERR_CUDA, std::string("scratch clear: ") + cudaGetErrorString(e));
-    check_labels_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(4 * dev_sms, (int64_t)(nvox / 4096) + 1)), 256, 0,
-                          st>>>(d_labels, nvox, (unsigned)nc, d_counts);
-    if ((e = cudaGetLastError()) != cudaSuccess ||
+    if ((e = (cudaError_t)check_labels(d_labels, nvox, (unsigned)nc, d_counts, dev_sms, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(hcount, d_counts, sizeof(hcount), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return set_error(RMS_ERR_CUDA, std::string("lattice check: ") + cudaGetErrorString(e));

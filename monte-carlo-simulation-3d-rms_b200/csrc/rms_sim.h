@@ -43,6 +43,7 @@ struct rms_sim {
     std::vector<uint8_t> labels;
     bool have_lattice = false;
     bool lattice_dirty = true;
+    bool host_stale = false;   // the device holds a newer lattice than `labels`
 
     // device resources (lazily created)
     rms_device_state* dev = nullptr;

@@ -109,3 +109,29 @@ def test_new_lattice_after_a_run_walks_the_new_lattice(precision):
     assert np.array_equal(got["npar_count"], want["npar_count"])
     assert_fp64_close(got["dx2"], want["dx2"], 1e-9, "dx2")
     assert_fp64_close(got["sigre"], want["sigre"], 1e-9, "sigre")
+
+
+def test_refused_lattice_after_a_run_keeps_the_previous_one():
+    """After a run, rms_sim_set_lattice checks the new lattice on the GPU: a
+    label >= Nc or a lattice with no labelled voxel is refused with
+    RMS_ERR_RANGE (the message names the first bad voxel, as the host check
+    does), and the simulation keeps walking the lattice it had."""
+    kw = dict(dt=2e-4, tn=500, npar=2000, res=0.1, diffusivity=[0.0, 2.0, 1.0], t2=[80.0, 80.0, 40.0],
+              bval=[1.0], bvec=[[1, 0, 0]], timepoints=500)
+    a = geometry.axon_lattice(16, 16, 24, 0.1, seed=1, exterior=2, r0=0.5)
+    b = geometry.axon_lattice(16, 16, 24, 0.1, seed=2, exterior=2, r0=0.7)
+    sim = engine.Sim(a, **kw)
+    sim.run(seed=4, precision="split")
+    sim.set_lattice(b)                      # accepted on the device
+    bad = b.copy()
+    bad[3, 4, 5] = 3
+    with pytest.raises(engine.RmsError) as e:
+        sim.set_lattice(bad)
+    assert e.value.code == -4 and "at voxel" in str(e.value) and str(3 * 16 * 24 + 4 * 24 + 5) in str(e.value)
+    with pytest.raises(engine.RmsError) as e:
+        sim.set_lattice(np.zeros_like(b))
+    assert e.value.code == -4
+    got = sim.run(seed=4, precision="compat").outputs()
+    want = engine.Sim(b, **kw).run(seed=4, precision="compat").outputs()
+    assert np.array_equal(got["npar_count"], want["npar_count"])
+    assert_fp64_close(got["dx2"], want["dx2"], 1e-9, "dx2")
