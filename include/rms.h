@@ -424,6 +424,21 @@ typedef struct rms_adjoint_grads {
 } rms_adjoint_grads;
 int rms_adjoint_run(rms_sim* sim, const rms_run_opts* opts, const double* g_sigw, rms_adjoint_grads* out);
 
+/* Jacobian of every waveform's signal sums with respect to the scalar
+ * parameters, in one adjoint run (three walks of each walker, as
+ * rms_adjoint_run).  No counterpart in the reference.  For waveform j and
+ * signal sum s (0: C_j, 1: S_j), row q = 2j + s of jac[2*nwave*RMS_JAC_COLS]
+ * holds d(sum)/d(parameter) in the columns below: the estimators of
+ * rms_adjoint_run with the loss L = that sum (D by time rescaling, kappa by
+ * forced draws and by the score function, T2 analytic; unused columns 0).
+ * sigw (optional, [nwave*2]) receives the run's signal sums. */
+#define RMS_JAC_D 0
+#define RMS_JAC_KAPPA 1
+#define RMS_JAC_KAPPA_SCORE 2
+#define RMS_JAC_T2 3             /* + compartment c, c < Nc */
+#define RMS_JAC_COLS 11
+int rms_adjoint_jacobian(rms_sim* sim, const rms_run_opts* opts, double* jac, double* sigw);
+
 /* ---- Multi-waveform phase contraction -------------------------------------
  * No counterpart in the reference (its only gradient form is the PGSE pair,
  * hpc_code/lib/main_PGSE.cu:336-346, summed per step per gradient).  For

@@ -111,6 +111,12 @@ struct AdjHooks {
     }
 };
 
+// JAC: instead of one weighted loss, the derivatives of every waveform's two
+// signal sums C_j, S_j with respect to D, kappa and T2 (Jacobian columns; the
+// sums at a.sums + kAdjSums, layout kJac* in rms_internal.h); dL/dwave is not
+// formed.  The R_j of the time rescaling go to dphi[] in pass 2 and the forced
+// walk's phases to dphi[] in pass 3, so phi[] keeps pass 1's phases.
+template <bool JAC>
 __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constant__ AdjArgs a) {
     constexpr int NC = kAdjNc, BITS = 4, NW = kAdjWaves;
     constexpr int kTab = 2 * NC + 2 * NC * NC;
@@ -151,6 +157,8 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
         float tr = 0.0f;   // this walker's time-rescaling derivative dL_w/d(eps)
         float Lkeep = 0.0f;   // this walker's loss (pass 1)
         int nb_w = 0;         // its Bernoulli draws (pass 1)
+        float s0keep = 0.0f;  // JAC: its T2 weight s0 (pass 1)
+        float wkeep = 0.0f;   // JAC: W - T / T2(c_T), the T2 weight's time-rescaling term (pass 1)
 
         for (int pass = 0; pass < (a.force ? 3 : 2); ++pass) {
             // pass 3 walks only the walkers that made a draw, and a warp with
@@ -194,8 +202,13 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                 DomainStream fs;
                 fs.init(a.seed, (uint64_t)w, kDomForce);
                 h.force_at = min((int)(fs.next() * (float)nb_w), nb_w - 1);
+            }
+            if (pass > 0) {
 #pragma unroll
-                for (int j = 0; j < NW; ++j) phi[j] = 0.0f;
+                for (int j = 0; j < NW; ++j) {
+                    if (JAC) dphi[j] = 0.0f;            // pass 2: R_j; pass 3: the forced phases
+                    else if (pass == 2) phi[j] = 0.0f;  // pass 3: the forced phases
+                }
             }
             float B0 = 0.0f, B1 = 0.0f, B2 = 0.0f;  // bin sums of the tangent
             int bin = 0, next_bin = a.bin_steps;
@@ -245,7 +258,9 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                         for (int j = 0; j < NW; ++j) {
                             if (j < a.nwave) {
                                 const double g0 = __ldg(wv + 3 * j), g1 = __ldg(wv + 3 * j + 1), g2 = __ldg(wv + 3 * j + 2);
-                                phi[j] += (float)(g0 * x0 + g1 * x1 + g2 * x2);
+                                const float inc = (float)(g0 * x0 + g1 * x1 + g2 * x2);
+                                if (JAC && pass == 2) dphi[j] += inc;
+                                else phi[j] += inc;
                                 if (p1st) dphi[j] += (float)((g0 * B0 + g1 * B1 + g2 * B2) * (double)a.res);
                             }
                         }
@@ -264,18 +279,21 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                                 const float q0 = (float)(__ldg(wv + 3 * j) - (last ? 0.0 : __ldg(wn + 3 * j)));
                                 const float q1 = (float)(__ldg(wv + 3 * j + 1) - (last ? 0.0 : __ldg(wn + 3 * j + 1)));
                                 const float q2 = (float)(__ldg(wv + 3 * j + 2) - (last ? 0.0 : __ldg(wn + 3 * j + 2)));
-                                tr = fmaf(aj[j] * tb, q0 * xe0 + q1 * xe1 + q2 * xe2, tr);
+                                if (JAC) dphi[j] = fmaf(tb, q0 * xe0 + q1 * xe1 + q2 * xe2, dphi[j]);   // R_j
+                                else tr = fmaf(aj[j] * tb, q0 * xe0 + q1 * xe1 + q2 * xe2, tr);
                             }
                         }
-                        // dL/dwave[bin][j] += a_jw X_wb, summed over the warp's walkers
-                        const float xs[3] = {(float)x0, (float)x1, (float)x2};
+                        if (!JAC) {
+                            // dL/dwave[bin][j] += a_jw X_wb, summed over the warp's walkers
+                            const float xs[3] = {(float)x0, (float)x1, (float)x2};
 #pragma unroll
-                        for (int ax = 0; ax < 3; ++ax) {
-                            float v[NW];
+                            for (int ax = 0; ax < 3; ++ax) {
+                                float v[NW];
 #pragma unroll
-                            for (int j = 0; j < NW; ++j) v[j] = aj[j] * xs[ax];
-                            const float r = warp_reduce_scatter16f(v, lane);
-                            if (lane < a.nwave) atomicAdd(a.dwave + ((size_t)bin * a.nwave + lane) * 3 + ax, r);
+                                for (int j = 0; j < NW; ++j) v[j] = aj[j] * xs[ax];
+                                const float r = warp_reduce_scatter16f(v, lane);
+                                if (lane < a.nwave) atomicAdd(a.dwave + ((size_t)bin * a.nwave + lane) * 3 + ax, r);
+                            }
                         }
                     }
                     P0 = P1 = P2 = 0.0;
@@ -307,10 +325,32 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                         atomicAdd(a.sums + kAdjSumSig + 2 * j, C);
                         atomicAdd(a.sums + kAdjSumSig + 2 * j + 1, S);
                     }
+                    if (JAC && j < a.nwave) {
+                        // score and residence sums of C_j and S_j
+                        const double Ew = active ? (double)h.E : 0.0;
+                        const double CE = warp_sum((double)(s0w * cs) * Ew), SE = warp_sum((double)(s0w * sn) * Ew);
+                        double* js = a.sums + kAdjSums;
+                        if (lane == 0) {
+                            atomicAdd(js + kJacE + 2 * j, CE);
+                            atomicAdd(js + kJacE + 2 * j + 1, SE);
+                        }
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            const float st = t_step[c];
+                            const double tcs = st > 0.0f ? (double)(h.tc[c] / st) : 0.0;
+                            const double CT = warp_sum((double)(s0w * cs) * tcs), ST = warp_sum((double)(s0w * sn) * tcs);
+                            if (lane == 0) {
+                                atomicAdd(js + kJacLT + (2 * j) * NC + c, CT);
+                                atomicAdd(js + kJacLT + (2 * j + 1) * NC + c, ST);
+                            }
+                        }
+                    }
                 }
                 // the T2 weight under time rescaling: dW/d(eps) = -W + T / T2(c_T)
-                tr += Lw * (float)(w64 - (double)a.tn * (double)(t_step[wk.ai] * t_k[wk.ai]));
+                wkeep = (float)(w64 - (double)a.tn * (double)(t_step[wk.ai] * t_k[wk.ai]));
+                tr += Lw * wkeep;
                 Lkeep = Lw;
+                s0keep = s0w;
                 nb_w = active ? h.nb : 0;
                 const double L = warp_sum((double)Lw), LE = warp_sum((double)Lw * (double)h.E),
                              GP = warp_sum((double)G), ES = warp_sum(active ? (double)h.E : 0.0);
@@ -330,6 +370,25 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
             } else if (pass == 1) {
                 const double TR = warp_sum((double)tr);
                 if (lane == 0) atomicAdd(a.sums + kAdjSumTR, TR);
+                if (JAC) {
+                    // dC_j/deps = -S_j dphi_j/deps - C_j dW/deps, dS_j/deps = C_j dphi_j/deps - S_j dW/deps,
+                    // dphi_j/deps = R_j - phi_j, -dW/deps = W - T / T2(c_T)
+#pragma unroll
+                    for (int j = 0; j < NW; ++j) {
+                        if (j < a.nwave) {
+                            float sn = 0.0f, cs = 0.0f;
+                            sincosf(phi[j], &sn, &cs);
+                            const float Cw = active ? s0keep * cs : 0.0f, Sw = active ? s0keep * sn : 0.0f;
+                            const float de = dphi[j] - phi[j];
+                            const double TC = warp_sum((double)(-Sw * de + Cw * wkeep));
+                            const double TS = warp_sum((double)(Cw * de + Sw * wkeep));
+                            if (lane == 0) {
+                                atomicAdd(a.sums + kAdjSums + kJacTR + 2 * j, TC);
+                                atomicAdd(a.sums + kAdjSums + kJacTR + 2 * j + 1, TS);
+                            }
+                        }
+                    }
+                }
             } else {
                 // nb_w Pij (1 - Pij) (L[crossed] - L[reflected]) of the forced walk
                 const float s0f = active ? (float)exp(-w64) : 0.0f;
@@ -343,9 +402,27 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
                     }
                 }
                 const float dL = h.xf ? Lkeep - Lf : Lf - Lkeep;
-                const double Fw = active ? (double)nb_w * (double)h.Pf * (1.0 - (double)h.Pf) * (double)dL : 0.0;
-                const double F = warp_sum(Fw);
+                const double wf = active ? (double)nb_w * (double)h.Pf * (1.0 - (double)h.Pf) : 0.0;
+                const double F = warp_sum(wf * (double)dL);
                 if (lane == 0) atomicAdd(a.sums + kAdjSumForce, F);
+                if (JAC) {
+                    // per waveform: C_j, S_j of the forced walk (phases in dphi[]) against pass 1's
+#pragma unroll
+                    for (int j = 0; j < NW; ++j) {
+                        if (j < a.nwave) {
+                            float sn, cs, snf, csf;
+                            sincosf(phi[j], &sn, &cs);
+                            sincosf(dphi[j], &snf, &csf);
+                            const float dC = s0f * csf - s0keep * cs, dS = s0f * snf - s0keep * sn;
+                            const double FC = warp_sum(wf * (double)(h.xf ? -dC : dC));
+                            const double FS = warp_sum(wf * (double)(h.xf ? -dS : dS));
+                            if (lane == 0) {
+                                atomicAdd(a.sums + kAdjSums + kJacF + 2 * j, FC);
+                                atomicAdd(a.sums + kAdjSums + kJacF + 2 * j + 1, FS);
+                            }
+                        }
+                    }
+                }
             }
         }
     }
@@ -353,14 +430,16 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
 
 }  // namespace
 
-int launch_adjoint(const AdjArgs& a, int grid, void* stream) {
-    adjoint_kernel<<<grid, kAdjBlock, 0, (cudaStream_t)stream>>>(a);
+int launch_adjoint(const AdjArgs& a, bool jac, int grid, void* stream) {
+    if (jac) adjoint_kernel<true><<<grid, kAdjBlock, 0, (cudaStream_t)stream>>>(a);
+    else adjoint_kernel<false><<<grid, kAdjBlock, 0, (cudaStream_t)stream>>>(a);
     return (int)cudaGetLastError();
 }
 
-int adjoint_blocks_per_sm() {
+int adjoint_blocks_per_sm(bool jac) {
     int n = 0;
-    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_kernel, kAdjBlock, 0);
+    const cudaError_t e = jac ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_kernel<true>, kAdjBlock, 0)
+                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_kernel<false>, kAdjBlock, 0);
     return e == cudaSuccess ? n : -1;
 }
 

@@ -1015,7 +1015,7 @@ int run_one(rms_sim* s, const rms_run_opts* o) {
 
 // Gradients of L = sum_j g_cos[j] C_j + g_sin[j] S_j for a waveform-mode
 // simulation, by the two-pass walk of rms_adjoint.cu.
-int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adjoint_grads* out) {
+int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adjoint_grads* out, double* jac) {
     if (s->mode != RMS_MODE_WAVEFORM) return set_error(RMS_ERR_ARG, "the adjoint differentiates a waveform-mode simulation");
     if (s->rule != RMS_RULE_REFLECT) return set_error(RMS_ERR_ARG, "the adjoint walks with reflecting membranes");
     if (s->nwave > kAdjWaves) return set_error(RMS_ERR_RANGE, "the adjoint takes at most 16 waveforms per run");
@@ -1078,8 +1078,9 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
     for (int j = 0; j < 2 * s->nwave; ++j) gup[j] = (float)(g_sigw ? g_sigw[j] : 0.0);
     RMS_CUDA(upload(d->adj_g, gup, st));
     const size_t ndw = (size_t)s->nbins * s->nwave * 3;
-    RMS_CUDA(d->adj_sums.ensure(sizeof(double) * kAdjSums));
-    RMS_CUDA(cudaMemsetAsync(d->adj_sums.p, 0, sizeof(double) * kAdjSums, st));
+    const int nsums = kAdjSums + (jac ? kJacSums : 0);
+    RMS_CUDA(d->adj_sums.ensure(sizeof(double) * nsums));
+    RMS_CUDA(cudaMemsetAsync(d->adj_sums.p, 0, sizeof(double) * nsums, st));
     RMS_CUDA(d->adj_dwave.ensure(sizeof(float) * ndw));
     RMS_CUDA(cudaMemsetAsync(d->adj_dwave.p, 0, sizeof(float) * ndw, st));
     RMS_CUDA(d->err.ensure(sizeof(int)));
@@ -1092,18 +1093,18 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
 
     int sms = 0;
     RMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    const int per_sm = adjoint_blocks_per_sm();
+    const int per_sm = adjoint_blocks_per_sm(jac != nullptr);
     if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
     const int64_t wpb = kAdjBlock / 32;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (a.ntiles + wpb - 1) / wpb));
     RMS_CUDA(cudaEventRecord(d->e0, st));
-    int e = launch_adjoint(a, grid, st);
+    int e = launch_adjoint(a, jac != nullptr, grid, st);
     if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch");
     RMS_CUDA(cudaEventRecord(d->e1, st));
-    std::vector<double> sums(kAdjSums);
+    std::vector<double> sums(nsums);
     std::vector<float> dw(ndw);
     int herr = 0;
-    RMS_CUDA(cudaMemcpyAsync(sums.data(), d->adj_sums.p, sizeof(double) * kAdjSums, cudaMemcpyDeviceToHost, st));
+    RMS_CUDA(cudaMemcpyAsync(sums.data(), d->adj_sums.p, sizeof(double) * nsums, cudaMemcpyDeviceToHost, st));
     RMS_CUDA(cudaMemcpyAsync(dw.data(), d->adj_dwave.p, sizeof(float) * ndw, cudaMemcpyDeviceToHost, st));
     RMS_CUDA(cudaMemcpyAsync(&herr, d->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     RMS_CUDA(cudaStreamSynchronize(st));
@@ -1147,6 +1148,26 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
     }
     if (out->sigw)
         for (int j = 0; j < 2 * s->nwave; ++j) out->sigw[j] = sums[kAdjSumSig + j];
+    if (jac) {
+        // each signal sum X_q (q = 2j + s) as the loss L = X_q: the formulas above with
+        // the walker sums of X_q
+        const double* js = sums.data() + kAdjSums;
+        const double N = (double)(w1 - w0);
+        for (int q = 0; q < 2 * s->nwave; ++q) {
+            double* row = jac + (size_t)q * RMS_JAC_COLS;
+            for (int k = 0; k < RMS_JAC_COLS; ++k) row[k] = 0.0;
+            const double Xq = sums[kAdjSumSig + q];
+            const double fq = js[kJacF + q];
+            const double sq = js[kJacE + q] - Xq / N * sums[kAdjSumE];
+            row[RMS_JAC_D] = (js[kJacTR + q] - (kap ? fq : 0.5 * fq)) / D;
+            row[RMS_JAC_KAPPA] = (kap && s->kappa > 0.0) ? fq / s->kappa : 0.0;
+            row[RMS_JAC_KAPPA_SCORE] = (kap && s->kappa > 0.0) ? sq / s->kappa : 0.0;
+            for (int c = 0; c < s->nc; ++c) {
+                const double T2 = s->t2[c];
+                row[RMS_JAC_T2 + c] = js[kJacLT + q * kAdjNc + c] * s->dt / (T2 * T2);
+            }
+        }
+    }
     return RMS_OK;
 }
 
@@ -1334,7 +1355,16 @@ int rms_adjoint_run(rms_sim* s, const rms_run_opts* opts, const double* g_sigw, 
     if (!s || !out) return set_error(RMS_ERR_ARG, "null argument");
     if (opts && opts->precision != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "the adjoint walks the SPLIT walk");
     if (opts && opts->traj_out) return set_error(RMS_ERR_ARG, "the adjoint writes no trajectory");
-    return run_adjoint(s, opts, g_sigw, out);
+    return run_adjoint(s, opts, g_sigw, out, nullptr);
+}
+
+int rms_adjoint_jacobian(rms_sim* s, const rms_run_opts* opts, double* jac, double* sigw) {
+    if (!s || !jac) return set_error(RMS_ERR_ARG, "null argument");
+    if (opts && opts->precision != RMS_PREC_SPLIT) return set_error(RMS_ERR_ARG, "the adjoint walks the SPLIT walk");
+    if (opts && opts->traj_out) return set_error(RMS_ERR_ARG, "the adjoint writes no trajectory");
+    rms_adjoint_grads g{};
+    g.sigw = sigw;
+    return run_adjoint(s, opts, nullptr, &g, jac);
 }
 
 int rms_sim_run(rms_sim* s, const rms_run_opts* opts) {

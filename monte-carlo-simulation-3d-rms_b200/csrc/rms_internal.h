@@ -138,6 +138,14 @@ constexpr int kAdjNc = 4;
 constexpr int kAdjSumL = 0, kAdjSumLE = 1, kAdjSumPath = 2, kAdjSumLT = 3, kAdjSumE = 3 + kAdjNc,
               kAdjSumSig = 4 + kAdjNc, kAdjSumTR = kAdjSumSig + 2 * kAdjWaves, kAdjSumForce = kAdjSumTR + 1;
 constexpr int kAdjSums = kAdjSumForce + 1;
+// Jacobian sums (rms_adjoint_jacobian), after the kAdjSums: for waveform j and
+// signal sum s (0: C_j = sum s0 cos phi_j, 1: S_j = sum s0 sin phi_j), q = 2j + s:
+//   kJacE + q           sum_w X_qw E_w (score of the permeation draws)
+//   kJacTR + q          sum_w dX_qw/deps (time rescaling)
+//   kJacF + q           sum_w nb_w Pij (1 - Pij) (X_qw[crossed] - X_qw[reflected]) (forced draws)
+//   kJacLT + q*NC + c   sum_w X_qw t_wc / step_c (residence in compartment c, steps)
+constexpr int kJacE = 0, kJacTR = 2 * kAdjWaves, kJacF = 4 * kAdjWaves, kJacLT = 6 * kAdjWaves;
+constexpr int kJacSums = kJacLT + 2 * kAdjWaves * kAdjNc;
 struct AdjArgs {
     const uint8_t* lat;          // padded 4-bit lattice with free-flight flags
     int n1, n2, n3, s0, s1;
@@ -154,8 +162,8 @@ struct AdjArgs {
     float* dwave;                // [bin][waveform][axis]: sum_w a_jw X_wb (um)
     int* err;
 };
-int launch_adjoint(const AdjArgs& a, int grid, void* stream);
-int adjoint_blocks_per_sm();
+int launch_adjoint(const AdjArgs& a, bool jac, int grid, void* stream);
+int adjoint_blocks_per_sm(bool jac);
 constexpr int kAdjBlock = 128;
 
 // Multi-waveform phase contraction (rms_contract.cu): out[j] = (sum_w cos phi,

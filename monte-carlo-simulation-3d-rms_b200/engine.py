@@ -33,7 +33,7 @@ EXPORTS = ("rms_sim_create", "rms_sim_load_dir", "rms_sim_set_lattice", "rms_sim
            "rms_sim_last_timing", "rms_batch_run", "rms_last_error", "rms_sim_destroy",
            "rms_rng_doubles", "rms_rng_floats", "rms_philox4x32_10", "rms_version",
            "rms_split_variant", "rms_rng_split", "rms_sim_run_noalloc", "rms_contract_phases",
-           "rms_adjoint_run", "rms_autotune", "rms_batch_graph_create", "rms_graph_run", "rms_graph_destroy",
+           "rms_adjoint_run", "rms_adjoint_jacobian", "rms_autotune", "rms_batch_graph_create", "rms_graph_run", "rms_graph_destroy",
            "rms_sim_cumulants", "rms_combine_cumulants", "rms_sim_set_tube_lattice",
            "rms_dki_shell", "rms_dki_lls", "rms_akc_shell", "rms_akc_lls")
 CONTRACT = {"fp32": 0, "bf16x3": 1, "bf16x3_presplit": 2}
@@ -141,6 +141,7 @@ def lib():
         L.rms_akc_lls.argtypes = [C.c_int, _DP, C.c_int, _DP, _DP, _DP]
         L.rms_autotune.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(RunOpts), C.POINTER(C.c_int), _DP]
         L.rms_adjoint_run.argtypes = [C.c_void_p, C.POINTER(RunOpts), _DP, C.POINTER(AdjointGrads)]
+        L.rms_adjoint_jacobian.argtypes = [C.c_void_p, C.POINTER(RunOpts), _DP, _DP]
         L.rms_contract_phases.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                           C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]
         _lib = L
@@ -190,6 +191,7 @@ class Sim:
         pj = _arr(pij) if pij is not None else None
         self._keep += [bv, bvc, gr, pj, wv]
         self.wave_shape = wv.shape if wv is not None else None
+        self.nc = int(nc or d.size)
         cfg = Config(MODE[mode], float(dt), int(tn), int(npar), int(nc or d.size), float(res),
                      int(shape[0]), int(shape[1]), int(shape[2]), _ptr(d), _ptr(t2a),
                      bv.size if mode == "narrow" else 0, _ptr(bv), _ptr(bvc),
@@ -218,6 +220,7 @@ class Sim:
         vals = open(os.path.join(path, "simParamInput.txt")).read().split()
         self.tn = int(vals[1])
         self.shape = tuple(int(v) for v in vals[-3:])
+        self.nc = int(vals[4 if mode == "narrow" else 3])
         return self
 
     def set_lattice(self, labels: np.ndarray):
@@ -274,6 +277,25 @@ class Sim:
         return dict(d_wave=dwave.reshape(nw, nb, 3), d_diffusivity=out.d_diffusivity, d_kappa=out.d_kappa,
                     d_t2=np.array(out.d_t2[:]), loss=out.loss, sigw=sigw.reshape(nw, 2),
                     d_diffusivity_pathwise=out.d_diffusivity_pathwise, d_kappa_score=out.d_kappa_score)
+
+    JAC_COLS = {"D": 0, "kappa": 1, "kappa_score": 2, "T2": 3}
+
+    def jacobian(self, seed: int = 0, device: int = 0, stream=None, walker_range=None) -> dict:
+        """d(signal sums)/d(D, kappa, T2) for every waveform in one adjoint run
+        (rms_adjoint_jacobian): arrays [nwave, 2] (cos sum, sin sum) per
+        parameter -- "D", "kappa" (forced draws), "kappa_score", and "T2"
+        [nwave, 2, nc] -- and the run's own sums "sigw" [nwave, 2]."""
+        if self.wave_shape is None:
+            raise ValueError("the adjoint needs a waveform-mode simulation")
+        nw = self.wave_shape[0]
+        opts = _opts(seed, "split", device, stream, walker_range=walker_range)
+        jac = np.zeros(2 * nw * 11)
+        sigw = np.zeros(2 * nw)
+        _check(lib().rms_adjoint_jacobian(self._h, C.byref(opts), _ptr(jac), _ptr(sigw)))
+        j = jac.reshape(nw, 2, 11)
+        nc = self.nc
+        return dict(D=j[:, :, 0].copy(), kappa=j[:, :, 1].copy(), kappa_score=j[:, :, 2].copy(),
+                    T2=j[:, :, 3:3 + nc].copy(), sigw=sigw.reshape(nw, 2))
 
     def cumulants(self, dirs=None):
         """(D, K), [timepoints, ndir], along unit directions dirs [ndir, 3]

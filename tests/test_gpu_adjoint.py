@@ -200,6 +200,31 @@ def test_kappa_gradient_permeable_axon():
     assert np.std(adjs) < np.std(scores), (adjs, scores)
 
 
+@pytest.mark.parametrize("kappa", [0.05, 0.0])
+def test_jacobian_rows_equal_one_hot_adjoints(kappa):
+    """rms_adjoint_jacobian's row for each waveform's cos and sin sum equals
+    rms_adjoint_run with a unit weight on that sum (the same walkers and
+    estimators; only the order of FP32 operations differs), for D, kappa
+    (forced draws and score function) and T2; with kappa = 0 no draw is made
+    and the kappa columns are 0."""
+    wave = base_waves()
+    n = 16384
+    sim = make(wave, kappa=kappa, npar=n)
+    J = sim.jacobian(seed=5)
+    for j in range(wave.shape[0]):
+        for sk in range(2):
+            g = np.zeros((wave.shape[0], 2))
+            g[j, sk] = 1.0
+            r = sim.adjoint(g.reshape(-1), seed=5)
+            assert J["D"][j, sk] == pytest.approx(r["d_diffusivity"], rel=1e-3, abs=1e-6 * n), (j, sk)
+            assert J["kappa"][j, sk] == pytest.approx(r["d_kappa"], rel=1e-3, abs=1e-6 * n), (j, sk)
+            assert J["kappa_score"][j, sk] == pytest.approx(r["d_kappa_score"], rel=1e-6, abs=1e-9 * n), (j, sk)
+            np.testing.assert_allclose(J["T2"][j, sk], r["d_t2"][:3], rtol=1e-6, atol=1e-12 * n)
+    np.testing.assert_allclose(J["sigw"], r["sigw"], rtol=1e-12)
+    if kappa == 0.0:
+        assert not J["kappa"].any() and not J["kappa_score"].any()
+
+
 def test_torch_autograd_through_rotations():
     import torch
     from rms_b200 import adjoint
