@@ -116,11 +116,26 @@ struct AdjHooks {
 // sums at a.sums + kAdjSums, layout kJac* in rms_internal.h); dL/dwave is not
 // formed.  The R_j of the time rescaling go to dphi[] in pass 2 and the forced
 // walk's phases to dphi[] in pass 3, so phi[] keeps pass 1's phases.
+// One float per waveform for the calling lane, in shared memory: column
+// threadIdx.x of a [NW][kAdjBlock] block (consecutive lanes, consecutive
+// banks).  The walker's phases, tangents and a_jw are read and written only at
+// bin ends and pass ends, so they need not hold registers through the step loop.
+struct LaneArr {
+    float* p;
+    __device__ __forceinline__ float& operator[](int j) const { return p[j * kAdjBlock]; }
+};
+
+// Resident blocks per SM: at least 5 for the weighted-loss form (96 registers,
+// no spills); the Jacobian form takes the compiler's choice (123 registers, 4
+// blocks).  Measured on the configs[3] job, 1e6 walkers: weighted 428 ms
+// (518 ms at 4 blocks), Jacobian 390 ms (416 ms when held to 4 blocks at 115
+// registers); with the per-lane arrays in registers (3 blocks) 541 / 474 ms.
 template <bool JAC>
-__global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constant__ AdjArgs a) {
+__global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const __grid_constant__ AdjArgs a) {
     constexpr int NC = kAdjNc, BITS = 4, NW = kAdjWaves;
     constexpr int kTab = 2 * NC + 2 * NC * NC;
     __shared__ float s_tab[kTab];
+    __shared__ float s_lane[3][NW][kAdjBlock];   // per lane: phi, dphi, aj (LaneArr)
     for (int i = threadIdx.x; i < kTab; i += blockDim.x)
         s_tab[i] = i < NC ? a.step[i]
                           : (i < 2 * NC ? a.kexp[i - NC]
@@ -143,7 +158,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_kernel(const __grid_constan
         const int64_t w = a.walker_begin + tile * 32 + lane;
         const bool live = w < a.walker_end;
         const uint32_t wlo = (uint32_t)w, whi = (uint32_t)((uint64_t)w >> 32);
-        float phi[NW], dphi[NW], aj[NW];
+        const LaneArr phi{&s_lane[0][0][threadIdx.x]}, dphi{&s_lane[1][0][threadIdx.x]}, aj{&s_lane[2][0][threadIdx.x]};
 #pragma unroll
         for (int j = 0; j < NW; ++j) phi[j] = dphi[j] = aj[j] = 0.0f;
         AdjHooks<NC> h;

@@ -1408,6 +1408,7 @@ int rms_sim_set_tube_lattice(rms_sim* s, const double* r2, const double* cx, con
         // the device already holds these labels; the packed form is rebuilt at the next run
         s->have_lattice = true;
         s->lattice_dirty = false;
+        s->host_stale = false;
         d->labels_bytes = nvox;
         d->packed_valid = false;
         return RMS_OK;
