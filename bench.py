@@ -614,7 +614,10 @@ def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
+    # under torchrun the ranks' exchange goes through NCCL even for one rank,
+    # so a one-GPU torchrun run walks the same code path as several GPUs
+    dist_on = world > 1 or "TORCHELASTIC_RUN_ID" in os.environ
+    if dist_on:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     lab, sim_kw, per_gpu, cfg = workload(args.workload, world, args.walkers, args.tn, args.timepoints,
@@ -630,18 +633,18 @@ def run_ours(args):
     precision = args.precision
 
     def barrier():
-        if world > 1:
+        if dist_on:
             dist.barrier()
 
     def max_over_ranks(*vals):
-        if world == 1:
+        if not dist_on:
             return vals
         t = torch.tensor(vals, dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return tuple(float(x) for x in t)
 
     def sum_over_ranks(x):
-        if world == 1:
+        if not dist_on:
             return x
         t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
         dist.all_reduce(t)
@@ -710,7 +713,7 @@ def run_ours(args):
         job.reload_inputs()
         job.run(3000 + i, precision)
         out = job.outputs()
-        if world > 1:
+        if dist_on:
             # the whole job's result: rank-order sum of the shards' accumulators
             from rms_b200 import shards
             out = shards.gather_sum({k: v for k, v in out.items() if not k.endswith("td")}, device="cuda")
@@ -801,7 +804,7 @@ def run_ours(args):
         }
         print(json.dumps(line), flush=True)
     job.close()
-    if world > 1:
+    if dist_on:
         dist.destroy_process_group()
 
 
