@@ -1212,11 +1212,14 @@ int set_lattice_on_device(rms_sim* s, const uint8_t* labels, size_t n) {
     unsigned long long hcount[2] = {0, 0};
     RMS_CUDA(cudaMemsetAsync(d->counts.p, 0, sizeof(hcount), d->own));
     RMS_CUDA(cudaMemcpyAsync(d->stage.p, labels, n, cudaMemcpyHostToDevice, d->own));
-    const int e = check_labels(d->stage.as<uint8_t>(), n, (unsigned)s->nc, d->counts.as<unsigned long long>(), sms,
-                               d->own);
-    if (e) return cuda_fail((cudaError_t)e, "lattice check launch");
-    RMS_CUDA(cudaMemcpyAsync(hcount, d->counts.p, sizeof(hcount), cudaMemcpyDeviceToHost, d->own));
-    RMS_CUDA(cudaStreamSynchronize(d->own));
+    // from here the stream reads the caller's buffer: every return waits for it
+    cudaError_t e = (cudaError_t)check_labels(d->stage.as<uint8_t>(), n, (unsigned)s->nc,
+                                              d->counts.as<unsigned long long>(), sms, d->own);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hcount, d->counts.p, sizeof(hcount), cudaMemcpyDeviceToHost, d->own);
+    const cudaError_t es = cudaStreamSynchronize(d->own);
+    if (e != cudaSuccess) return cuda_fail(e, "lattice check");
+    if (es != cudaSuccess) return cuda_fail(es, "lattice upload");
     if (hcount[0] || hcount[1] == 0 || (double)hcount[1] / (double)n < 1e-7) {
         // refused: the host scan names the first offending voxel
         const int rc = validate_lattice(labels, n, s->nc);
