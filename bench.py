@@ -808,7 +808,8 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-ADJOINT_METRIC = "walker-steps/s of the adjoint (both passes) of the waveform-mode signal"
+ADJOINT_METRIC = ("walker-steps/s of the forward walk differentiated by the adjoint (all its passes in the "
+                  "time) of the waveform-mode signal")
 
 
 def run_adjoint_bench(args):
@@ -905,7 +906,7 @@ def run_adjoint_bench(args):
     out["D"]["pathwise"] = {"value": r["d_diffusivity_pathwise"], "std_err": se_p,
                             "rel_err_vs_slope": abs(r["d_diffusivity_pathwise"] / out["D"]["slope_5pct"] - 1)}
     per_dir = per_direction_checks(s0, signal, npar, nw, par, h)
-    ws = npar * tn * 2
+    ws = npar * tn   # the forward walk's walker-steps: the adjoint re-walks them two or three times
     line = {
         "metric": ADJOINT_METRIC, "value": ws / (adj_ms * 1e-3), "unit": "walker-steps/s", "n_gpus": 1, "steps": 1,
         "warmup": args.warmup, "ms_per_step": adj_ms, "higher_is_better": True, "scaling": "weak",

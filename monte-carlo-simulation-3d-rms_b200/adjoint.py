@@ -77,3 +77,18 @@ def waveform_signal(wave: torch.Tensor, D: torch.Tensor, kappa: torch.Tensor, t2
     """Normalised signal [nwave, 2] of waveforms ``wave`` [nwave, nbins, 3]
     (phase per um per ms, i.e. gamma g), differentiable in all four inputs."""
     return _WaveformSignal.apply(wave, D, kappa, t2, setup)
+
+
+def signal_jacobian(wave: torch.Tensor, D: float, kappa: float, t2, setup: WalkSetup) -> dict:
+    """d(normalised signal)/d(D, kappa, T2) for every waveform in one reverse
+    pass (rms_adjoint_jacobian) instead of one backward pass per signal:
+    tensors "D", "kappa", "kappa_score" [nwave, 2] (cos and sin parts) and "T2"
+    [nwave, 2, nc], and the signal itself, "signal" [nwave, 2], for the walk
+    ``waveform_signal`` evaluates with the same setup."""
+    t2a = torch.as_tensor(t2, dtype=torch.float64).cpu().numpy()
+    sim = setup.sim(wave.detach().cpu().double().numpy(), float(D), float(kappa), t2a)
+    J = sim.jacobian(seed=setup.seed, device=setup.device)
+    sim.close()
+    out = {k: torch.from_numpy(J[k] / setup.npar) for k in ("D", "kappa", "kappa_score", "T2")}
+    out["signal"] = torch.from_numpy(J["sigw"] / setup.npar)
+    return out

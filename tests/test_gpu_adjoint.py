@@ -247,3 +247,12 @@ def test_torch_autograd_through_rotations():
     got = float((g.grad.numpy() * d).sum())
     assert abs(got / want - 1) < 0.01, (got, want)
     assert t2.grad.shape == (3,) and np.isfinite(D.grad.item()) and np.isfinite(kap.grad.item())
+    # the one-pass Jacobian contracted with the loss weights is the backward pass's gradient
+    J = adjoint.signal_jacobian(wave.detach(), 2.0, 0.05, [1e6, 80.0, 60.0], setup)
+    Wt = torch.from_numpy(WEIGHTS)
+    # the adjoint forms s0 cos(phi) in FP32, the forward walk in FP64
+    np.testing.assert_allclose(J["signal"].numpy(), S.detach().numpy(), rtol=1e-5, atol=1e-9)
+    assert float((J["D"] * Wt).sum()) == pytest.approx(D.grad.item(), rel=1e-3, abs=1e-9)
+    assert float((J["kappa"] * Wt).sum()) == pytest.approx(kap.grad.item(), rel=1e-3, abs=1e-9)
+    np.testing.assert_allclose((J["T2"] * Wt[:, :, None]).sum(dim=(0, 1)).numpy(), t2.grad.numpy(), rtol=1e-5,
+                               atol=1e-10)
