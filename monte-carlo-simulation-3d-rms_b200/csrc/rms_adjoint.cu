@@ -127,9 +127,10 @@ struct LaneArr {
 
 // Resident blocks per SM: at least 5 for the weighted-loss form (96 registers,
 // no spills); the Jacobian form takes the compiler's choice (123 registers, 4
-// blocks).  Measured on the configs[3] job, 1e6 walkers: weighted 428 ms
-// (518 ms at 4 blocks), Jacobian 390 ms (416 ms when held to 4 blocks at 115
-// registers); with the per-lane arrays in registers (3 blocks) 541 / 474 ms.
+// blocks).  Measured on a 64x64x512 axon, 1e6 walkers x 5000 steps, 16
+// waveforms: weighted 428 ms (518 ms at 4 blocks), Jacobian 390 ms (416 ms
+// when held to 4 blocks at 115 registers); with the per-lane arrays in
+// registers (3 blocks) 541 / 474 ms.
 template <bool JAC>
 __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const __grid_constant__ AdjArgs a) {
     constexpr int NC = kAdjNc, BITS = 4, NW = kAdjWaves;
