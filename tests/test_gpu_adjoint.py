@@ -200,6 +200,32 @@ def test_kappa_gradient_permeable_axon():
     assert np.std(adjs) < np.std(scores), (adjs, scores)
 
 
+def test_jacobian_rows_equal_the_oracle():
+    """rms_adjoint_jacobian's rows against the oracle's FP64 adjoint
+    (or_adjoint_split) with a unit weight on each signal sum, on flat planes
+    with partial permeation (kappa = 0.05), where the FP32 and FP64 walks
+    cannot part: D (time rescaling), kappa (forced draws and score function)
+    and T2 agree to FP32 accuracy."""
+    import pyoracle
+    wave = base_waves()
+    n, D, kap, t2 = 4096, 2.0, 0.05, (1e6, 70.0, 60.0)
+    lab = planes()
+    sim = make(wave, D=D, kappa=kap, t2=t2, lab=lab, npar=n)
+    J = sim.jacobian(seed=5)
+    step, t2s, pij, td = pyoracle.reference_tables(DT, RES, [0.0, D, D], list(t2), 100, TN, kappa=kap)
+    job = pyoracle.Job(lab, dt=DT, tn=TN, npar=n, res=RES, step=step, t2_steps=t2s, pij=pij, seed=5, timepoints=100,
+                       td=td, wave=wave, boundary=pyoracle.BOUNDARY_PERIODIC)
+    for j in range(wave.shape[0]):
+        for sk in range(2):
+            g = np.zeros((wave.shape[0], 2))
+            g[j, sk] = 1.0
+            sums = pyoracle.adjoint_split(job, g.reshape(-1))
+            want = pyoracle.adjoint_gradients(job, sums, D, t2, kappa=kap)
+            for key, col in (("d_diffusivity", "D"), ("d_kappa", "kappa"), ("d_kappa_score", "kappa_score")):
+                assert J[col][j, sk] == pytest.approx(want[key], rel=1e-2, abs=1e-5 * n), (j, sk, key)
+            np.testing.assert_allclose(J["T2"][j, sk], want["d_t2"], rtol=2e-3, atol=1e-9 * n)
+
+
 @pytest.mark.parametrize("kappa", [0.05, 0.0])
 def test_jacobian_rows_equal_one_hot_adjoints(kappa):
     """rms_adjoint_jacobian's row for each waveform's cos and sin sum equals
