@@ -131,12 +131,24 @@ struct LaneArr {
 // waveforms: weighted 428 ms (518 ms at 4 blocks), Jacobian 390 ms (416 ms
 // when held to 4 blocks at 115 registers); with the per-lane arrays in
 // registers (3 blocks) 541 / 474 ms.
-template <bool JAC>
-__global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const __grid_constant__ AdjArgs a) {
+//
+// FORM 0 walks all passes in this launch.  FORM 1 walks passes 1 and 2 only:
+// pass 1 counts the permeation draws made before every checkpoint step (a
+// multiple of 3, 32 and the bin length, where no partial sum is in flight)
+// and picks each walker's forced draw and the last checkpoint before it; pass
+// 2 saves the walker's state there (the phases so far re-accumulated in pass
+// 1's order, so they are pass 1's bit for bit) and lists the walker under that
+// resume step.  FORM 2 walks the forced walks of those lists, 32 walkers of
+// one resume step per warp, each from its saved state -- so a warp no longer
+// walks from step 0 because one lane's draw came early.  The sums are the
+// single launch's, up to the order of the FP64 atomics.
+template <bool JAC, int FORM>
+__global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjoint_kernel(const __grid_constant__ AdjArgs a) {
     constexpr int NC = kAdjNc, BITS = 4, NW = kAdjWaves;
     constexpr int kTab = 2 * NC + 2 * NC * NC;
     __shared__ float s_tab[kTab];
-    __shared__ float s_lane[3][NW][kAdjBlock];   // per lane: phi, dphi, aj (LaneArr)
+    // per lane: phi, dphi, aj (LaneArr); FORM 1: + the phases up to the checkpoint
+    __shared__ float s_lane[FORM == 1 ? 4 : 3][NW][kAdjBlock];
     for (int i = threadIdx.x; i < kTab; i += blockDim.x)
         s_tab[i] = i < NC ? a.step[i]
                           : (i < 2 * NC ? a.kexp[i - NC]
@@ -155,13 +167,31 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const _
     const uint8_t* lat = a.lat;
     const int s0 = a.s0, s1 = a.s1;
 
-    for (int64_t tile = warp_global; tile < a.ntiles; tile += nwarps) {
-        const int64_t w = a.walker_begin + tile * 32 + lane;
-        const bool live = w < a.walker_end;
+    for (int64_t tile = warp_global; tile < (FORM == 2 ? a.ngtiles : a.ntiles); tile += nwarps) {
+        int64_t w;
+        bool live;
+        int gb = 0;   // FORM 2: the resume bucket of this tile
+        int64_t wr = 0;   // the walker's index within the launch
+        if (FORM == 2) {
+            const AdjTile t = a.gtiles[tile];
+            gb = t.bucket;
+            const int e = t.first + lane;
+            live = e < a.bcount[gb];
+            wr = live ? (int64_t)a.blist[(size_t)gb * a.nwalk + e] : 0;
+        } else {
+            wr = tile * 32 + lane;
+            live = a.walker_begin + wr < a.walker_end;
+        }
+        w = a.walker_begin + wr;
         const uint32_t wlo = (uint32_t)w, whi = (uint32_t)((uint64_t)w >> 32);
         const LaneArr phi{&s_lane[0][0][threadIdx.x]}, dphi{&s_lane[1][0][threadIdx.x]}, aj{&s_lane[2][0][threadIdx.x]};
+        const LaneArr phc{&s_lane[FORM == 1 ? 3 : 0][0][threadIdx.x]};   // FORM 1 only
 #pragma unroll
         for (int j = 0; j < NW; ++j) phi[j] = dphi[j] = aj[j] = 0.0f;
+        if (FORM == 1) {
+#pragma unroll
+            for (int j = 0; j < NW; ++j) phc[j] = 0.0f;
+        }
         AdjHooks<NC> h;
 #pragma unroll
         for (int c = 0; c < NC; ++c) h.tc[c] = 0.0f;
@@ -175,16 +205,31 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const _
         int nb_w = 0;         // its Bernoulli draws (pass 1)
         float s0keep = 0.0f;  // JAC: its T2 weight s0 (pass 1)
         float wkeep = 0.0f;   // JAC: W - T / T2(c_T), the T2 weight's time-rescaling term (pass 1)
+        int nb_at[kAdjCkMax];  // FORM 1: draws before checkpoint c (step c * ck_every)
+        int ck_r = 0;          // FORM 1: the checkpoint the forced walk resumes from
+        int kf = 0;            // FORM 1: the forced draw
+        if (FORM == 2 && live) {
+            // what pass 1 left for this walker (FORM 1's summary)
+            const size_t nw = (size_t)a.nwalk;
+            Lkeep = __uint_as_float(a.ws[0 * nw + wr]);
+            nb_w = (int)a.ws[1 * nw + wr];
+            s0keep = __uint_as_float(a.ws[4 * nw + wr]);
+            if (JAC) {
+#pragma unroll
+                for (int j = 0; j < NW; ++j) phi[j] = __uint_as_float(a.ws[(5 + j) * nw + wr]);
+            }
+        }
 
-        for (int pass = 0; pass < (a.force ? 3 : 2); ++pass) {
+        for (int pass = (FORM == 2 ? 2 : 0); pass < (FORM == 0 ? (a.force ? 3 : 2) : (FORM == 1 ? 2 : 3)); ++pass) {
             // pass 3 walks only the walkers that made a draw, and a warp with
             // none of them skips it
-            if (pass == 2 && !__any_sync(kFullMask, live && nb_w > 0)) break;
+            if (FORM == 0 && pass == 2 && !__any_sync(kFullMask, live && nb_w > 0)) break;
             // start position: uniform in the labelled voxels (the split walk's draws)
             bool active = live && (pass < 2 || nb_w > 0);
+            const bool resume = FORM == 2 && gb > 0;   // from a saved state, not from the start
             float f0 = 0.5f, f1 = 0.5f, f2 = 0.5f;
             unsigned lin = 0;
-            if (active) {
+            if (active && !resume) {
                 DomainStream init;
                 init.init(a.seed, (uint64_t)w, kDomInit);
                 long long tries = 0;
@@ -199,9 +244,9 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const _
                     if (++tries >= kInitTryCap) { atomicOr(a.err, kErrInitCap); active = false; break; }
                 }
             }
-            const int ai0 = active ? label_at<BITS>(lat, lin) : 0;
-            SplitWalker wk{lin, active ? cell_at<BITS>(lat, lin) : 0u, f0, f1, f2, 0, 0, 0, f0, f1, f2, ai0,
-                        t_step[ai0], t_k[ai0], 0.0f};
+            const int ai0 = (active && !resume) ? label_at<BITS>(lat, lin) : 0;
+            SplitWalker wk{lin, (active && !resume) ? cell_at<BITS>(lat, lin) : 0u, f0, f1, f2, 0, 0, 0, f0, f1, f2,
+                        ai0, t_step[ai0], t_k[ai0], 0.0f};
             const SplitGeom geo{lat, s0, s1, a.nite, (bool)a.flight, (bool)a.same_cross, mirror};
             auto nsize = [&](int axis) { return axis == 0 ? a.n1 : (axis == 1 ? a.n2 : a.n3); };
             DomainStream perm;
@@ -226,14 +271,70 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const _
                     else if (pass == 2) phi[j] = 0.0f;  // pass 3: the forced phases
                 }
             }
+            int i_start = 0;
+            if (resume) {
+                // the state pass 2 saved at step gb * ck_every (layout: FORM 1's save below)
+                i_start = gb * a.ck_every;
+                if (active) {
+                    const size_t nw = (size_t)a.nwalk;
+                    const uint32_t* c = a.ck + wr;
+                    wk.lin = c[0 * nw]; wk.cell = c[1 * nw];
+                    wk.o0 = __uint_as_float(c[2 * nw]); wk.o1 = __uint_as_float(c[3 * nw]);
+                    wk.o2 = __uint_as_float(c[4 * nw]);
+                    wk.D0 = (int)c[5 * nw]; wk.D1 = (int)c[6 * nw]; wk.D2 = (int)c[7 * nw];
+                    wk.Fm0 = __uint_as_float(c[8 * nw]); wk.Fm1 = __uint_as_float(c[9 * nw]);
+                    wk.Fm2 = __uint_as_float(c[10 * nw]);
+                    wk.ai = (int)c[11 * nw];
+                    wk.cur_step = __uint_as_float(c[12 * nw]); wk.cur_k = __uint_as_float(c[13 * nw]);
+                    wk.w32 = __uint_as_float(c[14 * nw]);
+                    perm.block = c[15 * nw]; perm.q1 = c[16 * nw]; perm.q2 = c[17 * nw]; perm.q3 = c[18 * nw];
+                    perm.left = (int)c[19 * nw];
+                    w64 = __hiloint2double((int)c[21 * nw], (int)c[20 * nw]);
+                    h.nb = (int)c[22 * nw];
+#pragma unroll
+                    for (int j = 0; j < NW; ++j) {
+                        const float v = __uint_as_float(c[(23 + j) * nw]);
+                        if (JAC) dphi[j] = v;
+                        else phi[j] = v;
+                    }
+                }
+            }
             float B0 = 0.0f, B1 = 0.0f, B2 = 0.0f;  // bin sums of the tangent
-            int bin = 0, next_bin = a.bin_steps;
+            int bin = i_start / a.bin_steps, next_bin = (i_start / a.bin_steps + 1) * a.bin_steps;
             float q0 = 0.0f, q1 = 0.0f, q2 = 0.0f, q3 = 0.0f;   // the split walk's direction stream
             int phase = 0;
-            uint32_t dblk = 0u;
+            uint32_t dblk = (uint32_t)(i_start / 3);
             const bool p1st = (pass == 0);
+            int next_ck = (FORM == 1) ? 0 : -1;   // FORM 1: the next checkpoint step
+            int ck_n = 0;
 
-            for (int i = 0; i < a.tn; ++i) {
+            for (int i = i_start; i < a.tn; ++i) {
+                if (FORM == 1 && i == next_ck) {
+                    // a checkpoint step: no partial sum is in flight here
+                    if (p1st) {
+                        if (ck_n < kAdjCkMax) nb_at[ck_n] = h.nb;
+                        ++ck_n;
+                    } else if (active && nb_w > 0 && ck_r > 0 && i == ck_r * a.ck_every) {
+                        const size_t nw = (size_t)a.nwalk;
+                        uint32_t* c = a.ck + wr;
+                        c[0 * nw] = wk.lin; c[1 * nw] = wk.cell;
+                        c[2 * nw] = __float_as_uint(wk.o0); c[3 * nw] = __float_as_uint(wk.o1);
+                        c[4 * nw] = __float_as_uint(wk.o2);
+                        c[5 * nw] = (uint32_t)wk.D0; c[6 * nw] = (uint32_t)wk.D1; c[7 * nw] = (uint32_t)wk.D2;
+                        c[8 * nw] = __float_as_uint(wk.Fm0); c[9 * nw] = __float_as_uint(wk.Fm1);
+                        c[10 * nw] = __float_as_uint(wk.Fm2);
+                        c[11 * nw] = (uint32_t)wk.ai;
+                        c[12 * nw] = __float_as_uint(wk.cur_step); c[13 * nw] = __float_as_uint(wk.cur_k);
+                        c[14 * nw] = __float_as_uint(wk.w32);
+                        c[15 * nw] = perm.block; c[16 * nw] = perm.q1; c[17 * nw] = perm.q2; c[18 * nw] = perm.q3;
+                        c[19 * nw] = (uint32_t)perm.left;
+                        c[20 * nw] = (uint32_t)__double2loint(w64); c[21 * nw] = (uint32_t)__double2hiint(w64);
+                        c[22 * nw] = (uint32_t)h.nb;
+#pragma unroll
+                        for (int j = 0; j < NW; ++j) c[(23 + j) * nw] = __float_as_uint(phc[j]);
+                    }
+                    next_ck += a.ck_every;
+                }
                 float u1, u2;
                 if (phase == 0) {
                     float u[6];
@@ -282,6 +383,17 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const _
                         }
                         B0 = B1 = B2 = 0.0f;
                     } else {
+                        if (FORM == 1 && i < ck_r * a.ck_every) {
+                            // the phases up to the checkpoint, as pass 1 summed them
+#pragma unroll
+                            for (int j = 0; j < NW; ++j) {
+                                if (j < a.nwave) {
+                                    const double g0 = __ldg(wv + 3 * j), g1 = __ldg(wv + 3 * j + 1),
+                                                 g2 = __ldg(wv + 3 * j + 2);
+                                    phc[j] += (float)(g0 * x0 + g1 * x1 + g2 * x2);
+                                }
+                            }
+                        }
                         // time rescaling: at the end of bin b (time t = (b + 1) bin_steps dt)
                         // sum_j a_jw t (g_j,b - g_j,b+1) . x(t), g_j,nbins = 0
                         const float xe0 = ((float)D0 + (o0 - Fm0)) * a.res, xe1 = ((float)D1 + (o1 - Fm1)) * a.res,
@@ -368,6 +480,29 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const _
                 Lkeep = Lw;
                 s0keep = s0w;
                 nb_w = active ? h.nb : 0;
+                if (FORM == 1) {
+                    // the forced draw (as pass 3 picks it) and the last checkpoint before it
+                    if (nb_w > 0) {
+                        DomainStream fs;
+                        fs.init(a.seed, (uint64_t)w, kDomForce);
+                        kf = min((int)(fs.next() * (float)nb_w), nb_w - 1);
+                        const int nck = min(ck_n, kAdjCkMax);
+                        for (int c = 1; c < nck; ++c)
+                            if (nb_at[c] <= kf) ck_r = c;
+                    }
+                    if (live) {
+                        const size_t nw = (size_t)a.nwalk;
+                        a.ws[0 * nw + wr] = __float_as_uint(Lkeep);
+                        a.ws[1 * nw + wr] = (uint32_t)nb_w;
+                        a.ws[2 * nw + wr] = (uint32_t)kf;
+                        a.ws[3 * nw + wr] = (uint32_t)ck_r;
+                        a.ws[4 * nw + wr] = __float_as_uint(s0w);
+                        if (JAC) {
+#pragma unroll
+                            for (int j = 0; j < NW; ++j) a.ws[(5 + j) * nw + wr] = __float_as_uint(phi[j]);
+                        }
+                    }
+                }
                 const double L = warp_sum((double)Lw), LE = warp_sum((double)Lw * (double)h.E),
                              GP = warp_sum((double)G), ES = warp_sum(active ? (double)h.E : 0.0);
                 if (lane == 0) {
@@ -386,6 +521,11 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const _
             } else if (pass == 1) {
                 const double TR = warp_sum((double)tr);
                 if (lane == 0) atomicAdd(a.sums + kAdjSumTR, TR);
+                if (FORM == 1 && live && nb_w > 0) {
+                    // this walker's forced walk, listed under its resume step
+                    const int e = atomicAdd(a.bcount + ck_r, 1);
+                    a.blist[(size_t)ck_r * a.nwalk + e] = (int)wr;
+                }
                 if (JAC) {
                     // dC_j/deps = -S_j dphi_j/deps - C_j dW/deps, dS_j/deps = C_j dphi_j/deps - S_j dW/deps,
                     // dphi_j/deps = R_j - phi_j, -dW/deps = W - T / T2(c_T)
@@ -446,17 +586,29 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? 1 : 5) adjoint_kernel(const _
 
 }  // namespace
 
-int launch_adjoint(const AdjArgs& a, bool jac, int grid, void* stream) {
-    if (jac) adjoint_kernel<true><<<grid, kAdjBlock, 0, (cudaStream_t)stream>>>(a);
-    else adjoint_kernel<false><<<grid, kAdjBlock, 0, (cudaStream_t)stream>>>(a);
+template <bool JAC>
+static int launch_form(const AdjArgs& a, int form, int grid, cudaStream_t st) {
+    if (form == 0) adjoint_kernel<JAC, 0><<<grid, kAdjBlock, 0, st>>>(a);
+    else if (form == 1) adjoint_kernel<JAC, 1><<<grid, kAdjBlock, 0, st>>>(a);
+    else adjoint_kernel<JAC, 2><<<grid, kAdjBlock, 0, st>>>(a);
     return (int)cudaGetLastError();
 }
 
-int adjoint_blocks_per_sm(bool jac) {
+template <bool JAC>
+static int blocks_form(int form) {
     int n = 0;
-    const cudaError_t e = jac ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_kernel<true>, kAdjBlock, 0)
-                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_kernel<false>, kAdjBlock, 0);
+    const cudaError_t e =
+        form == 0   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_kernel<JAC, 0>, kAdjBlock, 0)
+        : form == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_kernel<JAC, 1>, kAdjBlock, 0)
+                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, adjoint_kernel<JAC, 2>, kAdjBlock, 0);
     return e == cudaSuccess ? n : -1;
 }
+
+int launch_adjoint(const AdjArgs& a, bool jac, int form, int grid, void* stream) {
+    return jac ? launch_form<true>(a, form, grid, (cudaStream_t)stream)
+               : launch_form<false>(a, form, grid, (cudaStream_t)stream);
+}
+
+int adjoint_blocks_per_sm(bool jac, int form) { return jac ? blocks_form<true>(form) : blocks_form<false>(form); }
 
 }  // namespace rms

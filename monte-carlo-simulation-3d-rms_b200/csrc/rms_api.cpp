@@ -78,7 +78,7 @@ struct rms_device_state {
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     DevBuf labels, packed, axons, wavef, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
-        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave, stage, counts;
+        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave, adj_ck, adj_ws, adj_blist, adj_bcount, adj_gtiles, stage, counts;
     HostPinned h_out, h_axons;
     size_t labels_bytes = 0;
     bool packed_valid = false;
@@ -88,7 +88,8 @@ struct rms_device_state {
         if (device >= 0) cudaSetDevice(device);
         for (DevBuf* b : {&labels, &packed, &axons, &wavef, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
-                          &tr_vox, &tr_ev, &tr_pos, &adj_g, &adj_sums, &adj_dwave, &stage, &counts})
+                          &tr_vox, &tr_ev, &tr_pos, &adj_g, &adj_sums, &adj_dwave, &adj_ck, &adj_ws, &adj_blist,
+                          &adj_bcount, &adj_gtiles, &stage, &counts})
             b->release();
         h_out.release();
         h_axons.release();
@@ -1093,13 +1094,79 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
 
     int sms = 0;
     RMS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    const int per_sm = adjoint_blocks_per_sm(jac != nullptr);
-    if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
     const int64_t wpb = kAdjBlock / 32;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (a.ntiles + wpb - 1) / wpb));
+    auto grid_for = [&](int form, int64_t tiles, int& grid) -> int {
+        const int per_sm = adjoint_blocks_per_sm(jac != nullptr, form);
+        if (per_sm <= 0) return set_error(RMS_ERR_CUDA, "occupancy query failed (kernel image missing for this GPU?)");
+        grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (tiles + wpb - 1) / wpb));
+        return RMS_OK;
+    };
+    // Grouped forced walks: checkpoints every E steps, E a multiple of 3 (the
+    // direction blocks), 32 (the float folds) and the bin length, with at most
+    // kAdjCkMax of them; each forced walk resumes from the last checkpoint
+    // before its forced draw, 32 walkers of one resume step per warp.
+    int64_t base = 96;   // lcm(3, 32)
+    {
+        int64_t x = base, y = a.bin_steps;
+        while (y) { const int64_t t = x % y; x = y; y = t; }
+        base = base / x * a.bin_steps;
+    }
+    const int64_t ck_every = base * std::max<int64_t>(1, (s->tn + base * kAdjCkMax - 1) / (base * kAdjCkMax));
+    const int nbk = (int)((s->tn - 1) / ck_every + 1);
+    const char* genv = std::getenv("RMS_ADJOINT_GROUPED");
+    bool grouped = a.force && nbk >= 2 && !(genv && genv[0] == '0');
+    const int64_t nwalk = w1 - w0;
+    if (grouped) {
+        // (kAdjCkWords + kAdjWsWords + nbk) words per walker; without room for
+        // them the single launch walks the forced walks instead
+        grouped = d->adj_ck.ensure(sizeof(uint32_t) * kAdjCkWords * (size_t)nwalk) == cudaSuccess &&
+                  d->adj_ws.ensure(sizeof(uint32_t) * kAdjWsWords * (size_t)nwalk) == cudaSuccess &&
+                  d->adj_blist.ensure(sizeof(int) * (size_t)nbk * (size_t)nwalk) == cudaSuccess;
+        if (!grouped) {
+            (void)cudaGetLastError();   // the failed allocation is not sticky; clear it
+            d->adj_ck.release();
+            d->adj_ws.release();
+            d->adj_blist.release();
+        }
+    }
+    int grid = 0;
+    if (grouped) {
+        a.ck_every = (int)ck_every;
+        a.nbk = nbk;
+        a.nwalk = nwalk;
+        RMS_CUDA(d->adj_bcount.ensure(sizeof(int) * kAdjCkMax));
+        RMS_CUDA(cudaMemsetAsync(d->adj_bcount.p, 0, sizeof(int) * kAdjCkMax, st));
+        a.ck = d->adj_ck.as<uint32_t>();
+        a.ws = d->adj_ws.as<uint32_t>();
+        a.blist = d->adj_blist.as<int>();
+        a.bcount = d->adj_bcount.as<int>();
+        rc = grid_for(1, a.ntiles, grid);
+        if (rc) return rc;
+    } else {
+        rc = grid_for(0, a.ntiles, grid);
+        if (rc) return rc;
+    }
     RMS_CUDA(cudaEventRecord(d->e0, st));
-    int e = launch_adjoint(a, jac != nullptr, grid, st);
+    int e = launch_adjoint(a, jac != nullptr, grouped ? 1 : 0, grid, st);
     if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch");
+    if (grouped) {
+        // the bucket sizes decide the forced walks' tiles: longest walks first
+        std::vector<int> cnt(nbk);
+        RMS_CUDA(cudaMemcpyAsync(cnt.data(), d->adj_bcount.p, sizeof(int) * nbk, cudaMemcpyDeviceToHost, st));
+        RMS_CUDA(cudaStreamSynchronize(st));
+        std::vector<AdjTile> tiles;
+        for (int b = 0; b < nbk; ++b)
+            for (int f = 0; f < cnt[b]; f += 32) tiles.push_back(AdjTile{b, f});
+        if (!tiles.empty()) {
+            RMS_CUDA(upload(d->adj_gtiles, tiles, st));
+            a.gtiles = d->adj_gtiles.as<AdjTile>();
+            a.ngtiles = (int64_t)tiles.size();
+            rc = grid_for(2, a.ngtiles, grid);
+            if (rc) return rc;
+            e = launch_adjoint(a, jac != nullptr, 2, grid, st);
+            if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch (forced walks)");
+        }
+    }
     RMS_CUDA(cudaEventRecord(d->e1, st));
     std::vector<double> sums(nsums);
     std::vector<float> dw(ndw);

@@ -146,6 +146,7 @@ constexpr int kAdjSums = kAdjSumForce + 1;
 //   kJacLT + q*NC + c   sum_w X_qw t_wc / step_c (residence in compartment c, steps)
 constexpr int kJacE = 0, kJacTR = 2 * kAdjWaves, kJacF = 4 * kAdjWaves, kJacLT = 6 * kAdjWaves;
 constexpr int kJacSums = kJacLT + 2 * kAdjWaves * kAdjNc;
+struct AdjTile { int bucket, first; };   // 32 entries of one bucket list
 struct AdjArgs {
     const uint8_t* lat;          // padded 4-bit lattice with free-flight flags
     int n1, n2, n3, s0, s1;
@@ -159,11 +160,27 @@ struct AdjArgs {
     const double* wave;          // [bin][waveform][axis], x dt
     const float* gup;            // [waveform][2]: dL/d(sum cos), dL/d(sum sin)
     double* sums;                // [kAdjSums]
+    // grouped forced walks (adjoint_kernel FORM 1 and 2): checkpoint every
+    // ck_every steps (nbk buckets of resume steps b * ck_every); per walker of
+    // the launch (nwalk) its checkpoint ck[word][walker] and summary
+    // ws[word][walker]; bucket lists blist[b][nwalk] with counts bcount[b];
+    // FORM 2 walks the tiles gtiles[t] = (bucket, first entry)
+    int ck_every, nbk;
+    int64_t nwalk;
+    uint32_t* ck;
+    uint32_t* ws;
+    int* blist;
+    int* bcount;
+    const struct AdjTile* gtiles;
+    int64_t ngtiles;
     float* dwave;                // [bin][waveform][axis]: sum_w a_jw X_wb (um)
     int* err;
 };
-int launch_adjoint(const AdjArgs& a, bool jac, int grid, void* stream);
-int adjoint_blocks_per_sm(bool jac);
+// form 0: all passes in one launch; 1: passes 1 and 2 with checkpoints and
+// buckets for the forced walks; 2: the forced walks, grouped by resume step
+constexpr int kAdjCkWords = 23 + kAdjWaves, kAdjWsWords = 5 + kAdjWaves, kAdjCkMax = 16;
+int launch_adjoint(const AdjArgs& a, bool jac, int form, int grid, void* stream);
+int adjoint_blocks_per_sm(bool jac, int form);
 constexpr int kAdjBlock = 128;
 
 // Multi-waveform phase contraction (rms_contract.cu): out[j] = (sum_w cos phi,

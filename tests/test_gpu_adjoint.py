@@ -282,3 +282,42 @@ def test_torch_autograd_through_rotations():
     assert float((J["kappa"] * Wt).sum()) == pytest.approx(kap.grad.item(), rel=1e-3, abs=1e-9)
     np.testing.assert_allclose((J["T2"] * Wt[:, :, None]).sum(dim=(0, 1)).numpy(), t2.grad.numpy(), rtol=1e-5,
                                atol=1e-10)
+
+
+@pytest.mark.parametrize("boundary,shard", [("periodic", None), ("mirror", None), ("periodic", (5000, 16384))])
+def test_grouped_forced_walks_equal_the_single_launch(monkeypatch, boundary, shard):
+    """The forced walks grouped by resume step (two launches: passes 1-2 with
+    checkpoints, then the forced walks from their checkpoints) give the
+    single launch's gradients and Jacobian: the same walkers, draws and FP32
+    arithmetic; the order of the FP64 sums differs, and the phases carried
+    over a checkpoint are summed in a second copy of the same FP32 code (so
+    the forced-draw sums, kappa and D, are held to 1e-5).  2000 steps of
+    20-step bins checkpoint every 480 steps (5 resume steps); also on a
+    walker shard that does not start at walker 0."""
+    wave = base_waves()
+    n = 16384
+
+    def both(grouped):
+        monkeypatch.setenv("RMS_ADJOINT_GROUPED", "1" if grouped else "0")
+        sim = engine.Sim(lattice(), dt=DT, tn=TN, npar=n, res=RES, diffusivity=[0.0, 2.0, 2.0],
+                         t2=[1e6, 80.0, 60.0], wave=wave, timepoints=100, permeation="kappa", kappa=0.05,
+                         boundary=boundary)
+        r = sim.adjoint(WEIGHTS.reshape(-1) / n, seed=5, walker_range=shard)
+        J = sim.jacobian(seed=5, walker_range=shard)
+        sim.close()
+        return r, J
+
+    r1, J1 = both(True)
+    r0, J0 = both(False)
+    assert r0["d_kappa"] != 0.0
+    for k in ("loss", "d_diffusivity_pathwise", "d_kappa_score"):
+        assert r1[k] == pytest.approx(r0[k], rel=1e-9, abs=1e-15), k
+    for k in ("d_diffusivity", "d_kappa"):
+        assert r1[k] == pytest.approx(r0[k], rel=1e-5, abs=1e-12), k
+    np.testing.assert_allclose(r1["d_wave"], r0["d_wave"], rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(r1["d_t2"], r0["d_t2"], rtol=1e-9, atol=1e-15)
+    np.testing.assert_allclose(r1["sigw"], r0["sigw"], rtol=1e-12)
+    for k in ("kappa_score", "T2", "sigw"):
+        np.testing.assert_allclose(J1[k], J0[k], rtol=1e-9, atol=1e-12 * n, err_msg=k)
+    for k in ("D", "kappa"):
+        np.testing.assert_allclose(J1[k], J0[k], rtol=1e-5, atol=1e-9 * n, err_msg=k)
