@@ -27,6 +27,9 @@
 //    L_w[reflected]): the weak derivative of the Bernoulli draws, an unbiased
 //    estimate of dL/dlog P that measures what a crossing changes instead of
 //    correlating the loss with rare crossings as the score function does.
+//    A forced walk repeats its unforced walk up to the forced draw, so with
+//    several checkpoints in the run it is walked from the last one before that
+//    draw, in a second launch over walkers grouped by resume step (FORM below).
 //
 // The host turns the sums into dL/dwave, dL/dT2_c (analytic), dL/dkappa
 // (dP/dkappa = P/kappa: the forced-draw sum / kappa; the score function
@@ -46,6 +49,8 @@
 // the function the forward run evaluates.
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 
 #include "philox.cuh"
 #include "rms_internal.h"
@@ -127,27 +132,32 @@ struct LaneArr {
 
 // Resident blocks per SM: at least 5 for the weighted-loss form (96 registers,
 // no spills); the Jacobian form takes the compiler's choice (123 registers, 4
-// blocks).  Measured on a 64x64x512 axon, 1e6 walkers x 5000 steps, 16
-// waveforms: weighted 428 ms (518 ms at 4 blocks), Jacobian 390 ms (416 ms
-// when held to 4 blocks at 115 registers); with the per-lane arrays in
-// registers (3 blocks) 541 / 474 ms.
+// blocks) except FORMs 1 and 2, held to 4 blocks (unbounded they took 248 and
+// 134 registers).
+// Measured on a 64x64x512 axon, 1e6 walkers x 5000 steps, 16 waveforms, all
+// passes in one launch: weighted 428 ms (518 ms at 4 blocks), Jacobian 390 ms
+// (416 ms when held to 4 blocks at 115 registers); with the per-lane arrays
+// in registers (3 blocks) 541 / 474 ms.  With the forced walks grouped (FORM 1
+// then FORM 2, 11 resume steps 480 steps apart): 310 / 308 ms.
 //
-// FORM 0 walks all passes in this launch.  FORM 1 walks passes 1 and 2 only:
-// pass 1 counts the permeation draws made before every checkpoint step (a
-// multiple of 3, 32 and the bin length, where no partial sum is in flight)
-// and picks each walker's forced draw and the last checkpoint before it; pass
-// 2 saves the walker's state there (the phases so far re-accumulated in pass
-// 1's order, so they are pass 1's bit for bit) and lists the walker under that
-// resume step.  FORM 2 walks the forced walks of those lists, 32 walkers of
-// one resume step per warp, each from its saved state -- so a warp no longer
-// walks from step 0 because one lane's draw came early.  The sums are the
-// single launch's, up to the order of the FP64 atomics.
+// FORM 0 walks all passes in this launch.  FORM 1 walks pass 1 only and
+// leaves in memory what passes 2 and 3 need: the bin displacement sums X_wb
+// and a_jw (weighted form; adjoint_dwave_kernel forms dL/dwave from them),
+// the time-rescaling sums R_j summed in pass 1 from the displacement at each
+// bin end (a_jw multiplies them only at the end), and the walker's state at
+// every checkpoint step (a multiple of 3, 32 and the bin length, where no
+// partial sum is in flight).  At the end it picks the forced draw and the last
+// checkpoint before it and lists the walker under that resume step.  FORM 2
+// walks the forced walks of those lists, 32 walkers of one resume step per
+// warp, each from its checkpoint -- so a warp no longer walks from step 0
+// because one lane's draw came early.  The sums are the single launch's up to
+// the order of the float and FP64 sums.
 template <bool JAC, int FORM>
-__global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjoint_kernel(const __grid_constant__ AdjArgs a) {
+__global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM > 0 ? 4 : 1) : 5) adjoint_kernel(const __grid_constant__ AdjArgs a) {
     constexpr int NC = kAdjNc, BITS = 4, NW = kAdjWaves;
     constexpr int kTab = 2 * NC + 2 * NC * NC;
     __shared__ float s_tab[kTab];
-    // per lane: phi, dphi, aj (LaneArr); FORM 1: + the phases up to the checkpoint
+    // per lane: phi, dphi, aj (LaneArr); FORM 1: + the time-rescaling sums R_j
     __shared__ float s_lane[FORM == 1 ? 4 : 3][NW][kAdjBlock];
     for (int i = threadIdx.x; i < kTab; i += blockDim.x)
         s_tab[i] = i < NC ? a.step[i]
@@ -167,17 +177,25 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
     const uint8_t* lat = a.lat;
     const int s0 = a.s0, s1 = a.s1;
 
-    for (int64_t tile = warp_global; tile < (FORM == 2 ? a.ngtiles : a.ntiles); tile += nwarps) {
+    for (int64_t tile = warp_global; tile < a.ntiles; tile += nwarps) {
         int64_t w;
         bool live;
         int gb = 0;   // FORM 2: the resume bucket of this tile
         int64_t wr = 0;   // the walker's index within the launch
         if (FORM == 2) {
-            const AdjTile t = a.gtiles[tile];
-            gb = t.bucket;
-            const int e = t.first + lane;
-            live = e < a.bcount[gb];
-            wr = live ? (int64_t)a.blist[(size_t)gb * a.nwalk + e] : 0;
+            // tile -> (bucket, first entry): the buckets' tiles in order
+            int64_t t = tile;
+            int cnt = 0;
+            for (gb = 0; gb < a.nbk; ++gb) {
+                cnt = __ldg(a.bcount + gb);
+                const int64_t nt = (cnt + 31) / 32;
+                if (t < nt) break;
+                t -= nt;
+            }
+            if (gb >= a.nbk) break;   // past the last listed walker (tiles only grow)
+            const int64_t e = t * 32 + lane;
+            live = e < cnt;
+            wr = live ? (int64_t)__ldg(a.blist + (size_t)gb * a.nwalk + e) : 0;
         } else {
             wr = tile * 32 + lane;
             live = a.walker_begin + wr < a.walker_end;
@@ -185,12 +203,12 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
         w = a.walker_begin + wr;
         const uint32_t wlo = (uint32_t)w, whi = (uint32_t)((uint64_t)w >> 32);
         const LaneArr phi{&s_lane[0][0][threadIdx.x]}, dphi{&s_lane[1][0][threadIdx.x]}, aj{&s_lane[2][0][threadIdx.x]};
-        const LaneArr phc{&s_lane[FORM == 1 ? 3 : 0][0][threadIdx.x]};   // FORM 1 only
+        const LaneArr rr{&s_lane[FORM == 1 ? 3 : 0][0][threadIdx.x]};   // FORM 1 only
 #pragma unroll
         for (int j = 0; j < NW; ++j) phi[j] = dphi[j] = aj[j] = 0.0f;
         if (FORM == 1) {
 #pragma unroll
-            for (int j = 0; j < NW; ++j) phc[j] = 0.0f;
+            for (int j = 0; j < NW; ++j) rr[j] = 0.0f;
         }
         AdjHooks<NC> h;
 #pragma unroll
@@ -206,21 +224,19 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
         float s0keep = 0.0f;  // JAC: its T2 weight s0 (pass 1)
         float wkeep = 0.0f;   // JAC: W - T / T2(c_T), the T2 weight's time-rescaling term (pass 1)
         int nb_at[kAdjCkMax];  // FORM 1: draws before checkpoint c (step c * ck_every)
-        int ck_r = 0;          // FORM 1: the checkpoint the forced walk resumes from
-        int kf = 0;            // FORM 1: the forced draw
         if (FORM == 2 && live) {
             // what pass 1 left for this walker (FORM 1's summary)
             const size_t nw = (size_t)a.nwalk;
             Lkeep = __uint_as_float(a.ws[0 * nw + wr]);
             nb_w = (int)a.ws[1 * nw + wr];
-            s0keep = __uint_as_float(a.ws[4 * nw + wr]);
+            s0keep = __uint_as_float(a.ws[2 * nw + wr]);
             if (JAC) {
 #pragma unroll
-                for (int j = 0; j < NW; ++j) phi[j] = __uint_as_float(a.ws[(5 + j) * nw + wr]);
+                for (int j = 0; j < NW; ++j) phi[j] = __uint_as_float(a.ws[(3 + j) * nw + wr]);
             }
         }
 
-        for (int pass = (FORM == 2 ? 2 : 0); pass < (FORM == 0 ? (a.force ? 3 : 2) : (FORM == 1 ? 2 : 3)); ++pass) {
+        for (int pass = (FORM == 2 ? 2 : 0); pass < (FORM == 0 ? (a.force ? 3 : 2) : (FORM == 1 ? 1 : 3)); ++pass) {
             // pass 3 walks only the walkers that made a draw, and a warp with
             // none of them skips it
             if (FORM == 0 && pass == 2 && !__any_sync(kFullMask, live && nb_w > 0)) break;
@@ -273,11 +289,11 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
             }
             int i_start = 0;
             if (resume) {
-                // the state pass 2 saved at step gb * ck_every (layout: FORM 1's save below)
+                // the state pass 1 saved at step gb * ck_every (layout: FORM 1's save below)
                 i_start = gb * a.ck_every;
                 if (active) {
                     const size_t nw = (size_t)a.nwalk;
-                    const uint32_t* c = a.ck + wr;
+                    const uint32_t* c = a.ck + (size_t)(gb - 1) * kAdjCkWords * nw + wr;
                     wk.lin = c[0 * nw]; wk.cell = c[1 * nw];
                     wk.o0 = __uint_as_float(c[2 * nw]); wk.o1 = __uint_as_float(c[3 * nw]);
                     wk.o2 = __uint_as_float(c[4 * nw]);
@@ -310,13 +326,12 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
 
             for (int i = i_start; i < a.tn; ++i) {
                 if (FORM == 1 && i == next_ck) {
-                    // a checkpoint step: no partial sum is in flight here
-                    if (p1st) {
-                        if (ck_n < kAdjCkMax) nb_at[ck_n] = h.nb;
-                        ++ck_n;
-                    } else if (active && nb_w > 0 && ck_r > 0 && i == ck_r * a.ck_every) {
+                    // a checkpoint step: no partial sum is in flight here; the
+                    // state at checkpoint c >= 1 goes to slot c - 1
+                    if (ck_n < kAdjCkMax) nb_at[ck_n] = h.nb;
+                    if (a.force && ck_n > 0 && ck_n < kAdjCkMax && live) {
                         const size_t nw = (size_t)a.nwalk;
-                        uint32_t* c = a.ck + wr;
+                        uint32_t* c = a.ck + (size_t)(ck_n - 1) * kAdjCkWords * nw + wr;
                         c[0 * nw] = wk.lin; c[1 * nw] = wk.cell;
                         c[2 * nw] = __float_as_uint(wk.o0); c[3 * nw] = __float_as_uint(wk.o1);
                         c[4 * nw] = __float_as_uint(wk.o2);
@@ -331,8 +346,9 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
                         c[20 * nw] = (uint32_t)__double2loint(w64); c[21 * nw] = (uint32_t)__double2hiint(w64);
                         c[22 * nw] = (uint32_t)h.nb;
 #pragma unroll
-                        for (int j = 0; j < NW; ++j) c[(23 + j) * nw] = __float_as_uint(phc[j]);
+                        for (int j = 0; j < NW; ++j) c[(23 + j) * nw] = __float_as_uint(phi[j]);
                     }
+                    ++ck_n;
                     next_ck += a.ck_every;
                 }
                 float u1, u2;
@@ -382,18 +398,34 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
                             }
                         }
                         B0 = B1 = B2 = 0.0f;
-                    } else {
-                        if (FORM == 1 && i < ck_r * a.ck_every) {
-                            // the phases up to the checkpoint, as pass 1 summed them
+                        if (FORM == 1) {
+                            // X_wb for dL/dwave, and R_j += t (g_j,b - g_j,b+1) . x(t) as pass 2 sums it
+                            if (!JAC && live) {
+                                const size_t nw = (size_t)a.nwalk;
+                                float* xb = a.xbin + (size_t)bin * 3 * nw + wr;
+                                xb[0] = (float)x0;
+                                xb[nw] = (float)x1;
+                                xb[2 * nw] = (float)x2;
+                            }
+                            const float xe0 = ((float)D0 + (o0 - Fm0)) * a.res,
+                                        xe1 = ((float)D1 + (o1 - Fm1)) * a.res,
+                                        xe2 = ((float)D2 + (o2 - Fm2)) * a.res;
+                            const float tb = (float)(i + 1);
+                            const double* wn = wv + a.nwave * 3;
+                            const bool last = bin + 1 >= a.nbins;
 #pragma unroll
                             for (int j = 0; j < NW; ++j) {
                                 if (j < a.nwave) {
-                                    const double g0 = __ldg(wv + 3 * j), g1 = __ldg(wv + 3 * j + 1),
-                                                 g2 = __ldg(wv + 3 * j + 2);
-                                    phc[j] += (float)(g0 * x0 + g1 * x1 + g2 * x2);
+                                    const float q0 = (float)(__ldg(wv + 3 * j) - (last ? 0.0 : __ldg(wn + 3 * j)));
+                                    const float q1 =
+                                        (float)(__ldg(wv + 3 * j + 1) - (last ? 0.0 : __ldg(wn + 3 * j + 1)));
+                                    const float q2 =
+                                        (float)(__ldg(wv + 3 * j + 2) - (last ? 0.0 : __ldg(wn + 3 * j + 2)));
+                                    rr[j] = fmaf(tb, q0 * xe0 + q1 * xe1 + q2 * xe2, rr[j]);
                                 }
                             }
                         }
+                    } else {
                         // time rescaling: at the end of bin b (time t = (b + 1) bin_steps dt)
                         // sum_j a_jw t (g_j,b - g_j,b+1) . x(t), g_j,nbins = 0
                         const float xe0 = ((float)D0 + (o0 - Fm0)) * a.res, xe1 = ((float)D1 + (o1 - Fm1)) * a.res,
@@ -448,6 +480,10 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
                     aj[j] = s0w * (gs * cs - gc * sn);
                     G += aj[j] * dphi[j];
                     tr -= aj[j] * phi[j];
+                    if (FORM == 1 && !JAC && j < a.nwave) {
+                        tr = fmaf(aj[j], rr[j], tr);   // pass 2's time-rescaling sum
+                        if (live) a.ajw[(size_t)j * a.nwalk + wr] = aj[j];
+                    }
                     const double C = warp_sum((double)(s0w * cs)), S = warp_sum((double)(s0w * sn));
                     if (lane == 0 && j < a.nwave) {
                         atomicAdd(a.sums + kAdjSumSig + 2 * j, C);
@@ -481,26 +517,46 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
                 s0keep = s0w;
                 nb_w = active ? h.nb : 0;
                 if (FORM == 1) {
-                    // the forced draw (as pass 3 picks it) and the last checkpoint before it
-                    if (nb_w > 0) {
+                    // pass 2's sums from what pass 1 kept
+                    const double TR = warp_sum((double)tr);
+                    if (lane == 0) atomicAdd(a.sums + kAdjSumTR, TR);
+                    if (JAC) {
+#pragma unroll
+                        for (int j = 0; j < NW; ++j) {
+                            if (j < a.nwave) {
+                                float sn = 0.0f, cs = 0.0f;
+                                sincosf(phi[j], &sn, &cs);
+                                const float Cw = active ? s0keep * cs : 0.0f, Sw = active ? s0keep * sn : 0.0f;
+                                const float de = rr[j] - phi[j];
+                                const double TC = warp_sum((double)(-Sw * de + Cw * wkeep));
+                                const double TS = warp_sum((double)(Cw * de + Sw * wkeep));
+                                if (lane == 0) {
+                                    atomicAdd(a.sums + kAdjSums + kJacTR + 2 * j, TC);
+                                    atomicAdd(a.sums + kAdjSums + kJacTR + 2 * j + 1, TS);
+                                }
+                            }
+                        }
+                    }
+                    if (a.force && live && nb_w > 0) {
+                        // the forced draw (as pass 3 picks it), the last checkpoint
+                        // before it, and this walker listed under that resume step
                         DomainStream fs;
                         fs.init(a.seed, (uint64_t)w, kDomForce);
-                        kf = min((int)(fs.next() * (float)nb_w), nb_w - 1);
+                        const int kf = min((int)(fs.next() * (float)nb_w), nb_w - 1);
                         const int nck = min(ck_n, kAdjCkMax);
+                        int ck_r = 0;
                         for (int c = 1; c < nck; ++c)
                             if (nb_at[c] <= kf) ck_r = c;
-                    }
-                    if (live) {
                         const size_t nw = (size_t)a.nwalk;
                         a.ws[0 * nw + wr] = __float_as_uint(Lkeep);
                         a.ws[1 * nw + wr] = (uint32_t)nb_w;
-                        a.ws[2 * nw + wr] = (uint32_t)kf;
-                        a.ws[3 * nw + wr] = (uint32_t)ck_r;
-                        a.ws[4 * nw + wr] = __float_as_uint(s0w);
+                        a.ws[2 * nw + wr] = __float_as_uint(s0w);
                         if (JAC) {
 #pragma unroll
-                            for (int j = 0; j < NW; ++j) a.ws[(5 + j) * nw + wr] = __float_as_uint(phi[j]);
+                            for (int j = 0; j < NW; ++j) a.ws[(3 + j) * nw + wr] = __float_as_uint(phi[j]);
                         }
+                        const int e = atomicAdd(a.bcount + ck_r, 1);
+                        a.blist[(size_t)ck_r * a.nwalk + e] = (int)wr;
                     }
                 }
                 const double L = warp_sum((double)Lw), LE = warp_sum((double)Lw * (double)h.E),
@@ -521,11 +577,6 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
             } else if (pass == 1) {
                 const double TR = warp_sum((double)tr);
                 if (lane == 0) atomicAdd(a.sums + kAdjSumTR, TR);
-                if (FORM == 1 && live && nb_w > 0) {
-                    // this walker's forced walk, listed under its resume step
-                    const int e = atomicAdd(a.bcount + ck_r, 1);
-                    a.blist[(size_t)ck_r * a.nwalk + e] = (int)wr;
-                }
                 if (JAC) {
                     // dC_j/deps = -S_j dphi_j/deps - C_j dW/deps, dS_j/deps = C_j dphi_j/deps - S_j dW/deps,
                     // dphi_j/deps = R_j - phi_j, -dW/deps = W - T / T2(c_T)
@@ -584,7 +635,70 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM == 1 ? 4 : 1) : 5) adjo
     }
 }
 
+// dL/dwave from pass 1's records: dwave[b][j][ax] += sum_w a_jw X_wb,ax over
+// the launch's walkers (xbin [bin][axis][walker], ajw [waveform][walker]).
+// Each block takes kDwSlab walkers (kDwPer per thread, their a_jw in
+// registers) and rows [r0, r1) of the bin x axis table; per row a warp
+// reduce-scatter and a sum over the block's warps leave one float atomic per
+// waveform.  HBM-bound: the X table is read once (12 bytes per walker per bin).
+constexpr int kDwBlock = 256, kDwPer = 4, kDwSlab = kDwBlock * kDwPer;
+
+__global__ void __launch_bounds__(kDwBlock) adjoint_dwave_kernel(const float* __restrict__ xbin,
+                                                                const float* __restrict__ ajw, int64_t nwalk,
+                                                                int nwave, int nrows, int rows_per_block,
+                                                                float* __restrict__ dwave) {
+    constexpr int NW = kAdjWaves;
+    __shared__ float red[2][kDwBlock / 32][NW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t w0 = (int64_t)blockIdx.x * kDwSlab + threadIdx.x;
+    float av[kDwPer][NW];
+#pragma unroll
+    for (int k = 0; k < kDwPer; ++k) {
+        const int64_t w = w0 + (int64_t)k * kDwBlock;
+#pragma unroll
+        for (int j = 0; j < NW; ++j) av[k][j] = (w < nwalk && j < nwave) ? __ldg(ajw + (size_t)j * nwalk + w) : 0.0f;
+    }
+    const int r0 = blockIdx.y * rows_per_block, r1 = min(nrows, r0 + rows_per_block);
+    for (int r = r0; r < r1; ++r) {
+        float acc[NW];
+#pragma unroll
+        for (int j = 0; j < NW; ++j) acc[j] = 0.0f;
+        const float* xr = xbin + (size_t)r * nwalk;
+#pragma unroll
+        for (int k = 0; k < kDwPer; ++k) {
+            const int64_t w = w0 + (int64_t)k * kDwBlock;
+            const float x = w < nwalk ? __ldcs(xr + w) : 0.0f;
+#pragma unroll
+            for (int j = 0; j < NW; ++j) acc[j] = fmaf(av[k][j], x, acc[j]);
+        }
+        const float v = warp_reduce_scatter16f(acc, lane);   // lanes l, l ^ 16: waveform l & 15
+        const int buf = r & 1;
+        if (lane < 16) red[buf][warp][lane] = v;
+        __syncthreads();
+        if (threadIdx.x < nwave) {
+            float t = 0.0f;
+#pragma unroll
+            for (int q = 0; q < kDwBlock / 32; ++q) t += red[buf][q][threadIdx.x];
+            const int b = r / 3, ax = r - 3 * b;
+            atomicAdd(dwave + ((size_t)b * nwave + threadIdx.x) * 3 + ax, t);
+        }
+    }
+}
+
 }  // namespace
+
+int launch_adjoint_dwave(const AdjArgs& a, int sms, void* stream) {
+    const int nrows = a.nbins * 3;
+    const int slabs = (int)((a.nwalk + kDwSlab - 1) / kDwSlab);
+    // enough blocks for every SM: split the rows when the walkers are few
+    const int want = 4 * sms;
+    const int groups = std::max(1, std::min(nrows, (want + slabs - 1) / slabs));
+    const int per = (nrows + groups - 1) / groups;
+    const dim3 grid((unsigned)slabs, (unsigned)((nrows + per - 1) / per));
+    adjoint_dwave_kernel<<<grid, kDwBlock, 0, (cudaStream_t)stream>>>(a.xbin, a.ajw, a.nwalk, a.nwave, nrows, per,
+                                                                     a.dwave);
+    return (int)cudaGetLastError();
+}
 
 template <bool JAC>
 static int launch_form(const AdjArgs& a, int form, int grid, cudaStream_t st) {

@@ -78,7 +78,8 @@ struct rms_device_state {
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     DevBuf labels, packed, axons, wavef, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
-        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave, adj_ck, adj_ws, adj_blist, adj_bcount, adj_gtiles, stage, counts;
+        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave, adj_ck, adj_ws, adj_blist, adj_bcount, adj_xbin, adj_ajw, stage,
+        counts;
     HostPinned h_out, h_axons;
     size_t labels_bytes = 0;
     bool packed_valid = false;
@@ -89,7 +90,7 @@ struct rms_device_state {
         for (DevBuf* b : {&labels, &packed, &axons, &wavef, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
                           &tr_vox, &tr_ev, &tr_pos, &adj_g, &adj_sums, &adj_dwave, &adj_ck, &adj_ws, &adj_blist,
-                          &adj_bcount, &adj_gtiles, &stage, &counts})
+                          &adj_bcount, &adj_xbin, &adj_ajw, &stage, &counts})
             b->release();
         h_out.release();
         h_axons.release();
@@ -1101,10 +1102,13 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
         grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, (tiles + wpb - 1) / wpb));
         return RMS_OK;
     };
-    // Grouped forced walks: checkpoints every E steps, E a multiple of 3 (the
-    // direction blocks), 32 (the float folds) and the bin length, with at most
-    // kAdjCkMax of them; each forced walk resumes from the last checkpoint
-    // before its forced draw, 32 walkers of one resume step per warp.
+    // Pass 1 alone, then the forced walks grouped by resume step.  Checkpoints
+    // every E steps, E a multiple of 3 (the direction blocks), 32 (the float
+    // folds) and the bin length, at most kAdjCkMax of them; each forced walk
+    // resumes from the last checkpoint before its forced draw.  Per walker:
+    // the checkpoints, the summary, a bucket entry per resume step and
+    // (weighted form) X_wb and a_jw; the walkers go in chunks that fit the
+    // scratch budget (half the free memory, at most 16 GiB).
     int64_t base = 96;   // lcm(3, 32)
     {
         int64_t x = base, y = a.bin_steps;
@@ -1113,58 +1117,79 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
     }
     const int64_t ck_every = base * std::max<int64_t>(1, (s->tn + base * kAdjCkMax - 1) / (base * kAdjCkMax));
     const int nbk = (int)((s->tn - 1) / ck_every + 1);
-    const char* genv = std::getenv("RMS_ADJOINT_GROUPED");
-    bool grouped = a.force && nbk >= 2 && !(genv && genv[0] == '0');
     const int64_t nwalk = w1 - w0;
+    const size_t per_walker =
+        (jac ? 0 : sizeof(float) * ((size_t)3 * s->nbins + s->nwave)) +
+        (a.force ? sizeof(uint32_t) * ((size_t)kAdjCkWords * (nbk - 1) + kAdjWsWords + nbk) : 0);
+    size_t mfree = 0, mtotal = 0;
+    if (cudaMemGetInfo(&mfree, &mtotal) != cudaSuccess) {
+        (void)cudaGetLastError();
+        mfree = 0;
+    }
+    const size_t budget = std::min<size_t>(mfree / 2, (size_t)16 << 30);
+    int64_t chunk = std::min<int64_t>(nwalk, (int64_t)(budget / std::max<size_t>(per_walker, 1)));
+    if (chunk < nwalk) chunk = chunk / 32 * 32;
+    const char* genv = std::getenv("RMS_ADJOINT_GROUPED");
+    bool grouped = !(genv && genv[0] == '0') && chunk >= std::min<int64_t>(nwalk, 65536);
     if (grouped) {
-        // (kAdjCkWords + kAdjWsWords + nbk) words per walker; without room for
-        // them the single launch walks the forced walks instead
-        grouped = d->adj_ck.ensure(sizeof(uint32_t) * kAdjCkWords * (size_t)nwalk) == cudaSuccess &&
-                  d->adj_ws.ensure(sizeof(uint32_t) * kAdjWsWords * (size_t)nwalk) == cudaSuccess &&
-                  d->adj_blist.ensure(sizeof(int) * (size_t)nbk * (size_t)nwalk) == cudaSuccess;
-        if (!grouped) {
-            (void)cudaGetLastError();   // the failed allocation is not sticky; clear it
-            d->adj_ck.release();
-            d->adj_ws.release();
-            d->adj_blist.release();
+        const size_t nwc = (size_t)chunk;
+        bool ok = true;
+        if (!jac) {
+            ok = ok && d->adj_xbin.ensure(sizeof(float) * 3 * (size_t)s->nbins * nwc) == cudaSuccess;
+            ok = ok && d->adj_ajw.ensure(sizeof(float) * (size_t)s->nwave * nwc) == cudaSuccess;
+        }
+        if (a.force) {
+            ok = ok && d->adj_ck.ensure(sizeof(uint32_t) * kAdjCkWords * (size_t)(nbk - 1) * nwc) == cudaSuccess;
+            ok = ok && d->adj_ws.ensure(sizeof(uint32_t) * kAdjWsWords * nwc) == cudaSuccess;
+            ok = ok && d->adj_blist.ensure(sizeof(int) * (size_t)nbk * nwc) == cudaSuccess;
+            ok = ok && d->adj_bcount.ensure(sizeof(int) * kAdjCkMax) == cudaSuccess;
+        }
+        if (!ok) {
+            // without room for the records the single launch walks all passes
+            (void)cudaGetLastError();   // a failed allocation is not sticky; clear it
+            for (DevBuf* b : {&d->adj_xbin, &d->adj_ajw, &d->adj_ck, &d->adj_ws, &d->adj_blist}) b->release();
+            grouped = false;
         }
     }
-    int grid = 0;
-    if (grouped) {
+    RMS_CUDA(cudaEventRecord(d->e0, st));
+    if (!grouped) {
+        int grid = 0;
+        rc = grid_for(0, a.ntiles, grid);
+        if (rc) return rc;
+        const int e = launch_adjoint(a, jac != nullptr, 0, grid, st);
+        if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch");
+    } else {
         a.ck_every = (int)ck_every;
         a.nbk = nbk;
-        a.nwalk = nwalk;
-        RMS_CUDA(d->adj_bcount.ensure(sizeof(int) * kAdjCkMax));
-        RMS_CUDA(cudaMemsetAsync(d->adj_bcount.p, 0, sizeof(int) * kAdjCkMax, st));
+        a.xbin = d->adj_xbin.as<float>();
+        a.ajw = d->adj_ajw.as<float>();
         a.ck = d->adj_ck.as<uint32_t>();
         a.ws = d->adj_ws.as<uint32_t>();
         a.blist = d->adj_blist.as<int>();
         a.bcount = d->adj_bcount.as<int>();
-        rc = grid_for(1, a.ntiles, grid);
-        if (rc) return rc;
-    } else {
-        rc = grid_for(0, a.ntiles, grid);
-        if (rc) return rc;
-    }
-    RMS_CUDA(cudaEventRecord(d->e0, st));
-    int e = launch_adjoint(a, jac != nullptr, grouped ? 1 : 0, grid, st);
-    if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch");
-    if (grouped) {
-        // the bucket sizes decide the forced walks' tiles: longest walks first
-        std::vector<int> cnt(nbk);
-        RMS_CUDA(cudaMemcpyAsync(cnt.data(), d->adj_bcount.p, sizeof(int) * nbk, cudaMemcpyDeviceToHost, st));
-        RMS_CUDA(cudaStreamSynchronize(st));
-        std::vector<AdjTile> tiles;
-        for (int b = 0; b < nbk; ++b)
-            for (int f = 0; f < cnt[b]; f += 32) tiles.push_back(AdjTile{b, f});
-        if (!tiles.empty()) {
-            RMS_CUDA(upload(d->adj_gtiles, tiles, st));
-            a.gtiles = d->adj_gtiles.as<AdjTile>();
-            a.ngtiles = (int64_t)tiles.size();
-            rc = grid_for(2, a.ngtiles, grid);
+        for (int64_t c0 = w0; c0 < w1; c0 += chunk) {
+            a.walker_begin = c0;
+            a.walker_end = std::min<int64_t>(w1, c0 + chunk);
+            a.nwalk = a.walker_end - a.walker_begin;
+            a.ntiles = (a.nwalk + 31) / 32;
+            if (a.force) RMS_CUDA(cudaMemsetAsync(d->adj_bcount.p, 0, sizeof(int) * kAdjCkMax, st));
+            int grid = 0;
+            rc = grid_for(1, a.ntiles, grid);
             if (rc) return rc;
-            e = launch_adjoint(a, jac != nullptr, 2, grid, st);
-            if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch (forced walks)");
+            int e = launch_adjoint(a, jac != nullptr, 1, grid, st);
+            if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch (pass 1)");
+            if (!jac) {
+                e = launch_adjoint_dwave(a, sms, st);
+                if (e) return cuda_fail((cudaError_t)e, "adjoint dL/dwave launch");
+            }
+            if (a.force) {
+                // the buckets' tiles: at most one partial tile per bucket beyond nwalk / 32
+                a.ntiles = a.nwalk / 32 + nbk;
+                rc = grid_for(2, a.ntiles, grid);
+                if (rc) return rc;
+                e = launch_adjoint(a, jac != nullptr, 2, grid, st);
+                if (e) return cuda_fail((cudaError_t)e, "adjoint kernel launch (forced walks)");
+            }
         }
     }
     RMS_CUDA(cudaEventRecord(d->e1, st));

@@ -146,7 +146,6 @@ constexpr int kAdjSums = kAdjSumForce + 1;
 //   kJacLT + q*NC + c   sum_w X_qw t_wc / step_c (residence in compartment c, steps)
 constexpr int kJacE = 0, kJacTR = 2 * kAdjWaves, kJacF = 4 * kAdjWaves, kJacLT = 6 * kAdjWaves;
 constexpr int kJacSums = kJacLT + 2 * kAdjWaves * kAdjNc;
-struct AdjTile { int bucket, first; };   // 32 entries of one bucket list
 struct AdjArgs {
     const uint8_t* lat;          // padded 4-bit lattice with free-flight flags
     int n1, n2, n3, s0, s1;
@@ -160,26 +159,29 @@ struct AdjArgs {
     const double* wave;          // [bin][waveform][axis], x dt
     const float* gup;            // [waveform][2]: dL/d(sum cos), dL/d(sum sin)
     double* sums;                // [kAdjSums]
-    // grouped forced walks (adjoint_kernel FORM 1 and 2): checkpoint every
-    // ck_every steps (nbk buckets of resume steps b * ck_every); per walker of
-    // the launch (nwalk) its checkpoint ck[word][walker] and summary
-    // ws[word][walker]; bucket lists blist[b][nwalk] with counts bcount[b];
-    // FORM 2 walks the tiles gtiles[t] = (bucket, first entry)
+    // pass 1 alone, then the forced walks grouped (adjoint_kernel FORM 1 and
+    // 2): checkpoint every ck_every steps (nbk resume steps b * ck_every); per
+    // walker of the launch (nwalk): its states at checkpoints 1..nbk-1,
+    // ck[checkpoint - 1][word][walker]; its summary ws[word][walker]; bucket
+    // lists blist[b][nwalk] with counts bcount[b]; weighted form: the bin
+    // displacement sums xbin[bin][axis][walker] (um) and a_jw, ajw[j][walker]
     int ck_every, nbk;
     int64_t nwalk;
     uint32_t* ck;
     uint32_t* ws;
     int* blist;
     int* bcount;
-    const struct AdjTile* gtiles;
-    int64_t ngtiles;
+    float* xbin;
+    float* ajw;
     float* dwave;                // [bin][waveform][axis]: sum_w a_jw X_wb (um)
     int* err;
 };
-// form 0: all passes in one launch; 1: passes 1 and 2 with checkpoints and
-// buckets for the forced walks; 2: the forced walks, grouped by resume step
-constexpr int kAdjCkWords = 23 + kAdjWaves, kAdjWsWords = 5 + kAdjWaves, kAdjCkMax = 16;
+// form 0: all passes in one launch; 1: pass 1 with checkpoints, X_wb, a_jw
+// and the buckets of the forced walks; 2: the forced walks, grouped by resume
+// step.  launch_adjoint_dwave: dL/dwave from form 1's X_wb and a_jw.
+constexpr int kAdjCkWords = 23 + kAdjWaves, kAdjWsWords = 3 + kAdjWaves, kAdjCkMax = 16;
 int launch_adjoint(const AdjArgs& a, bool jac, int form, int grid, void* stream);
+int launch_adjoint_dwave(const AdjArgs& a, int sms, void* stream);
 int adjoint_blocks_per_sm(bool jac, int form);
 constexpr int kAdjBlock = 128;
 

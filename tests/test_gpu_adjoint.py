@@ -286,14 +286,16 @@ def test_torch_autograd_through_rotations():
 
 @pytest.mark.parametrize("boundary,shard", [("periodic", None), ("mirror", None), ("periodic", (5000, 16384))])
 def test_grouped_forced_walks_equal_the_single_launch(monkeypatch, boundary, shard):
-    """The forced walks grouped by resume step (two launches: passes 1-2 with
-    checkpoints, then the forced walks from their checkpoints) give the
-    single launch's gradients and Jacobian: the same walkers, draws and FP32
-    arithmetic; the order of the FP64 sums differs, and the phases carried
-    over a checkpoint are summed in a second copy of the same FP32 code (so
-    the forced-draw sums, kappa and D, are held to 1e-5).  2000 steps of
-    20-step bins checkpoint every 480 steps (5 resume steps); also on a
-    walker shard that does not start at walker 0."""
+    """The default reverse pass (pass 1 alone, recording the bin displacement
+    sums, a_jw, the time-rescaling sums and the checkpoints; dL/dwave reduced
+    from the records; then the forced walks grouped by resume step, each from
+    its checkpoint) gives the single launch's gradients and Jacobian: the same
+    walkers, draws and FP32 walk.  The forced walks and the Jacobian's
+    time-rescaling sums are the same FP32 arithmetic (only the FP64 sums'
+    order differs); dL/dwave and the weighted time-rescaling sum are summed in
+    another order (float).  2000 steps of 20-step bins checkpoint every 480
+    steps (5 resume steps); also on a walker shard that does not start at
+    walker 0."""
     wave = base_waves()
     n = 16384
 
@@ -310,14 +312,32 @@ def test_grouped_forced_walks_equal_the_single_launch(monkeypatch, boundary, sha
     r1, J1 = both(True)
     r0, J0 = both(False)
     assert r0["d_kappa"] != 0.0
-    for k in ("loss", "d_diffusivity_pathwise", "d_kappa_score"):
-        assert r1[k] == pytest.approx(r0[k], rel=1e-9, abs=1e-15), k
-    for k in ("d_diffusivity", "d_kappa"):
-        assert r1[k] == pytest.approx(r0[k], rel=1e-5, abs=1e-12), k
-    np.testing.assert_allclose(r1["d_wave"], r0["d_wave"], rtol=1e-6, atol=1e-9)
+    for k in ("loss", "d_diffusivity_pathwise", "d_kappa_score", "d_kappa"):
+        assert r1[k] == pytest.approx(r0[k], rel=1e-7, abs=1e-15), k
+    assert r1["d_diffusivity"] == pytest.approx(r0["d_diffusivity"], rel=1e-4), "d_diffusivity"
+    scale = np.abs(r0["d_wave"]).max()
+    np.testing.assert_allclose(r1["d_wave"], r0["d_wave"], rtol=0, atol=1e-5 * scale)
     np.testing.assert_allclose(r1["d_t2"], r0["d_t2"], rtol=1e-9, atol=1e-15)
     np.testing.assert_allclose(r1["sigw"], r0["sigw"], rtol=1e-12)
-    for k in ("kappa_score", "T2", "sigw"):
-        np.testing.assert_allclose(J1[k], J0[k], rtol=1e-9, atol=1e-12 * n, err_msg=k)
-    for k in ("D", "kappa"):
-        np.testing.assert_allclose(J1[k], J0[k], rtol=1e-5, atol=1e-9 * n, err_msg=k)
+    for k in ("D", "kappa", "kappa_score", "T2", "sigw"):
+        np.testing.assert_allclose(J1[k], J0[k], rtol=1e-7, atol=1e-12 * n, err_msg=k)
+
+
+def test_grouped_reverse_pass_without_permeation(monkeypatch):
+    """Impermeable membranes (kappa = 0): no forced walks; the records of
+    pass 1 still give the single launch's dL/dwave, D and T2 gradients."""
+    wave = base_waves()
+    n = 16384
+    out = []
+    for grouped in ("1", "0"):
+        monkeypatch.setenv("RMS_ADJOINT_GROUPED", grouped)
+        sim = make(wave, kappa=0.0, npar=n)
+        out.append((sim.adjoint(WEIGHTS.reshape(-1) / n, seed=5), sim.jacobian(seed=5)))
+        sim.close()
+    (r1, J1), (r0, J0) = out
+    assert r1["d_kappa"] == 0.0 and r0["d_kappa"] == 0.0
+    assert r1["d_diffusivity"] == pytest.approx(r0["d_diffusivity"], rel=1e-4)
+    scale = np.abs(r0["d_wave"]).max()
+    np.testing.assert_allclose(r1["d_wave"], r0["d_wave"], rtol=0, atol=1e-5 * scale)
+    for k in ("D", "T2", "sigw"):
+        np.testing.assert_allclose(J1[k], J0[k], rtol=1e-7, atol=1e-12 * n, err_msg=k)
