@@ -408,8 +408,15 @@ int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint
  *                          length (flat membranes, periodic walls), blind to
  *                          the jumps above; the T2 weight's dependence on D
  *                          through residence times is not included
- * Each walker is walked two or three times from its random streams (nothing
- * stored; the third walk only with permeation draws).  d_wave
+ * Each walker is walked once, recording its bin displacement sums (12 bytes
+ * per bin) and its state every ck steps (at most 16 checkpoints; ck a multiple
+ * of 96 and of the bin length); with permeation draws each walker that made a
+ * draw is walked once more from the last checkpoint before its forced draw.
+ * The records go in device scratch held by the simulation (walkers in chunks
+ * of at most half the free memory and 16 GiB); where even 65536 walkers'
+ * records do not fit, or with RMS_ADJOINT_GROUPED=0 in the environment, each
+ * walker is walked two or three times from its random streams instead, with
+ * nothing stored (the same gradients up to the order of float sums).  d_wave
  * (caller-allocated host array) and sigw (optional, [nwave*2], the run's own
  * signal sums) may be NULL. */
 typedef struct rms_adjoint_grads {
@@ -425,8 +432,7 @@ typedef struct rms_adjoint_grads {
 int rms_adjoint_run(rms_sim* sim, const rms_run_opts* opts, const double* g_sigw, rms_adjoint_grads* out);
 
 /* Jacobian of every waveform's signal sums with respect to the scalar
- * parameters, in one adjoint run (three walks of each walker, as
- * rms_adjoint_run).  No counterpart in the reference.  For waveform j and
+ * parameters, in one adjoint run (the walks of rms_adjoint_run).  No counterpart in the reference.  For waveform j and
  * signal sum s (0: C_j, 1: S_j), row q = 2j + s of jac[2*nwave*RMS_JAC_COLS]
  * holds d(sum)/d(parameter) in the columns below: the estimators of
  * rms_adjoint_run with the loss L = that sum (D by time rescaling, kappa by

@@ -4,8 +4,8 @@
 // For the split walk in waveform mode (rms_walk_split.cu) with signals
 // C_j = sum_w s0_w cos phi_jw, S_j = sum_w s0_w sin phi_jw and upstream weights
 // (gC_j, gS_j), the loss is L = sum_w L_w, L_w = s0_w sum_j (gC_j cos phi_jw +
-// gS_j sin phi_jw).  Each walker is walked twice from its counter-based random
-// streams -- nothing of the trajectory is stored:
+// gS_j sin phi_jw).  The estimators, as three walks of each walker from its
+// counter-based random streams (FORM 0, nothing of the trajectory stored):
 //
 //  pass 1 accumulates phi_jw; the tangent dphi_jw/dl of the phase with respect
 //    to the step length l with the event sequence frozen (the displacement's
@@ -27,9 +27,12 @@
 //    L_w[reflected]): the weak derivative of the Bernoulli draws, an unbiased
 //    estimate of dL/dlog P that measures what a crossing changes instead of
 //    correlating the loss with rare crossings as the score function does.
-//    A forced walk repeats its unforced walk up to the forced draw, so with
-//    several checkpoints in the run it is walked from the last one before that
-//    draw, in a second launch over walkers grouped by resume step (FORM below).
+//  By default (FORMs 1 and 2 below) pass 1 also records what pass 2 reads
+//    (X_wb; the time-rescaling sums, linear in a_jw) so pass 2 is not walked,
+//    and the walker's state at checkpoints: a forced walk repeats its
+//    unforced walk up to the forced draw, so it is walked from the last
+//    checkpoint before that draw, in a second launch over walkers grouped by
+//    resume step.
 //
 // The host turns the sums into dL/dwave, dL/dT2_c (analytic), dL/dkappa
 // (dP/dkappa = P/kappa: the forced-draw sum / kappa; the score function
@@ -44,7 +47,7 @@
 // walk at voxel corners, mirror walls and changed permeation draws, which the
 // pathwise derivative through the step length (events frozen, also summed)
 // does not; it is exact for the continuum process and carries the walk's
-// time-discretisation error.  Both passes walk the split walk's step
+// time-discretisation error.  All passes walk the split walk's step
 // (split_step.cuh: same streams, same arithmetic), so the gradients belong to
 // the function the forward run evaluates.
 #include <cuda_runtime.h>
@@ -119,8 +122,9 @@ struct AdjHooks {
 // JAC: instead of one weighted loss, the derivatives of every waveform's two
 // signal sums C_j, S_j with respect to D, kappa and T2 (Jacobian columns; the
 // sums at a.sums + kAdjSums, layout kJac* in rms_internal.h); dL/dwave is not
-// formed.  The R_j of the time rescaling go to dphi[] in pass 2 and the forced
-// walk's phases to dphi[] in pass 3, so phi[] keeps pass 1's phases.
+// formed.  The R_j of the time rescaling go to dphi[] in pass 2 (FORM 1: to
+// their own array in pass 1) and the forced walk's phases to dphi[] in pass 3,
+// so phi[] keeps pass 1's phases.
 // One float per waveform for the calling lane, in shared memory: column
 // threadIdx.x of a [NW][kAdjBlock] block (consecutive lanes, consecutive
 // banks).  The walker's phases, tangents and a_jw are read and written only at
@@ -137,8 +141,9 @@ struct LaneArr {
 // Measured on a 64x64x512 axon, 1e6 walkers x 5000 steps, 16 waveforms, all
 // passes in one launch: weighted 428 ms (518 ms at 4 blocks), Jacobian 390 ms
 // (416 ms when held to 4 blocks at 115 registers); with the per-lane arrays
-// in registers (3 blocks) 541 / 474 ms.  With the forced walks grouped (FORM 1
-// then FORM 2, 11 resume steps 480 steps apart): 310 / 308 ms.
+// in registers (3 blocks) 541 / 474 ms.  FORM 1, the dL/dwave reduction and
+// FORM 2 (11 resume steps 480 steps apart): 183 / 187 ms (forward walk 154 ms;
+// with pass 2 still walked and the forced walks grouped, 310 / 308 ms).
 //
 // FORM 0 walks all passes in this launch.  FORM 1 walks pass 1 only and
 // leaves in memory what passes 2 and 3 need: the bin displacement sums X_wb
@@ -638,18 +643,67 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM > 0 ? 4 : 1) : 5) adjoi
 // dL/dwave from pass 1's records: dwave[b][j][ax] += sum_w a_jw X_wb,ax over
 // the launch's walkers (xbin [bin][axis][walker], ajw [waveform][walker]).
 // Each block takes kDwSlab walkers (kDwPer per thread, their a_jw in
-// registers) and rows [r0, r1) of the bin x axis table; per row a warp
-// reduce-scatter and a sum over the block's warps leave one float atomic per
-// waveform.  HBM-bound: the X table is read once (12 bytes per walker per bin).
-constexpr int kDwBlock = 256, kDwPer = 4, kDwSlab = kDwBlock * kDwPer;
+// registers) and rows [r0, r1) of the bin x axis table, kDwRows rows per
+// step; per row a warp reduce-scatter, and per step one barrier and a sum over
+// the block's warps leave one float atomic per row and waveform.  The next
+// step's rows are loaded while this step's are summed (two register sets), so
+// the X table streams from HBM instead of waiting out one load latency per
+// row; it is read once (12 bytes per walker per bin).
+constexpr int kDwBlock = 256, kDwPer = 4, kDwRows = 4, kDwSlab = kDwBlock * kDwPer;
 
-__global__ void __launch_bounds__(kDwBlock) adjoint_dwave_kernel(const float* __restrict__ xbin,
-                                                                const float* __restrict__ ajw, int64_t nwalk,
-                                                                int nwave, int nrows, int rows_per_block,
-                                                                float* __restrict__ dwave) {
+__device__ __forceinline__ void dw_load(float (&xv)[kDwRows][kDwPer], const float* __restrict__ xbin, int64_t nwalk,
+                                        int64_t w0, int rg, int r1) {
+#pragma unroll
+    for (int g = 0; g < kDwRows; ++g) {
+        const int r = rg + g;
+#pragma unroll
+        for (int k = 0; k < kDwPer; ++k) {
+            const int64_t w = w0 + (int64_t)k * kDwBlock;
+            xv[g][k] = (r < r1 && w < nwalk) ? __ldcs(xbin + (size_t)r * nwalk + w) : 0.0f;
+        }
+    }
+}
+
+__device__ __forceinline__ void dw_rows(const float (&xv)[kDwRows][kDwPer], const float (&av)[kDwPer][kAdjWaves],
+                                        float (&red)[kDwRows][kDwBlock / 32][kAdjWaves], int rg, int r1, int nwave,
+                                        float* __restrict__ dwave) {
     constexpr int NW = kAdjWaves;
-    __shared__ float red[2][kDwBlock / 32][NW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int g = 0; g < kDwRows; ++g) {
+        float acc[NW];
+#pragma unroll
+        for (int j = 0; j < NW; ++j) acc[j] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < kDwPer; ++k) {
+#pragma unroll
+            for (int j = 0; j < NW; ++j) acc[j] = fmaf(av[k][j], xv[g][k], acc[j]);
+        }
+        const float v = warp_reduce_scatter16f(acc, lane);   // lanes l, l ^ 16: waveform l & 15
+        if (lane < 16) red[g][warp][lane] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kDwRows * 16) {
+        const int g = threadIdx.x >> 4, j = threadIdx.x & 15, r = rg + g;
+        if (j < nwave && r < r1) {
+            float t = 0.0f;
+#pragma unroll
+            for (int q = 0; q < kDwBlock / 32; ++q) t += red[g][q][j];
+            const int b = r / 3, ax = r - 3 * b;
+            atomicAdd(dwave + ((size_t)b * nwave + j) * 3 + ax, t);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kDwBlock, 2) adjoint_dwave_kernel(const float* __restrict__ xbin,
+                                                                   const float* __restrict__ ajw, int64_t nwalk,
+                                                                   int nwave, int nrows, int rows_per_block,
+                                                                   float* __restrict__ dwave) {
+    constexpr int NW = kAdjWaves;
+    // red[s]: the warps' row sums of every other step (one barrier per step:
+    // a buffer is written again only after the next step's barrier, which its
+    // readers pass after reading it)
+    __shared__ float red[2][kDwRows][kDwBlock / 32][NW];
     const int64_t w0 = (int64_t)blockIdx.x * kDwSlab + threadIdx.x;
     float av[kDwPer][NW];
 #pragma unroll
@@ -659,29 +713,13 @@ __global__ void __launch_bounds__(kDwBlock) adjoint_dwave_kernel(const float* __
         for (int j = 0; j < NW; ++j) av[k][j] = (w < nwalk && j < nwave) ? __ldg(ajw + (size_t)j * nwalk + w) : 0.0f;
     }
     const int r0 = blockIdx.y * rows_per_block, r1 = min(nrows, r0 + rows_per_block);
-    for (int r = r0; r < r1; ++r) {
-        float acc[NW];
-#pragma unroll
-        for (int j = 0; j < NW; ++j) acc[j] = 0.0f;
-        const float* xr = xbin + (size_t)r * nwalk;
-#pragma unroll
-        for (int k = 0; k < kDwPer; ++k) {
-            const int64_t w = w0 + (int64_t)k * kDwBlock;
-            const float x = w < nwalk ? __ldcs(xr + w) : 0.0f;
-#pragma unroll
-            for (int j = 0; j < NW; ++j) acc[j] = fmaf(av[k][j], x, acc[j]);
-        }
-        const float v = warp_reduce_scatter16f(acc, lane);   // lanes l, l ^ 16: waveform l & 15
-        const int buf = r & 1;
-        if (lane < 16) red[buf][warp][lane] = v;
-        __syncthreads();
-        if (threadIdx.x < nwave) {
-            float t = 0.0f;
-#pragma unroll
-            for (int q = 0; q < kDwBlock / 32; ++q) t += red[buf][q][threadIdx.x];
-            const int b = r / 3, ax = r - 3 * b;
-            atomicAdd(dwave + ((size_t)b * nwave + threadIdx.x) * 3 + ax, t);
-        }
+    float xa[kDwRows][kDwPer], xb[kDwRows][kDwPer];
+    dw_load(xa, xbin, nwalk, w0, r0, r1);
+    for (int rg = r0; rg < r1; rg += 2 * kDwRows) {
+        dw_load(xb, xbin, nwalk, w0, rg + kDwRows, r1);
+        dw_rows(xa, av, red[0], rg, r1, nwave, dwave);
+        dw_load(xa, xbin, nwalk, w0, rg + 2 * kDwRows, r1);
+        dw_rows(xb, av, red[1], rg + kDwRows, r1, nwave, dwave);
     }
 }
 
@@ -690,7 +728,7 @@ __global__ void __launch_bounds__(kDwBlock) adjoint_dwave_kernel(const float* __
 int launch_adjoint_dwave(const AdjArgs& a, int sms, void* stream) {
     const int nrows = a.nbins * 3;
     const int slabs = (int)((a.nwalk + kDwSlab - 1) / kDwSlab);
-    // enough blocks for every SM: split the rows when the walkers are few
+    // two waves of the 2 resident blocks per SM at least: split the rows when the walkers are few
     const int want = 4 * sms;
     const int groups = std::max(1, std::min(nrows, (want + slabs - 1) / slabs));
     const int per = (nrows + groups - 1) / groups;
