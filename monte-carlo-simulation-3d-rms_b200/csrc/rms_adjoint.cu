@@ -142,7 +142,7 @@ struct LaneArr {
 // passes in one launch: weighted 428 ms (518 ms at 4 blocks), Jacobian 390 ms
 // (416 ms when held to 4 blocks at 115 registers); with the per-lane arrays
 // in registers (3 blocks) 541 / 474 ms.  FORM 1, the dL/dwave reduction and
-// FORM 2 (11 resume steps 480 steps apart): 183 / 187 ms (forward walk 154 ms;
+// FORM 2 (11 resume steps 480 steps apart): 176 / 187 ms (forward walk 154 ms;
 // with pass 2 still walked and the forced walks grouped, 310 / 308 ms).
 //
 // FORM 0 walks all passes in this launch.  FORM 1 walks pass 1 only and
