@@ -839,6 +839,19 @@ def run_adjoint_bench(args):
                           wave=np.einsum("jab,nb->jna", R, gg), timepoints=1000, boundary="periodic",
                           permeation="kappa", kappa=kappa)
 
+    if args.launches_once:
+        # one forward walk, one weighted reverse pass and one Jacobian, nothing
+        # else: the launch list of the job for a profiler
+        s1 = sim(g, **par)
+        s1.run(seed=9, precision="split")
+        fwd = s1.timing()[0]
+        s1.adjoint(W.reshape(-1) / npar, seed=9)
+        adj = s1.timing()[0]
+        s1.jacobian(seed=9)
+        print(json.dumps({"workload": "adjoint, one of each", "walkers": npar, "forward_ms": fwd, "adjoint_ms": adj,
+                          "jacobian_ms": s1.timing()[0]}), flush=True)
+        return
+
     def signal(gg=g, D=par["D"], kappa=par["kappa"], t2=par["t2"], seed=9):
         """Normalised signal per direction, [nw, 2] (cos, sin sums / walkers)."""
         s_ = sim(gg, D, kappa, t2)
@@ -1162,6 +1175,8 @@ def main():
                     choices=["production", "production-full", "batch", "single", "contraction", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--walkers", type=int, default=None, help="walkers per GPU (smaller case, e.g. for ncu)")
+    ap.add_argument("--launches-once", action="store_true",
+                    help="adjoint workload: one forward walk, reverse pass and Jacobian only (for a launch list)")
     ap.add_argument("--plain-steps", type=int, default=1,
                     help="timed runs of the plain FP64 walk on the same job (0: none)")
     ap.add_argument("--scaling", default="strong", choices=["strong", "weak"],

@@ -224,8 +224,9 @@ int rms_sim_get_trace_positions(const rms_sim* sim, double* pos, size_t nwalkers
 int rms_sim_write_dir(const rms_sim* sim, const char* dir);
 
 /* Device time of the last run's walk kernel and of the whole run (ms), from
- * CUDA events on the run's stream.  Replaces the clock() print of
- * main.cu:536-540. */
+ * CUDA events on the run's stream; after rms_adjoint_run or
+ * rms_adjoint_jacobian, both hold the reverse pass's time.  Replaces the
+ * clock() print of main.cu:536-540. */
 int rms_sim_last_timing(const rms_sim* sim, double* walk_ms, double* run_ms);
 
 /* Run several simulations (e.g. one per axon) on one device.  Simulation k

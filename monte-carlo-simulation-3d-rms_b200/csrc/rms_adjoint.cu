@@ -137,12 +137,14 @@ struct LaneArr {
 // Resident blocks per SM: at least 5 for the weighted-loss form (96 registers,
 // no spills); the Jacobian form takes the compiler's choice (123 registers, 4
 // blocks) except FORMs 1 and 2, held to 4 blocks (unbounded they took 248 and
-// 134 registers).
+// 134 registers).  FORM 1 of the weighted form also runs at 4 blocks: at 5
+// (96 registers, 116 bytes spilled) the job below took 175 ms, at 4 (128
+// registers, 48 bytes) 155 ms.
 // Measured on a 64x64x512 axon, 1e6 walkers x 5000 steps, 16 waveforms, all
 // passes in one launch: weighted 428 ms (518 ms at 4 blocks), Jacobian 390 ms
 // (416 ms when held to 4 blocks at 115 registers); with the per-lane arrays
 // in registers (3 blocks) 541 / 474 ms.  FORM 1, the dL/dwave reduction and
-// FORM 2 (11 resume steps 480 steps apart): 176 / 187 ms (forward walk 154 ms;
+// FORM 2 (11 resume steps 480 steps apart): 155 / 149 ms (forward walk 154 ms;
 // with pass 2 still walked and the forced walks grouped, 310 / 308 ms).
 //
 // FORM 0 walks all passes in this launch.  FORM 1 walks pass 1 only and
@@ -158,7 +160,7 @@ struct LaneArr {
 // because one lane's draw came early.  The sums are the single launch's up to
 // the order of the float and FP64 sums.
 template <bool JAC, int FORM>
-__global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM > 0 ? 4 : 1) : 5) adjoint_kernel(const __grid_constant__ AdjArgs a) {
+__global__ void __launch_bounds__(kAdjBlock, FORM == 1 ? 4 : (JAC ? (FORM > 0 ? 4 : 1) : 5)) adjoint_kernel(const __grid_constant__ AdjArgs a) {
     constexpr int NC = kAdjNc, BITS = 4, NW = kAdjWaves;
     constexpr int kTab = 2 * NC + 2 * NC * NC;
     __shared__ float s_tab[kTab];
@@ -390,6 +392,7 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM > 0 ? 4 : 1) : 5) adjoi
                 if (event) {
                     const double x0 = P0 * (double)a.res, x1 = P1 * (double)a.res, x2 = P2 * (double)a.res;
                     const double* wv = a.wave + (size_t)bin * a.nwave * 3;
+                    const float4* wq = a.wq + (size_t)bin * a.nwave * 2;   // [j]: g_j,b - g_j,b+1; g_j,b res
                     if (pass != 1) {
                         // the phases (pass 1: and their tangents; pass 3: of the forced walk)
 #pragma unroll
@@ -399,7 +402,10 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM > 0 ? 4 : 1) : 5) adjoi
                                 const float inc = (float)(g0 * x0 + g1 * x1 + g2 * x2);
                                 if (JAC && pass == 2) dphi[j] += inc;
                                 else phi[j] += inc;
-                                if (p1st) dphi[j] += (float)((g0 * B0 + g1 * B1 + g2 * B2) * (double)a.res);
+                                if (p1st) {
+                                    const float4 gr = __ldg(wq + 2 * j + 1);
+                                    dphi[j] += fmaf(gr.z, B2, fmaf(gr.y, B1, gr.x * B0));
+                                }
                             }
                         }
                         B0 = B1 = B2 = 0.0f;
@@ -416,17 +422,11 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM > 0 ? 4 : 1) : 5) adjoi
                                         xe1 = ((float)D1 + (o1 - Fm1)) * a.res,
                                         xe2 = ((float)D2 + (o2 - Fm2)) * a.res;
                             const float tb = (float)(i + 1);
-                            const double* wn = wv + a.nwave * 3;
-                            const bool last = bin + 1 >= a.nbins;
 #pragma unroll
                             for (int j = 0; j < NW; ++j) {
                                 if (j < a.nwave) {
-                                    const float q0 = (float)(__ldg(wv + 3 * j) - (last ? 0.0 : __ldg(wn + 3 * j)));
-                                    const float q1 =
-                                        (float)(__ldg(wv + 3 * j + 1) - (last ? 0.0 : __ldg(wn + 3 * j + 1)));
-                                    const float q2 =
-                                        (float)(__ldg(wv + 3 * j + 2) - (last ? 0.0 : __ldg(wn + 3 * j + 2)));
-                                    rr[j] = fmaf(tb, q0 * xe0 + q1 * xe1 + q2 * xe2, rr[j]);
+                                    const float4 q = __ldg(wq + 2 * j);
+                                    rr[j] = fmaf(tb, q.x * xe0 + q.y * xe1 + q.z * xe2, rr[j]);
                                 }
                             }
                         }
@@ -436,16 +436,12 @@ __global__ void __launch_bounds__(kAdjBlock, JAC ? (FORM > 0 ? 4 : 1) : 5) adjoi
                         const float xe0 = ((float)D0 + (o0 - Fm0)) * a.res, xe1 = ((float)D1 + (o1 - Fm1)) * a.res,
                                     xe2 = ((float)D2 + (o2 - Fm2)) * a.res;
                         const float tb = (float)(i + 1);   // steps (the waveform table carries dt)
-                        const double* wn = wv + a.nwave * 3;
-                        const bool last = bin + 1 >= a.nbins;
 #pragma unroll
                         for (int j = 0; j < NW; ++j) {
                             if (j < a.nwave) {
-                                const float q0 = (float)(__ldg(wv + 3 * j) - (last ? 0.0 : __ldg(wn + 3 * j)));
-                                const float q1 = (float)(__ldg(wv + 3 * j + 1) - (last ? 0.0 : __ldg(wn + 3 * j + 1)));
-                                const float q2 = (float)(__ldg(wv + 3 * j + 2) - (last ? 0.0 : __ldg(wn + 3 * j + 2)));
-                                if (JAC) dphi[j] = fmaf(tb, q0 * xe0 + q1 * xe1 + q2 * xe2, dphi[j]);   // R_j
-                                else tr = fmaf(aj[j] * tb, q0 * xe0 + q1 * xe1 + q2 * xe2, tr);
+                                const float4 q = __ldg(wq + 2 * j);
+                                if (JAC) dphi[j] = fmaf(tb, q.x * xe0 + q.y * xe1 + q.z * xe2, dphi[j]);   // R_j
+                                else tr = fmaf(aj[j] * tb, q.x * xe0 + q.y * xe1 + q.z * xe2, tr);
                             }
                         }
                         if (!JAC) {

@@ -78,8 +78,8 @@ struct rms_device_state {
     cudaStream_t own = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     DevBuf labels, packed, axons, wavef, tables, tablesf, slots, sig_slots, vscr, qtab, bvec, grad, gpair, ev_step,
-        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave, adj_ck, adj_ws, adj_blist, adj_bcount, adj_xbin, adj_ajw, stage,
-        counts;
+        ev_pair, ev_coef, out, out_sig, err, tr_init, tr_vox, tr_ev, tr_pos, adj_g, adj_sums, adj_dwave, adj_ck, adj_ws, adj_blist, adj_bcount, adj_xbin, adj_ajw, adj_wq,
+        stage, counts;
     HostPinned h_out, h_axons;
     size_t labels_bytes = 0;
     bool packed_valid = false;
@@ -90,7 +90,7 @@ struct rms_device_state {
         for (DevBuf* b : {&labels, &packed, &axons, &wavef, &tables, &tablesf, &slots, &sig_slots, &vscr, &qtab, &bvec, &grad,
                           &gpair, &ev_step, &ev_pair, &ev_coef, &out, &out_sig, &err, &tr_init,
                           &tr_vox, &tr_ev, &tr_pos, &adj_g, &adj_sums, &adj_dwave, &adj_ck, &adj_ws, &adj_blist,
-                          &adj_bcount, &adj_xbin, &adj_ajw, &stage, &counts})
+                          &adj_bcount, &adj_xbin, &adj_ajw, &adj_wq, &stage, &counts})
             b->release();
         h_out.release();
         h_axons.release();
@@ -215,6 +215,7 @@ void zero_results(rms_sim* s) {
     s->trace_n = 0;
     s->walk_ms = s->run_ms = 0.0;
     s->have_results = true;
+    s->have_timing = true;
 }
 
 // The walkers a batch call walks in simulation s: all of them, or the call's
@@ -793,6 +794,7 @@ int finish_launch(std::vector<LaunchJob>& jobs, LaunchPlan& p, bool events) {
         sk->last_grid = p.grid;
         sk->last_block = p.block;
         sk->have_results = true;
+        sk->have_timing = true;
     }
     return RMS_OK;
 }
@@ -1076,6 +1078,19 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
             for (int k = 0; k < 3; ++k)
                 wf[((size_t)b * s->nwave + j) * 3 + k] = s->wave[((size_t)j * s->nbins + b) * 3 + k] * s->dt;
     RMS_CUDA(upload(d->wavef, wf, st));
+    // the float terms of the time rescaling and of the step-length tangent:
+    // (float)(g_b - g_b+1) with g_nbins = 0, and (float)(g_b res)
+    std::vector<float> wq((size_t)s->nbins * s->nwave * 8, 0.0f);
+    for (int b = 0; b < s->nbins; ++b)
+        for (int j = 0; j < s->nwave; ++j)
+            for (int k = 0; k < 3; ++k) {
+                const double g = wf[((size_t)b * s->nwave + j) * 3 + k];
+                const double gn = b + 1 < s->nbins ? wf[((size_t)(b + 1) * s->nwave + j) * 3 + k] : 0.0;
+                float* e = wq.data() + ((size_t)b * s->nwave + j) * 8;
+                e[k] = (float)(g - gn);
+                e[4 + k] = (float)(g * (double)x.res);
+            }
+    RMS_CUDA(upload(d->adj_wq, wq, st));
     std::vector<float> gup((size_t)2 * s->nwave);
     for (int j = 0; j < 2 * s->nwave; ++j) gup[j] = (float)(g_sigw ? g_sigw[j] : 0.0);
     RMS_CUDA(upload(d->adj_g, gup, st));
@@ -1088,6 +1103,7 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
     RMS_CUDA(d->err.ensure(sizeof(int)));
     RMS_CUDA(cudaMemsetAsync(d->err.p, 0, sizeof(int), st));
     a.wave = d->wavef.as<double>();
+    a.wq = d->adj_wq.as<float4>();
     a.gup = d->adj_g.as<float>();
     a.sums = d->adj_sums.as<double>();
     a.dwave = d->adj_dwave.as<float>();
@@ -1206,6 +1222,7 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
     RMS_CUDA(cudaEventElapsedTime(&ms, d->e0, d->e1));
     s->walk_ms = ms;
     s->run_ms = ms;
+    s->have_timing = true;
 
     // dL/dwave: phase_j = dt sum_b wave_j,b . X_b
     if (out->d_wave)
@@ -1712,7 +1729,7 @@ int rms_sim_write_dir(const rms_sim* s, const char* dir) {
 
 int rms_sim_last_timing(const rms_sim* s, double* walk_ms, double* run_ms) {
     if (!s) return set_error(RMS_ERR_ARG, "null sim");
-    if (!s->have_results) return set_error(RMS_ERR_STATE, "no run yet");
+    if (!s->have_timing) return set_error(RMS_ERR_STATE, "no run yet");
     if (walk_ms) *walk_ms = s->walk_ms;
     if (run_ms) *run_ms = s->run_ms;
     return RMS_OK;

@@ -157,6 +157,7 @@ struct AdjArgs {
     int force;                   // a third pass: one permeation decision per walker forced the other way
     float step[kAdjNc], kexp[kAdjNc], pij[kAdjNc * kAdjNc], ratio[kAdjNc * kAdjNc];
     const double* wave;          // [bin][waveform][axis], x dt
+    const float4* wq;            // [bin][waveform][2]: (g_b - g_b+1, 0), (g_b res, 0) as floats (g_nbins = 0)
     const float* gup;            // [waveform][2]: dL/d(sum cos), dL/d(sum sin)
     double* sums;                // [kAdjSums]
     // pass 1 alone, then the forced walks grouped (adjoint_kernel FORM 1 and

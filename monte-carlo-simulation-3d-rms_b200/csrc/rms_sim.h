@@ -50,6 +50,7 @@ struct rms_sim {
 
     // results of the last run
     bool have_results = false;
+    bool have_timing = false;   // walk_ms / run_ms hold a run's or an adjoint's times
     std::vector<double> sig0, dx2, dx4, sigre, sig, sigw, npar_count;
     int64_t trace_n = 0;
     std::vector<int32_t> tr_init, tr_vox;

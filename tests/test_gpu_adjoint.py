@@ -341,3 +341,13 @@ def test_grouped_reverse_pass_without_permeation(monkeypatch):
     np.testing.assert_allclose(r1["d_wave"], r0["d_wave"], rtol=0, atol=1e-5 * scale)
     for k in ("D", "T2", "sigw"):
         np.testing.assert_allclose(J1[k], J0[k], rtol=1e-7, atol=1e-12 * n, err_msg=k)
+
+
+def test_timing_reports_the_reverse_pass_on_a_fresh_simulation():
+    """rms_sim_last_timing after an adjoint call on a simulation that has not
+    run forward: the reverse pass's device time, positive."""
+    sim = make(base_waves(), npar=4096)
+    sim.adjoint(WEIGHTS.reshape(-1) / 4096, seed=5)
+    walk_ms, run_ms = sim.timing()
+    assert walk_ms > 0.0 and run_ms > 0.0
+    sim.close()
