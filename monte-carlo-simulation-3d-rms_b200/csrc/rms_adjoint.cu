@@ -159,8 +159,10 @@ struct LaneArr {
 // warp, each from its checkpoint -- so a warp no longer walks from step 0
 // because one lane's draw came early.  The sums are the single launch's up to
 // the order of the float and FP64 sums.
+constexpr int adj_min_blocks(bool jac, int form) { return form == 1 ? 4 : (jac ? (form == 2 ? 4 : 1) : 5); }
+
 template <bool JAC, int FORM>
-__global__ void __launch_bounds__(kAdjBlock, FORM == 1 ? 4 : (JAC ? (FORM > 0 ? 4 : 1) : 5)) adjoint_kernel(const __grid_constant__ AdjArgs a) {
+__global__ void __launch_bounds__(kAdjBlock, adj_min_blocks(JAC, FORM)) adjoint_kernel(const __grid_constant__ AdjArgs a) {
     constexpr int NC = kAdjNc, BITS = 4, NW = kAdjWaves;
     constexpr int kTab = 2 * NC + 2 * NC * NC;
     __shared__ float s_tab[kTab];
