@@ -142,6 +142,10 @@ def test_results_before_run_are_an_error():
     with pytest.raises(engine.RmsError) as e:
         s.get("sig0")
     assert e.value.code == -7
+    # no run and no reverse pass yet: no times either
+    with pytest.raises(engine.RmsError) as e:
+        s.timing()
+    assert e.value.code == -7
 
 
 @pytest.mark.parametrize("case", ["narrow_3comp", "pgse_3comp"])
