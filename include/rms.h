@@ -414,7 +414,8 @@ int rms_sim_run_noalloc(const rms_sim* sim, const rms_run_opts* opts, const uint
  * of 96 and of the bin length); with permeation draws each walker that made a
  * draw is walked once more from the last checkpoint before its forced draw.
  * The records go in device scratch held by the simulation (walkers in chunks
- * of at most half the free memory and 16 GiB); where even 65536 walkers'
+ * of at most half the free memory and 16 GiB, or RMS_ADJOINT_SCRATCH_MB
+ * mebibytes when that is set and smaller); where even 65536 walkers'
  * records do not fit, or with RMS_ADJOINT_GROUPED=0 in the environment, each
  * walker is walked two or three times from its random streams instead, with
  * nothing stored (the same gradients up to the order of float sums).  d_wave

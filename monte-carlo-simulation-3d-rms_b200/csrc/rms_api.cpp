@@ -1124,7 +1124,8 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
     // resumes from the last checkpoint before its forced draw.  Per walker:
     // the checkpoints, the summary, a bucket entry per resume step and
     // (weighted form) X_wb and a_jw; the walkers go in chunks that fit the
-    // scratch budget (half the free memory, at most 16 GiB).
+    // scratch budget (half the free memory, at most 16 GiB, or less with
+    // RMS_ADJOINT_SCRATCH_MB).
     int64_t base = 96;   // lcm(3, 32)
     {
         int64_t x = base, y = a.bin_steps;
@@ -1142,7 +1143,11 @@ int run_adjoint(rms_sim* s, const rms_run_opts* o, const double* g_sigw, rms_adj
         (void)cudaGetLastError();
         mfree = 0;
     }
-    const size_t budget = std::min<size_t>(mfree / 2, (size_t)16 << 30);
+    size_t budget = std::min<size_t>(mfree / 2, (size_t)16 << 30);
+    if (const char* cap = std::getenv("RMS_ADJOINT_SCRATCH_MB")) {
+        const long long mb = std::atoll(cap);
+        if (mb > 0) budget = std::min<size_t>(budget, (size_t)mb << 20);
+    }
     int64_t chunk = std::min<int64_t>(nwalk, (int64_t)(budget / std::max<size_t>(per_walker, 1)));
     if (chunk < nwalk) chunk = chunk / 32 * 32;
     const char* genv = std::getenv("RMS_ADJOINT_GROUPED");

@@ -351,3 +351,36 @@ def test_timing_reports_the_reverse_pass_on_a_fresh_simulation():
     walk_ms, run_ms = sim.timing()
     assert walk_ms > 0.0 and run_ms > 0.0
     sim.close()
+
+
+def test_reverse_pass_in_walker_chunks_equals_one_chunk(monkeypatch):
+    """200000 walkers with the scratch capped at 130 MiB against one chunk.
+    Records per walker: 1936 bytes for the weighted form (100 bins x 3
+    floats, a_jw, 4 checkpoints, the summary and bucket entries) -- chunks of
+    70,400, 70,400 and 59,200 walkers; 720 bytes for the Jacobian -- 189,312
+    and 10,688.  The chunks' sums add up to the whole run's gradients and
+    Jacobian (float and FP64 sums in another order only)."""
+    wave = base_waves()
+    n = 200000
+
+    def run(cap):
+        if cap:
+            monkeypatch.setenv("RMS_ADJOINT_SCRATCH_MB", str(cap))
+        else:
+            monkeypatch.delenv("RMS_ADJOINT_SCRATCH_MB", raising=False)
+        sim = make(wave, npar=n)
+        r = sim.adjoint(WEIGHTS.reshape(-1) / n, seed=5)
+        J = sim.jacobian(seed=5)
+        sim.close()
+        return r, J
+
+    r1, J1 = run(130)
+    r0, J0 = run(0)
+    for k in ("loss", "d_diffusivity_pathwise", "d_kappa_score", "d_kappa"):
+        assert r1[k] == pytest.approx(r0[k], rel=1e-7, abs=1e-15), k
+    assert r1["d_diffusivity"] == pytest.approx(r0["d_diffusivity"], rel=1e-5), "d_diffusivity"
+    scale = np.abs(r0["d_wave"]).max()
+    np.testing.assert_allclose(r1["d_wave"], r0["d_wave"], rtol=0, atol=1e-5 * scale)
+    np.testing.assert_allclose(r1["d_t2"], r0["d_t2"], rtol=1e-9, atol=1e-15)
+    for k in ("D", "kappa", "kappa_score", "T2", "sigw"):
+        np.testing.assert_allclose(J1[k], J0[k], rtol=1e-7, atol=1e-12 * n, err_msg=k)
