@@ -4,9 +4,11 @@
 of s0 (cos phase_j, sin phase_j) per waveform j, shape [nwave, 2] -- as a
 differentiable function of the waveforms, the diffusivity D (shared by every
 labelled compartment), the membrane permeability kappa and the per-compartment
-T2.  The forward pass is the split walk (rms_sim_run); the backward pass walks
-the same walkers again from their counter-based random streams
-(rms_adjoint_run) instead of storing trajectories.  Gradients: exact pathwise
+T2.  The forward pass is the split walk (rms_sim_run); the backward pass
+(rms_adjoint_run) walks the same walkers again from their counter-based random
+streams, keeping per-bin displacement sums and a few checkpoints per walker in
+device memory, and walks each walker that made a permeation draw once more
+from a checkpoint.  Gradients: exact pathwise
 for the waveforms, analytic for T2, time rescaling (minus the kappa term) for
 D, forced permeation draws (the weak derivative of the Bernoulli draws) for
 kappa.  torch is the plumbing here; all arithmetic runs in librms.
