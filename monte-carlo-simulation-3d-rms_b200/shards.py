@@ -43,3 +43,25 @@ def gather_sum(fields: dict, group=None, device=None) -> dict:
         out[k] = total[off:off + a.size].reshape(a.shape)
         off += a.size
     return out
+
+
+# rms_adjoint_run's outputs that are sums over walkers: a shard's values add up
+# to the whole job's (dL/dwave, D by time rescaling and pathwise, kappa by
+# forced draws, T2, the loss and the signal sums)
+ADJOINT_SUMS = ("d_wave", "d_diffusivity", "d_diffusivity_pathwise", "d_kappa", "d_t2", "loss", "sigw")
+
+
+def adjoint_sum(grads: dict, group=None, device=None) -> dict:
+    """The whole job's adjoint from one rank's walker shard (Sim.adjoint with
+    walker_range = that shard): every walker sum added over ranks in rank
+    order.  d_kappa_score, whose baseline is the shard's own mean loss, is
+    summed too: the sum of the shards' score estimates, unbiased like each of
+    them, though not the single run's value.  Every rank passes the same
+    keys (the fields present in grads are summed)."""
+    fields = {k: np.asarray(grads[k], dtype=np.float64) for k in ADJOINT_SUMS + ("d_kappa_score",) if k in grads}
+    tot = gather_sum(fields, group=group, device=device)
+    out = dict(grads)
+    for k, v in tot.items():
+        out[k] = float(v) if np.ndim(grads[k]) == 0 else v
+    return out
+

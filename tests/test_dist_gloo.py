@@ -113,6 +113,64 @@ def test_two_rank_shards_sum_to_the_whole_job():
         np.testing.assert_allclose(got[k], whole[k], rtol=1e-12, atol=1e-12 * np.abs(whole[k]).max())
 
 
+def _adjoint_job():
+    """Permeable flat planes (kappa = 0.05), 2 waveforms of 20 bins."""
+    from rms_b200 import waveforms
+    lab = np.full((12, 8, 8), 2, dtype=np.uint8)
+    lab[(np.arange(12) // 3) % 2 == 0] = 1
+    dt, tn, nb = 5e-4, 400, 20
+    wave = waveforms.scale_to_b(waveforms.random_smooth(2, nb, 1.0, seed=7), dt * tn / nb, [0.5, 1.0])
+    step, t2s, pij, td = pyoracle.reference_tables(dt, 0.1, [0.0, 2.0, 2.0], [1e6, 70.0, 60.0], 20, tn, kappa=0.05)
+    job = pyoracle.Job(lab, dt=dt, tn=tn, npar=96, res=0.1, step=step, t2_steps=t2s, pij=pij, seed=3,
+                       timepoints=20, td=td, wave=wave, boundary=pyoracle.BOUNDARY_PERIODIC)
+    gup = np.array([0.3, -1.1, 0.7, 0.2]) / job.npar
+    return job, gup
+
+
+def _adjoint_grads(job, gup, w0, w1):
+    sums = pyoracle.adjoint_split(job, gup, w0, w1)
+    return pyoracle.adjoint_gradients(job, sums, 2.0, [1e6, 70.0, 60.0], kappa=0.05, nwalk=w1 - w0)
+
+
+def _adjoint_rank(rank, world, port, q):
+    """One rank's walker shard of the reverse pass (the oracle's FP64 adjoint
+    standing in for rms_adjoint_run with walker_range), then
+    shards.adjoint_sum."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    job, gup = _adjoint_job()
+    w0, w1 = shards.split_range(job.npar, rank, world)
+    tot = shards.adjoint_sum(_adjoint_grads(job, gup, w0, w1))
+    if rank == 0:
+        q.put(tot)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_adjoint_shards_sum_to_the_whole_job():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_adjoint_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    job, gup = _adjoint_job()
+    whole = _adjoint_grads(job, gup, 0, job.npar)
+    assert whole["d_kappa"] != 0.0   # permeation draws were forced
+    for k in ("d_diffusivity", "d_diffusivity_pathwise", "d_kappa", "loss"):
+        assert got[k] == pytest.approx(whole[k], rel=1e-12, abs=1e-15), k
+    for k in ("d_wave", "d_t2"):
+        np.testing.assert_allclose(got[k], whole[k], rtol=1e-12, atol=1e-12 * np.abs(whole[k]).max(), err_msg=k)
+    # the score with per-shard baselines: the sum of the two shards' estimates
+    halves = [_adjoint_grads(job, gup, *shards.split_range(job.npar, r, 2))["d_kappa_score"] for r in range(2)]
+    assert got["d_kappa_score"] == pytest.approx(sum(halves), rel=1e-12, abs=1e-15)
+
+
 def test_shard_ranges_cover_the_job():
     for npar, world in ((10, 3), (1, 2), (1000003, 8)):
         rs = [shards.split_range(npar, r, world) for r in range(world)]
